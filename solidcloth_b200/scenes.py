@@ -1,0 +1,258 @@
+"""Synthetic cloth workloads with the shapes of the benchmark configurations.
+
+Every array here is float32 / uint32 and produced deterministically from a
+seed, so the CUDA library, the CPU oracle and the reference build all receive
+bit-identical inputs. Nothing in this module touches a GPU.
+
+Configurations (sizes, materials and colliders of the benchmark set):
+  cfg0  32x32 grid, 1 m, two corners pinned, FEM + bends, no collisions, 4 x 10
+  cfg1  128x128 grid, 1 m, 0.4 m above a sphere (r 0.3) sampled as a 64^3 SDF,
+        self-collision, thickness 5 mm, friction 0.3, 8 x 15
+  cfg2  256x256 grid, 1.5 m, dropped 0.5 m onto a level-5 icosphere mesh
+        (r 0.25) standing on a ground plane, mesh + self contacts, 8 x 20
+  cfg3  512 independent cloths, side 16..128 log-uniform, sphere SDF 32^3 each,
+        1-4 pinned corners, self-collision, 8 x 15
+Mapping choices (documented where the reference needs an interpretation):
+  * unit = 1 (SI gravity), FEM on, dihedral bends on;
+  * E = 1e3 enters only the shear compliance; Poisson 0.3;
+  * bend stiffness 1e-3 is the projection factor s = 0.0005 * b, so b = 2.0;
+  * lumped masses from areal density 0.1 kg/m^2; pinned vertices get mass 0
+    (-> inverse mass 0, as ClothModel::SetMasses does);
+  * +-1e-3 m uniform noise on positions after the grid is built;
+  * fixed iteration counts (the reference's FEM early exit is bypassed).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+import numpy as np
+
+CF_VERTICES, CF_TRIANGLES, CF_SELF, CF_WALLS, CF_EDGES = 1, 2, 4, 8, 16
+
+
+@dataclass
+class Params:
+    unit: float = 1.0
+    thickness: float = 0.3
+    tolerance: float = 0.2
+    shear: float = 1e3
+    bend: float = 2.0
+    stretch: float = 2e10
+    poisson: float = 0.3
+    friction: float = 0.4
+    iterations: int = 10
+    substeps: int = 4
+    flags: int = 0
+    fem: bool = True
+    dihedral: bool = True
+    fixed_iterations: bool = True
+    drag: float = 1.0
+
+    def as_array(self) -> np.ndarray:
+        return np.array([self.unit, self.thickness, self.tolerance, self.shear, self.bend,
+                         self.stretch, self.poisson, self.friction, self.iterations,
+                         self.substeps, self.flags, float(self.fem), float(self.dihedral),
+                         float(self.fixed_iterations), self.drag], dtype=np.float32)
+
+
+@dataclass
+class SDFGrid:
+    cells: tuple
+    box: np.ndarray          # (6,) min xyz, max xyz
+    values: np.ndarray       # (cells+1)^3 float32, x fastest
+
+
+@dataclass
+class MeshCollider:
+    vertices: np.ndarray     # (V, 3) float32
+    indices: np.ndarray      # (T*3,) uint32
+
+
+@dataclass
+class Scene:
+    name: str
+    n: int                   # vertices per side
+    inc: float               # grid spacing
+    offset: np.ndarray       # (3,)
+    attached: bool
+    params: Params
+    masses: np.ndarray       # (n*n,) float32, 0 at pinned vertices
+    positions: np.ndarray    # (n*n, 3) float32 (noisy initial positions)
+    dt: float = 1.0 / 60.0
+    frames: int = 120
+    walls: Optional[np.ndarray] = None
+    spheres: List[tuple] = field(default_factory=list)
+    sdfs: List[SDFGrid] = field(default_factory=list)
+    meshes: List[MeshCollider] = field(default_factory=list)
+    ccd: bool = False
+
+    @property
+    def num_vertices(self) -> int:
+        return self.n * self.n
+
+
+def grid_positions(n: int, inc: float, offset) -> np.ndarray:
+    """Flat horizontal grid positions exactly as ClothPatch::Init(grid) computes
+    them in float32 (Physics/ClothPatch.cpp:150-190): column j at
+    x_j = x_{j-1} + inc starting from -0.5*n*inc, row i at startY + inc*i."""
+    off = np.asarray(offset, dtype=np.float32)
+    pos = np.zeros((n * n, 3), dtype=np.float32)
+    x = np.float32(np.float32(-0.5) * np.float32(n)) * np.float32(inc)
+    start = x
+    for j in range(n):
+        base = j * n
+        for i in range(n):
+            z = start if i == 0 else np.float32(start + np.float32(np.float32(inc) * np.float32(i)))
+            pos[base + i] = (np.float32(x + off[0]), np.float32(np.float32(0) + off[1]),
+                             np.float32(z + off[2]))
+        x = np.float32(x + np.float32(inc))
+    return pos
+
+
+def grid_triangles(n: int) -> np.ndarray:
+    """Triangle list of ClothPatch::Init(grid), alternating diagonals
+    (Physics/ClothPatch.cpp:205-221)."""
+    tris = []
+    for j in range(1, n):
+        for i in range(1, n):
+            idx = j * n + i
+            a, b, c, d = idx - n - 1, idx - n, idx, idx - 1
+            if (i & 1) == (j & 1):
+                tris += [(a, c, b), (a, d, c)]
+            else:
+                tris += [(b, d, c), (d, b, a)]
+    return np.asarray(tris, dtype=np.uint32)
+
+
+def lumped_masses(n: int, inc: float, density: float, pinned) -> np.ndarray:
+    tris = grid_triangles(n)
+    area = np.float32(0.5 * inc * inc)
+    m = np.zeros(n * n, dtype=np.float64)
+    for k in range(3):
+        np.add.at(m, tris[:, k], density * float(area) / 3.0)
+    m = m.astype(np.float32)
+    for p in pinned:
+        m[p] = 0.0
+    return m
+
+
+def corner_pins(n: int, corners) -> List[int]:
+    """Corner vertex ids: 0 = (j=0,i=0), 1 = (j=0,i=n-1), 2 = (j=n-1,i=0), 3 = (j=n-1,i=n-1).
+    ClothPatch::Init(attached=true) pins corners 1 and 3."""
+    ids = [0, n - 1, (n - 1) * n, n * n - 1]
+    return [ids[c] for c in corners]
+
+
+def sphere_sdf(center, radius: float, cells: int, margin: float) -> SDFGrid:
+    """Analytic sphere distance sampled at the grid points of SDF::Create(cells,
+    cells, cells, box) (Geometry/SDF.cpp:10-40, GetPosAt SDF.h:64-70)."""
+    c = np.asarray(center, dtype=np.float32)
+    half = np.float32(radius + margin)
+    bmin = (c - half).astype(np.float32)
+    bmax = (c + half).astype(np.float32)
+    ext = (bmax - bmin).astype(np.float32)
+    inv = np.float32(1.0) / np.float32(cells)
+    steps = (ext * inv).astype(np.float32)
+    ax = np.arange(cells + 1, dtype=np.float32)
+    gx = (ax * steps[0] + bmin[0]).astype(np.float32)
+    gy = (ax * steps[1] + bmin[1]).astype(np.float32)
+    gz = (ax * steps[2] + bmin[2]).astype(np.float32)
+    Z, Y, X = np.meshgrid(gz, gy, gx, indexing="ij")
+    d = np.sqrt((X.astype(np.float64) - c[0]) ** 2 + (Y.astype(np.float64) - c[1]) ** 2 +
+                (Z.astype(np.float64) - c[2]) ** 2) - radius
+    vals = d.astype(np.float32).reshape(-1)          # x fastest (z outermost)
+    return SDFGrid((cells, cells, cells), np.concatenate([bmin, bmax]).astype(np.float32), vals)
+
+
+def icosphere(level: int, radius: float, center) -> MeshCollider:
+    """Icosahedron subdivided `level` times and projected to the sphere
+    (level 5 -> 10,242 vertices, 20,480 triangles), outward winding."""
+    t = (1.0 + 5 ** 0.5) / 2.0
+    verts = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t),
+             (0, -1, -t), (0, 1, -t), (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    verts = [np.array(v, dtype=np.float64) / np.linalg.norm(v) for v in verts]
+    faces = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4),
+             (11, 10, 2), (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8),
+             (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    for _ in range(level):
+        cache = {}
+
+        def mid(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in cache:
+                m = verts[a] + verts[b]
+                verts.append(m / np.linalg.norm(m))
+                cache[key] = len(verts) - 1
+            return cache[key]
+
+        nf = []
+        for a, b, c in faces:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        faces = nf
+    v = (np.asarray(verts) * radius + np.asarray(center, dtype=np.float64)).astype(np.float32)
+    return MeshCollider(v, np.asarray(faces, dtype=np.uint32).reshape(-1))
+
+
+def _noise(rng: np.random.Generator, shape, amp: float) -> np.ndarray:
+    return rng.uniform(-amp, amp, size=shape).astype(np.float32)
+
+
+def make_grid_scene(name: str, n: int, side: float, height: float, params: Params,
+                    pinned_corners=(), seed: int = 0, frames: int = 120,
+                    center_xz=(0.0, 0.0)) -> Scene:
+    inc = float(np.float32(side / (n - 1)))
+    # centre the grid: column/row coordinates start at -0.5*n*inc
+    off = np.array([0.5 * inc + center_xz[0], height, 0.5 * inc + center_xz[1]], dtype=np.float32)
+    pins = corner_pins(n, pinned_corners)
+    masses = lumped_masses(n, inc, 0.1, pins)
+    rng = np.random.default_rng(seed)
+    pos = grid_positions(n, inc, off)
+    pos = (pos + _noise(rng, pos.shape, 1e-3)).astype(np.float32)
+    attached = tuple(sorted(pinned_corners)) == (1, 3)
+    return Scene(name, n, inc, off, attached, params, masses, pos, frames=frames)
+
+
+def cfg0(seed: int = 0) -> Scene:
+    p = Params(iterations=10, substeps=4, flags=0)
+    return make_grid_scene("cfg0_32x32_pinned", 32, 1.0, 0.0, p, pinned_corners=(1, 3), seed=seed, frames=120)
+
+
+def cfg1(seed: int = 1, n: int = 128, ccd: bool = False) -> Scene:
+    p = Params(thickness=0.005, tolerance=0.005, friction=0.3, iterations=15, substeps=8,
+               flags=CF_VERTICES | CF_SELF)
+    s = make_grid_scene(f"cfg1_{n}x{n}_sphere_sdf_self", n, 1.0, 0.3 + 0.4, p, seed=seed, frames=300)
+    s.sdfs.append(sphere_sdf((0.0, 0.0, 0.0), 0.3, 63, 0.1))
+    s.ccd = ccd
+    return s
+
+
+def cfg2(seed: int = 2, n: int = 256, level: int = 5) -> Scene:
+    p = Params(thickness=0.005, tolerance=0.005, friction=0.3, iterations=20, substeps=8,
+               flags=CF_VERTICES | CF_TRIANGLES | CF_EDGES | CF_SELF | CF_WALLS)
+    s = make_grid_scene(f"cfg2_{n}x{n}_icosphere_mesh_self", n, 1.5, 0.5 + 0.5, p, seed=seed, frames=300)
+    s.walls = np.array([-20.0, 0.0, -20.0, 20.0, 20.0, 20.0], dtype=np.float32)
+    s.meshes.append(icosphere(level, 0.25, (0.0, 0.25, 0.0)))
+    return s
+
+
+def cfg3_instances(count: int = 512, seed: int = 3, lo: int = 16, hi: int = 128) -> List[Scene]:
+    rng = np.random.default_rng(seed)
+    sides = np.exp(rng.uniform(np.log(lo), np.log(hi), size=count)).round().astype(int)
+    scenes = []
+    for k in range(count):
+        n = int(np.clip(sides[k], lo, hi))
+        r = float(rng.uniform(0.1, 0.4))
+        npins = int(rng.integers(1, 5))
+        corners = tuple(sorted(rng.choice(4, size=npins, replace=False).tolist()))
+        p = Params(thickness=0.005, tolerance=0.005, friction=0.3, iterations=15, substeps=8,
+                   flags=CF_VERTICES | CF_SELF)
+        s = make_grid_scene(f"cfg3_inst{k}_{n}", n, 1.0, r + 0.4, p, pinned_corners=corners,
+                            seed=seed * 100003 + k, frames=200)
+        s.sdfs.append(sphere_sdf((0.0, 0.0, 0.0), r, 31, 0.1))
+        scenes.append(s)
+    return scenes
+
+
+CONFIGS = {"cfg0": cfg0, "cfg1": cfg1, "cfg2": cfg2}
