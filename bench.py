@@ -1,0 +1,327 @@
+"""Cloth-step benchmark: vertex-substeps/s on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config cfg1]
+
+Workload (default): the 128x128 drape onto a 64^3 sphere SDF with self-collision,
+8 substeps x 15 iterations per frame (scenes.cfg1). One "step" is one frame,
+i.e. one scStepCloth(1/60) call = 8 substeps. Multi-GPU (torchrun, one process
+per GPU) runs independent replicas (a single cloth does not shard): scaling is
+weak and `value` is the sum over ranks of the device-timed throughput, using the
+max time over ranks.
+
+Timing: W untimed frames, then K frames each bracketed by CUDA events on the
+patch's stream; L2 is flushed (a 256 MiB write) before every timed frame,
+outside the events. `e2e` runs K more frames through the C ABI with host
+buffers: the state is uploaded from pinned host memory before each frame and
+read back after it, wall-clock timed.
+
+--impl reference times the SolidCloth reference's own CPU step (compiled from
+its sources into oracle/_ref) on the host cores, one substep per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "cloth vertex-substeps/s on 1 B200; learned vs plain iters at equal residual"
+UNIT = "vertex-substeps/s"
+
+
+def _args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="cfg1", choices=["cfg0", "cfg1", "cfg2"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def _scene(name):
+    from solidcloth_b200 import scenes
+    return scenes.CONFIGS[name]()
+
+
+def _workload(sc):
+    return {"workload": f"{sc.name}: {sc.n}x{sc.n} grid ({sc.num_vertices} vertices), "
+                        f"{sc.params.substeps} substeps x {sc.params.iterations} iterations per frame, dt 1/60",
+            "flags": sc.params.flags, "colliders": {"sdf": len(sc.sdfs), "mesh": len(sc.meshes),
+                                                      "walls": sc.walls is not None},
+            "iterations": "fixed", "l2": "flushed (256 MiB write) before every timed frame",
+            "step": "one frame = one scStepCloth call"}
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index),
+                 "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in Path(self.path).read_text().splitlines():
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 9:
+                    rows.append(f)
+        except Exception:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for k, n in enumerate(names):
+                if r[5 + k].lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def cpu_reference_rate(sc, substeps: int, threads: int | None = None):
+    """Time the reference's own CPU step (oracle/_ref) on a bounded sample:
+    `substeps` substeps of the scene after one untimed substep."""
+    import ctypes as C
+    from oracle.bridge import RefCloth, _load, REF_LIB
+    if threads:
+        RefCloth.set_threads(threads)
+    cores = _load(REF_LIB, "ref_").ref_max_threads()
+    r = RefCloth.from_scene(sc)
+    h = sc.dt / sc.params.substeps
+    # one substep per call: a patch with numSteps = 1 and dt = h
+    pa = sc.params.as_array().copy()
+    pa[9] = 1
+    r._fn("set_params")(r.h, pa.ctypes.data_as(C.POINTER(C.c_float)), pa.size)
+    r.step(h)
+    t0 = time.perf_counter()
+    for _ in range(substeps):
+        r.step(h)
+    dt = time.perf_counter() - t0
+    r.close()
+    return sc.num_vertices * substeps / dt, dt, int(cores)
+
+
+def run_reference(args):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return
+    sc = _scene(args.config)
+    from oracle.bridge import available
+    if not available("ref"):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libscref.so not built (reference sources absent at build time)"}))
+        return
+    from oracle.bridge import RefCloth, _load, REF_LIB
+    lib = _load(REF_LIB, "ref_")
+    cores = lib.ref_max_threads()
+    r = RefCloth.from_scene(sc)
+    import ctypes as C
+    h = sc.dt / sc.params.substeps
+    pa = sc.params.as_array().copy()
+    pa[9] = 1
+    r._fn("set_params")(r.h, pa.ctypes.data_as(C.POINTER(C.c_float)), pa.size)
+    for _ in range(args.warmup):
+        r.step(h)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        r.step(h)
+        times.append(time.perf_counter() - t0)
+    tot = sum(times)
+    value = sc.num_vertices * args.steps / tot
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+            "data": "synthetic", "config": dict(_workload(sc), step="one substep (reference CPU)"),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                             "sample": f"{args.steps} substeps of {sc.name} after {args.warmup} warm-up substeps, "
+                                       f"OpenMP threads = {cores}"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def run_ours(args):
+    import torch
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    from solidcloth_b200 import api
+    sc = _scene(args.config)
+    w, p = api.load_scene(sc)
+    stream = torch.cuda.ExternalStream(p.cuda_stream(), device=torch.device("cuda", local))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    for _ in range(args.warmup):
+        p.step(sc.dt)
+    p.synchronize()
+    st = p.status()
+    kernels_per_frame = p.graph_kernel_count()
+
+    def barrier():
+        if ws > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    with Clocks(local) as clk:
+        barrier()
+        with torch.cuda.stream(stream):
+            for k in range(args.steps):
+                flush.fill_(float(k))
+                starts[k].record(stream)
+                p.step(sc.dt)
+                ends[k].record(stream)
+        barrier()
+    ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    tot_ms = float(sum(ms))
+    if ws > 1:
+        t = torch.tensor([tot_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        tot_ms = float(t.item())
+    vsub = sc.num_vertices * sc.params.substeps
+    value = ws * vsub * args.steps / (tot_ms * 1e-3)
+    status = st | p.status()
+
+    # end to end through the C ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        pos = torch.empty((sc.num_vertices, 3), dtype=torch.float32).pin_memory().numpy()
+        prev = torch.empty_like(torch.from_numpy(pos)).pin_memory().numpy()
+        vel = torch.empty_like(torch.from_numpy(pos)).pin_memory().numpy()
+        pos[:] = p.model.positions()
+        prev[:] = p.model.prev_positions()
+        vel[:] = p.model.velocities()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            p.model.set_state(pos, prev, vel)
+            p.step(sc.dt)
+            pos[:] = p.model.positions()
+            prev[:] = p.model.prev_positions()
+            vel[:] = p.model.velocities()
+        barrier()
+        e2e_s = time.perf_counter() - t0
+        if ws > 1:
+            t = torch.tensor([e2e_s], device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e = {"value": ws * vsub * args.steps / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": 3 * 16 * sc.num_vertices,
+               "d2h_bytes_per_step": 3 * 16 * sc.num_vertices,
+               "path": "scSetParticleState -> scStepCloth -> scGetParticlePositions/Prev/Velocities"}
+
+    # roofline of the dominant constraint sweep (FEM), timed alone with events
+    T = len(p.model.tris())
+    fem_ms = p.profile_sweep(0, reps=50)
+    bend_ms = p.profile_sweep(1, reps=50)
+    B = len(p.model.bends())
+    peak, peak_kind = _peaks()
+    fem_bytes = 144 * T
+    achieved = fem_bytes / (fem_ms * 1e-3) / 1e9
+    traffic = None
+    tj = ROOT / "profiles" / "traffic.json"
+    if tj.exists():
+        try:
+            traffic = json.loads(tj.read_text()).get(f"{args.config}_fem_sweep_bytes")
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "kernel": "k_fem (one FEM sweep = all colours of one iteration)",
+                "algorithmic_bytes_per_launch": fem_bytes, "ms_per_sweep": fem_ms,
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                "bend_sweep": {"ms": bend_ms, "achieved_gbs": 144 * B / (bend_ms * 1e-3) / 1e9}}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            from oracle.bridge import available
+            if available("ref"):
+                nsub = 2 if sc.num_vertices > 4096 else 32
+                v, secs, cores = cpu_reference_rate(sc, nsub)
+                cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
+                       "sample": f"{nsub} substeps of {sc.name} after one untimed substep ({secs:.1f} s), "
+                                 f"the reference's own C++ (oracle/_ref, OpenMP {cores} threads)"}
+        except Exception as e:  # reported, not fatal
+            cpu = {"value": None, "unit": UNIT, "cores": None, "kind": "reference", "sample": f"failed: {e}"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+                "config": _workload(sc), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": kernels_per_frame * args.steps, "kernels_per_frame": kernels_per_frame,
+                "clocks": clk.summary(), "device_status": status}
+        print(json.dumps(line))
+    p.free()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    args = _args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

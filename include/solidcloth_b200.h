@@ -1,0 +1,229 @@
+/*
+ * solidcloth_b200.h — C ABI of the B200 cloth step (libsolidcloth_b200.so).
+ *
+ * Drop-in for the SolidCloth "ClothAPI" (Demo/ClothAPI.h:65-146): the same sc*
+ * entry points, handle structs and argument meaning, so a caller that binds the
+ * reference's ClothLib binds this library by changing the library name. Where
+ * the reference passes C++ references (Vector3&, int&) this header declares the
+ * ABI-identical pointers; Math::Vector3 is 3 packed floats (scVector3) and
+ * Geometry::Aabb3 two of them (scAabb3).
+ *
+ * Differences, all additive or forced by the absence of C++ types in a C ABI:
+ *   - scCreateSDF(Geometry::SDF*) / scCreateMesh(Geometry::Mesh*) take caller-owned
+ *     C++ objects in the reference; here the grid / mesh data are passed as
+ *     arrays (scCreateSDFGrid, scCreateMeshCollider).
+ *   - scComputeStrainMap fills a caller array instead of a std::vector.
+ *   - The step runs asynchronously on the patch's CUDA stream; every getter
+ *     synchronises first, so results are visible exactly as in the reference.
+ *   - Errors: the reference has none (invalid handles are UB). Every entry point
+ *     here records failures; scGetLastError() returns and clears the last one.
+ * Each declaration cites the reference declaration it replaces.
+ */
+#ifndef SOLIDCLOTH_B200_H
+#define SOLIDCLOTH_B200_H
+
+#include <stdbool.h>
+
+#if defined(_WIN32)
+#define SCEXP __declspec(dllexport)
+#else
+#define SCEXP __attribute__((visibility("default")))
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef void* scHandle;                                 /* Demo/ClothAPI.h:9 */
+typedef struct scClothPatch { void* ptr; } scClothPatch; /* Demo/ClothAPI.h:11-17 */
+typedef struct scCollisionWorld { void* ptr; } scCollisionWorld; /* :19-22 */
+typedef struct scMesh { void* ptr; } scMesh;            /* :24-27 */
+typedef struct scModel { void* ptr; } scModel;          /* :29-32 */
+typedef struct scVector3 { float x, y, z; } scVector3;  /* Math::Vector3 */
+typedef struct scVector2 { float x, y; } scVector2;     /* Math::Vector2 */
+typedef struct scAabb3 { scVector3 min, max; } scAabb3; /* Geometry::Aabb3 */
+typedef struct scQuaternion { float s; scVector3 v; } scQuaternion; /* Math::Quaternion */
+
+enum scCollFlags                                        /* Demo/ClothAPI.h:34-41 */
+{
+    scCollisionFlagVertices = 1,
+    scCollisionFlagTriangles = 2,
+    scCollisionFlagSelf = 4,
+    scCollisionFlagWalls = 8,
+    scCollisionFlagEdges = 16,
+};
+
+enum scCollidableType                                   /* Demo/ClothAPI.h:43-53 */
+{
+    scCollidableTypeInvalid,
+    scCollidableTypeWalls,
+    scCollidableTypeSlab,
+    scCollidableTypeSphere,
+    scCollidableTypeMesh,
+    scCollidableTypeBox,
+    scCollidableTypeCapsule,
+    scCollidableTypeSDF,
+};
+
+/* ---- collision world (Demo/ClothAPI.h:68-74) ---- */
+SCEXP scCollisionWorld scCreateCollisionWorld(void);
+SCEXP void scFreeCollisionWorld(scCollisionWorld collWorld);
+SCEXP void scClearCollidables(scCollisionWorld collWorld);
+SCEXP int scGetNumCollidables(scCollisionWorld collWorld);
+/* Transfers ownership of the collidable to the world (Demo/ClothAPI.cpp:38-43). */
+SCEXP void scAddCollidable(scCollisionWorld collWorld, scHandle collidable);
+SCEXP scHandle scGetCollidable(scCollisionWorld collWorld, int i);
+
+/* ---- collidables (Demo/ClothAPI.h:77-87) ---- */
+SCEXP scHandle scCreateWalls(scAabb3 box);
+SCEXP scHandle scCreateSphere(scVector3 center, float radius);
+/* Stored and reported by scGetCapsuleInfo; the GPU step ignores capsules. */
+SCEXP scHandle scCreateCapsule(scVector3 c, float rad, float halfHeight, scQuaternion quat);
+/* Replaces scCreateSDF(Geometry::SDF*) (Demo/ClothAPI.h:80): a (nx+1)(ny+1)(nz+1)
+   float grid over `box`, x fastest, as Geometry::SDF::Create(nx, ny, nz, box) +
+   values + ComputeGradient() (Geometry/SDF.cpp:10-56,210-256). Values are copied. */
+SCEXP scHandle scCreateSDFGrid(int nx, int ny, int nz, scAabb3 box, const float* values);
+/* Replaces scCreateMesh(Geometry::Mesh*) (Demo/ClothAPI.h:81): a triangle mesh
+   prepared as Demo/ClothDemo.cpp:100-103 does (normals, edges, edge one-rings).
+   Arrays are copied. */
+SCEXP scHandle scCreateMeshCollider(const float* vertices, int numVertices, const unsigned* indices, int numIndices);
+SCEXP int scGetCollidableType(scHandle collidable);
+/* Opaque here: the reference returns its Geometry::AabbTree*, a C++ type. */
+SCEXP void* scGetMeshTree(scHandle collMesh);
+SCEXP void scGetWallsInfo(scHandle walls, scAabb3* box);
+SCEXP void scGetSphereInfo(scHandle sphere, float* radius, scVector3* center);
+SCEXP void scGetCapsuleInfo(scHandle capsule, float* radius, float* halfHeight, scVector3* center, scQuaternion* rot);
+
+/* ---- cloth patch (Demo/ClothAPI.h:91-99) ---- */
+SCEXP scClothPatch scCreateClothPatch(scCollisionWorld collWorld);
+SCEXP void scFreeClothPatch(scClothPatch patch);
+SCEXP scModel scGetClothModel(scClothPatch patch);
+SCEXP scMesh scGetClothMesh(scClothPatch patch);
+SCEXP void scInitCloth(scClothPatch patch, int divX, int divY, float inc, scVector3 offset, bool horizontal, bool attached);
+/* The hot entry point: ClothPatch::Step (Demo/ClothAPI.cpp:146-150). */
+SCEXP void scStepCloth(scClothPatch patch, float dt);
+SCEXP void scUpdateClothMesh(scClothPatch patch);
+/* Replaces scComputeStrainMap(patch, std::vector<Vector3>&): colors has one
+   scVector3 per particle. */
+SCEXP void scComputeStrainMap(scClothPatch patch, scVector3* colors);
+
+/* ---- cloth model (Demo/ClothAPI.h:102-138) ---- */
+SCEXP int scGetNumParticles(scModel model);
+SCEXP void scGetParticlePos(scModel model, int i, scVector3* pos);
+SCEXP float scGetParticleInvMass(scModel model, int i);
+SCEXP int scGetNumTris(scModel model);
+SCEXP void scGetTriangle(scModel model, int i, int* i1, int* i2, int* i3);
+SCEXP void scGetTriangleInfo(scModel model, int i, float* invDet, scVector2* du, scVector2* dv, scVector2* s);
+SCEXP int scGetNumQuads(scModel model);
+SCEXP void scGetQuad(scModel model, int i, int* i1, int* i2, int* i3, int* i4);
+SCEXP int scGetNumLinks(scModel model);
+SCEXP void scGetLink(scModel model, int i, int* i1, int* i2);
+SCEXP int scGetNumContacts(scModel model);
+SCEXP void scGetContact(scModel model, int i, scVector3* point, scVector3* normal);
+SCEXP int scGetNumTriContacts(scModel model);
+SCEXP void scGetTriContact(scModel model, int i, scVector3* point, scVector3* normal);
+SCEXP int scGetCollisionFlags(scModel model);
+SCEXP void scSetCollisionFlags(scModel model, int val);
+SCEXP float scGetThickness(scModel model);
+SCEXP void scSetThickness(scModel model, float val);
+SCEXP float scGetTolerance(scModel model);
+SCEXP void scSetTolerance(scModel model, float val);
+SCEXP float scGetFriction(scModel model);
+SCEXP void scSetFriction(scModel model, float val);
+SCEXP int scGetNumIterations(scModel model);
+SCEXP void scSetNumIterations(scModel model, int val);
+SCEXP bool scGetUseFEM(scModel model);
+SCEXP void scSetUseFEM(scModel model, bool val);
+/* Opaque here (Demo/ClothAPI.h:134 returns Geometry::AabbTree*). */
+SCEXP void* scGetClothTree(scModel model);
+SCEXP void scAddMouseSpring(scModel model, int i1, int i2, int i3, scVector3 coords, scVector3 p);
+SCEXP void scUpdateMouseSpring(scModel model, scVector3 p);
+SCEXP void scRemoveMouseSpring(scModel model);
+
+/* ---- mesh (Demo/ClothAPI.h:141-145); borrowed pointers, valid until the next
+   scUpdateClothMesh / scInitCloth / scFreeClothPatch ---- */
+SCEXP int scGetMeshVertexCount(scMesh mesh);
+SCEXP int scGetMeshIndexCount(scMesh mesh);
+SCEXP scVector3* scGetMeshNormalBuffer(scMesh mesh);
+SCEXP scVector3* scGetMeshVertexBuffer(scMesh mesh);
+SCEXP unsigned int* scGetMeshIndexBuffer(scMesh mesh);
+
+/* ---- additions: setters the reference has only on the C++ ClothModel /
+   ClothPatch (Physics/ClothModel.h:110-146, Physics/ClothPatch.h:49-50) ---- */
+SCEXP void scSetUnit(scModel model, float val);
+SCEXP float scGetUnit(scModel model);
+SCEXP void scSetShearStiffness(scModel model, float val);
+SCEXP void scSetBendStiffness(scModel model, float val);
+SCEXP void scSetStretchStiffness(scModel model, float val);
+SCEXP void scSetPoisson(scModel model, float val);
+SCEXP void scSetDragCoeff(scModel model, float val);
+SCEXP void scSetDihedral(scModel model, bool val);
+SCEXP void scSetSelfShrink(scModel model, float val);
+SCEXP void scSetNumSteps(scClothPatch patch, int val);
+SCEXP int scGetNumSteps(scClothPatch patch);
+/* ClothModel::SetMasses (Physics/ClothModel.cpp:45-52): mass 0 pins a particle. */
+SCEXP void scSetMasses(scModel model, const float* masses);
+SCEXP void scSetParticleInvMass(scModel model, int i, float invMass);
+/* ClothModel::SetPositions (Physics/ClothModel.cpp:38-43), bulk xyz; also sets
+   the previous positions, as a freshly initialised patch has them equal. */
+SCEXP void scSetParticlePositions(scModel model, const float* xyz);
+SCEXP void scGetParticlePositions(scModel model, float* xyz);
+SCEXP void scGetParticleVelocities(scModel model, float* xyz);
+SCEXP void scGetParticlePrevPositions(scModel model, float* xyz);
+SCEXP void scSetParticleState(scModel model, const float* pos, const float* prev, const float* vel);
+/* Fixed iteration count: bypasses the GS early exit (Physics/ClothPBD.cpp:357),
+   which in FEM mode otherwise stops after one iteration without contacts. */
+SCEXP void scSetFixedIterations(scModel model, bool val);
+/* Continuous vertex-triangle / edge-edge self-collision
+   (Physics/SelfCollisionDetector.cpp), appended to the self contacts each substep. */
+SCEXP void scSetSelfCCD(scModel model, bool val);
+SCEXP int scGetSolverIterations(scModel model);
+
+/* ---- additions: inspection for parity checks ---- */
+/* kind 0: FEM triangles, 1: bends. Writes the solve order (a permutation) and
+   returns the number of colours; colourStart gets numColours+1 offsets if not NULL. */
+SCEXP int scGetConstraintOrder(scModel model, int kind, int* order, int* colourStart);
+SCEXP int scGetNumBends(scModel model);
+SCEXP void scGetBends(scModel model, unsigned* idx4);
+SCEXP int scGetNumEdges(scModel model);
+SCEXP void scGetEdges(scModel model, int* e4);
+/* kind 0 vertex, 1 triangle, 2 edge, 3 self vertex-triangle, 4 self edge-edge */
+SCEXP int scGetNumContactsOfKind(scModel model, int kind);
+/* self contacts (kind 3/4): idx4 = i1..i4, f7 = normal xyz, w1, w2, w3, side */
+SCEXP void scGetSelfContacts(scModel model, int kind, int* idx4, float* f7);
+/* vertex contacts in list order: idx2 = particle, feature; f6 = point, normal */
+SCEXP void scGetVertexContacts(scModel model, int* idx2, float* f6);
+/* triangle contacts: idx4 = i1 i2 i3 feature; f9 = point normal w */
+SCEXP void scGetTriContacts(scModel model, int* idx4, float* f9);
+/* edge contacts: idx3 = i1 i2 feature; f8 = point normal w1 w2 */
+SCEXP void scGetEdgeContacts(scModel model, int* idx3, float* f8);
+/* continuous-collision broad-phase pairs of the last substep:
+   kind 0 -> (vertex, triangle), kind 1 -> (edge, edge); returns the count */
+SCEXP int scGetCCDCandidates(scModel model, int kind, int* pairs, int cap);
+/* collision-mesh (prev positions) vertex normals as of the last mesh update */
+SCEXP void scGetCollisionMeshNormals(scModel model, float* xyz);
+
+/* ---- additions: errors and synchronisation ---- */
+SCEXP int scGetLastError(void);
+SCEXP const char* scGetLastErrorString(void);
+/* device-side status bits of the last steps (overflow of fixed-capacity
+   contact slots etc.); clears them */
+SCEXP int scGetStatus(scClothPatch patch);
+SCEXP void scSynchronize(scClothPatch patch);
+
+/* ---- additions: measurement ---- */
+/* the patch's CUDA stream (cudaStream_t), for events around scStepCloth */
+SCEXP void* scGetCudaStream(scClothPatch patch);
+/* kernel nodes in the frame graph of the last scStepCloth (launches per frame) */
+SCEXP int scGetGraphKernelCount(scClothPatch patch);
+/* Time `reps` back-to-back constraint sweeps (kind 0: all FEM colours of one
+   iteration, 1: all bend colours) captured as one graph, with CUDA events on
+   the patch stream; returns milliseconds per sweep, or a negative value on error.
+   Particle positions are modified. */
+SCEXP float scProfileSweep(scClothPatch patch, int kind, int reps);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SOLIDCLOTH_B200_H */

@@ -1783,10 +1783,16 @@ struct Cloth
         for (auto& p : ee) ee_test(p.first, p.second);
     }
 
+    /* The continuous detector run inside a step. Candidate pairs are taken in
+       the canonical order the GPU produces them: (vertex, triangle) ascending
+       for vertex-triangle pairs, (edge, higher edge) for edge-edge pairs. */
     void ccd_detect()
     {
         std::vector<std::pair<int, int>> vt, ee;
         broadphase(thickness + tolerance * 0.5f, vt, ee);
+        std::sort(vt.begin(), vt.end(), [](const std::pair<int, int>& a, const std::pair<int, int>& b) {
+            return a.second < b.second || (a.second == b.second && a.first < b.first);
+        });
         narrow(vt, ee);
     }
 };

@@ -1,0 +1,420 @@
+"""Python binding of the C ABI (include/solidcloth_b200.h) over ctypes.
+
+The classes mirror the reference's C++ objects that ClothDemo drives directly
+(Physics/CollisionWorld.h, Physics/ClothPatch.h, Physics/ClothModel.h) and call
+the same sc* entry points a ctypes / cgo / JNI caller of the reference's
+ClothLib would bind. There is no CPU fallback: if the CUDA library is not built
+or no CUDA device is usable, constructing a patch raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+from .scenes import Scene
+
+LIB_PATH = Path(__file__).resolve().parent / "lib" / "libsolidcloth_b200.so"
+
+
+class scVector3(C.Structure):
+    _fields_ = [("x", C.c_float), ("y", C.c_float), ("z", C.c_float)]
+
+
+class scVector2(C.Structure):
+    _fields_ = [("x", C.c_float), ("y", C.c_float)]
+
+
+class scAabb3(C.Structure):
+    _fields_ = [("min", scVector3), ("max", scVector3)]
+
+
+class scQuaternion(C.Structure):
+    _fields_ = [("s", C.c_float), ("v", scVector3)]
+
+
+class _Handle(C.Structure):
+    _fields_ = [("ptr", C.c_void_p)]
+
+
+scClothPatch = scCollisionWorld = scMesh = scModel = _Handle
+_f = C.POINTER(C.c_float)
+_i = C.POINTER(C.c_int)
+_u = C.POINTER(C.c_uint)
+
+# name -> (argtypes, restype)
+SIGNATURES = {
+    "scCreateCollisionWorld": ([], scCollisionWorld),
+    "scFreeCollisionWorld": ([scCollisionWorld], None),
+    "scClearCollidables": ([scCollisionWorld], None),
+    "scGetNumCollidables": ([scCollisionWorld], C.c_int),
+    "scAddCollidable": ([scCollisionWorld, C.c_void_p], None),
+    "scGetCollidable": ([scCollisionWorld, C.c_int], C.c_void_p),
+    "scCreateWalls": ([scAabb3], C.c_void_p),
+    "scCreateSphere": ([scVector3, C.c_float], C.c_void_p),
+    "scCreateCapsule": ([scVector3, C.c_float, C.c_float, scQuaternion], C.c_void_p),
+    "scCreateSDFGrid": ([C.c_int, C.c_int, C.c_int, scAabb3, _f], C.c_void_p),
+    "scCreateMeshCollider": ([_f, C.c_int, _u, C.c_int], C.c_void_p),
+    "scGetCollidableType": ([C.c_void_p], C.c_int),
+    "scGetMeshTree": ([C.c_void_p], C.c_void_p),
+    "scGetWallsInfo": ([C.c_void_p, C.POINTER(scAabb3)], None),
+    "scGetSphereInfo": ([C.c_void_p, _f, C.POINTER(scVector3)], None),
+    "scGetCapsuleInfo": ([C.c_void_p, _f, _f, C.POINTER(scVector3), C.POINTER(scQuaternion)], None),
+    "scCreateClothPatch": ([scCollisionWorld], scClothPatch),
+    "scFreeClothPatch": ([scClothPatch], None),
+    "scGetClothModel": ([scClothPatch], scModel),
+    "scGetClothMesh": ([scClothPatch], scMesh),
+    "scInitCloth": ([scClothPatch, C.c_int, C.c_int, C.c_float, scVector3, C.c_bool, C.c_bool], None),
+    "scStepCloth": ([scClothPatch, C.c_float], None),
+    "scUpdateClothMesh": ([scClothPatch], None),
+    "scComputeStrainMap": ([scClothPatch, C.POINTER(scVector3)], None),
+    "scGetNumParticles": ([scModel], C.c_int),
+    "scGetParticlePos": ([scModel, C.c_int, C.POINTER(scVector3)], None),
+    "scGetParticleInvMass": ([scModel, C.c_int], C.c_float),
+    "scGetNumTris": ([scModel], C.c_int),
+    "scGetTriangle": ([scModel, C.c_int, _i, _i, _i], None),
+    "scGetTriangleInfo": ([scModel, C.c_int, _f, C.POINTER(scVector2), C.POINTER(scVector2), C.POINTER(scVector2)], None),
+    "scGetNumQuads": ([scModel], C.c_int),
+    "scGetQuad": ([scModel, C.c_int, _i, _i, _i, _i], None),
+    "scGetNumLinks": ([scModel], C.c_int),
+    "scGetLink": ([scModel, C.c_int, _i, _i], None),
+    "scGetNumContacts": ([scModel], C.c_int),
+    "scGetContact": ([scModel, C.c_int, C.POINTER(scVector3), C.POINTER(scVector3)], None),
+    "scGetNumTriContacts": ([scModel], C.c_int),
+    "scGetTriContact": ([scModel, C.c_int, C.POINTER(scVector3), C.POINTER(scVector3)], None),
+    "scGetCollisionFlags": ([scModel], C.c_int),
+    "scSetCollisionFlags": ([scModel, C.c_int], None),
+    "scGetThickness": ([scModel], C.c_float),
+    "scSetThickness": ([scModel, C.c_float], None),
+    "scGetTolerance": ([scModel], C.c_float),
+    "scSetTolerance": ([scModel, C.c_float], None),
+    "scGetFriction": ([scModel], C.c_float),
+    "scSetFriction": ([scModel, C.c_float], None),
+    "scGetNumIterations": ([scModel], C.c_int),
+    "scSetNumIterations": ([scModel, C.c_int], None),
+    "scGetUseFEM": ([scModel], C.c_bool),
+    "scSetUseFEM": ([scModel, C.c_bool], None),
+    "scGetClothTree": ([scModel], C.c_void_p),
+    "scAddMouseSpring": ([scModel, C.c_int, C.c_int, C.c_int, scVector3, scVector3], None),
+    "scUpdateMouseSpring": ([scModel, scVector3], None),
+    "scRemoveMouseSpring": ([scModel], None),
+    "scGetMeshVertexCount": ([scMesh], C.c_int),
+    "scGetMeshIndexCount": ([scMesh], C.c_int),
+    "scGetMeshNormalBuffer": ([scMesh], C.POINTER(scVector3)),
+    "scGetMeshVertexBuffer": ([scMesh], C.POINTER(scVector3)),
+    "scGetMeshIndexBuffer": ([scMesh], C.POINTER(C.c_uint)),
+    "scSetUnit": ([scModel, C.c_float], None),
+    "scGetUnit": ([scModel], C.c_float),
+    "scSetShearStiffness": ([scModel, C.c_float], None),
+    "scSetBendStiffness": ([scModel, C.c_float], None),
+    "scSetStretchStiffness": ([scModel, C.c_float], None),
+    "scSetPoisson": ([scModel, C.c_float], None),
+    "scSetDragCoeff": ([scModel, C.c_float], None),
+    "scSetDihedral": ([scModel, C.c_bool], None),
+    "scSetSelfShrink": ([scModel, C.c_float], None),
+    "scSetNumSteps": ([scClothPatch, C.c_int], None),
+    "scGetNumSteps": ([scClothPatch], C.c_int),
+    "scSetMasses": ([scModel, _f], None),
+    "scSetParticleInvMass": ([scModel, C.c_int, C.c_float], None),
+    "scSetParticlePositions": ([scModel, _f], None),
+    "scGetParticlePositions": ([scModel, _f], None),
+    "scGetParticleVelocities": ([scModel, _f], None),
+    "scGetParticlePrevPositions": ([scModel, _f], None),
+    "scSetParticleState": ([scModel, _f, _f, _f], None),
+    "scSetFixedIterations": ([scModel, C.c_bool], None),
+    "scSetSelfCCD": ([scModel, C.c_bool], None),
+    "scGetSolverIterations": ([scModel], C.c_int),
+    "scGetConstraintOrder": ([scModel, C.c_int, _i, _i], C.c_int),
+    "scGetNumBends": ([scModel], C.c_int),
+    "scGetBends": ([scModel, _u], None),
+    "scGetNumEdges": ([scModel], C.c_int),
+    "scGetEdges": ([scModel, _i], None),
+    "scGetNumContactsOfKind": ([scModel, C.c_int], C.c_int),
+    "scGetSelfContacts": ([scModel, C.c_int, _i, _f], None),
+    "scGetVertexContacts": ([scModel, _i, _f], None),
+    "scGetTriContacts": ([scModel, _i, _f], None),
+    "scGetEdgeContacts": ([scModel, _i, _f], None),
+    "scGetCCDCandidates": ([scModel, C.c_int, _i, C.c_int], C.c_int),
+    "scGetCollisionMeshNormals": ([scModel, _f], None),
+    "scGetLastError": ([], C.c_int),
+    "scGetLastErrorString": ([], C.c_char_p),
+    "scGetStatus": ([scClothPatch], C.c_int),
+    "scSynchronize": ([scClothPatch], None),
+    "scGetCudaStream": ([scClothPatch], C.c_void_p),
+    "scGetGraphKernelCount": ([scClothPatch], C.c_int),
+    "scProfileSweep": ([scClothPatch, C.c_int, C.c_int], C.c_float),
+}
+
+_lib = None
+
+
+def lib():
+    """Load the CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m solidcloth_b200.build`")
+        L = C.CDLL(str(LIB_PATH))
+        for name, (args, res) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def _fp(a):
+    return a.ctypes.data_as(_f)
+
+
+def _check(what: str):
+    L = lib()
+    msg = L.scGetLastErrorString()
+    err = L.scGetLastError()
+    if err:
+        raise RuntimeError(f"{what}: error {err}: {msg.decode() if msg else ''}")
+
+
+def v3(x) -> scVector3:
+    return scVector3(float(x[0]), float(x[1]), float(x[2]))
+
+
+class CollisionWorld:
+    """Physics::CollisionWorld (Physics/CollisionWorld.h:10-29)."""
+
+    def __init__(self):
+        self.h = lib().scCreateCollisionWorld()
+
+    def add_walls(self, box6):
+        b = scAabb3(v3(box6[:3]), v3(box6[3:]))
+        lib().scAddCollidable(self.h, lib().scCreateWalls(b))
+
+    def add_sphere(self, center, radius):
+        lib().scAddCollidable(self.h, lib().scCreateSphere(v3(center), float(radius)))
+
+    def add_sdf(self, grid):
+        vals = np.ascontiguousarray(grid.values, np.float32)
+        b = scAabb3(v3(grid.box[:3]), v3(grid.box[3:]))
+        h = lib().scCreateSDFGrid(grid.cells[0], grid.cells[1], grid.cells[2], b, _fp(vals))
+        _check("scCreateSDFGrid")
+        lib().scAddCollidable(self.h, h)
+
+    def add_mesh(self, mesh):
+        v = np.ascontiguousarray(mesh.vertices, np.float32)
+        idx = np.ascontiguousarray(mesh.indices, np.uint32)
+        h = lib().scCreateMeshCollider(_fp(v), v.shape[0], idx.ctypes.data_as(_u), idx.size)
+        _check("scCreateMeshCollider")
+        lib().scAddCollidable(self.h, h)
+
+    def clear(self):
+        lib().scClearCollidables(self.h)
+
+    @property
+    def num_collidables(self):
+        return lib().scGetNumCollidables(self.h)
+
+    def free(self):
+        if self.h is not None:
+            lib().scFreeCollisionWorld(self.h)
+            self.h = None
+
+
+class ClothModel:
+    """Physics::ClothModel as seen through the scModel handle."""
+
+    def __init__(self, handle, patch):
+        self.h = handle
+        self.patch = patch
+
+    @property
+    def num_particles(self):
+        return lib().scGetNumParticles(self.h)
+
+    def set_params(self, p):
+        L = lib()
+        L.scSetUnit(self.h, p.unit)
+        L.scSetThickness(self.h, p.thickness)
+        L.scSetTolerance(self.h, p.tolerance)
+        L.scSetShearStiffness(self.h, p.shear)
+        L.scSetBendStiffness(self.h, p.bend)
+        L.scSetStretchStiffness(self.h, p.stretch)
+        L.scSetPoisson(self.h, p.poisson)
+        L.scSetFriction(self.h, p.friction)
+        L.scSetNumIterations(self.h, int(p.iterations))
+        L.scSetCollisionFlags(self.h, int(p.flags))
+        L.scSetUseFEM(self.h, bool(p.fem))
+        L.scSetDihedral(self.h, bool(p.dihedral))
+        L.scSetFixedIterations(self.h, bool(p.fixed_iterations))
+        L.scSetDragCoeff(self.h, p.drag)
+        _check("set_params")
+
+    def set_masses(self, masses):
+        m = np.ascontiguousarray(masses, np.float32)
+        lib().scSetMasses(self.h, _fp(m))
+        _check("scSetMasses")
+
+    def set_positions(self, pos):
+        p = np.ascontiguousarray(pos, np.float32)
+        lib().scSetParticlePositions(self.h, _fp(p))
+        _check("scSetParticlePositions")
+
+    def set_state(self, pos, prev, vel):
+        a, b, c = (np.ascontiguousarray(x, np.float32) for x in (pos, prev, vel))
+        lib().scSetParticleState(self.h, _fp(a), _fp(b), _fp(c))
+        _check("scSetParticleState")
+
+    def _get3(self, fn):
+        out = np.zeros((self.num_particles, 3), np.float32)
+        getattr(lib(), fn)(self.h, _fp(out))
+        return out
+
+    def positions(self):
+        return self._get3("scGetParticlePositions")
+
+    def velocities(self):
+        return self._get3("scGetParticleVelocities")
+
+    def prev_positions(self):
+        return self._get3("scGetParticlePrevPositions")
+
+    def collision_mesh_normals(self):
+        return self._get3("scGetCollisionMeshNormals")
+
+    def inv_masses(self):
+        return np.array([lib().scGetParticleInvMass(self.h, i) for i in range(self.num_particles)], np.float32)
+
+    def set_ccd(self, on: bool):
+        lib().scSetSelfCCD(self.h, bool(on))
+
+    def constraint_order(self, kind):
+        n = lib().scGetNumTris(self.h) if kind == 0 else lib().scGetNumBends(self.h)
+        order = np.zeros(n, np.int32)
+        start = np.zeros(70, np.int32)
+        nc = lib().scGetConstraintOrder(self.h, kind, order.ctypes.data_as(_i), start.ctypes.data_as(_i))
+        return order, start[:nc + 1].copy()
+
+    def tris(self):
+        n = lib().scGetNumTris(self.h)
+        out = np.zeros((n, 3), np.int32)
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        for t in range(n):
+            lib().scGetTriangle(self.h, t, C.byref(a), C.byref(b), C.byref(c))
+            out[t] = (a.value, b.value, c.value)
+        return out
+
+    def bends(self):
+        n = lib().scGetNumBends(self.h)
+        out = np.zeros((n, 4), np.uint32)
+        lib().scGetBends(self.h, out.ctypes.data_as(_u))
+        return out
+
+    def edges(self):
+        n = lib().scGetNumEdges(self.h)
+        out = np.zeros((n, 4), np.int32)
+        lib().scGetEdges(self.h, out.ctypes.data_as(_i))
+        return out
+
+    def contacts(self, kind):
+        """kind 0 vertex, 1 tri, 2 edge, 3 self VT, 4 self EE (oracle layout)."""
+        L = lib()
+        n = L.scGetNumContactsOfKind(self.h, kind)
+        if kind == 0:
+            a = np.zeros((n, 2), np.int32); f = np.zeros((n, 6), np.float32)
+            L.scGetVertexContacts(self.h, a.ctypes.data_as(_i), _fp(f))
+        elif kind == 1:
+            a = np.zeros((n, 4), np.int32); f = np.zeros((n, 9), np.float32)
+            L.scGetTriContacts(self.h, a.ctypes.data_as(_i), _fp(f))
+        elif kind == 2:
+            a = np.zeros((n, 3), np.int32); f = np.zeros((n, 8), np.float32)
+            L.scGetEdgeContacts(self.h, a.ctypes.data_as(_i), _fp(f))
+        else:
+            a = np.zeros((n, 4), np.int32); f = np.zeros((n, 7), np.float32)
+            L.scGetSelfContacts(self.h, kind, a.ctypes.data_as(_i), _fp(f))
+        return a, f
+
+    def ccd_candidates(self, kind, cap=1 << 24):
+        out = np.zeros((cap, 2), np.int32)
+        n = lib().scGetCCDCandidates(self.h, kind, out.ctypes.data_as(_i), cap)
+        return out[:min(n, cap)].copy()
+
+    def solver_iterations(self):
+        return lib().scGetSolverIterations(self.h)
+
+
+class ClothPatch:
+    """Physics::ClothPatch (Physics/ClothPatch.h:24-72) on one GPU."""
+
+    def __init__(self, world: CollisionWorld):
+        self.world = world
+        self.h = lib().scCreateClothPatch(world.h)
+        _check("scCreateClothPatch")
+        self.model = ClothModel(lib().scGetClothModel(self.h), self)
+
+    def init_grid(self, div_x, div_y, inc, offset, horizontal=True, attached=False):
+        lib().scInitCloth(self.h, int(div_x), int(div_y), float(inc), v3(offset), bool(horizontal), bool(attached))
+        _check("scInitCloth")
+
+    def set_num_steps(self, n):
+        lib().scSetNumSteps(self.h, int(n))
+
+    def step(self, dt):
+        lib().scStepCloth(self.h, float(dt))
+        _check("scStepCloth")
+
+    def update_mesh(self):
+        lib().scUpdateClothMesh(self.h)
+        _check("scUpdateClothMesh")
+
+    def synchronize(self):
+        lib().scSynchronize(self.h)
+
+    def status(self):
+        return lib().scGetStatus(self.h)
+
+    def cuda_stream(self) -> int:
+        return lib().scGetCudaStream(self.h) or 0
+
+    def graph_kernel_count(self) -> int:
+        return lib().scGetGraphKernelCount(self.h)
+
+    def profile_sweep(self, kind: int, reps: int = 50) -> float:
+        ms = lib().scProfileSweep(self.h, int(kind), int(reps))
+        _check("scProfileSweep")
+        return float(ms)
+
+    def mesh_buffers(self):
+        L = lib()
+        m = L.scGetClothMesh(self.h)
+        nv, ni = L.scGetMeshVertexCount(m), L.scGetMeshIndexCount(m)
+        v = np.ctypeslib.as_array(C.cast(L.scGetMeshVertexBuffer(m), _f), shape=(nv, 3)).copy()
+        nb = L.scGetMeshNormalBuffer(m)
+        n = np.ctypeslib.as_array(C.cast(nb, _f), shape=(nv, 3)).copy() if nb else None
+        idx = np.ctypeslib.as_array(L.scGetMeshIndexBuffer(m), shape=(ni,)).copy()
+        return v, n, idx
+
+    def free(self):
+        if self.h is not None:
+            lib().scFreeClothPatch(self.h)
+            self.h = None
+
+
+def load_scene(scene: Scene, ccd: bool | None = None):
+    """Build world + patch for a scenes.Scene exactly as the oracles do."""
+    w = CollisionWorld()
+    if scene.walls is not None:
+        w.add_walls(scene.walls)
+    for (c, r) in scene.spheres:
+        w.add_sphere(c, r)
+    for g in scene.sdfs:
+        w.add_sdf(g)
+    for m in scene.meshes:
+        w.add_mesh(m)
+    p = ClothPatch(w)
+    p.model.set_params(scene.params)
+    p.set_num_steps(scene.params.substeps)
+    p.init_grid(scene.n, scene.n, scene.inc, scene.offset, True, scene.attached)
+    p.model.set_masses(scene.masses)
+    p.model.set_positions(scene.positions)
+    p.model.set_ccd(scene.ccd if ccd is None else ccd)
+    return w, p

@@ -1,0 +1,610 @@
+// capi.cu — the extern "C" sc* entry points (include/solidcloth_b200.h), each a
+// thin shim over the host objects in cloth.h, mirroring Demo/ClothAPI.cpp.
+#include "cloth.h"
+#include "../../include/solidcloth_b200.h"
+#include <cstring>
+#include <cmath>
+
+using namespace sc;
+
+namespace {
+
+ClothPatch* P(scClothPatch p) { return (ClothPatch*)p.ptr; }
+ClothModel* M(scModel m) { return (ClothModel*)m.ptr; }
+CollisionWorld* W(scCollisionWorld w) { return (CollisionWorld*)w.ptr; }
+V3 v3(scVector3 a) { return mk(a.x, a.y, a.z); }
+scVector3 sv(V3 a) { scVector3 r = {a.x, a.y, a.z}; return r; }
+
+bool check_model(ClothModel* m, int i = -1)
+{
+    if (!m) { set_error(SC_ERR_ARG, "null model handle"); return false; }
+    if (i >= 0 && i >= m->N) { set_error(SC_ERR_ARG, "particle index out of range"); return false; }
+    return true;
+}
+
+void host_sync(ClothModel* m) { if (m && m->owner) m->owner->sync(); }
+
+template <typename T>
+std::vector<T> dl(const T* d, size_t n)
+{
+    std::vector<T> h(n);
+    if (n) cudaMemcpy(h.data(), d, sizeof(T) * n, cudaMemcpyDeviceToHost);
+    return h;
+}
+
+int dcount(const int* d)
+{
+    int v = 0;
+    if (d) cudaMemcpy(&v, d, sizeof(int), cudaMemcpyDeviceToHost);
+    return v;
+}
+
+} // namespace
+
+extern "C" {
+
+// ------------------------------------------------------------------ world
+scCollisionWorld scCreateCollisionWorld(void) { scCollisionWorld w; w.ptr = new CollisionWorld(); return w; }
+void scFreeCollisionWorld(scCollisionWorld w) { delete W(w); }
+void scClearCollidables(scCollisionWorld w) { if (W(w)) { W(w)->list.clear(); W(w)->version++; } }
+int scGetNumCollidables(scCollisionWorld w) { return W(w) ? (int)W(w)->list.size() : 0; }
+void scAddCollidable(scCollisionWorld w, scHandle c)
+{
+    if (!W(w) || !c) { set_error(SC_ERR_ARG, "null handle"); return; }
+    W(w)->list.push_back(std::shared_ptr<Collidable>((Collidable*)c));
+    W(w)->version++;
+}
+scHandle scGetCollidable(scCollisionWorld w, int i)
+{
+    if (!W(w) || i < 0 || i >= (int)W(w)->list.size()) { set_error(SC_ERR_ARG, "collidable index out of range"); return nullptr; }
+    return W(w)->list[i].get();
+}
+
+// -------------------------------------------------------------- collidables
+scHandle scCreateWalls(scAabb3 box)
+{
+    WallsC* w = new WallsC();
+    w->type = CT_WALLS;
+    w->box.lo = v3(box.min); w->box.hi = v3(box.max);
+    return w;
+}
+
+scHandle scCreateSphere(scVector3 center, float radius)
+{
+    SphereC* s = new SphereC();
+    s->type = CT_SPHERE;
+    s->center = v3(center);
+    s->radius = radius;
+    return s;
+}
+
+scHandle scCreateCapsule(scVector3 c, float rad, float halfHeight, scQuaternion q)
+{
+    CapsuleC* k = new CapsuleC();
+    k->type = CT_CAPSULE;
+    k->center = v3(c); k->r = rad; k->hh = halfHeight;
+    k->rot[0] = q.s; k->rot[1] = q.v.x; k->rot[2] = q.v.y; k->rot[3] = q.v.z;
+    return k;
+}
+
+// SDF::Create + CacheData + ComputeGradient (Geometry/SDF.cpp:10-40,210-256)
+scHandle scCreateSDFGrid(int nx, int ny, int nz, scAabb3 box, const float* values)
+{
+    if (nx < 1 || ny < 1 || nz < 1 || !values) { set_error(SC_ERR_ARG, "bad SDF grid"); return nullptr; }
+    SDFC* s = new SDFC();
+    s->type = CT_SDF;
+    s->nc[0] = nx; s->nc[1] = ny; s->nc[2] = nz;
+    s->box.lo = v3(box.min); s->box.hi = v3(box.max);
+    V3 ext = s->box.hi - s->box.lo;
+    V3 inv = mk(1.f / nx, 1.f / ny, 1.f / nz);
+    s->steps = mk(ext.x * inv.x, ext.y * inv.y, ext.z * inv.z);
+    size_t n = (size_t)(nx + 1) * (ny + 1) * (nz + 1);
+    s->values.assign(values, values + n);
+    s->compute_gradient();
+    return s;
+}
+
+scHandle scCreateMeshCollider(const float* vertices, int nv, const unsigned* indices, int ni)
+{
+    if (!vertices || !indices || nv <= 0 || ni <= 0 || ni % 3) { set_error(SC_ERR_ARG, "bad mesh"); return nullptr; }
+    MeshC* m = new MeshC();
+    m->type = CT_MESH;
+    m->mesh.verts.resize(nv);
+    for (int i = 0; i < nv; i++) m->mesh.verts[i] = mk(vertices[3 * i], vertices[3 * i + 1], vertices[3 * i + 2]);
+    m->mesh.idx.assign(indices, indices + ni);
+    m->mesh.compute_normals();
+    m->mesh.construct_edges();
+    m->mesh.construct_rings(false, true);
+    return m;
+}
+
+int scGetCollidableType(scHandle c) { return c ? ((Collidable*)c)->type : CT_INVALID; }
+void* scGetMeshTree(scHandle c)
+{
+    Collidable* k = (Collidable*)c;
+    if (!k || k->type != CT_MESH) return nullptr;
+    MeshC* m = (MeshC*)k;
+    return m->built ? (void*)&m->tree : nullptr;
+}
+void scGetWallsInfo(scHandle c, scAabb3* box)
+{
+    Collidable* k = (Collidable*)c;
+    if (!k || k->type != CT_WALLS || !box) return;
+    box->min = sv(((WallsC*)k)->box.lo); box->max = sv(((WallsC*)k)->box.hi);
+}
+void scGetSphereInfo(scHandle c, float* radius, scVector3* center)
+{
+    Collidable* k = (Collidable*)c;
+    if (!k || k->type != CT_SPHERE) return;
+    if (radius) *radius = ((SphereC*)k)->radius;
+    if (center) *center = sv(k->center);
+}
+void scGetCapsuleInfo(scHandle c, float* radius, float* halfHeight, scVector3* center, scQuaternion* rot)
+{
+    Collidable* k = (Collidable*)c;
+    if (!k || k->type != CT_CAPSULE) return;
+    CapsuleC* cap = (CapsuleC*)k;
+    if (radius) *radius = cap->r;
+    if (halfHeight) *halfHeight = cap->hh;
+    if (center) *center = sv(cap->center);
+    if (rot) { rot->s = cap->rot[0]; rot->v.x = cap->rot[1]; rot->v.y = cap->rot[2]; rot->v.z = cap->rot[3]; }
+}
+
+// ------------------------------------------------------------------ patch
+scClothPatch scCreateClothPatch(scCollisionWorld w)
+{
+    scClothPatch p; p.ptr = nullptr;
+    if (!W(w)) { set_error(SC_ERR_ARG, "null world"); return p; }
+    p.ptr = new ClothPatch(*W(w));
+    return p;
+}
+void scFreeClothPatch(scClothPatch p) { delete P(p); }
+scModel scGetClothModel(scClothPatch p) { scModel m; m.ptr = P(p) ? &P(p)->model : nullptr; return m; }
+scMesh scGetClothMesh(scClothPatch p) { scMesh m; m.ptr = P(p) ? &P(p)->mesh : nullptr; return m; }
+
+void scInitCloth(scClothPatch p, int divX, int divY, float inc, scVector3 offset, bool horizontal, bool attached)
+{
+    if (!P(p)) { set_error(SC_ERR_ARG, "null patch"); return; }
+    P(p)->init_grid(divX, divY, inc, v3(offset), horizontal, attached);
+}
+
+void scStepCloth(scClothPatch p, float dt)
+{
+    if (!P(p)) { set_error(SC_ERR_ARG, "null patch"); return; }
+    P(p)->step(dt);
+}
+
+void scUpdateClothMesh(scClothPatch p) { if (P(p)) P(p)->update_mesh(); }
+
+// ClothPatch::ComputeStrainMap (Physics/ClothPatch.cpp:337-381)
+void scComputeStrainMap(scClothPatch p, scVector3* colors)
+{
+    if (!P(p) || !colors) return;
+    ClothModel& m = P(p)->model;
+    host_sync(&m);
+    std::vector<V3> col(m.N, mk(0, 0, 0));
+    const float PI = 3.1415926535897932384626433832795f;
+    for (const FemHost& t : m.tris)
+    {
+        V3 dx1 = m.hpos[t.i2] - m.hpos[t.i1], dx2 = m.hpos[t.i3] - m.hpos[t.i1];
+        V3 wu = t.invDet * (t.dv2 * dx1 - t.dv1 * dx2);
+        V3 wv = t.invDet * (-t.du2 * dx1 + t.du1 * dx2);
+        float euu = 0.5f * (dot(wu, wu) - 1), evv = 0.5f * (dot(wv, wv) - 1), euv = dot(wu, wv);
+        float s = sqrtf(euu * euu + evv * evv + euv * euv);
+        V3 e1 = normalized(dx1), e2 = normalized(m.hpos[t.i3] - m.hpos[t.i2]), e3 = normalized(-dx2);
+        float t1 = (float)acos(-dot(e1, e3)), t2 = (float)acos(-dot(e1, e2)), t3 = (float)acos(-dot(e2, e3));
+        s *= 10.f;
+        V3 c = mk(s, 0, s);
+        col[t.i1] += (t1 / PI) * c; col[t.i2] += (t2 / PI) * c; col[t.i3] += (t3 / PI) * c;
+    }
+    for (int i = 0; i < m.N; i++) colors[i] = sv(col[i]);
+}
+
+// ------------------------------------------------------------------ model
+int scGetNumParticles(scModel m) { return M(m) ? M(m)->N : 0; }
+void scGetParticlePos(scModel m, int i, scVector3* pos)
+{
+    if (!check_model(M(m), i) || !pos) return;
+    host_sync(M(m));
+    *pos = sv(M(m)->hpos[i]);
+}
+float scGetParticleInvMass(scModel m, int i)
+{
+    if (!check_model(M(m), i)) return 0.f;
+    host_sync(M(m));
+    return M(m)->invMass[i];
+}
+int scGetNumTris(scModel m) { return M(m) ? (int)M(m)->tris.size() : 0; }
+void scGetTriangle(scModel m, int i, int* i1, int* i2, int* i3)
+{
+    if (!M(m) || i < 0 || i >= (int)M(m)->tris.size()) { set_error(SC_ERR_ARG, "triangle index out of range"); return; }
+    const FemHost& t = M(m)->tris[i];
+    if (i1) *i1 = t.i1; if (i2) *i2 = t.i2; if (i3) *i3 = t.i3;
+}
+void scGetTriangleInfo(scModel m, int i, float* invDet, scVector2* du, scVector2* dv, scVector2* s)
+{
+    if (!M(m) || i < 0 || i >= (int)M(m)->tris.size()) { set_error(SC_ERR_ARG, "triangle index out of range"); return; }
+    const FemHost& t = M(m)->tris[i];
+    if (invDet) *invDet = t.invDet;
+    if (du) { du->x = t.du1; du->y = t.du2; }
+    if (dv) { dv->x = t.dv1; dv->y = t.dv2; }
+    if (s) { s->x = t.su; s->y = t.sv; }
+}
+int scGetNumQuads(scModel m) { return M(m) ? (int)M(m)->quads.size() : 0; }
+void scGetQuad(scModel m, int i, int* i1, int* i2, int* i3, int* i4)
+{
+    if (!M(m) || i < 0 || i >= (int)M(m)->quads.size()) { set_error(SC_ERR_ARG, "quad index out of range"); return; }
+    uint4 q = M(m)->quads[i];
+    if (i1) *i1 = q.x; if (i2) *i2 = q.y; if (i3) *i3 = q.z; if (i4) *i4 = q.w;
+}
+int scGetNumLinks(scModel m) { return M(m) ? (int)M(m)->links.size() : 0; }
+void scGetLink(scModel m, int i, int* i1, int* i2)
+{
+    if (!M(m) || i < 0 || i >= (int)M(m)->links.size()) { set_error(SC_ERR_ARG, "link index out of range"); return; }
+    if (i1) *i1 = M(m)->links[i].x; if (i2) *i2 = M(m)->links[i].y;
+}
+
+// vertex contacts in list order: collider, then particle, then slot
+static std::vector<VC> vertex_contacts(ClothModel* m, std::vector<int>* owner)
+{
+    std::vector<VC> out;
+    if (!m->buf.vc || m->buf.numVColl == 0) return out;
+    host_sync(m);
+    std::vector<uint8_t> cnt = dl(m->buf.vcCount, (size_t)m->buf.numVColl * m->N);
+    size_t total = 0;
+    for (auto& g : m->vcollHost) total += (size_t)g.kmax * m->N;
+    std::vector<VC> slots = dl(m->buf.vc, total);
+    for (int ci = 0; ci < m->buf.numVColl; ci++)
+    {
+        const VColl& g = m->vcollHost[ci];
+        for (int i = 0; i < m->N; i++)
+            for (int k = 0; k < cnt[(size_t)ci * m->N + i]; k++)
+            {
+                out.push_back(slots[g.slotBase + (size_t)i * g.kmax + k]);
+                if (owner) owner->push_back(i);
+            }
+    }
+    return out;
+}
+
+int scGetNumContacts(scModel m) { return M(m) ? (int)vertex_contacts(M(m), nullptr).size() : 0; }
+void scGetContact(scModel m, int i, scVector3* point, scVector3* normal)
+{
+    if (!M(m)) return;
+    std::vector<VC> v = vertex_contacts(M(m), nullptr);
+    if (i < 0 || i >= (int)v.size()) { set_error(SC_ERR_ARG, "contact index out of range"); return; }
+    if (point) *point = {v[i].point.x, v[i].point.y, v[i].point.z};
+    if (normal) *normal = {v[i].normal.x, v[i].normal.y, v[i].normal.z};
+}
+int scGetNumTriContacts(scModel m)
+{
+    if (!M(m) || !M(m)->buf.tcCount) return 0;
+    host_sync(M(m));
+    return dcount(M(m)->buf.tcCount);
+}
+void scGetTriContact(scModel m, int i, scVector3* point, scVector3* normal)
+{
+    int n = scGetNumTriContacts(m);
+    if (i < 0 || i >= n) { set_error(SC_ERR_ARG, "contact index out of range"); return; }
+    TC t;
+    cudaMemcpy(&t, M(m)->buf.tcList + i, sizeof(TC), cudaMemcpyDeviceToHost);
+    if (point) *point = {t.point.x, t.point.y, t.point.z};
+    if (normal) *normal = {t.normal.x, t.normal.y, t.normal.z};
+}
+
+#define SC_GETSET(Name, field, type)                                             \
+    type scGet##Name(scModel m) { return M(m) ? (type)M(m)->prm.field : (type)0; } \
+    void scSet##Name(scModel m, type v) { if (M(m)) { M(m)->prm.field = v; M(m)->touch(); } }
+
+SC_GETSET(CollisionFlags, flags, int)
+SC_GETSET(Thickness, thickness, float)
+SC_GETSET(Tolerance, tolerance, float)
+SC_GETSET(Friction, friction, float)
+SC_GETSET(NumIterations, iterations, int)
+SC_GETSET(UseFEM, fem, bool)
+SC_GETSET(Unit, unit, float)
+
+void* scGetClothTree(scModel m) { return M(m) ? (void*)&M(m)->triBvh : nullptr; }
+
+void scAddMouseSpring(scModel m, int i1, int i2, int i3, scVector3 coords, scVector3 p)
+{
+    if (!check_model(M(m))) return;
+    (void)i1; (void)i2; (void)i3; (void)coords; (void)p;
+    set_error(SC_ERR_UNSUPPORTED, "mouse spring is interactive-only and not part of the GPU step");
+}
+void scUpdateMouseSpring(scModel m, scVector3 p) { (void)m; (void)p; }
+void scRemoveMouseSpring(scModel m) { (void)m; }
+
+// ------------------------------------------------------------------- mesh
+int scGetMeshVertexCount(scMesh mesh) { return mesh.ptr ? (int)((HMesh*)mesh.ptr)->verts.size() : 0; }
+int scGetMeshIndexCount(scMesh mesh) { return mesh.ptr ? (int)((HMesh*)mesh.ptr)->idx.size() : 0; }
+scVector3* scGetMeshNormalBuffer(scMesh mesh)
+{
+    HMesh* h = (HMesh*)mesh.ptr;
+    return (h && !h->normals.empty()) ? (scVector3*)h->normals.data() : nullptr;
+}
+scVector3* scGetMeshVertexBuffer(scMesh mesh)
+{
+    HMesh* h = (HMesh*)mesh.ptr;
+    return (h && !h->verts.empty()) ? (scVector3*)h->verts.data() : nullptr;
+}
+unsigned int* scGetMeshIndexBuffer(scMesh mesh)
+{
+    HMesh* h = (HMesh*)mesh.ptr;
+    return (h && !h->idx.empty()) ? (unsigned int*)h->idx.data() : nullptr;
+}
+
+// --------------------------------------------------------------- additions
+void scSetShearStiffness(scModel m, float v) { if (M(m)) { M(m)->prm.shear = v; M(m)->touch(); } }
+void scSetBendStiffness(scModel m, float v) { if (M(m)) { M(m)->prm.bend = v; M(m)->touch(); } }
+void scSetStretchStiffness(scModel m, float v) { if (M(m)) { M(m)->prm.stretch = v; M(m)->touch(); } }
+void scSetPoisson(scModel m, float v) { if (M(m)) { M(m)->prm.poisson = v; M(m)->touch(); } }
+void scSetDragCoeff(scModel m, float v) { if (M(m)) { M(m)->prm.drag = v; M(m)->touch(); } }
+void scSetDihedral(scModel m, bool v) { if (M(m)) { M(m)->prm.dihedral = v; M(m)->touch(); } }
+void scSetSelfShrink(scModel m, float v) { if (M(m)) { M(m)->prm.selfShrink = v; M(m)->touch(); } }
+void scSetNumSteps(scClothPatch p, int v)
+{
+    if (!P(p) || v < 1) { set_error(SC_ERR_ARG, "substeps must be >= 1"); return; }
+    P(p)->numSteps = v;
+}
+int scGetNumSteps(scClothPatch p) { return P(p) ? P(p)->numSteps : 0; }
+
+void scSetMasses(scModel m, const float* masses)
+{
+    if (!check_model(M(m)) || !masses) return;
+    host_sync(M(m));
+    for (int i = 0; i < M(m)->N; i++) M(m)->invMass[i] = masses[i] == 0.f ? 0.f : 1.f / masses[i];
+    M(m)->upload_state(M(m)->owner->stream);
+}
+void scSetParticleInvMass(scModel m, int i, float w)
+{
+    if (!check_model(M(m), i)) return;
+    host_sync(M(m));
+    M(m)->invMass[i] = w;
+    M(m)->upload_state(M(m)->owner->stream);
+}
+void scSetParticlePositions(scModel m, const float* xyz)
+{
+    if (!check_model(M(m)) || !xyz) return;
+    host_sync(M(m));
+    for (int i = 0; i < M(m)->N; i++)
+    {
+        M(m)->hpos[i] = mk(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
+        M(m)->hprev[i] = M(m)->hpos[i];
+    }
+    M(m)->upload_state(M(m)->owner->stream);
+}
+void scSetParticleState(scModel m, const float* pos, const float* prev, const float* vel)
+{
+    if (!check_model(M(m)) || !pos || !prev || !vel) return;
+    host_sync(M(m));
+    for (int i = 0; i < M(m)->N; i++)
+    {
+        M(m)->hpos[i] = mk(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+        M(m)->hprev[i] = mk(prev[3 * i], prev[3 * i + 1], prev[3 * i + 2]);
+        M(m)->hvel[i] = mk(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]);
+    }
+    M(m)->upload_state(M(m)->owner->stream);
+}
+static void get3(scModel m, float* xyz, int which)
+{
+    if (!check_model(M(m)) || !xyz) return;
+    host_sync(M(m));
+    const std::vector<V3>& v = which == 0 ? M(m)->hpos : (which == 1 ? M(m)->hvel : M(m)->hprev);
+    memcpy(xyz, v.data(), sizeof(float) * 3 * M(m)->N);
+}
+void scGetParticlePositions(scModel m, float* xyz) { get3(m, xyz, 0); }
+void scGetParticleVelocities(scModel m, float* xyz) { get3(m, xyz, 1); }
+void scGetParticlePrevPositions(scModel m, float* xyz) { get3(m, xyz, 2); }
+void scSetFixedIterations(scModel m, bool v) { if (M(m)) { M(m)->prm.fixedIterations = v; M(m)->touch(); } }
+void scSetSelfCCD(scModel m, bool v) { if (M(m)) { M(m)->prm.ccd = v; M(m)->touch(); } }
+int scGetSolverIterations(scModel m)
+{
+    if (!M(m) || !M(m)->dc.scal) return 0;
+    host_sync(M(m));
+    float v = 0;
+    cudaMemcpy(&v, M(m)->dc.scal + 9, sizeof(float), cudaMemcpyDeviceToHost);
+    return (int)v;
+}
+
+int scGetConstraintOrder(scModel m, int kind, int* order, int* colourStart)
+{
+    if (!M(m)) return 0;
+    const std::vector<int>& o = kind == 0 ? M(m)->triOrder : M(m)->bendOrder;
+    const std::vector<int>& s = kind == 0 ? M(m)->triColourStart : M(m)->bendColourStart;
+    if (order) memcpy(order, o.data(), sizeof(int) * o.size());
+    if (colourStart) memcpy(colourStart, s.data(), sizeof(int) * s.size());
+    return (int)s.size() - 1;
+}
+int scGetNumBends(scModel m) { return M(m) ? (int)M(m)->bends.size() : 0; }
+void scGetBends(scModel m, unsigned* idx4)
+{
+    if (!M(m) || !idx4) return;
+    memcpy(idx4, M(m)->bends.data(), sizeof(uint4) * M(m)->bends.size());
+}
+int scGetNumEdges(scModel m) { return (M(m) && M(m)->owner) ? (int)M(m)->owner->mesh.edges.size() : 0; }
+void scGetEdges(scModel m, int* e4)
+{
+    if (!M(m) || !e4) return;
+    const auto& E = M(m)->owner->mesh.edges;
+    for (size_t i = 0; i < E.size(); i++) { e4[4 * i] = E[i].i1; e4[4 * i + 1] = E[i].i2; e4[4 * i + 2] = E[i].t1; e4[4 * i + 3] = E[i].t2; }
+}
+
+int scGetNumContactsOfKind(scModel m, int kind)
+{
+    ClothModel* c = M(m);
+    if (!c || !c->buf.tcCount) return 0;
+    host_sync(c);
+    switch (kind)
+    {
+    case 0: return (int)vertex_contacts(c, nullptr).size();
+    case 1: return dcount(c->buf.tcCount);
+    case 2: return dcount(c->buf.ecCount);
+    case 3: return dcount(c->buf.stCount);
+    case 4: return dcount(c->buf.seCount);
+    }
+    return 0;
+}
+
+void scGetSelfContacts(scModel m, int kind, int* idx4, float* f7)
+{
+    ClothModel* c = M(m);
+    if (!c || !c->buf.stCount) return;
+    int n = scGetNumContactsOfKind(m, kind);
+    std::vector<SCt> v = dl(kind == 3 ? c->buf.stList : c->buf.seList, n);
+    for (int i = 0; i < n; i++)
+    {
+        if (idx4) { idx4[4 * i] = v[i].idx.x; idx4[4 * i + 1] = v[i].idx.y; idx4[4 * i + 2] = v[i].idx.z; idx4[4 * i + 3] = v[i].idx.w; }
+        if (f7)
+        {
+            float* f = f7 + 7 * i;
+            f[0] = v[i].normal.x; f[1] = v[i].normal.y; f[2] = v[i].normal.z;
+            f[3] = v[i].w.x; f[4] = v[i].w.y; f[5] = v[i].w.z; f[6] = v[i].side;
+        }
+    }
+}
+
+void scGetVertexContacts(scModel m, int* idx2, float* f6)
+{
+    if (!M(m)) return;
+    std::vector<int> owner;
+    std::vector<VC> v = vertex_contacts(M(m), &owner);
+    for (size_t i = 0; i < v.size(); i++)
+    {
+        if (idx2) { idx2[2 * i] = owner[i]; idx2[2 * i + 1] = v[i].feature; }
+        if (f6)
+        {
+            float* f = f6 + 6 * i;
+            f[0] = v[i].point.x; f[1] = v[i].point.y; f[2] = v[i].point.z;
+            f[3] = v[i].normal.x; f[4] = v[i].normal.y; f[5] = v[i].normal.z;
+        }
+    }
+}
+
+void scGetTriContacts(scModel m, int* idx4, float* f9)
+{
+    ClothModel* c = M(m);
+    if (!c || !c->buf.tcCount) return;
+    int n = scGetNumContactsOfKind(m, 1);
+    std::vector<TC> v = dl(c->buf.tcList, n);
+    for (int i = 0; i < n; i++)
+    {
+        if (idx4) { idx4[4 * i] = v[i].idx.x; idx4[4 * i + 1] = v[i].idx.y; idx4[4 * i + 2] = v[i].idx.z; idx4[4 * i + 3] = v[i].feature; }
+        if (f9)
+        {
+            float* f = f9 + 9 * i;
+            f[0] = v[i].point.x; f[1] = v[i].point.y; f[2] = v[i].point.z;
+            f[3] = v[i].normal.x; f[4] = v[i].normal.y; f[5] = v[i].normal.z;
+            f[6] = v[i].w.x; f[7] = v[i].w.y; f[8] = v[i].w.z;
+        }
+    }
+}
+
+void scGetEdgeContacts(scModel m, int* idx3, float* f8)
+{
+    ClothModel* c = M(m);
+    if (!c || !c->buf.ecCount) return;
+    int n = scGetNumContactsOfKind(m, 2);
+    std::vector<EC> v = dl(c->buf.ecList, n);
+    for (int i = 0; i < n; i++)
+    {
+        if (idx3) { idx3[3 * i] = v[i].idx.x; idx3[3 * i + 1] = v[i].idx.y; idx3[3 * i + 2] = v[i].feature; }
+        if (f8)
+        {
+            float* f = f8 + 8 * i;
+            f[0] = v[i].point.x; f[1] = v[i].point.y; f[2] = v[i].point.z;
+            f[3] = v[i].normal.x; f[4] = v[i].normal.y; f[5] = v[i].normal.z;
+            f[6] = v[i].w.x; f[7] = v[i].w.y;
+        }
+    }
+}
+
+int scGetCCDCandidates(scModel m, int kind, int* pairs, int cap)
+{
+    ClothModel* c = M(m);
+    if (!c || !c->buf.ccdVtPairCount || !c->prm.ccd) return 0;
+    host_sync(c);
+    int n = dcount(kind == 0 ? c->buf.ccdVtPairCount : c->buf.ccdEePairCount);
+    int lim = kind == 0 ? c->buf.ccdVtCap : c->buf.ccdEeCap;
+    int k = std::min(std::min(n, lim), cap);
+    if (pairs && k > 0)
+        cudaMemcpy(pairs, kind == 0 ? c->buf.ccdVtPairs : c->buf.ccdEePairs, sizeof(int2) * k, cudaMemcpyDeviceToHost);
+    return n;
+}
+
+void scGetCollisionMeshNormals(scModel m, float* xyz)
+{
+    ClothModel* c = M(m);
+    if (!c || !xyz || !c->dc.prevN) return;
+    host_sync(c);
+    std::vector<float4> n = dl(c->dc.prevN, c->N);
+    for (int i = 0; i < c->N; i++) { xyz[3 * i] = n[i].x; xyz[3 * i + 1] = n[i].y; xyz[3 * i + 2] = n[i].z; }
+}
+
+int scGetLastError(void)
+{
+    int e = last_error();
+    set_error(SC_OK, "");
+    return e;
+}
+const char* scGetLastErrorString(void) { return last_error_string(); }
+
+int scGetStatus(scClothPatch p)
+{
+    if (!P(p) || !P(p)->model.dc.status) return 0;
+    P(p)->sync();
+    int s = 0;
+    cudaMemcpy(&s, P(p)->model.dc.status, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaMemset(P(p)->model.dc.status, 0, sizeof(int));
+    return s;
+}
+
+void scSynchronize(scClothPatch p) { if (P(p)) P(p)->sync(); }
+
+void* scGetCudaStream(scClothPatch p) { return P(p) ? (void*)P(p)->stream : nullptr; }
+
+int scGetGraphKernelCount(scClothPatch p)
+{
+    if (!P(p) || !P(p)->graph) return 0;
+    return P(p)->graphKernelCount;
+}
+
+float scProfileSweep(scClothPatch p, int kind, int reps)
+{
+    ClothPatch* cp = P(p);
+    if (!cp || cp->model.N == 0 || reps < 1) { set_error(SC_ERR_ARG, "bad profile request"); return -1.f; }
+    ClothModel& m = cp->model;
+    cp->sync();
+    const SolverParams P0 = m.solver_params(1.f / 480.f);
+    cudaStream_t s = cp->stream;
+    cudaGraph_t g;
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return -1.f;
+    for (int r = 0; r < reps; r++)
+    {
+        if (kind == 0)
+            for (size_t c = 0; c + 1 < m.triColourStart.size(); c++)
+                launch_fem(s, m.dc, P0, m.triColourStart[c], m.triColourStart[c + 1] - m.triColourStart[c]);
+        else
+            for (size_t c = 0; c + 1 < m.bendColourStart.size(); c++)
+                launch_bends(s, m.dc, P0, m.bendColourStart[c], m.bendColourStart[c + 1] - m.bendColourStart[c], 0);
+    }
+    if (cudaStreamEndCapture(s, &g) != cudaSuccess) return -1.f;
+    cudaGraphExec_t ge;
+    if (cudaGraphInstantiate(&ge, g, 0) != cudaSuccess) { cudaGraphDestroy(g); return -1.f; }
+    cudaGraphDestroy(g);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0); cudaEventCreate(&e1);
+    cudaGraphLaunch(ge, s);                 // warm-up
+    cudaEventRecord(e0, s);
+    cudaGraphLaunch(ge, s);
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0); cudaEventDestroy(e1);
+    cudaGraphExecDestroy(ge);
+    cp->hostStateDirty = true;
+    return ms / reps;
+}
+
+} // extern "C"

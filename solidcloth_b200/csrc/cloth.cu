@@ -1,0 +1,1010 @@
+// cloth.cu — host side of the cloth step: set-up (grid, FEM rest data, edges,
+// bends, colouring, BVH topology, collider trees), device buffers, and the CUDA
+// graph that runs one frame (ClothPatch::Step) on a private stream.
+#include "cloth.h"
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <cstdio>
+#include <numeric>
+#include <mutex>
+
+namespace sc {
+
+static inline float bits_f(uint32_t u) { float f; memcpy(&f, &u, 4); return f; }
+
+// ------------------------------------------------------------------ errors
+static thread_local int g_err = SC_OK;
+static thread_local std::string g_errMsg;
+
+void set_error(int code, const std::string& msg)
+{
+    g_err = code;
+    g_errMsg = msg;
+}
+int last_error() { return g_err; }
+const char* last_error_string() { return g_errMsg.c_str(); }
+
+#define SC_CUDA(x)                                                                     \
+    do {                                                                               \
+        cudaError_t e_ = (x);                                                          \
+        if (e_ != cudaSuccess) {                                                       \
+            set_error(SC_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_));   \
+            return false;                                                              \
+        }                                                                              \
+    } while (0)
+
+// -------------------------------------------------------------------- mesh
+// Mesh::ComputeNormals, angle weighted (Geometry/Mesh.cpp:10-63)
+void HMesh::compute_normals()
+{
+    normals.assign(verts.size(), mk(0, 0, 0));
+    triN.resize(idx.size() / 3);
+    for (size_t i = 0; i < idx.size(); i += 3)
+    {
+        const int i1 = idx[i], i2 = idx[i + 1], i3 = idx[i + 2];
+        V3 a = verts[i1], b = verts[i2], c = verts[i3];
+        V3 nt = normalized(cross(b - a, c - a));
+        triN[i / 3] = nt;
+        V3 e1 = normalized(b - a), e2 = normalized(c - b), e3 = normalized(a - c);
+        float c1 = -dot(e1, e3), c2 = -dot(e1, e2), c3 = -dot(e2, e3);
+        float s1 = len(cross(e1, -e3)), s2 = len(cross(e2, -e1)), s3 = len(cross(e3, -e1));
+        float t1 = std::fabs(c1) > 1 ? (float)std::fabs(std::atan2((double)s1, (double)c1)) : acosf(c1);
+        float t2 = std::fabs(c2) > 1 ? (float)std::fabs(std::atan2((double)s2, (double)c2)) : acosf(c2);
+        float t3 = std::fabs(c3) > 1 ? (float)std::fabs(std::atan2((double)s3, (double)c3)) : acosf(c3);
+        normals[i1] += t1 * nt;
+        normals[i2] += t2 * nt;
+        normals[i3] += t3 * nt;
+    }
+    for (size_t i = 0; i < verts.size(); i++)
+    {
+        if (len(normals[i]) == 0) continue;
+        normals[i] = normalized(normals[i]);
+    }
+}
+
+// Mesh::ConstructEdges (Geometry/Mesh.cpp:65-147). The half-edge array is sorted
+// with std::sort and the same (i1, i2) comparator as the reference, so the two
+// half-edges of each interior edge come out in the same (unstable) order and
+// t1/t2 — hence bend vertex order and edge normals — match it.
+void HMesh::construct_edges()
+{
+    edges.clear();
+    const int numEdges = (int)idx.size();
+    if (numEdges == 0) return;
+    std::vector<HEdge> dup(numEdges);
+    triE.assign(idx.size(), 0);
+    for (int i = 0; i < numEdges; i++)
+    {
+        int i1 = idx[i], i2;
+        if ((i + 1) % 3 == 0)
+        {
+            i2 = idx[i - 2];
+            triE[i / 3 * 3 + 2] = (uint32_t)i;
+            triE[i / 3 * 3 + 1] = (uint32_t)(i - 1);
+            triE[i / 3 * 3 + 0] = (uint32_t)(i - 2);
+        }
+        else
+            i2 = idx[i + 1];
+        bool swapped = false;
+        if (i1 > i2) { std::swap(i1, i2); swapped = true; }
+        HEdge e;
+        e.i1 = i1; e.i2 = i2; e.swapped = swapped; e.t1 = i / 3; e.t2 = -1;
+        e.n = triN[i / 3];
+        e.origIdx = i;
+        dup[i] = e;
+    }
+    std::sort(dup.begin(), dup.end(), [](const HEdge& a, const HEdge& b) {
+        return a.i1 < b.i1 || (a.i1 == b.i1 && a.i2 < b.i2);
+    });
+    HEdge cur = dup[0];
+    std::vector<int> map(dup.size(), -1);
+    map[cur.origIdx] = 0;
+    for (size_t i = 1; i < dup.size(); i++)
+    {
+        if (dup[i].i1 == dup[i - 1].i1 && dup[i].i2 == dup[i - 1].i2)
+        {
+            map[dup[i].origIdx] = (int)edges.size();
+            cur.t2 = dup[i].t1;
+            cur.n = normalized(triN[cur.t1] + triN[cur.t2]);
+            continue;
+        }
+        edges.push_back(cur);
+        cur = dup[i];
+        map[cur.origIdx] = (int)edges.size();
+    }
+    edges.push_back(cur);
+    for (size_t k = 0; k < triE.size(); k++) triE[k] = map[triE[k]];
+}
+
+void HMesh::construct_rings(bool vtx, bool edge)
+{
+    if (vtx) vtxRing.assign(verts.size(), {});
+    if (edge) edgeRing.assign(verts.size(), {});
+    for (size_t i = 0; i < edges.size(); i++)
+    {
+        if (vtx) { vtxRing[edges[i].i1].push_back(edges[i].i2); vtxRing[edges[i].i2].push_back(edges[i].i1); }
+        if (edge) { edgeRing[edges[i].i1].push_back((int)i); edgeRing[edges[i].i2].push_back((int)i); }
+    }
+}
+
+// --------------------------------------------------------------- SDF grid
+SDFC::~SDFC()
+{
+    if (valTex) cudaDestroyTextureObject(valTex);
+    if (gradTex) cudaDestroyTextureObject(gradTex);
+    if (valArr) cudaFreeArray(valArr);
+    if (gradArr) cudaFreeArray(gradArr);
+}
+
+// SDF::ComputeGradient, forward differences with the last layer copied
+// (Geometry/SDF.cpp:210-256)
+void SDFC::compute_gradient()
+{
+    const int nv0 = nc[0] + 1, nv1 = nc[1] + 1;
+    auto index = [&](int x, int y, int z) { return x + y * nv0 + z * nv0 * nv1; };
+    auto out = [&](int x, int y, int z) { return x > nc[0] || y > nc[1] || z > nc[2] || x < 0 || y < 0 || z < 0; };
+    auto val = [&](int x, int y, int z) { return out(x, y, z) ? 0.f : values[index(x, y, z)]; };
+    auto gat = [&](int x, int y, int z) { return out(x, y, z) ? mk(0, 0, 0) : grad[index(x, y, z)]; };
+    auto set = [&](int x, int y, int z, V3 g) { if (!out(x, y, z)) grad[index(x, y, z)] = g; };
+    grad.assign(values.size(), mk(0, 0, 0));
+    for (int x = 0; x < nc[0]; x++)
+    {
+        for (int y = 0; y < nc[1]; y++)
+        {
+            for (int z = 0; z < nc[2]; z++)
+            {
+                float v = val(x, y, z);
+                float dfdx = (val(x + 1, y, z) - v) / steps.x;
+                float dfdy = (val(x, y + 1, z) - v) / steps.y;
+                float dfdz = (val(x, y, z + 1) - v) / steps.z;
+                set(x, y, z, mk(dfdx, dfdy, dfdz));
+            }
+            set(x, y, nc[2], gat(x, y, nc[2] - 1));
+        }
+        for (int z = 0; z <= nc[2]; z++) set(x, nc[1], z, gat(x, nc[1] - 1, z));
+    }
+    for (int y = 0; y <= nc[1]; y++)
+        for (int z = 0; z <= nc[2]; z++) set(nc[0], y, z, gat(nc[0] - 1, y, z));
+}
+
+bool SDFC::upload(int dev)
+{
+    if (device == dev && valTex) return true;
+    const int nx = nc[0] + 1, ny = nc[1] + 1, nz = nc[2] + 1;
+    cudaExtent ext = make_cudaExtent(nx, ny, nz);
+    cudaChannelFormatDesc cdv = cudaCreateChannelDesc<float>();
+    cudaChannelFormatDesc cdg = cudaCreateChannelDesc<float4>();
+    SC_CUDA(cudaMalloc3DArray(&valArr, &cdv, ext));
+    SC_CUDA(cudaMalloc3DArray(&gradArr, &cdg, ext));
+    std::vector<float4> g4(grad.size());
+    for (size_t i = 0; i < grad.size(); i++) g4[i] = make_float4(grad[i].x, grad[i].y, grad[i].z, 0.f);
+    cudaMemcpy3DParms p = {};
+    p.srcPtr = make_cudaPitchedPtr((void*)values.data(), nx * sizeof(float), nx, ny);
+    p.dstArray = valArr; p.extent = ext; p.kind = cudaMemcpyHostToDevice;
+    SC_CUDA(cudaMemcpy3D(&p));
+    cudaMemcpy3DParms q = {};
+    q.srcPtr = make_cudaPitchedPtr((void*)g4.data(), nx * sizeof(float4), nx, ny);
+    q.dstArray = gradArr; q.extent = ext; q.kind = cudaMemcpyHostToDevice;
+    SC_CUDA(cudaMemcpy3D(&q));
+    cudaTextureDesc td = {};
+    for (int k = 0; k < 3; k++) td.addressMode[k] = cudaAddressModeBorder;   // 0 outside, as SDF::GetValue(int)
+    td.filterMode = cudaFilterModePoint;                                      // exact samples; blend in FP32
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 0;
+    cudaResourceDesc rd = {};
+    rd.resType = cudaResourceTypeArray;
+    rd.res.array.array = valArr;
+    SC_CUDA(cudaCreateTextureObject(&valTex, &rd, &td, nullptr));
+    rd.res.array.array = gradArr;
+    SC_CUDA(cudaCreateTextureObject(&gradTex, &rd, &td, nullptr));
+    device = dev;
+    return true;
+}
+
+// ----------------------------------------------------------- mesh collider
+MeshC::~MeshC() { if (dmem) cudaFree(dmem); }
+
+// Geometry::ComputeMeshTree + SplitNode, exclusive child assignment,
+// maxPrims 40 (Geometry/AabbTree.cpp:9-178)
+void MeshC::build_tree(float tol)
+{
+    tree.clear();
+    MeshTreeNode root;
+    root.box = Box::empty();
+    for (V3 v : mesh.verts) { root.box.lo = vmin(root.box.lo, v); root.box.hi = vmax(root.box.hi, v); }
+    for (uint32_t i = 0; i < (uint32_t)mesh.ntris(); i++) root.tris.push_back(i);
+    for (uint32_t i = 0; i < (uint32_t)mesh.verts.size(); i++) root.verts.push_back(i);
+    for (uint32_t i = 0; i < (uint32_t)mesh.edges.size(); i++) root.edges.push_back(i);
+    tree.push_back(root);
+    struct Item { int node, level; };
+    // recursion order of SplitNode: node, then left subtree, then right subtree
+    std::vector<Item> stack{{0, 1}};
+    const int maxLevel = 20;
+    while (!stack.empty())
+    {
+        Item it = stack.back();
+        stack.pop_back();
+        const int ni = it.node;
+        const size_t maxPrims = 40;
+        if (tree[ni].tris.size() < maxPrims && tree[ni].verts.size() < maxPrims && tree[ni].edges.size() < maxPrims) continue;
+        V3 ext = tree[ni].box.hi - tree[ni].box.lo;
+        int dir = 0;
+        float m = ext.x;
+        if (ext.y > m) { m = ext.y; dir = 1; }
+        if (ext.z > m) { m = ext.z; dir = 2; }
+        const float center = 0.5f * (comp(tree[ni].box.lo, dir) + comp(tree[ni].box.hi, dir));
+        MeshTreeNode L, R;
+        L.box = Box::empty(); R.box = Box::empty();
+        for (uint32_t t : tree[ni].tris)
+        {
+            Box b = Box::empty();
+            b.add(mesh.verts[mesh.idx[3 * t]]); b.add(mesh.verts[mesh.idx[3 * t + 1]]); b.add(mesh.verts[mesh.idx[3 * t + 2]]);
+            b.extrude(tol);
+            if (comp(b.lo, dir) <= center) { L.tris.push_back(t); L.box.add(b); }
+            else { R.tris.push_back(t); R.box.add(b); }
+        }
+        for (uint32_t e : tree[ni].edges)
+        {
+            Box b = Box::empty();
+            b.add(mesh.verts[mesh.edges[e].i1]); b.add(mesh.verts[mesh.edges[e].i2]);
+            b.extrude(tol);
+            if (comp(b.lo, dir) <= center) { L.edges.push_back(e); L.box.add(b); }
+            else { R.edges.push_back(e); R.box.add(b); }
+        }
+        for (uint32_t v : tree[ni].verts)
+        {
+            Box b = Box::empty();
+            b.add(mesh.verts[v]);
+            b.extrude(tol);
+            if (comp(mesh.verts[v], dir) <= center) { L.verts.push_back(v); L.box.add(b); }
+            else { R.verts.push_back(v); R.box.add(b); }
+        }
+        tree[ni].tris.clear(); tree[ni].edges.clear(); tree[ni].verts.clear();
+        int l = -1, r = -1;
+        if (!(L.tris.empty() && L.verts.empty() && L.edges.empty())) { tree.push_back(L); l = (int)tree.size() - 1; }
+        if (!(R.tris.empty() && R.verts.empty() && R.edges.empty())) { tree.push_back(R); r = (int)tree.size() - 1; }
+        tree[ni].left = l; tree[ni].right = r;
+        if (it.level < maxLevel)
+        {
+            if (r >= 0) stack.push_back({r, it.level + 1});
+            if (l >= 0) stack.push_back({l, it.level + 1});
+        }
+    }
+    built = true;
+}
+
+bool MeshC::upload(int devId)
+{
+    if (device == devId && dmem) return true;
+    const int V = (int)mesh.verts.size(), T = mesh.ntris(), E = (int)mesh.edges.size();
+    const int M = (int)tree.size();
+    std::vector<float4> v(V), n(V), en(E), lo(M), hi(M);
+    std::vector<int4> edge(E), pr(M);
+    std::vector<int2> ch(M), er(M);
+    std::vector<uint32_t> tris, verts, edges;
+    for (int i = 0; i < V; i++) { v[i] = f4(mesh.verts[i], 0); n[i] = f4(mesh.normals[i], 0); }
+    for (int e = 0; e < E; e++)
+    {
+        const HEdge& h = mesh.edges[e];
+        edge[e] = make_int4((int)h.i1, (int)h.i2, h.t1, h.t2);
+        en[e] = f4(h.n, 0);
+    }
+    for (int k = 0; k < M; k++)
+    {
+        const MeshTreeNode& t = tree[k];
+        lo[k] = f4(t.box.lo, 0); hi[k] = f4(t.box.hi, 0);
+        ch[k] = make_int2(t.left, t.right);
+        pr[k] = make_int4((int)tris.size(), (int)t.tris.size(), (int)verts.size(), (int)t.verts.size());
+        er[k] = make_int2((int)edges.size(), (int)t.edges.size());
+        tris.insert(tris.end(), t.tris.begin(), t.tris.end());
+        verts.insert(verts.end(), t.verts.begin(), t.verts.end());
+        edges.insert(edges.end(), t.edges.begin(), t.edges.end());
+    }
+    // one allocation, 256-byte aligned sub-buffers
+    size_t off = 0;
+    auto take = [&](size_t bytes) { size_t o = off; off += (bytes + 255) & ~size_t(255); return o; };
+    size_t oV = take(V * 16), oN = take(V * 16), oEN = take(E * 16), oT = take(T * 12), oE = take(E * 16);
+    size_t oLo = take(M * 16), oHi = take(M * 16), oCh = take(M * 8), oPr = take(M * 16), oEr = take(M * 8);
+    size_t oTr = take(tris.size() * 4 + 4), oVe = take(verts.size() * 4 + 4), oEd = take(edges.size() * 4 + 4);
+    SC_CUDA(cudaMalloc(&dmem, off));
+    char* d = (char*)dmem;
+    SC_CUDA(cudaMemcpy(d + oV, v.data(), V * 16, cudaMemcpyHostToDevice));
+    SC_CUDA(cudaMemcpy(d + oN, n.data(), V * 16, cudaMemcpyHostToDevice));
+    SC_CUDA(cudaMemcpy(d + oEN, en.data(), E * 16, cudaMemcpyHostToDevice));
+    SC_CUDA(cudaMemcpy(d + oT, mesh.idx.data(), T * 12, cudaMemcpyHostToDevice));
+    SC_CUDA(cudaMemcpy(d + oE, edge.data(), E * 16, cudaMemcpyHostToDevice));
+    SC_CUDA(cudaMemcpy(d + oLo, lo.data(), M * 16, cudaMemcpyHostToDevice));
+    SC_CUDA(cudaMemcpy(d + oHi, hi.data(), M * 16, cudaMemcpyHostToDevice));
+    SC_CUDA(cudaMemcpy(d + oCh, ch.data(), M * 8, cudaMemcpyHostToDevice));
+    SC_CUDA(cudaMemcpy(d + oPr, pr.data(), M * 16, cudaMemcpyHostToDevice));
+    SC_CUDA(cudaMemcpy(d + oEr, er.data(), M * 8, cudaMemcpyHostToDevice));
+    if (!tris.empty()) SC_CUDA(cudaMemcpy(d + oTr, tris.data(), tris.size() * 4, cudaMemcpyHostToDevice));
+    if (!verts.empty()) SC_CUDA(cudaMemcpy(d + oVe, verts.data(), verts.size() * 4, cudaMemcpyHostToDevice));
+    if (!edges.empty()) SC_CUDA(cudaMemcpy(d + oEd, edges.data(), edges.size() * 4, cudaMemcpyHostToDevice));
+    dev.V = V; dev.T = T; dev.E = E;
+    dev.v = (const float4*)(d + oV); dev.n = (const float4*)(d + oN); dev.en = (const float4*)(d + oEN);
+    dev.tri = (const uint32_t*)(d + oT); dev.edge = (const int4*)(d + oE);
+    dev.tree.numNodes = M;
+    dev.tree.lo = (const float4*)(d + oLo); dev.tree.hi = (const float4*)(d + oHi);
+    dev.tree.children = (const int2*)(d + oCh); dev.tree.primRange = (const int4*)(d + oPr);
+    dev.tree.edgeRange = (const int2*)(d + oEr);
+    dev.tree.tris = (const uint32_t*)(d + oTr); dev.tree.verts = (const uint32_t*)(d + oVe);
+    dev.tree.edges = (const uint32_t*)(d + oEd);
+    device = devId;
+    return true;
+}
+
+// --------------------------------------------------------------- LBVH host
+static uint32_t expand_bits(uint32_t v)
+{
+    v = (v * 0x00010001u) & 0xFF0000FFu;
+    v = (v * 0x00000101u) & 0x0F00F00Fu;
+    v = (v * 0x00000011u) & 0xC30C30C3u;
+    v = (v * 0x00000005u) & 0x49249249u;
+    return v;
+}
+
+// Linear BVH over primitive centroids: Morton-ordered primitives, median
+// splits (balanced), nodes emitted in depth-first preorder so traversal needs
+// no stack (escape index = first node after the subtree). The topology is
+// built once from the rest shape; every substep only refits the boxes.
+void LBVHHost::build(const std::vector<V3>& cen)
+{
+    const int n = (int)cen.size();
+    numLeaves = n;
+    numNodes = n > 0 ? 2 * n - 1 : 0;
+    child.assign(numNodes, 0); escape.assign(numNodes, 0); parent.assign(numNodes, -1); leafNode.assign(n, 0);
+    if (n == 0) return;
+    V3 lo = cen[0], hi = cen[0];
+    for (const V3& c : cen) { lo = vmin(lo, c); hi = vmax(hi, c); }
+    std::vector<std::pair<uint32_t, int>> key(n);
+    for (int i = 0; i < n; i++)
+    {
+        auto q = [](float v, float a, float b) {
+            float t = (b > a) ? (v - a) / (b - a) : 0.5f;
+            int x = (int)(t * 1023.f);
+            return (uint32_t)std::max(0, std::min(1023, x));
+        };
+        uint32_t m = (expand_bits(q(cen[i].x, lo.x, hi.x)) << 2) | (expand_bits(q(cen[i].y, lo.y, hi.y)) << 1) |
+                     expand_bits(q(cen[i].z, lo.z, hi.z));
+        key[i] = {m, i};
+    }
+    std::sort(key.begin(), key.end());
+    int next = 0;
+    // iterative preorder build over (range, parent, is-right-child) jobs
+    struct Job { int lo, hi, par; bool right; };
+    std::vector<Job> jobs{{0, n, -1, false}};
+    while (!jobs.empty())
+    {
+        Job j = jobs.back();
+        jobs.pop_back();
+        int node = next++;
+        parent[node] = j.par;
+        if (j.right && j.par >= 0) child[j.par] = node;
+        if (j.hi - j.lo == 1)
+        {
+            child[node] = ~key[j.lo].second;
+            leafNode[key[j.lo].second] = node;
+            escape[node] = node + 1;
+            continue;
+        }
+        int mid = (j.lo + j.hi) / 2;
+        escape[node] = node + 2 * (j.hi - j.lo) - 1;     // subtree of k leaves has 2k-1 nodes
+        jobs.push_back({mid, j.hi, node, true});
+        jobs.push_back({j.lo, mid, node, false});
+    }
+}
+
+// ------------------------------------------------------------------ model
+ClothModel::~ClothModel() { release_device(); }
+
+void* ClothModel::dalloc(size_t bytes, bool contact)
+{
+    void* p = nullptr;
+    if (bytes == 0) bytes = 16;
+    if (cudaMalloc(&p, bytes) != cudaSuccess)
+    {
+        set_error(SC_ERR_CUDA, "cudaMalloc failed");
+        return nullptr;
+    }
+    cudaMemset(p, 0, bytes);
+    (contact ? bufAllocs : allocs).push_back(p);
+    return p;
+}
+
+void ClothModel::release_buffers()
+{
+    for (void* p : bufAllocs) cudaFree(p);
+    bufAllocs.clear();
+    buf = Buffers{};
+    bufWorldVersion = ~0ull;
+}
+
+void ClothModel::release_device()
+{
+    release_buffers();
+    for (void* p : allocs) cudaFree(p);
+    allocs.clear();
+    dc = DevCloth{};
+}
+
+SolverParams ClothModel::solver_params(float h) const
+{
+    SolverParams P;
+    P.unit = prm.unit; P.thickness = prm.thickness; P.tolerance = prm.tolerance; P.shear = prm.shear;
+    P.bend = prm.bend; P.poisson = prm.poisson; P.friction = prm.friction; P.drag = prm.drag;
+    P.selfShrink = prm.selfShrink;
+    P.h = h; P.h2 = h * h; P.invH = 1.f / h;
+    // epsilonUV = 1 / shear modulus (Physics/ClothPBD.cpp:56)
+    P.epsUV = 2 * (1 + prm.poisson) / (std::max(prm.shear, 0.1f) * prm.unit * prm.unit);
+    P.iterations = prm.iterations; P.flags = prm.flags; P.fem = prm.fem; P.dihedral = prm.dihedral;
+    P.fixedIterations = prm.fixedIterations; P.bendFreq = prm.bendFreq;
+    P.selfThreshold = prm.selfThreshold;
+    return P;
+}
+
+// Greedy colouring in index order on the particle-sharing graph: each
+// constraint takes the lowest colour unused by earlier constraints on its
+// particles. Solve order = (colour, index).
+template <int K, typename Get>
+static void greedy_colour(int n, int N, Get verts, std::vector<int>& order, std::vector<int>& start)
+{
+    std::vector<uint64_t> used(N, 0);
+    std::vector<int> col(n, 0);
+    int maxc = 0;
+    for (int i = 0; i < n; i++)
+    {
+        uint32_t v[K];
+        verts(i, v);
+        uint64_t u = 0;
+        for (int k = 0; k < K; k++) u |= used[v[k]];
+        int c = 0;
+        while (c < 64 && (u >> c & 1ull)) c++;
+        if (c >= 64) c = 63;
+        col[i] = c;
+        maxc = std::max(maxc, c + 1);
+        for (int k = 0; k < K; k++) used[v[k]] |= 1ull << c;
+    }
+    order.resize(n);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return col[a] < col[b]; });
+    start.assign(maxc + 1, 0);
+    for (int i = 0; i < n; i++) start[col[i] + 1]++;
+    for (int c = 0; c < maxc; c++) start[c + 1] += start[c];
+}
+
+void ClothModel::colour_constraints()
+{
+    greedy_colour<3>((int)tris.size(), N, [&](int i, uint32_t* v) { v[0] = tris[i].i1; v[1] = tris[i].i2; v[2] = tris[i].i3; },
+                     triOrder, triColourStart);
+    greedy_colour<4>((int)bends.size(), N, [&](int i, uint32_t* v) { v[0] = bends[i].x; v[1] = bends[i].y; v[2] = bends[i].z; v[3] = bends[i].w; },
+                     bendOrder, bendColourStart);
+}
+
+bool ClothModel::upload_topology(const HMesh& mesh)
+{
+    release_device();
+    SC_CUDA(cudaGetDevice(&device));
+    const int T = (int)tris.size(), E = (int)mesh.edges.size(), B = (int)bends.size();
+    dc.N = N; dc.T = T; dc.E = E; dc.B = B;
+    colour_constraints();
+    // particle state
+    dc.pos = (float4*)dalloc(sizeof(float4) * N);
+    dc.prev = (float4*)dalloc(sizeof(float4) * N);
+    dc.vel = (float4*)dalloc(sizeof(float4) * N);
+    // FEM records in colour order
+    std::vector<float4> fem(3 * (size_t)T);
+    for (int k = 0; k < T; k++)
+    {
+        const FemHost& t = tris[triOrder[k]];
+        fem[3 * k] = make_float4(bits_f(t.i1), bits_f(t.i2), bits_f(t.i3), t.du1);
+        fem[3 * k + 1] = make_float4(t.du2, t.dv1, t.dv2, t.invDet);
+        fem[3 * k + 2] = make_float4(t.lu2, t.lv2, t.lu0 * t.lv0, t.area);
+    }
+    float4* dfem = (float4*)dalloc(sizeof(float4) * 3 * (size_t)T);
+    SC_CUDA(cudaMemcpy(dfem, fem.data(), sizeof(float4) * 3 * (size_t)T, cudaMemcpyHostToDevice));
+    dc.fem = dfem;
+    std::vector<uint4> bd(B);
+    for (int k = 0; k < B; k++) bd[k] = bends[bendOrder[k]];
+    uint4* dbend = (uint4*)dalloc(sizeof(uint4) * B);
+    if (B) SC_CUDA(cudaMemcpy(dbend, bd.data(), sizeof(uint4) * B, cudaMemcpyHostToDevice));
+    dc.bend = dbend;
+    // collision-mesh topology
+    uint32_t* dtri = (uint32_t*)dalloc(sizeof(uint32_t) * 3 * (size_t)T);
+    SC_CUDA(cudaMemcpy(dtri, mesh.idx.data(), sizeof(uint32_t) * 3 * (size_t)T, cudaMemcpyHostToDevice));
+    dc.tri = dtri;
+    uint32_t* dtriE = (uint32_t*)dalloc(sizeof(uint32_t) * 3 * (size_t)T);
+    SC_CUDA(cudaMemcpy(dtriE, mesh.triE.data(), sizeof(uint32_t) * 3 * (size_t)T, cudaMemcpyHostToDevice));
+    dc.triE = dtriE;
+    std::vector<int4> ed(E);
+    std::vector<uint8_t> sw(E);
+    for (int e = 0; e < E; e++)
+    {
+        ed[e] = make_int4((int)mesh.edges[e].i1, (int)mesh.edges[e].i2, mesh.edges[e].t1, mesh.edges[e].t2);
+        sw[e] = mesh.edges[e].swapped ? 1 : 0;
+    }
+    int4* dedge = (int4*)dalloc(sizeof(int4) * E);
+    SC_CUDA(cudaMemcpy(dedge, ed.data(), sizeof(int4) * E, cudaMemcpyHostToDevice));
+    dc.edge = dedge;
+    uint8_t* dsw = (uint8_t*)dalloc(E);
+    SC_CUDA(cudaMemcpy(dsw, sw.data(), E, cudaMemcpyHostToDevice));
+    dc.edgeSwapped = dsw;
+    auto csr = [&](const std::vector<std::vector<int>>& lists, const int*& startOut, const int*& dataOut) -> bool {
+        std::vector<int> st(N + 1, 0), data;
+        for (int i = 0; i < N; i++) { st[i + 1] = st[i] + (int)lists[i].size(); data.insert(data.end(), lists[i].begin(), lists[i].end()); }
+        int* ds = (int*)dalloc(sizeof(int) * (N + 1));
+        int* dd = (int*)dalloc(sizeof(int) * (data.size() + 1));
+        SC_CUDA(cudaMemcpy(ds, st.data(), sizeof(int) * (N + 1), cudaMemcpyHostToDevice));
+        if (!data.empty()) SC_CUDA(cudaMemcpy(dd, data.data(), sizeof(int) * data.size(), cudaMemcpyHostToDevice));
+        startOut = ds; dataOut = dd;
+        return true;
+    };
+    if (!csr(mesh.vtxRing, dc.vRingStart, dc.vRing)) return false;
+    if (!csr(mesh.edgeRing, dc.eRingStart, dc.eRing)) return false;
+    {
+        std::vector<int> st(N + 1, 0);
+        std::vector<int2> vt(3 * (size_t)T);
+        for (int t = 0; t < T; t++) for (int k = 0; k < 3; k++) st[mesh.idx[3 * t + k] + 1]++;
+        for (int i = 0; i < N; i++) st[i + 1] += st[i];
+        std::vector<int> cur(st.begin(), st.end() - 1);
+        for (int t = 0; t < T; t++) for (int k = 0; k < 3; k++) vt[cur[mesh.idx[3 * t + k]]++] = make_int2(t, k);
+        int* ds = (int*)dalloc(sizeof(int) * (N + 1));
+        int2* dv = (int2*)dalloc(sizeof(int2) * 3 * (size_t)T);
+        SC_CUDA(cudaMemcpy(ds, st.data(), sizeof(int) * (N + 1), cudaMemcpyHostToDevice));
+        SC_CUDA(cudaMemcpy(dv, vt.data(), sizeof(int2) * 3 * (size_t)T, cudaMemcpyHostToDevice));
+        dc.vTriStart = ds; dc.vTri = dv;
+    }
+    std::vector<uint8_t> border(N, 0);
+    for (int i = 0; i < N; i++) for (int e : mesh.edgeRing[i]) if (mesh.edges[e].t2 < 0) border[i] = 1;
+    uint8_t* dborder = (uint8_t*)dalloc(N);
+    SC_CUDA(cudaMemcpy(dborder, border.data(), N, cudaMemcpyHostToDevice));
+    dc.vBorder = dborder;
+    dc.prevN = (float4*)dalloc(sizeof(float4) * N);
+    dc.prevTriN = (float4*)dalloc(sizeof(float4) * T);
+    dc.meshN = (float4*)dalloc(sizeof(float4) * N);
+    dc.meshTriN = (float4*)dalloc(sizeof(float4) * T);
+    dc.triAngles = (float4*)dalloc(sizeof(float4) * T);
+    dc.scal = (float*)dalloc(sizeof(float) * 16);
+    dc.status = (int*)dalloc(sizeof(int) * 4);
+    {
+        // collision-mesh normals as of the initial mesh (ClothPatch::Init copies
+        // mMesh, normals included, into mPrevMesh)
+        std::vector<float4> n4(N), t4(T);
+        for (int i = 0; i < N; i++) n4[i] = f4(mesh.normals[i], 0);
+        for (int t = 0; t < T; t++) t4[t] = f4(mesh.triN[t], 0);
+        SC_CUDA(cudaMemcpy(dc.prevN, n4.data(), sizeof(float4) * N, cudaMemcpyHostToDevice));
+        SC_CUDA(cudaMemcpy(dc.prevTriN, t4.data(), sizeof(float4) * T, cudaMemcpyHostToDevice));
+        SC_CUDA(cudaMemcpy(dc.meshN, n4.data(), sizeof(float4) * N, cudaMemcpyHostToDevice));
+        SC_CUDA(cudaMemcpy(dc.meshTriN, t4.data(), sizeof(float4) * T, cudaMemcpyHostToDevice));
+    }
+    // BVH topologies from the rest shape
+    auto mkbvh = [&](const std::vector<V3>& cen, DevBVH& out, DevBVH* shareTopo) -> bool {
+        LBVHHost h;
+        h.build(cen);
+        out.numLeaves = h.numLeaves; out.numNodes = h.numNodes;
+        if (shareTopo)
+        {
+            out.child = shareTopo->child; out.escape = shareTopo->escape; out.parent = shareTopo->parent; out.leafNode = shareTopo->leafNode;
+        }
+        else
+        {
+            int* d = (int*)dalloc(sizeof(int) * (3 * (size_t)h.numNodes + h.numLeaves + 4));
+            SC_CUDA(cudaMemcpy(d, h.child.data(), sizeof(int) * h.numNodes, cudaMemcpyHostToDevice));
+            SC_CUDA(cudaMemcpy(d + h.numNodes, h.escape.data(), sizeof(int) * h.numNodes, cudaMemcpyHostToDevice));
+            SC_CUDA(cudaMemcpy(d + 2 * h.numNodes, h.parent.data(), sizeof(int) * h.numNodes, cudaMemcpyHostToDevice));
+            SC_CUDA(cudaMemcpy(d + 3 * h.numNodes, h.leafNode.data(), sizeof(int) * h.numLeaves, cudaMemcpyHostToDevice));
+            out.child = d; out.escape = d + h.numNodes; out.parent = d + 2 * h.numNodes; out.leafNode = d + 3 * h.numNodes;
+        }
+        out.lo = (float4*)dalloc(sizeof(float4) * h.numNodes);
+        out.hi = (float4*)dalloc(sizeof(float4) * h.numNodes);
+        out.visit = (int*)dalloc(sizeof(int) * h.numNodes);
+        return true;
+    };
+    std::vector<V3> tc(T), ec(E);
+    for (int t = 0; t < T; t++)
+        tc[t] = (1.f / 3.f) * (hpos[mesh.idx[3 * t]] + hpos[mesh.idx[3 * t + 1]] + hpos[mesh.idx[3 * t + 2]]);
+    for (int e = 0; e < E; e++) ec[e] = 0.5f * (hpos[mesh.edges[e].i1] + hpos[mesh.edges[e].i2]);
+    if (!mkbvh(tc, triBvh, nullptr)) return false;
+    if (!mkbvh(ec, edgeBvh, nullptr)) return false;
+    if (!mkbvh(tc, sweptTriBvh, &triBvh)) return false;
+    if (!mkbvh(ec, sweptEdgeBvh, &edgeBvh)) return false;
+    bufWorldVersion = ~0ull;
+    return true;
+}
+
+void ClothModel::upload_state(cudaStream_t s)
+{
+    std::vector<float4> p(N), q(N), v(N);
+    for (int i = 0; i < N; i++)
+    {
+        p[i] = f4(hpos[i], invMass[i]);
+        q[i] = f4(hprev[i], 0.f);
+        v[i] = f4(hvel[i], 0.f);
+    }
+    cudaMemcpyAsync(dc.pos, p.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dc.prev, q.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dc.vel, v.data(), sizeof(float4) * N, cudaMemcpyHostToDevice, s);
+    cudaStreamSynchronize(s);
+}
+
+void ClothModel::download_state(cudaStream_t s)
+{
+    std::vector<float4> p(N), q(N), v(N);
+    cudaMemcpyAsync(p.data(), dc.pos, sizeof(float4) * N, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(q.data(), dc.prev, sizeof(float4) * N, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(v.data(), dc.vel, sizeof(float4) * N, cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    for (int i = 0; i < N; i++)
+    {
+        hpos[i] = mk(p[i]); invMass[i] = p[i].w;
+        hprev[i] = mk(q[i]);
+        hvel[i] = mk(v[i]);
+    }
+}
+
+// Contact buffers depend on the world's colliders, the collision flags and the
+// continuous-collision switch; they are (re)allocated before a graph capture.
+bool ClothModel::ensure_buffers(const CollisionWorld& world, cudaStream_t s)
+{
+    const bool ccd = prm.ccd;
+    if (bufWorldVersion == world.version && bufFlags == prm.flags && bufCcd == ccd && buf.vc) return true;
+    release_buffers();
+    const int T = dc.T, E = dc.E;
+    vcollHost.clear();
+    std::vector<DevMesh> meshes;
+    int slotBase = 0;
+    for (auto& cp : world.list)
+    {
+        Collidable* c = cp.get();
+        VColl g = {};
+        g.type = c->type;
+        if (c->type == CT_WALLS)
+        {
+            WallsC* w = (WallsC*)c;
+            g.kmax = WALL_SLOTS;
+            g.a = f4(w->box.lo, 0); g.b = f4(w->box.hi, 0);
+        }
+        else if (c->type == CT_SPHERE)
+        {
+            SphereC* sp = (SphereC*)c;
+            g.kmax = 1;
+            g.a = f4(sp->center, sp->radius);
+        }
+        else if (c->type == CT_SDF)
+        {
+            SDFC* sd = (SDFC*)c;
+            if (!sd->upload(device)) return false;
+            g.kmax = 1;
+            g.val = sd->valTex; g.grad = sd->gradTex;
+            g.sdfLo = f4(sd->box.lo, 0); g.sdfSteps = f4(sd->steps, 0);
+            g.sdfCells = make_int4(sd->nc[0], sd->nc[1], sd->nc[2], 0);
+        }
+        else if (c->type == CT_MESH)
+        {
+            MeshC* m = (MeshC*)c;
+            // CollisionMesh::Update builds the tree once with the current
+            // thickness (Physics/Common.h:124-137)
+            if (!m->built) m->build_tree(prm.thickness);
+            if (!m->upload(device)) return false;
+            g.kmax = 1;
+            g.mesh = (int)meshes.size();
+            meshes.push_back(m->dev);
+        }
+        else
+        {
+            set_error(SC_ERR_UNSUPPORTED, "collidable type not supported by the GPU step (capsule/box/slab); it is ignored");
+            continue;
+        }
+        g.slotBase = slotBase;
+        slotBase += g.kmax * N;
+        vcollHost.push_back(g);
+    }
+    const int nv = (int)vcollHost.size();
+    int nTE = 0;
+    for (auto& g : vcollHost) if (g.type == CT_SPHERE || g.type == CT_SDF || g.type == CT_MESH) nTE++;
+    buf.numVColl = nv;
+    buf.vcCount = (uint8_t*)dalloc((size_t)std::max(1, nv) * N, true);
+    buf.vc = (VC*)dalloc(sizeof(VC) * (size_t)std::max(1, slotBase), true);
+    VColl* dcoll = (VColl*)dalloc(sizeof(VColl) * std::max(1, nv), true);
+    if (nv) SC_CUDA(cudaMemcpy(dcoll, vcollHost.data(), sizeof(VColl) * nv, cudaMemcpyHostToDevice));
+    buf.vcoll = dcoll;
+    DevMesh* dmeshes = (DevMesh*)dalloc(sizeof(DevMesh) * std::max<size_t>(1, meshes.size()), true);
+    if (!meshes.empty()) SC_CUDA(cudaMemcpy(dmeshes, meshes.data(), sizeof(DevMesh) * meshes.size(), cudaMemcpyHostToDevice));
+    buf.meshes = dmeshes;
+    buf.numMeshes = (int)meshes.size();
+    // triangle / edge contacts
+    const int nTc = (prm.flags & CF_TRIANGLES) ? nTE : 0, nEc = (prm.flags & CF_EDGES) ? nTE : 0;
+    buf.tcCap = std::max(1, nTc * T);
+    buf.ecCap = std::max(1, nEc * E);
+    buf.tcSlot = (TC*)dalloc(sizeof(TC) * (size_t)buf.tcCap, true);
+    buf.tcFlag = (int*)dalloc(sizeof(int) * (size_t)buf.tcCap, true);
+    buf.tcList = (TC*)dalloc(sizeof(TC) * (size_t)buf.tcCap, true);
+    buf.ecSlot = (EC*)dalloc(sizeof(EC) * (size_t)buf.ecCap, true);
+    buf.ecFlag = (int*)dalloc(sizeof(int) * (size_t)buf.ecCap, true);
+    buf.ecList = (EC*)dalloc(sizeof(EC) * (size_t)buf.ecCap, true);
+    int* counts = (int*)dalloc(sizeof(int) * 16, true);
+    buf.tcCount = counts; buf.ecCount = counts + 1; buf.stCount = counts + 2; buf.seCount = counts + 3;
+    buf.ccdVtPairCount = counts + 4; buf.ccdEePairCount = counts + 5; buf.scanTot = counts + 8;
+    // self contacts
+    const bool self = (prm.flags & CF_SELF) != 0;
+    buf.ccdVtCap = ccd ? std::max(1, N * KCCD) : 1;
+    buf.ccdEeCap = ccd ? std::max(1, E * KCCD) : 1;
+    buf.stCap = (self ? N * KVT : 1) + (ccd ? buf.ccdVtCap : 0);
+    buf.seCap = (self ? E : 1) + (ccd ? buf.ccdEeCap : 0);
+    buf.stCnt = (int*)dalloc(sizeof(int) * N, true);
+    buf.stSlot = (SCt*)dalloc(sizeof(SCt) * (size_t)(self ? N * KVT : 1), true);
+    buf.stList = (SCt*)dalloc(sizeof(SCt) * (size_t)buf.stCap, true);
+    buf.seFlag = (int*)dalloc(sizeof(int) * E, true);
+    buf.seSlot = (SCt*)dalloc(sizeof(SCt) * (size_t)E, true);
+    buf.seList = (SCt*)dalloc(sizeof(SCt) * (size_t)buf.seCap, true);
+    buf.ccdVtCnt = (int*)dalloc(sizeof(int) * N, true);
+    buf.ccdEeCnt = (int*)dalloc(sizeof(int) * E, true);
+    buf.ccdVtCand = (int*)dalloc(sizeof(int) * (size_t)(ccd ? N * KCCD : 1), true);
+    buf.ccdEeCand = (int*)dalloc(sizeof(int) * (size_t)(ccd ? E * KCCD : 1), true);
+    buf.ccdVtPairs = (int2*)dalloc(sizeof(int2) * (size_t)buf.ccdVtCap, true);
+    buf.ccdEePairs = (int2*)dalloc(sizeof(int2) * (size_t)buf.ccdEeCap, true);
+    buf.ccdVtHit = (int*)dalloc(sizeof(int) * (size_t)buf.ccdVtCap, true);
+    buf.ccdEeHit = (int*)dalloc(sizeof(int) * (size_t)buf.ccdEeCap, true);
+    buf.ccdVtRec = (SCt*)dalloc(sizeof(SCt) * (size_t)buf.ccdVtCap, true);
+    buf.ccdEeRec = (SCt*)dalloc(sizeof(SCt) * (size_t)buf.ccdEeCap, true);
+    // colouring
+    buf.vmin = (unsigned long long*)dalloc(sizeof(unsigned long long) * N, true);
+    SC_CUDA(cudaMemset(buf.vmin, 0xff, sizeof(unsigned long long) * N));
+    buf.colourCap = buf.ecCap + buf.tcCap + buf.stCap + buf.seCap;
+    buf.colour = (int*)dalloc(sizeof(int) * (size_t)buf.colourCap, true);
+    buf.order = (int*)dalloc(sizeof(int) * (size_t)buf.colourCap, true);
+    buf.colourStart = (int*)dalloc(sizeof(int) * 4 * (MAX_COLOURS + 1), true);
+    // scans
+    size_t maxScan = std::max<size_t>({(size_t)N, (size_t)E, (size_t)buf.tcCap, (size_t)buf.ecCap,
+                                       (size_t)buf.ccdVtCap, (size_t)buf.ccdEeCap});
+    buf.scanOff = (int*)dalloc(sizeof(int) * (maxScan + 1), true);
+    buf.scanBlock = (int*)dalloc(sizeof(int) * (maxScan / 1024 + 8), true);
+    bufWorldVersion = world.version;
+    bufFlags = prm.flags;
+    bufCcd = ccd;
+    (void)s;
+    return true;
+}
+
+// ------------------------------------------------------------------ patch
+ClothPatch::ClothPatch(CollisionWorld& w) : world(w), model(this)
+{
+    cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
+}
+
+ClothPatch::~ClothPatch()
+{
+    if (graph) cudaGraphExecDestroy(graph);
+    if (stream) { cudaStreamSynchronize(stream); cudaStreamDestroy(stream); }
+}
+
+// ClothModel::AddTriangle: FEM rest data from the uv parameterisation
+// (Physics/ClothModel.cpp:54-92)
+static FemHost make_triangle(const ClothModel& m, uint32_t i1, uint32_t i2, uint32_t i3)
+{
+    FemHost t = {};
+    t.i1 = i1; t.i2 = i2; t.i3 = i3;
+    float d1x = m.uvx[i2] - m.uvx[i1], d1y = m.uvy[i2] - m.uvy[i1];
+    float d2x = m.uvx[i3] - m.uvx[i1], d2y = m.uvy[i3] - m.uvy[i1];
+    t.du1 = d1x; t.du2 = d2x; t.dv1 = d1y; t.dv2 = d2y;
+    t.det = t.du1 * t.dv2 - t.du2 * t.dv1;
+    t.invDet = 0.f;
+    if (t.det != 0) t.invDet = 1.f / t.det;
+    V3 dx1 = m.hpos[i2] - m.hpos[i1], dx2 = m.hpos[i3] - m.hpos[i1];
+    V3 wu = t.invDet * (t.dv2 * dx1 - t.dv1 * dx2);
+    V3 wv = t.invDet * (-t.du2 * dx1 + t.du1 * dx2);
+    t.lu0 = len(wu);
+    t.lv0 = len(wv);
+    if (t.lu0 != 0) t.su = 1.f / t.lu0;
+    if (t.lv0 != 0) t.sv = 1.f / t.lv0;
+    t.area = 0.5f * t.det;
+    t.lu2 = t.lu0 * t.lu0;
+    t.lv2 = t.lv0 * t.lv0;
+    return t;
+}
+
+// ClothPatch::Init(divX, divY, inc, offset, horizontal, attached)
+// (Physics/ClothPatch.cpp:135-246). The vertical layout's random incline is
+// not reproduced (horizontal = false lays the grid in the XY plane with z = 0).
+bool ClothPatch::init_grid(int divX, int divY, float inc, V3 offset, bool horizontal, bool attached)
+{
+    if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
+    if (divX < 2 || divY < 2) { set_error(SC_ERR_ARG, "grid needs at least 2x2 vertices"); return false; }
+    ClothModel& m = model;
+    const int N = divX * divY;
+    m.N = N;
+    m.hpos.assign(N, mk(0, 0, 0)); m.hprev.assign(N, mk(0, 0, 0)); m.hvel.assign(N, mk(0, 0, 0));
+    m.invMass.assign(N, 1.f); m.uvx.assign(N, 0.f); m.uvy.assign(N, 0.f);
+    m.tris.clear(); m.bends.clear(); m.links.clear(); m.quads.clear();
+    mesh = HMesh();
+    isQuadMesh = true;
+    const bool dihedral = m.prm.dihedral;
+    auto addLink = [&](uint32_t a, uint32_t b) {
+        // ClothModel::AddLink (Physics/ClothModel.inl:12-31): skipped when both pinned
+        if (m.invMass[a] == 0 && m.invMass[b] == 0) return;
+        m.links.push_back(make_uint2(a, b));
+    };
+    float x = -0.5f * divX * inc;
+    const float startY = x;
+    for (int j = 0, base = 0; j < divX; j++, base += divY)
+    {
+        m.hpos[base] = horizontal ? mk(x, 0, startY) + offset : mk(x, startY, 0) + offset;
+        m.hprev[base] = m.hpos[base];
+        m.uvx[base] = x; m.uvy[base] = 0;
+        if (base >= divY)
+        {
+            addLink(base - divY, base);
+            addLink(base - divY + 1, base);
+            if (base >= 2 * divY && !dihedral) addLink(base - 2 * divY, base);
+        }
+        for (int i = 1; i < divY; i++)
+        {
+            const int idx = base + i;
+            m.hpos[idx] = horizontal ? mk(x, 0, startY + inc * i) + offset : mk(x, startY + inc * i, 0) + offset;
+            m.hprev[idx] = m.hpos[idx];
+            m.uvx[idx] = x; m.uvy[idx] = inc * i;
+            addLink(idx - 1, idx);
+            if (idx > base + 1 && !dihedral) addLink(idx - 2, idx);
+            if (idx >= divY)
+            {
+                addLink(idx - divY, idx);
+                if (i < divY - 1) addLink(idx - divY + 1, idx);
+                if (j > 1 && !dihedral) addLink(idx - 2 * divY, idx);
+            }
+            if (idx > divY)
+            {
+                addLink(idx - divY - 1, idx);
+                const uint32_t a = idx - divY - 1, b = idx - divY, c = idx, d = idx - 1;
+                m.quads.push_back(make_uint4(a, b, c, d));
+                uint32_t t[6];
+                if ((i & 1) == (j & 1)) { uint32_t u[6] = {a, c, b, a, d, c}; memcpy(t, u, sizeof(t)); }
+                else { uint32_t u[6] = {b, d, c, d, b, a}; memcpy(t, u, sizeof(t)); }
+                for (int k = 0; k < 2; k++)
+                {
+                    m.tris.push_back(make_triangle(m, t[3 * k], t[3 * k + 1], t[3 * k + 2]));
+                    mesh.idx.push_back(t[3 * k]); mesh.idx.push_back(t[3 * k + 1]); mesh.idx.push_back(t[3 * k + 2]);
+                }
+            }
+        }
+        if (attached && (j == 0 || j == divX - 1)) m.invMass[base + divY - 1] = 0.f;
+        x += inc;
+    }
+    mesh.verts = m.hpos;
+    mesh.compute_normals();
+    mesh.construct_edges();
+    mesh.construct_rings(true, true);
+    // ClothModel::AddBendConstraint for every interior edge (Physics/ClothModel.cpp:94-126)
+    for (const HEdge& e : mesh.edges)
+    {
+        if (e.t2 < 0) continue;
+        auto opp = [&](int t) -> uint32_t {
+            const FemHost& tr = m.tris[t];
+            if (tr.i1 != e.i1 && tr.i1 != e.i2) return tr.i1;
+            if (tr.i2 != e.i1 && tr.i2 != e.i2) return tr.i2;
+            return tr.i3;
+        };
+        m.bends.push_back(make_uint4(e.i1, e.i2, opp(e.t1), opp(e.t2)));
+    }
+    prevMesh = mesh;
+    if (!m.upload_topology(mesh)) return false;
+    m.upload_state(stream);
+    hostStateDirty = false;
+    return true;
+}
+
+void ClothPatch::sync()
+{
+    cudaStreamSynchronize(stream);
+    if (hostStateDirty)
+    {
+        model.download_state(stream);
+        hostStateDirty = false;
+    }
+}
+
+// One substep (ClothModelPBD::Step) recorded into the capture stream.
+void ClothPatch::record_substep(float h)
+{
+    ClothModel& m = model;
+    const SolverParams P = m.solver_params(h);
+    const DevCloth& c = m.dc;
+    Buffers& b = m.buf;
+    cudaStream_t s = stream;
+    launch_predict(s, c, P);
+    // ClothModel::DetectCollisions (Physics/ClothCollision.cpp:17-48)
+    launch_vertex_colliders(s, c, P, b, m.vcollHost.data());
+    launch_tri_edge_colliders(s, c, P, b, m.vcollHost.data(), (int)m.vcollHost.size(), m.prm.flags);
+    const bool self = (m.prm.flags & CF_SELF) != 0, ccd = m.prm.ccd;
+    if (self)
+    {
+        launch_bvh_refit(s, m.triBvh, c, 0, 0.f);
+        launch_bvh_refit(s, m.edgeBvh, c, 1, 0.f);
+        launch_self_proximity(s, c, P, b, m.triBvh, m.edgeBvh);
+    }
+    if (ccd)
+    {
+        const float tol = m.prm.thickness + m.prm.tolerance * 0.5f;
+        launch_bvh_refit(s, m.sweptTriBvh, c, 2, tol);
+        launch_bvh_refit(s, m.sweptEdgeBvh, c, 3, tol);
+        launch_ccd(s, c, P, b, m.sweptTriBvh, m.sweptEdgeBvh);
+    }
+    if (self || ccd) launch_compact_self(s, c, b, ccd);
+    else cudaMemsetAsync(b.stCount, 0, 2 * sizeof(int), s);
+    launch_colour_contacts(s, c, b);
+    // ClothModelPBD::SolveGS (Physics/ClothPBD.cpp:324-369)
+    launch_reset_gs(s, c);
+    for (int k = 0; k < m.prm.iterations; k++)
+    {
+        if (m.prm.fem)
+            for (size_t col = 0; col + 1 < m.triColourStart.size(); col++)
+                launch_fem(s, c, P, m.triColourStart[col], m.triColourStart[col + 1] - m.triColourStart[col]);
+        if (m.prm.dihedral && k % m.prm.bendFreq == 0)
+            for (size_t col = 0; col + 1 < m.bendColourStart.size(); col++)
+                launch_bends(s, c, P, m.bendColourStart[col], m.bendColourStart[col + 1] - m.bendColourStart[col], col == 0);
+        launch_solve_vertex_contacts(s, c, P, b);
+        launch_solve_multi_contacts(s, c, P, b, k);
+    }
+    launch_velocity(s, c, P);
+}
+
+// ClothPatch::Step (Physics/ClothPatch.cpp:323-335): numSteps substeps of dt/n,
+// launched as one CUDA graph (captured on first use and whenever a parameter,
+// the collision world or dt changes). Asynchronous: readers synchronise.
+bool ClothPatch::step(float dt)
+{
+    ClothModel& m = model;
+    if (m.N == 0) { set_error(SC_ERR_STATE, "cloth not initialised"); return false; }
+    if (!m.prm.fem && m.prm.iterations > 0)
+    {
+        set_error(SC_ERR_UNSUPPORTED, "mass-spring (links) solver is not implemented on the GPU; enable FEM");
+        return false;
+    }
+    if (!m.ensure_buffers(world, stream)) return false;
+    const int n = numSteps;
+    const float h = dt / n;
+    if (!graph || graphDt != dt || graphSteps != n || graphParamVersion != m.paramVersion || graphWorldVersion != world.version)
+    {
+        if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
+        cudaGraph_t g;
+        SC_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        for (int i = 0; i < n; i++) record_substep(h);
+        SC_CUDA(cudaStreamEndCapture(stream, &g));
+        size_t numNodes = 0;
+        cudaGraphGetNodes(g, nullptr, &numNodes);
+        std::vector<cudaGraphNode_t> nodes(numNodes);
+        if (numNodes) cudaGraphGetNodes(g, nodes.data(), &numNodes);
+        graphKernelCount = 0;
+        for (size_t k = 0; k < numNodes; k++)
+        {
+            cudaGraphNodeType t;
+            if (cudaGraphNodeGetType(nodes[k], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) graphKernelCount++;
+        }
+        cudaError_t e = cudaGraphInstantiate(&graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) { set_error(SC_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e)); graph = nullptr; return false; }
+        graphDt = dt; graphSteps = n; graphParamVersion = m.paramVersion; graphWorldVersion = world.version;
+    }
+    SC_CUDA(cudaGraphLaunch(graph, stream));
+    hostStateDirty = true;
+    return true;
+}
+
+// ClothPatch::UpdateMesh (Physics/ClothPatch.cpp:266-273): render mesh from the
+// current positions, both meshes' normals recomputed; the collision mesh's
+// normals feed the next substeps' Voronoi tests.
+void ClothPatch::update_mesh()
+{
+    ClothModel& m = model;
+    if (m.N == 0) return;
+    launch_normals(stream, m.dc, false, m.dc.pos);
+    launch_normals(stream, m.dc, true, m.dc.prev);
+    sync();
+    std::vector<float4> n(m.N);
+    cudaMemcpy(n.data(), m.dc.meshN, sizeof(float4) * m.N, cudaMemcpyDeviceToHost);
+    mesh.verts = m.hpos;
+    mesh.normals.resize(m.N);
+    for (int i = 0; i < m.N; i++) mesh.normals[i] = mk(n[i]);
+}
+
+} // namespace sc

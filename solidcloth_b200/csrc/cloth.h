@@ -1,0 +1,194 @@
+// cloth.h — host-side objects behind the C ABI: collision world, collidables,
+// cloth model and cloth patch (the roles of Physics/CollisionWorld.h,
+// Physics/Common.h, Physics/ClothModel.h and Physics/ClothPatch.h).
+#pragma once
+#include "launch.h"
+#include <memory>
+#include <vector>
+#include <string>
+#include <cstdint>
+
+namespace sc {
+
+// ------------------------------------------------------------ host mesh
+struct HEdge
+{
+    V3 n = {0, 0, 0};
+    uint32_t i1 = 0, i2 = 0;
+    int t1 = -1, t2 = -1;
+    int origIdx = 0;
+    bool swapped = false;
+};
+
+struct HMesh
+{
+    std::vector<V3> verts;
+    std::vector<uint32_t> idx;
+    std::vector<V3> normals, triN;
+    std::vector<uint32_t> triE;          // 3 per triangle
+    std::vector<HEdge> edges;
+    std::vector<std::vector<int>> vtxRing, edgeRing;
+    int ntris() const { return (int)idx.size() / 3; }
+    void compute_normals();              // Mesh::ComputeNormals
+    void construct_edges();              // Mesh::ConstructEdges
+    void construct_rings(bool vtx, bool edge);
+};
+
+// ------------------------------------------------------------ colliders
+enum CollidableType { CT_INVALID, CT_WALLS, CT_SLAB, CT_SPHERE, CT_MESH, CT_BOX, CT_CAPSULE, CT_SDF };
+
+struct Collidable
+{
+    int type = CT_INVALID;
+    float rot[4] = {1, 0, 0, 0};       // quaternion (s, x, y, z)
+    V3 center = {0, 0, 0};
+    virtual ~Collidable() {}
+};
+
+struct WallsC : Collidable { Box box; };
+struct SphereC : Collidable { float radius = 0; };
+struct CapsuleC : Collidable { float r = 0, hh = 0; };
+
+struct SDFC : Collidable
+{
+    int nc[3] = {0, 0, 0};
+    Box box;
+    V3 steps = {0, 0, 0};
+    std::vector<float> values;
+    std::vector<V3> grad;
+    // per-device texture objects
+    int device = -1;
+    cudaArray_t valArr = nullptr, gradArr = nullptr;
+    cudaTextureObject_t valTex = 0, gradTex = 0;
+    ~SDFC();
+    void compute_gradient();             // SDF::ComputeGradient
+    bool upload(int dev);
+};
+
+struct MeshTreeNode { Box box; std::vector<uint32_t> tris, verts, edges; int left = -1, right = -1; };
+
+struct MeshC : Collidable
+{
+    HMesh mesh;
+    std::vector<MeshTreeNode> tree;      // Geometry::ComputeMeshTree, built lazily
+    bool built = false;
+    int device = -1;
+    // device copies
+    void* dmem = nullptr;
+    DevMesh dev{};
+    ~MeshC();
+    void build_tree(float tol);
+    bool upload(int dev);
+};
+
+struct CollisionWorld
+{
+    std::vector<std::shared_ptr<Collidable>> list;
+    uint64_t version = 0;
+};
+
+// ------------------------------------------------------------ cloth
+struct HostParams
+{
+    // defaults of ClothModel::ClothModel (Physics/ClothModel.cpp:10-36)
+    float unit = 10, thickness = 0.3f, tolerance = 0.2f, shear = 5e8f, bend = 5.f, stretch = 2e10f;
+    float poisson = 0.5f, friction = 0.4f, area = 10.f, drag = 1.f, selfShrink = .9f, selfSoften = .1f;
+    float selfThreshold = 0.003f;
+    int iterations = 50, flags = 0, bendFreq = 2;
+    bool fem = false, dihedral = true, fixedIterations = false, ccd = false;
+};
+
+struct FemHost { uint32_t i1, i2, i3; float du1, du2, dv1, dv2, det, invDet, lu0, lv0, su, sv, lu2, lv2, area; };
+
+struct LBVHHost
+{
+    std::vector<int> child, escape, parent, leafNode;
+    int numLeaves = 0, numNodes = 0;
+    void build(const std::vector<V3>& centroids);
+};
+
+class ClothPatch;
+
+class ClothModel
+{
+public:
+    explicit ClothModel(ClothPatch* owner) : owner(owner) {}
+    ~ClothModel();
+
+    ClothPatch* owner;
+    HostParams prm;
+    uint64_t paramVersion = 1;
+
+    // host topology and rest data
+    int N = 0;
+    std::vector<V3> hpos, hprev, hvel;
+    std::vector<float> invMass;
+    std::vector<float> uvx, uvy;
+    std::vector<FemHost> tris;
+    std::vector<uint4> bends;
+    std::vector<uint2> links;
+    std::vector<uint4> quads;
+    std::vector<int> triOrder, bendOrder;      // colour order
+    std::vector<int> triColourStart, bendColourStart;
+    bool mouseActive = false;
+
+    // device
+    int device = -1;
+    std::vector<void*> allocs;
+    DevCloth dc{};
+    DevBVH triBvh{}, edgeBvh{}, sweptTriBvh{}, sweptEdgeBvh{};
+    Buffers buf{};
+    std::vector<VColl> vcollHost;
+    std::vector<void*> bufAllocs;
+    uint64_t bufWorldVersion = ~0ull;
+    int bufFlags = -1;
+    bool bufCcd = false;
+
+    void* dalloc(size_t bytes, bool contactBuffer = false);
+    void release_device();
+    void release_buffers();
+    bool upload_topology(const HMesh& mesh);
+    bool ensure_buffers(const CollisionWorld& world, cudaStream_t s);
+    void download_state(cudaStream_t s);
+    void upload_state(cudaStream_t s);
+    SolverParams solver_params(float h) const;
+    void colour_constraints();
+    void touch() { paramVersion++; }
+};
+
+class ClothPatch
+{
+public:
+    explicit ClothPatch(CollisionWorld& w);
+    ~ClothPatch();
+
+    CollisionWorld& world;
+    ClothModel model;
+    HMesh mesh, prevMesh;     // render mesh and collision mesh (host mirrors)
+    int numSteps = 1;
+    bool isQuadMesh = true;
+    cudaStream_t stream = nullptr;
+
+    // cached CUDA graph of one frame
+    cudaGraphExec_t graph = nullptr;
+    float graphDt = -1.f;
+    int graphSteps = -1;
+    uint64_t graphParamVersion = 0, graphWorldVersion = ~0ull;
+    bool hostStateDirty = false;   // host copies older than the device state
+    int graphKernelCount = 0;
+
+    bool init_grid(int divX, int divY, float inc, V3 offset, bool horizontal, bool attached);
+    bool step(float dt);
+    void update_mesh();
+    void record_substep(float h);
+    void sync();
+};
+
+// error reporting (thread-local last error, plus device status bits)
+void set_error(int code, const std::string& msg);
+int last_error();
+const char* last_error_string();
+
+enum ErrorCodes { SC_OK = 0, SC_ERR_CUDA = 1, SC_ERR_ARG = 2, SC_ERR_STATE = 3, SC_ERR_UNSUPPORTED = 4, SC_ERR_DEVICE_STATUS = 5 };
+
+} // namespace sc

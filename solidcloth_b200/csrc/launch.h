@@ -1,0 +1,85 @@
+// launch.h — host-callable launchers for the cloth-step kernels (step_kernels.cu).
+#pragma once
+#include "sc_internal.cuh"
+
+namespace sc {
+
+constexpr int KVT = 16;        // self vertex-triangle contact slots per vertex
+constexpr int KCAND = 192;     // BVH candidates kept per proximity query
+constexpr int KRES = 48;       // distinct features tracked per vertex for the dedup
+constexpr int KCCD = 64;       // continuous-collision candidates per query
+constexpr int MAX_COLOURS = 64;// independent-set colouring rounds per contact class
+constexpr int WALL_SLOTS = 5;
+
+// Vertex contact slot (walls, sphere, SDF, mesh vertex contacts).
+struct VC { float4 point; float4 normal; float2 lam; int feature; int mesh; };
+// Triangle contact (cloth triangle vs collider vertex / sphere / SDF).
+struct TC { uint4 idx; float4 point; float4 normal; float4 w; float2 lam; int feature; int mesh; };
+// Edge contact (cloth edge vs collider edge / sphere).
+struct EC { uint4 idx; float4 point; float4 normal; float4 w; float2 lam; int feature; int mesh; };
+// Self contact (vertex-triangle: i1..i3 triangle, i4 vertex; edge-edge: (i1,i2) x (i3,i4)).
+struct SCt { uint4 idx; float4 normal; float4 w; float2 lam; float side; float error; };
+
+// Vertex collider descriptor (world order).
+struct VColl
+{
+    int type;        // 1 walls, 3 sphere, 7 sdf, 4 mesh
+    int slotBase;    // first slot of this collider in the vertex-contact slot array
+    int kmax;        // slots per vertex
+    int mesh;        // mesh collider index for type 4
+    float4 a, b;     // walls: lo, hi; sphere: centre (a.xyz), radius (a.w)
+    cudaTextureObject_t val, grad; // sdf
+    float4 sdfLo, sdfSteps;        // sdf box min, steps
+    int4 sdfCells;
+};
+
+struct Buffers
+{
+    // vertex contacts: counts[coll][N] (uint8), slots[slotBase + i*kmax + k]
+    uint8_t* vcCount;
+    VC* vc;
+    int numVColl;
+    const VColl* vcoll;       // device copy
+    // triangle / edge contacts: per-collider slot arrays, flags, dense lists
+    TC* tcSlot; int* tcFlag; TC* tcList; int* tcCount; int tcCap;
+    EC* ecSlot; int* ecFlag; EC* ecList; int* ecCount; int ecCap;
+    // self contacts
+    int* stCnt; SCt* stSlot; SCt* stList; int* stCount; int stCap;
+    int* seFlag; SCt* seSlot; SCt* seList; int* seCount; int seCap;
+    // continuous collision
+    int* ccdVtCnt; int* ccdVtCand; int* ccdEeCnt; int* ccdEeCand;
+    int2* ccdVtPairs; int2* ccdEePairs; int* ccdVtPairCount; int* ccdEePairCount; int ccdVtCap, ccdEeCap;
+    int* ccdVtHit; SCt* ccdVtRec; int* ccdEeHit; SCt* ccdEeRec;
+    // colouring scratch
+    unsigned long long* vmin;  // N, kept at ~0
+    int* colour; int* order; int* colourStart; int colourCap;
+    // scan scratch: block sums, per-item offsets, totals
+    int* scanBlock; int* scanOff; int* scanTot;
+    const DevMesh* meshes;     // device array
+    int numMeshes;
+};
+
+void launch_predict(cudaStream_t s, const DevCloth& c, const SolverParams& P);
+void launch_velocity(cudaStream_t s, const DevCloth& c, const SolverParams& P);
+void launch_fem(cudaStream_t s, const DevCloth& c, const SolverParams& P, int first, int count);
+void launch_bends(cudaStream_t s, const DevCloth& c, const SolverParams& P, int first, int count, int resetErr);
+void launch_normals(cudaStream_t s, const DevCloth& c, bool prevMesh, const float4* verts);
+void launch_vertex_colliders(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b, const VColl* hostColl);
+void launch_tri_edge_colliders(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b,
+                               const VColl* hostColl, int numColl, int flags);
+void launch_solve_vertex_contacts(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b);
+void launch_solve_multi_contacts(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b, int iter);
+void launch_colour_contacts(cudaStream_t s, const DevCloth& c, const Buffers& b);
+void launch_bvh_refit(cudaStream_t s, const DevBVH& bvh, const DevCloth& c, int kind, float tol);
+void launch_self_proximity(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b,
+                           const DevBVH& triBvh, const DevBVH& edgeBvh);
+void launch_ccd(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b,
+                const DevBVH& triBvh, const DevBVH& edgeBvh);
+void launch_compact_self(cudaStream_t s, const DevCloth& c, const Buffers& b, bool ccd);
+void launch_reset_gs(cudaStream_t s, const DevCloth& c);
+void launch_gs_exit_test(cudaStream_t s, const DevCloth& c, const SolverParams& P, int iter);
+
+// exclusive scan of n ints (out may alias nothing); total written to *total if not null
+void scan_ints(cudaStream_t s, const int* in, int* out, int n, int* total, int* tmp);
+
+} // namespace sc

@@ -1,0 +1,1899 @@
+// step_kernels.cu — sm_100a kernels of the per-substep PBD cloth step.
+//
+// One substep (ClothModelPBD::Step, Physics/ClothPBD.cpp:255-322) is, on the GPU:
+//   predict -> [collision mesh refit, detection into fixed slots, block-scan
+//   compaction, independent-set colouring of multi-particle contacts]
+//   -> iterations x (FEM colours, bend colours every 2nd iteration, vertex
+//   contacts, multi-particle contacts) -> velocity,
+// all captured once into a CUDA graph by the host (cloth.cu).
+//
+// Bit-exactness: compiled with -fmad=false and IEEE division/square root; the
+// arithmetic follows the reference's operation order (see scmath.cuh), so box
+// overlaps, contact regions, candidate pairs and CCD hits are decided exactly as
+// the reference decides them. acosf/atan2f are CUDA's and may differ from glibc's
+// by a few ulp (bend angles, angle-weighted normals).
+#include "launch.h"
+#include <cstdio>
+
+namespace sc {
+
+__device__ __forceinline__ V3 ld3(const float4* p, uint32_t i) { float4 a = p[i]; return mk(a.x, a.y, a.z); }
+__device__ __forceinline__ void st3(float4* p, uint32_t i, V3 v)
+{
+    float4 a = p[i]; a.x = v.x; a.y = v.y; a.z = v.z; p[i] = a;
+}
+__device__ __forceinline__ void atomic_max_pos(float* addr, float v)
+{
+    // non-negative floats order like their bit patterns
+    atomicMax((int*)addr, __float_as_int(v));
+}
+__device__ __forceinline__ bool gs_done(const DevCloth& c) { return c.scal[8] != 0.f; }
+
+static inline int blocks_for(int n, int t = 256) { int b = (n + t - 1) / t; return b < 1 ? 1 : b; }
+
+// --------------------------------------------------------------- predict
+// ClothModelPBD::Step, symplectic Euler part (Physics/ClothPBD.cpp:257-266);
+// also the max |pos - prev| used by the collision thresholds
+// (Physics/ClothCollision.cpp:91-100).
+__global__ void k_predict(DevCloth c, SolverParams P)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.N) return;
+    float4 p = c.pos[i];
+    c.prev[i] = make_float4(p.x, p.y, p.z, 0.f);
+    if (p.w == 0.f) return;
+    float4 v = c.vel[i];
+    const float hgx = P.h * 0.f, hgy = P.h * -9.8f, hgz = P.h * 0.f;
+    v.x += P.unit * hgx; v.y += P.unit * hgy; v.z += P.unit * hgz;
+    v.x = P.drag * v.x; v.y = P.drag * v.y; v.z = P.drag * v.z;
+    c.vel[i] = v;
+    V3 np = mk(p.x, p.y, p.z) + P.h * mk(v.x, v.y, v.z);
+    c.pos[i] = make_float4(np.x, np.y, np.z, p.w);
+    float tv = len(np - mk(p.x, p.y, p.z));
+    atomic_max_pos(&c.scal[0], tv);
+}
+
+// ClothModelPBD::Step, velocity update (Physics/ClothPBD.cpp:314-321)
+__global__ void k_velocity(DevCloth c, SolverParams P)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.N) return;
+    float4 p = c.pos[i];
+    if (p.w == 0.f) return;
+    float4 q = c.prev[i];
+    V3 v = P.invH * (mk(p.x, p.y, p.z) - mk(q.x, q.y, q.z));
+    c.vel[i] = make_float4(v.x, v.y, v.z, 0.f);
+}
+
+// ------------------------------------------------------------ FEM sweep
+// ClothModelPBD::SolveTriangles for the triangles of one colour
+// (Physics/ClothPBD.cpp:52-108): warp and weft hard, shear compliant.
+__global__ void __launch_bounds__(256) k_fem(DevCloth c, SolverParams P, int first, int count)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count || gs_done(c)) return;
+    k += first;
+    const float4 r0 = c.fem[3 * k], r1 = c.fem[3 * k + 1], r2 = c.fem[3 * k + 2];
+    const uint32_t i1 = __float_as_uint(r0.x), i2 = __float_as_uint(r0.y), i3 = __float_as_uint(r0.z);
+    const float du1 = r0.w, du2 = r1.x, dv1 = r1.y, dv2 = r1.z, invDet = r1.w;
+    const float lu2 = r2.x, lv2 = r2.y, lu0lv0 = r2.z, area = r2.w;
+    float4 a = c.pos[i1], b = c.pos[i2], d = c.pos[i3];
+    V3 x1 = mk(a.x, a.y, a.z), x2 = mk(b.x, b.y, b.z), x3 = mk(d.x, d.y, d.z);
+    const float w1 = a.w, w2 = b.w, w3 = d.w;
+    V3 dx1 = x2 - x1, dx2 = x3 - x1;
+    V3 wu = invDet * (dv2 * dx1 - dv1 * dx2);
+    V3 wv = invDet * (-du2 * dx1 + du1 * dx2);
+    float err, diag, lambda;
+    V3 q1, q2, q3;
+    // warp
+    q2 = (invDet * dv2) * wu;
+    q3 = (-invDet * dv1) * wu;
+    q1 = -q2 - q3;
+    diag = dot(w1 * q1, q1) + dot(w2 * q2, q2) + dot(w3 * q3, q3);
+    err = 0.5f * (dot(wu, wu) - lu2);
+    lambda = -err / diag;
+    x1 += (w1 * lambda) * q1; x2 += (w2 * lambda) * q2; x3 += (w3 * lambda) * q3;
+    // weft
+    q2 = (-invDet * du2) * wv;
+    q3 = (invDet * du1) * wv;
+    q1 = -q2 - q3;
+    diag = dot(w1 * q1, q1) + dot(w2 * q2, q2) + dot(w3 * q3, q3);
+    err = 0.5f * (dot(wv, wv) - lv2);
+    lambda = -err / diag;
+    x1 += (w1 * lambda) * q1; x2 += (w2 * lambda) * q2; x3 += (w3 * lambda) * q3;
+    // shear
+    q2 = dv2 * wv - du2 * wu;
+    q3 = -dv1 * wv + du1 * wu;
+    q1 = -q2 - q3;
+    diag = invDet * (dot(w1 * q1, q1) + dot(w2 * q2, q2) + dot(w3 * q3, q3));
+    err = dot(wu, wv);
+    float s = 1.f / (1.f + lu0lv0 * P.epsUV / (diag * P.h2 * area));
+    lambda = -s * err / diag;
+    x1 += (w1 * lambda) * q1; x2 += (w2 * lambda) * q2; x3 += (w3 * lambda) * q3;
+    c.pos[i1] = make_float4(x1.x, x1.y, x1.z, w1);
+    c.pos[i2] = make_float4(x2.x, x2.y, x2.z, w2);
+    c.pos[i3] = make_float4(x3.x, x3.y, x3.z, w3);
+}
+
+// ---------------------------------------------------------- bend sweep
+// SolveBends + EvaluateAngle + EvaluateGradient for one colour
+// (Physics/ClothPBD.cpp:110-224).
+__global__ void __launch_bounds__(256) k_bends(DevCloth c, SolverParams P, int first, int count)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count || gs_done(c)) return;
+    const uint4 bc = c.bend[first + k];
+    float4 a = c.pos[bc.x], b = c.pos[bc.y], d = c.pos[bc.z], e = c.pos[bc.w];
+    const float m1 = a.w, m2 = b.w, m3 = d.w, m4 = e.w;
+    if (m1 + m2 + m3 + m4 == 0) return;
+    V3 x1 = mk(a.x, a.y, a.z), x2 = mk(b.x, b.y, b.z), x3 = mk(d.x, d.y, d.z), x4 = mk(e.x, e.y, e.z);
+    V3 x12 = x2 - x1;
+    float l = len(x12);
+    V3 x13 = x3 - x1;
+    V3 n1 = cross(x12, x13);
+    float l1 = len(n1);
+    V3 x14 = x4 - x1;
+    V3 n2 = cross(x14, x12);
+    float l2 = len(n2);
+    float cosine, theta;
+    if (l1 == 0 || l2 == 0) { cosine = 1; theta = 0; }
+    else
+    {
+        float il1 = 1.f / l1, il2 = 1.f / l2;
+        cosine = dot(il1 * n1, il2 * n2);
+        cosine = mn(1.f, mx(-1.f, cosine));
+        theta = acosf(cosine);
+    }
+    if (fabsf(cosine) >= 1 - 0.001f) return;
+    float h1 = l1 / l, h2 = l2 / l;
+    float he = 0.5f * (h1 + h2);
+    float il1 = 1.f / l1, il2 = 1.f / l2;
+    V3 n1n = il1 * n1, n2n = il2 * n2;
+    V3 n1p = n1n - n2n * cosine;
+    V3 n2p = n2n - n1n * cosine;
+    float sine = sqrtf(1 - cosine * cosine);
+    V3 q3 = (il1 / sine / he) * cross(x12, n2p);
+    V3 q4 = (-il2 / sine / he) * cross(x12, n1p);
+    V3 q2 = (-il1 / sine / he) * cross(x13, n2p) + (il2 / sine / he) * cross(x14, n1p);
+    V3 q1 = -q2 - q3 - q4;
+    float diag = m1 * lensq(q1) + m2 * lensq(q2) + m3 * lensq(q3) + m4 * lensq(q4);
+    if (diag == 0) return;
+    float s = 0.0005f * P.bend;
+    float errv = fabsf(s * theta);
+    float lambda = -s * theta / he / diag;
+    x1 += (lambda * m1) * q1; x2 += (lambda * m2) * q2; x3 += (lambda * m3) * q3; x4 += (lambda * m4) * q4;
+    c.pos[bc.x] = make_float4(x1.x, x1.y, x1.z, m1);
+    c.pos[bc.y] = make_float4(x2.x, x2.y, x2.z, m2);
+    c.pos[bc.z] = make_float4(x3.x, x3.y, x3.z, m3);
+    c.pos[bc.w] = make_float4(x4.x, x4.y, x4.z, m4);
+    if (!P.fixedIterations) atomic_max_pos(&c.scal[2], errv);
+}
+
+// ----------------------------------------------------------- normals
+// Mesh::ComputeNormals (Geometry/Mesh.cpp:10-63): per-triangle unit normal and
+// corner angles, then a per-vertex gather in triangle order (the reference's
+// accumulation order), then normalisation.
+__global__ void k_tri_normals(const float4* verts, const uint32_t* tri, int T, float4* triN, float4* ang)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= T) return;
+    V3 a = ld3(verts, tri[3 * t]), b = ld3(verts, tri[3 * t + 1]), cc = ld3(verts, tri[3 * t + 2]);
+    V3 nt = normalized(cross(b - a, cc - a));
+    triN[t] = f4(nt, 0.f);
+    V3 e1 = normalized(b - a), e2 = normalized(cc - b), e3 = normalized(a - cc);
+    float c1 = -dot(e1, e3), c2 = -dot(e1, e2), c3 = -dot(e2, e3);
+    float s1 = len(cross(e1, -e3)), s2 = len(cross(e2, -e1)), s3 = len(cross(e3, -e1));
+    float t1 = fabsf(c1) > 1 ? fabsf((float)atan2((double)s1, (double)c1)) : acosf(c1);
+    float t2 = fabsf(c2) > 1 ? fabsf((float)atan2((double)s2, (double)c2)) : acosf(c2);
+    float t3 = fabsf(c3) > 1 ? fabsf((float)atan2((double)s3, (double)c3)) : acosf(c3);
+    ang[t] = make_float4(t1, t2, t3, 0.f);
+}
+
+__global__ void k_vertex_normals(int N, const int* start, const int2* vt, const float4* triN, const float4* ang, float4* out)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    V3 n = mk(0.f, 0.f, 0.f);
+    for (int k = start[i]; k < start[i + 1]; k++)
+    {
+        int2 tc = vt[k];
+        float4 a = ang[tc.x];
+        float w = tc.y == 0 ? a.x : (tc.y == 1 ? a.y : a.z);
+        n += w * ld3(triN, tc.x);
+    }
+    if (len(n) != 0) n = normalized(n);
+    out[i] = f4(n, 0.f);
+}
+
+// ------------------------------------------------------------ SDF grid
+// SDF::GetGridCoords / GetValue / GetGrad (Geometry/SDF.h:105-155): point
+// fetches from 3-D textures (border mode returns the reference's 0 outside the
+// grid) and the trilinear blend in FP32 registers in the reference's order.
+struct GridCoord { int x, y, z; float fx, fy, fz; };
+
+__device__ __forceinline__ GridCoord grid_coords(const VColl& g, V3 p)
+{
+    GridCoord r;
+    float rx = (p.x - g.sdfLo.x) / g.sdfSteps.x;
+    float ry = (p.y - g.sdfLo.y) / g.sdfSteps.y;
+    float rz = (p.z - g.sdfLo.z) / g.sdfSteps.z;
+    r.x = (int)floorf(rx); r.y = (int)floorf(ry); r.z = (int)floorf(rz);
+    r.fx = fabsf(rx - r.x); r.fy = fabsf(ry - r.y); r.fz = fabsf(rz - r.z);
+    return r;
+}
+
+__device__ __forceinline__ bool grid_out(const VColl& g, int x, int y, int z)
+{
+    return x > g.sdfCells.x || y > g.sdfCells.y || z > g.sdfCells.z || x < 0 || y < 0 || z < 0;
+}
+
+__device__ __forceinline__ float tv(const VColl& g, int x, int y, int z)
+{
+    return tex3D<float>(g.val, x + 0.5f, y + 0.5f, z + 0.5f);
+}
+__device__ __forceinline__ V3 tg(const VColl& g, int x, int y, int z)
+{
+    float4 a = tex3D<float4>(g.grad, x + 0.5f, y + 0.5f, z + 0.5f);
+    return mk(a.x, a.y, a.z);
+}
+
+__device__ float sdf_value(const VColl& g, V3 p)
+{
+    GridCoord q = grid_coords(g, p);
+    if (grid_out(g, q.x, q.y, q.z)) return FLT_MAX;
+    const float fx = q.fx, fy = q.fy, fz = q.fz;
+    const int x = q.x, y = q.y, z = q.z;
+    return (1.f - fx) * (1.f - fy) * (1.f - fz) * tv(g, x, y, z) +
+           (1.f - fx) * (1.f - fy) * fz * tv(g, x, y, z + 1) +
+           (1.f - fx) * fy * (1.f - fz) * tv(g, x, y + 1, z) +
+           (1.f - fx) * fy * fz * tv(g, x, y + 1, z + 1) +
+           fx * (1.f - fy) * (1.f - fz) * tv(g, x + 1, y, z) +
+           fx * (1.f - fy) * fz * tv(g, x + 1, y, z + 1) +
+           fx * fy * (1.f - fz) * tv(g, x + 1, y + 1, z) +
+           fx * fy * fz * tv(g, x + 1, y + 1, z + 1);
+}
+
+__device__ V3 sdf_grad(const VColl& g, V3 p)
+{
+    GridCoord q = grid_coords(g, p);
+    if (grid_out(g, q.x, q.y, q.z)) return mk(0.f, 0.f, 0.f);
+    const float fx = q.fx, fy = q.fy, fz = q.fz;
+    const int x = q.x, y = q.y, z = q.z;
+    return (1.f - fx) * (1.f - fy) * (1.f - fz) * tg(g, x, y, z) +
+           (1.f - fx) * (1.f - fy) * fz * tg(g, x, y, z + 1) +
+           (1.f - fx) * fy * (1.f - fz) * tg(g, x, y + 1, z) +
+           (1.f - fx) * fy * fz * tg(g, x, y + 1, z + 1) +
+           fx * (1.f - fy) * (1.f - fz) * tg(g, x + 1, y, z) +
+           fx * (1.f - fy) * fz * tg(g, x + 1, y, z + 1) +
+           fx * fy * (1.f - fz) * tg(g, x + 1, y + 1, z) +
+           fx * fy * fz * tg(g, x + 1, y + 1, z + 1);
+}
+
+// SphereSDF::QueryPoint / GridSDF::QueryPoint (Physics/ClothCollisionSDF.h:14-24,130-139)
+__device__ float query_point(const VColl& g, V3 p, V3& cp, V3& n, int& feature)
+{
+    if (g.type == 7)
+    {
+        float v = sdf_value(g, p);
+        V3 gr = normalized(sdf_grad(g, p));
+        n = gr;
+        cp = p - v * gr;
+        feature = -3;
+        return v;
+    }
+    V3 ctr = mk(g.a.x, g.a.y, g.a.z);
+    V3 delta = p - ctr;
+    float l = len(delta);
+    delta = (1.f / l) * delta;
+    n = delta;
+    cp = ctr + g.a.w * delta;
+    feature = -1;
+    return l - g.a.w;
+}
+
+// --------------------------------------------------- static mesh tree
+// ClosestPointOnMeshToPointRec / ToTriangleRec / ToSegmentEdgeRec
+// (Geometry/ClosestPointOnMesh.cpp:262-302,393-452,589-659) as an explicit-stack
+// depth-first search that visits nodes in exactly the recursion's order:
+// the nearer child first; the farther child is tested against the distance
+// found once the nearer subtree is done.
+constexpr int MESH_STACK = 48;
+
+struct PointHit { float dist; int tri; V3 cp, bary, normal; int region; };
+
+__device__ PointHit mesh_point_query(const DevMesh& m, V3 p, int* status)
+{
+    PointHit r; r.dist = FLT_MAX; r.tri = -1; r.region = -1;
+    r.cp = r.bary = r.normal = mk(0.f, 0.f, 0.f);
+    float minDist = FLT_MAX;
+    int stNode[MESH_STACK]; float stDist[MESH_STACK];
+    int sp = 0;
+    int node = 0;
+    while (true)
+    {
+        if (node >= 0)
+        {
+            int4 pr = m.tree.primRange[node];
+            for (int k = 0; k < pr.y; k++)
+            {
+                uint32_t t = m.tree.tris[pr.x + k];
+                V3 a = ld3(m.v, m.tri[3 * t]), b = ld3(m.v, m.tri[3 * t + 1]), cc = ld3(m.v, m.tri[3 * t + 2]);
+                V3 coords, pt;
+                int region = closest_point_triangle(p, a, b, cc, pt, coords);
+                V3 delta = p - pt;
+                float dist = len(delta);
+                if (dist == 0) continue;
+                if (dist < minDist)
+                {
+                    minDist = dist;
+                    r.dist = dist; r.tri = (int)t; r.cp = pt; r.bary = coords;
+                    r.normal = (1.f / dist) * delta; r.region = region;
+                }
+            }
+            int2 ch = m.tree.children[node];
+            if (ch.x >= 0 || ch.y >= 0)
+            {
+                Box bl, br;
+                float dl = FLT_MAX, dr = FLT_MAX;
+                if (ch.x >= 0) { bl.lo = ld3(m.tree.lo, ch.x); bl.hi = ld3(m.tree.hi, ch.x); dl = bl.dist(p); }
+                if (ch.y >= 0) { br.lo = ld3(m.tree.lo, ch.y); br.hi = ld3(m.tree.hi, ch.y); dr = br.dist(p); }
+                int nearN = ch.x, farN = ch.y; float nearD = dl, farD = dr;
+                if (!(dl < dr)) { nearN = ch.y; farN = ch.x; nearD = dr; farD = dl; }
+                if (sp < MESH_STACK) { stNode[sp] = farN; stDist[sp] = farD; sp++; }
+                else atomicOr(status, ST_MESH_STACK_OVERFLOW);
+                node = (nearD < minDist) ? nearN : -1;
+                continue;
+            }
+        }
+        // pop the next pending far child whose box is still within reach
+        node = -1;
+        while (sp > 0 && node < 0)
+        {
+            sp--;
+            if (stDist[sp] < minDist) node = stNode[sp];
+        }
+        if (node < 0) break;
+    }
+    return r;
+}
+
+struct VtxHit { float dist; int vertex; V3 cpMesh, cpTri, bary, normal; int region; };
+
+__device__ VtxHit mesh_triangle_query(const DevMesh& m, V3 a, V3 b, V3 cc, int* status)
+{
+    VtxHit r; r.dist = -FLT_MAX; r.vertex = -1; r.region = 0;
+    r.cpMesh = r.cpTri = r.bary = r.normal = mk(0.f, 0.f, 0.f);
+    float minDist = FLT_MAX;
+    Box tb = Box::empty(); tb.add(a); tb.add(b); tb.add(cc);
+    int stNode[MESH_STACK]; float stDist[MESH_STACK];
+    int sp = 0, node = 0;
+    while (true)
+    {
+        if (node >= 0)
+        {
+            int4 pr = m.tree.primRange[node];
+            for (int k = 0; k < pr.w; k++)
+            {
+                uint32_t v = m.tree.verts[pr.z + k];
+                V3 pv = ld3(m.v, v);
+                V3 bary, cp;
+                int region = closest_point_triangle(pv, a, b, cc, cp, bary);
+                V3 delta = cp - pv;
+                float dist = len(delta);
+                if (dist == 0) continue;
+                if (dist < minDist)
+                {
+                    minDist = dist;
+                    r.vertex = (int)v; r.cpMesh = pv; r.cpTri = cp; r.bary = bary;
+                    r.normal = (1.f / dist) * delta; r.dist = dist; r.region = region;
+                }
+            }
+            int2 ch = m.tree.children[node];
+            if (ch.x >= 0 || ch.y >= 0)
+            {
+                Box bl, br;
+                float dl = FLT_MAX, dr = FLT_MAX;
+                if (ch.x >= 0) { bl.lo = ld3(m.tree.lo, ch.x); bl.hi = ld3(m.tree.hi, ch.x); dl = bl.dist(tb); }
+                if (ch.y >= 0) { br.lo = ld3(m.tree.lo, ch.y); br.hi = ld3(m.tree.hi, ch.y); dr = br.dist(tb); }
+                int nearN = ch.x, farN = ch.y; float nearD = dl, farD = dr;
+                if (!(dl < dr)) { nearN = ch.y; farN = ch.x; nearD = dr; farD = dl; }
+                if (sp < MESH_STACK) { stNode[sp] = farN; stDist[sp] = farD; sp++; }
+                else atomicOr(status, ST_MESH_STACK_OVERFLOW);
+                node = (nearD < minDist) ? nearN : -1;
+                continue;
+            }
+        }
+        node = -1;
+        while (sp > 0 && node < 0) { sp--; if (stDist[sp] < minDist) node = stNode[sp]; }
+        if (node < 0) break;
+    }
+    return r;
+}
+
+struct SegHit { float dist; int edge; V3 cpMesh, cpSegm, normal; float cs0, cs1, cm0, cm1; int region; };
+
+// ComputeEdgeNormal (Geometry/ClosestPointOnMesh.cpp:483-497)
+__device__ __forceinline__ V3 mesh_edge_normal(const DevMesh& m, int e, float param)
+{
+    V3 n = ld3(m.en, e);
+    int4 ed = m.edge[e];
+    if (param == 0.f) n = ld3(m.n, ed.x);
+    if (param == 1.f) n = ld3(m.n, ed.y);
+    return n;
+}
+
+__device__ SegHit mesh_segment_query(const DevMesh& m, V3 p, V3 q, int* status)
+{
+    SegHit r; r.dist = -FLT_MAX; r.edge = -1; r.region = -1;
+    r.cpMesh = r.cpSegm = r.normal = mk(0.f, 0.f, 0.f);
+    r.cs0 = r.cs1 = r.cm0 = r.cm1 = 0.f;
+    float minDist = FLT_MAX;
+    Box eb = Box::empty(); eb.add(p); eb.add(q);
+    int stNode[MESH_STACK]; float stDist[MESH_STACK];
+    int sp = 0, node = 0;
+    while (true)
+    {
+        if (node >= 0)
+        {
+            int2 er = m.tree.edgeRange[node];
+            for (int k = 0; k < er.y; k++)
+            {
+                uint32_t e = m.tree.edges[er.x + k];
+                int4 ed = m.edge[e];
+                V3 a = ld3(m.v, ed.x), b = ld3(m.v, ed.y);
+                float ps, pm;
+                V3 cs, cm;
+                int region = closest_segm_segm(p, q, a, b, ps, pm, cs, cm);
+                V3 delta = cm - cs;
+                float dist = len(delta);
+                if (dist == 0) continue;
+                if (dist < minDist)
+                {
+                    minDist = dist;
+                    r.dist = dist; r.edge = (int)e; r.cpMesh = cm; r.cpSegm = cs;
+                    r.cs0 = 1.0f - ps; r.cs1 = ps; r.cm0 = 1.0f - pm; r.cm1 = pm;
+                    r.normal = mesh_edge_normal(m, (int)e, pm);
+                    r.region = region;
+                }
+            }
+            int2 ch = m.tree.children[node];
+            if (ch.x >= 0 || ch.y >= 0)
+            {
+                Box bl, br;
+                float dl = FLT_MAX, dr = FLT_MAX;
+                if (ch.x >= 0) { bl.lo = ld3(m.tree.lo, ch.x); bl.hi = ld3(m.tree.hi, ch.x); dl = bl.dist(eb); }
+                if (ch.y >= 0) { br.lo = ld3(m.tree.lo, ch.y); br.hi = ld3(m.tree.hi, ch.y); dr = br.dist(eb); }
+                int nearN = ch.x, farN = ch.y; float nearD = dl, farD = dr;
+                if (!(dl < dr)) { nearN = ch.y; farN = ch.x; nearD = dr; farD = dl; }
+                if (sp < MESH_STACK) { stNode[sp] = farN; stDist[sp] = farD; sp++; }
+                else atomicOr(status, ST_MESH_STACK_OVERFLOW);
+                node = (nearD < minDist) ? nearN : -1;
+                continue;
+            }
+        }
+        node = -1;
+        while (sp > 0 && node < 0) { sp--; if (stDist[sp] < minDist) node = stNode[sp]; }
+        if (node < 0) break;
+    }
+    return r;
+}
+
+// ------------------------------------------------- vertex contact detection
+// One thread per cloth vertex walks the world's colliders in order and writes
+// its vertex contacts into per-(collider, vertex) slots, reproducing
+// WallCollisions, SDFCollisions<Sphere/Grid> (vertex part) and the vertex part
+// of MeshCollisions (Physics/ClothCollision.cpp:89-135,199-220,438-470).
+__global__ void k_vertex_colliders(DevCloth c, SolverParams P, Buffers b)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.N) return;
+    const V3 pos = ld3(c.pos, i), prev = ld3(c.prev, i);
+    const float maxTv = c.scal[0];
+    const float radTolMesh = P.thickness + mx(P.tolerance, maxTv * 1.5f);
+    for (int ci = 0; ci < b.numVColl; ci++)
+    {
+        const VColl& g = b.vcoll[ci];
+        VC* slot = b.vc + g.slotBase + (size_t)i * g.kmax;
+        int n = 0;
+        auto add = [&](V3 p, V3 nn, int feature, int mesh) {
+            VC v;
+            v.point = f4(p, 0.f); v.normal = f4(nn, 0.f);
+            v.lam = make_float2(0.f, 0.f); v.feature = feature; v.mesh = mesh;
+            slot[n++] = v;
+        };
+        if (g.type == 1)
+        {
+            if (P.flags & CF_WALLS)
+            {
+                const float r = P.thickness + P.tolerance;
+                if (pos.y - r <= g.a.y) add(mk(pos.x, g.a.y, pos.z), mk(0, 1, 0), -1, -1);
+                if (pos.x - r <= g.a.x) add(mk(g.a.x, pos.y, pos.z), mk(1, 0, 0), -1, -1);
+                if (pos.x + r >= g.b.x) add(mk(g.b.x, pos.y, pos.z), mk(-1, 0, 0), -1, -1);
+                if (pos.z - r <= g.a.z) add(mk(pos.x, pos.y, g.a.z), mk(0, 0, 1), -1, -1);
+                if (pos.z + r >= g.b.z) add(mk(pos.x, pos.y, g.b.z), mk(0, 0, -1), -1, -1);
+            }
+        }
+        else if (g.type == 3 || g.type == 7)
+        {
+            if (P.flags & CF_VERTICES)
+            {
+                V3 p, nn; int feature;
+                float dist = query_point(g, prev, p, nn, feature);
+                float tvv = len(prev - pos);
+                float radTol = P.thickness + mx(P.tolerance, tvv * 1.1f);
+                if (dist < radTol && dist >= 0) add(p, nn, feature, -1);
+            }
+        }
+        else if (g.type == 4)
+        {
+            if (P.flags & CF_VERTICES)
+            {
+                PointHit h = mesh_point_query(b.meshes[g.mesh], prev, c.status);
+                if (h.dist < radTolMesh && h.dist >= 0) add(h.cp, h.normal, h.tri, g.mesh);
+            }
+        }
+        b.vcCount[(size_t)ci * c.N + i] = (uint8_t)n;
+    }
+}
+
+// GridSDF::QueryTriangle, Frank-Wolfe (Physics/ClothCollisionSDF.h:148-205)
+__device__ float sdf_query_triangle(const VColl& g, V3 a, V3 bb, V3 cc, V3& cpOut, V3& n, V3& coords)
+{
+    V3 cp = 0.33f * (a + bb + cc);
+    float distOld = 0;
+    for (int i = 1; i < 100; i++)
+    {
+        float dist = sdf_value(g, cp);
+        if (dist == FLT_MAX) return FLT_MAX;
+        V3 gr = sdf_grad(g, cp);
+        float dA = dot(a, gr), dB = dot(bb, gr), dC = dot(cc, gr);
+        float d = dA; V3 s = a;
+        if (dB < d) { d = dB; s = bb; }
+        if (dC < d) { d = dC; s = cc; }
+        if (distOld > 0)
+        {
+            float rel = fabsf(distOld - dist) / distOld;
+            if (rel < 0.0001f) break;
+        }
+        distOld = dist;
+        float alpha = 2.f / (i + 2.f);
+        cp += alpha * (s - cp);
+    }
+    float v = sdf_value(g, cp);
+    V3 gr = normalized(sdf_grad(g, cp));
+    n = gr;
+    cpOut = cp - v * gr;
+    V3 v0 = bb - a, v1 = cc - a, v2 = cp - a;
+    float d00 = lensq(v0), d01 = dot(v0, v1), d11 = lensq(v1), d20 = dot(v2, v0), d21 = dot(v2, v1);
+    float denom = d00 * d11 - d01 * d01;
+    coords.y = (d11 * d20 - d01 * d21) / denom;
+    coords.z = (d00 * d21 - d01 * d20) / denom;
+    coords.x = 1.f - coords.y - coords.z;
+    return v;
+}
+
+// Triangle and edge contacts against sphere / SDF / mesh colliders
+// (SDFCollisions edge + triangle parts, Physics/ClothCollision.cpp:472-579;
+// MeshCollisions triangle + edge parts, :137-196). One thread per cloth
+// triangle or edge per collider; results go to per-item slots.
+__global__ void k_tri_colliders(DevCloth c, SolverParams P, Buffers b, VColl g, int slotColl)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= c.T) return;
+    const uint32_t i1 = c.tri[3 * t], i2 = c.tri[3 * t + 1], i3 = c.tri[3 * t + 2];
+    const size_t slot = (size_t)slotColl * c.T + t;
+    b.tcFlag[slot] = 0;
+    V3 a = ld3(c.prev, i1), bb = ld3(c.prev, i2), cc = ld3(c.prev, i3);
+    float tv1 = len(ld3(c.prev, i1) - ld3(c.pos, i1));
+    float tv2 = len(ld3(c.prev, i2) - ld3(c.pos, i2));
+    float tv3 = len(ld3(c.prev, i3) - ld3(c.pos, i3));
+    float tvm = mx(tv1, mx(tv2, tv3));
+    TC rec;
+    rec.idx = make_uint4(i1, i2, i3, 0);
+    rec.lam = make_float2(0.f, 0.f);
+    if (g.type == 4)
+    {
+        // MeshCollisions: per-triangle threshold with 1.2 x travel (ClothCollision.cpp:137-160)
+        VtxHit h = mesh_triangle_query(b.meshes[g.mesh], a, bb, cc, c.status);
+        float rt = P.thickness + mx(P.tolerance, tvm * 1.2f);
+        if (h.dist < rt && h.dist >= 0)
+        {
+            rec.point = f4(h.cpMesh, 0.f); rec.normal = f4(h.normal, 0.f);
+            rec.w = make_float4(h.bary.x, h.bary.y, h.bary.z, 0.f);
+            rec.feature = h.vertex; rec.mesh = g.mesh;
+            b.tcSlot[slot] = rec; b.tcFlag[slot] = 1;
+        }
+        return;
+    }
+    const bool handleBorder = ((P.flags & CF_VERTICES) == 0) || ((P.flags & CF_EDGES) == 0);
+    const float eps = 0.001f;
+    V3 cp, n, coords;
+    float dist;
+    if (g.type == 7) dist = sdf_query_triangle(g, a, bb, cc, cp, n, coords);
+    else
+    {
+        V3 ctr = mk(g.a.x, g.a.y, g.a.z), pt;
+        closest_point_triangle(ctr, a, bb, cc, pt, coords);
+        V3 delta = pt - ctr;
+        float l = len(delta);
+        delta = (1.f / l) * delta;
+        n = delta;
+        cp = ctr + g.a.w * delta;
+        dist = l - g.a.w;
+    }
+    float radTol = P.thickness + mx(P.tolerance, tvm * 1.1f);
+    if (dist < radTol && dist >= 0 && ((coords.x > eps && coords.y > eps && coords.z > eps) || handleBorder))
+    {
+        rec.point = f4(cp, 0.f); rec.normal = f4(n, 0.f);
+        rec.w = make_float4(coords.x, coords.y, coords.z, 0.f);
+        rec.feature = -1; rec.mesh = -1;
+        b.tcSlot[slot] = rec; b.tcFlag[slot] = 1;
+    }
+}
+
+__global__ void k_edge_colliders(DevCloth c, SolverParams P, Buffers b, VColl g, int slotColl)
+{
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= c.E) return;
+    const int4 ed = c.edge[e];
+    const size_t slot = (size_t)slotColl * c.E + e;
+    b.ecFlag[slot] = 0;
+    V3 p = ld3(c.prev, ed.x), q = ld3(c.prev, ed.y);
+    EC rec;
+    rec.idx = make_uint4(ed.x, ed.y, 0, 0);
+    rec.lam = make_float2(0.f, 0.f);
+    if (g.type == 4)
+    {
+        const float radTol = P.thickness + mx(P.tolerance, c.scal[0] * 1.5f);
+        SegHit h = mesh_segment_query(b.meshes[g.mesh], p, q, c.status);
+        if (h.dist < radTol && h.dist >= 0)
+        {
+            rec.point = f4(h.cpMesh, 0.f); rec.normal = f4(h.normal, 0.f);
+            rec.w = make_float4(h.cs0, h.cs1, 0.f, 0.f);
+            rec.feature = h.edge; rec.mesh = g.mesh;
+            b.ecSlot[slot] = rec; b.ecFlag[slot] = 1;
+        }
+        return;
+    }
+    const bool handleBorder = (P.flags & CF_VERTICES) == 0;
+    const float eps = 0.02f;
+    float c0 = 0.f, c1 = 0.f, dist;
+    V3 cp = mk(0.f, 0.f, 0.f), n = mk(0.f, 0.f, 0.f);
+    if (g.type == 7) dist = 0.f; // GridSDF::QuerySegment is a stub returning 0
+    else
+    {
+        float t;
+        V3 ctr = mk(g.a.x, g.a.y, g.a.z);
+        V3 ps = closest_point_segment(ctr, p, q, t);
+        V3 delta = ps - ctr;
+        float l = len(delta);
+        delta = (1.f / l) * delta;
+        n = delta;
+        cp = ctr + g.a.w * delta;
+        c0 = 1.0f - t; c1 = t;
+        dist = l - g.a.w;
+    }
+    float tv1 = len(ld3(c.prev, ed.x) - ld3(c.pos, ed.x));
+    float tv2 = len(ld3(c.prev, ed.y) - ld3(c.pos, ed.y));
+    float radTol = P.thickness + mx(P.tolerance, mx(tv1, tv2) * 1.1f);
+    if (dist < radTol && dist >= 0 && ((c0 > eps && c0 < 1.f - eps && c1 > eps && c1 < 1.f - eps) || handleBorder))
+    {
+        rec.point = f4(cp, 0.f); rec.normal = f4(n, 0.f);
+        rec.w = make_float4(c0, c1, 0.f, 0.f);
+        rec.feature = -1; rec.mesh = -1;
+        b.ecSlot[slot] = rec; b.ecFlag[slot] = 1;
+    }
+}
+
+// --------------------------------------------------------- contact solves
+// ComputeTriangleNormal(mesh, tri, coords, false): vertex normals blended by the
+// barycentric coordinates (Geometry/ClosestPointOnMesh.cpp:37-60).
+__device__ __forceinline__ V3 blended_normal(const DevMesh& m, int t, V3 w)
+{
+    V3 n0 = ld3(m.n, m.tri[3 * t]), n1 = ld3(m.n, m.tri[3 * t + 1]), n2 = ld3(m.n, m.tri[3 * t + 2]);
+    return normalized(w.x * n0 + w.y * n1 + w.z * n2);
+}
+
+// SolveContactsPosition (Physics/ClothCollisionHandler.cpp:134-202): one thread
+// per particle processes that particle's contacts in list order (collider, slot),
+// which equals the reference's sequential order because every vertex contact
+// moves a single particle.
+__global__ void k_solve_vertex_contacts(DevCloth c, SolverParams P, Buffers b)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.N || gs_done(c)) return;
+    float err = 0.f;
+    float4 p4 = c.pos[i];
+    V3 p = mk(p4.x, p4.y, p4.z);
+    const V3 q = ld3(c.prev, i);
+    bool touched = false;
+    for (int ci = 0; ci < b.numVColl; ci++)
+    {
+        const VColl& g = b.vcoll[ci];
+        const int n = b.vcCount[(size_t)ci * c.N + i];
+        VC* slot = b.vc + g.slotBase + (size_t)i * g.kmax;
+        for (int k = 0; k < n; k++)
+        {
+            VC v = slot[k];
+            V3 point = mk(v.point.x, v.point.y, v.point.z), normal = mk(v.normal.x, v.normal.y, v.normal.z);
+            if (v.mesh >= 0)
+            {
+                const DevMesh& m = b.meshes[v.mesh];
+                int t = v.feature;
+                V3 coords, cp;
+                closest_point_triangle(p, ld3(m.v, m.tri[3 * t]), ld3(m.v, m.tri[3 * t + 1]), ld3(m.v, m.tri[3 * t + 2]), cp, coords);
+                point = cp;
+                normal = blended_normal(m, t, coords);
+                v.point = f4(point, 0.f); v.normal = f4(normal, 0.f);
+            }
+            V3 delta = p - point;
+            float l = dot(delta, normal);
+            V3 disp = normal;
+            if (l > P.thickness) { slot[k] = v; continue; }
+            float depth = P.thickness - l;
+            err = mx(err, fabsf(depth));
+            float dLambda = depth;
+            v.lam.x += dLambda;
+            disp = disp * dLambda;
+            V3 v12 = p - q - mk(0.f, 0.f, 0.f);
+            float vnrel = dot(normal, v12);
+            V3 vt = v12 - vnrel * normal;
+            float vtrel = len(vt);
+            const float limit = P.friction * v.lam.x;
+            if (vtrel > 0.001f)
+            {
+                float dLF = vtrel;
+                float l0 = v.lam.y;
+                v.lam.y = l0 + dLF;
+                if (v.lam.y >= limit) v.lam.y = limit;
+                dLF = v.lam.y - l0;
+                vt = vt * (1.0f / vtrel);
+                disp += -dLF * vt;
+            }
+            p += disp;
+            float4 vv = c.vel[i];
+            V3 nv = mk(vv.x, vv.y, vv.z) + P.invH * disp;
+            c.vel[i] = make_float4(nv.x, nv.y, nv.z, 0.f);
+            touched = true;
+            slot[k] = v;
+        }
+    }
+    if (touched) c.pos[i] = make_float4(p.x, p.y, p.z, p4.w);
+    if (!P.fixedIterations && err > 0.f) atomic_max_pos(&c.scal[3], err);
+}
+
+// SolveEdgeContacts for one contact (Physics/ClothCollisionHandler.cpp:289-362)
+__device__ float solve_edge_contact(const DevCloth& c, const SolverParams& P, const Buffers& b, EC& k)
+{
+    float4 a4 = c.pos[k.idx.x], b4 = c.pos[k.idx.y];
+    V3 x1 = mk(a4.x, a4.y, a4.z), x2 = mk(b4.x, b4.y, b4.z);
+    const float m1 = a4.w, m2 = b4.w;
+    float w1 = k.w.x, w2 = k.w.y;
+    V3 point = mk(k.point.x, k.point.y, k.point.z), normal = mk(k.normal.x, k.normal.y, k.normal.z);
+    V3 p = w1 * x1 + w2 * x2;
+    if (k.mesh >= 0)
+    {
+        const DevMesh& m = b.meshes[k.mesh];
+        int4 ed = m.edge[k.feature];
+        float s1, t;
+        closest_segm_segm(ld3(m.v, ed.x), ld3(m.v, ed.y), x1, x2, s1, t, point, p);
+        w1 = 1.0f - t; w2 = t;
+        k.point = f4(point, 0.f);
+    }
+    k.w.x = w1; k.w.y = w2;
+    const float len0 = P.thickness;
+    float l = dot(normal, p - point - mk(0.f, 0.f, 0.f));
+    if (l > len0) return -1.f;
+    float s = 1.f / (w1 * w1 / m1 + w2 * w2 / m2);
+    float depth = len0 - l;
+    float dLambda = s * depth;
+    k.lam.x += dLambda;
+    V3 disp = dLambda * normal;
+    if (P.friction != 0)
+    {
+        V3 p0 = w1 * ld3(c.prev, k.idx.x) + w2 * ld3(c.prev, k.idx.y);
+        V3 v12 = p - p0 - mk(0.f, 0.f, 0.f);
+        float vnrel = dot(normal, v12);
+        V3 vt = v12 - vnrel * normal;
+        float vtrel = len(vt);
+        const float limit = P.friction * k.lam.x;
+        if (vtrel > 0.001f)
+        {
+            float l0 = k.lam.y;
+            k.lam.y = l0 + vtrel;
+            if (k.lam.y >= limit) k.lam.y = limit;
+            dLambda = k.lam.y - l0;
+            vt = vt * (1.f / vtrel);
+            V3 pp = -s * dLambda * vt;
+            x1 += pp * (w1 * m1); x2 += pp * (w2 * m2);
+        }
+    }
+    x1 += disp * (w1 * m1); x2 += disp * (w2 * m2);
+    c.pos[k.idx.x] = make_float4(x1.x, x1.y, x1.z, m1);
+    c.pos[k.idx.y] = make_float4(x2.x, x2.y, x2.z, m2);
+    return depth;
+}
+
+// SolveTriContacts for one contact (Physics/ClothCollisionHandler.cpp:204-287)
+__device__ float solve_tri_contact(const DevCloth& c, const SolverParams& P, const Buffers& b, TC& k)
+{
+    float4 a4 = c.pos[k.idx.x], b4 = c.pos[k.idx.y], c4 = c.pos[k.idx.z];
+    V3 x1 = mk(a4.x, a4.y, a4.z), x2 = mk(b4.x, b4.y, b4.z), x3 = mk(c4.x, c4.y, c4.z);
+    const float m1 = a4.w, m2 = b4.w, m3 = c4.w;
+    V3 point = mk(k.point.x, k.point.y, k.point.z);
+    V3 coords, p;
+    closest_point_triangle(point, x1, x2, x3, p, coords);
+    const float w1 = coords.x, w2 = coords.y, w3 = coords.z;
+    k.w = make_float4(w1, w2, w3, 0.f);
+    V3 n = normalized(-cross(x2 - x1, x3 - x1));
+    V3 normal = n;
+    if (k.mesh >= 0 && k.feature >= 0)
+    {
+        V3 mnrm = ld3(b.meshes[k.mesh].n, k.feature);
+        if (dot(n, mnrm) < 0) normal = -n;
+    }
+    k.normal = f4(normal, 0.f);
+    const float len0 = P.thickness;
+    float l = dot(normal, p - point - mk(0.f, 0.f, 0.f));
+    if (l > len0) return -1.f;
+    float s = 1.f / (w1 * w1 / m1 + w2 * w2 / m2 + w3 * w3 / m3);
+    float depth = len0 - l;
+    float dLambda = s * depth;
+    k.lam.x += dLambda;
+    V3 disp = dLambda * normal;
+    if (P.friction != 0)
+    {
+        V3 p0 = w1 * ld3(c.prev, k.idx.x) + w2 * ld3(c.prev, k.idx.y) + w3 * ld3(c.prev, k.idx.z);
+        V3 v12 = p - p0 - mk(0.f, 0.f, 0.f);
+        float vnrel = dot(normal, v12);
+        V3 vt = v12 - vnrel * normal;
+        float vtrel = len(vt);
+        const float limit = P.friction * k.lam.x;
+        if (vtrel > 0.001f)
+        {
+            float l0 = k.lam.y;
+            k.lam.y = l0 + vtrel;
+            if (k.lam.y >= limit) k.lam.y = limit;
+            dLambda = k.lam.y - l0;
+            vt = vt * (1.f / vtrel);
+            V3 pp = -s * dLambda * vt;
+            x1 += pp * (w1 * m1); x2 += pp * (w2 * m2); x3 += pp * (w3 * m3);
+        }
+    }
+    x1 += disp * (w1 * m1); x2 += disp * (w2 * m2); x3 += disp * (w3 * m3);
+    c.pos[k.idx.x] = make_float4(x1.x, x1.y, x1.z, m1);
+    c.pos[k.idx.y] = make_float4(x2.x, x2.y, x2.z, m2);
+    c.pos[k.idx.z] = make_float4(x3.x, x3.y, x3.z, m3);
+    return depth;
+}
+
+// SolveSelfTrisPosition for one contact (Physics/ClothCollisionHandler.cpp:364-450)
+__device__ float solve_self_tri(const DevCloth& c, const SolverParams& P, SCt& k)
+{
+    const float soften = .9f;
+    float len0 = P.thickness * P.selfShrink;
+    float4 a4 = c.pos[k.idx.x], b4 = c.pos[k.idx.y], c4 = c.pos[k.idx.z], d4 = c.pos[k.idx.w];
+    V3 x1 = mk(a4.x, a4.y, a4.z), x2 = mk(b4.x, b4.y, b4.z), x3 = mk(c4.x, c4.y, c4.z), x4 = mk(d4.x, d4.y, d4.z);
+    const float m1 = a4.w, m2 = b4.w, m3 = c4.w, m4 = d4.w;
+    V3 p, coords;
+    closest_point_triangle(x4, x1, x2, x3, p, coords);
+    const float w1 = coords.x, w2 = coords.y, w3 = coords.z;
+    k.w.x = w1; k.w.y = w2; k.w.z = w3;
+    V3 delta = x4 - p;
+    V3 n = normalized(cross(x2 - x1, x3 - x1));
+    float side = signed_volume(x4, x1, x2, x3);
+    if (k.side * side <= 0) len0 = P.thickness * 0.1f;
+    if (dot(n, mk(k.normal.x, k.normal.y, k.normal.z)) < 0) n = -n;
+    float l = dot(n, delta);
+    if (l > len0) return -1.f;
+    float im = w1 * w1 * m1 + w2 * w2 * m2 + w3 * w3 * m3 + m4;
+    float s = 1.f / im;
+    float err = l - len0;
+    k.error = err;
+    float absErr = mx(0.f, -err);
+    float dLambda = soften * s * err;
+    V3 disp = dLambda * n;
+    k.lam.x += -dLambda / P.h;
+    x1 += disp * (w1 * m1);
+    x2 += disp * (w2 * m2);
+    x3 += disp * (w3 * m3);
+    x4 -= disp * m4;
+    c.pos[k.idx.x] = make_float4(x1.x, x1.y, x1.z, m1);
+    c.pos[k.idx.y] = make_float4(x2.x, x2.y, x2.z, m2);
+    c.pos[k.idx.z] = make_float4(x3.x, x3.y, x3.z, m3);
+    c.pos[k.idx.w] = make_float4(x4.x, x4.y, x4.z, m4);
+    return absErr;
+}
+
+// SolveSelfEdgesPosition for one contact (Physics/ClothCollisionHandler.cpp:453-542)
+__device__ float solve_self_edge(const DevCloth& c, const SolverParams& P, SCt& k)
+{
+    float thick = P.thickness * P.selfShrink;
+    const float soften = 0.9f;
+    float4 a4 = c.pos[k.idx.x], b4 = c.pos[k.idx.y], c4 = c.pos[k.idx.z], d4 = c.pos[k.idx.w];
+    V3 x1 = mk(a4.x, a4.y, a4.z), x2 = mk(b4.x, b4.y, b4.z), x3 = mk(c4.x, c4.y, c4.z), x4 = mk(d4.x, d4.y, d4.z);
+    const float m1 = a4.w, m2 = b4.w, m3 = c4.w, m4 = d4.w;
+    float side = signed_volume(x1, x2, x3, x4);
+    V3 p, q;
+    float t1, t2;
+    closest_segm_segm(x1, x2, x3, x4, t1, t2, p, q);
+    const float w1 = 1 - t1, w2 = 1 - t2;
+    k.w.x = w1; k.w.y = w2;
+    const float omw1 = 1.f - w1, omw2 = 1.f - w2;
+    V3 delta = q - p;
+    V3 n = normalized(delta);
+    if (dot(n, mk(k.normal.x, k.normal.y, k.normal.z)) < 0.0f) n = -n;
+    if (side * k.side < 0) thick = P.thickness * 0.1f;
+    float l = dot(n, delta);
+    if (l > thick) return -1.f;
+    float im = w1 * w1 * m1 + omw1 * omw1 * m2 + w2 * w2 * m3 + omw2 * omw2 * m4;
+    float s = 1.f / im;
+    float err = l - thick;
+    k.error = err;
+    float absErr = mx(0.f, -err);
+    float dLambda = -soften * s * err;
+    k.lam.x += dLambda / P.h;
+    V3 disp = dLambda * n;
+    x1 -= disp * (omw1 * m1);
+    x2 -= disp * (w1 * m2);
+    x3 += disp * (omw2 * m3);
+    x4 += disp * (w2 * m4);
+    c.pos[k.idx.x] = make_float4(x1.x, x1.y, x1.z, m1);
+    c.pos[k.idx.y] = make_float4(x2.x, x2.y, x2.z, m2);
+    c.pos[k.idx.z] = make_float4(x3.x, x3.y, x3.z, m3);
+    c.pos[k.idx.w] = make_float4(x4.x, x4.y, x4.z, m4);
+    return absErr;
+}
+
+// ------------------------------------------ colouring of multi-particle contacts
+// Deterministic independent-set colouring (Jones-Plassmann with hashed
+// priorities): in each round a contact whose key is the smallest among the
+// still-uncoloured contacts on every particle it touches takes the round's
+// colour. Contacts of one colour share no particle, so a colour is one
+// parallel sweep and the result equals the sequential sweep in
+// (colour, index) order, which is what the oracle's check mode runs.
+struct ClassView
+{
+    int kind;          // 0 edge, 1 tri, 2 self VT, 3 self EE
+    const int* count;
+    int* colour;
+    int* order;
+    int* start;        // MAX_COLOURS + 1
+};
+
+__device__ __forceinline__ int contact_verts(const Buffers& b, int kind, int i, uint32_t* v)
+{
+    if (kind == 0) { uint4 x = b.ecList[i].idx; v[0] = x.x; v[1] = x.y; return 2; }
+    if (kind == 1) { uint4 x = b.tcList[i].idx; v[0] = x.x; v[1] = x.y; v[2] = x.z; return 3; }
+    uint4 x = (kind == 2 ? b.stList[i].idx : b.seList[i].idx);
+    v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w; return 4;
+}
+
+__device__ void colour_class(const Buffers& b, const ClassView& cv, int* status)
+{
+    __shared__ int sHist[MAX_COLOURS + 1];
+    __shared__ int sCursor[MAX_COLOURS + 1];
+    __shared__ int sRemaining;
+    const int n = *cv.count;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) cv.colour[i] = -1;
+    if (threadIdx.x == 0) sRemaining = n;
+    __syncthreads();
+    int round = 0;
+    while (sRemaining > 0 && round < MAX_COLOURS - 1)
+    {
+        for (int i = threadIdx.x; i < n; i += blockDim.x)
+        {
+            if (cv.colour[i] >= 0) continue;
+            unsigned long long key = ((unsigned long long)mix32((uint32_t)i) << 32) | (uint32_t)i;
+            uint32_t v[4]; int nv = contact_verts(b, cv.kind, i, v);
+            for (int k = 0; k < nv; k++) atomicMin(&b.vmin[v[k]], key);
+        }
+        __syncthreads();
+        int mine = 0;
+        for (int i = threadIdx.x; i < n; i += blockDim.x)
+        {
+            if (cv.colour[i] >= 0) continue;
+            unsigned long long key = ((unsigned long long)mix32((uint32_t)i) << 32) | (uint32_t)i;
+            uint32_t v[4]; int nv = contact_verts(b, cv.kind, i, v);
+            bool ok = true;
+            for (int k = 0; k < nv; k++) ok = ok && (b.vmin[v[k]] == key);
+            if (ok) { cv.colour[i] = MAX_COLOURS + round; mine++; }   // tentative mark
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += blockDim.x)
+        {
+            int col = cv.colour[i];
+            if (col >= 0 && col != MAX_COLOURS + round) continue;
+            uint32_t v[4]; int nv = contact_verts(b, cv.kind, i, v);
+            for (int k = 0; k < nv; k++) b.vmin[v[k]] = ~0ull;
+            if (col == MAX_COLOURS + round) cv.colour[i] = round;
+        }
+        __shared__ int sCount;
+        if (threadIdx.x == 0) sCount = 0;
+        __syncthreads();
+        if (mine) atomicAdd(&sCount, mine);
+        __syncthreads();
+        if (threadIdx.x == 0) sRemaining -= sCount;
+        __syncthreads();
+        round++;
+    }
+    if (sRemaining > 0)
+    {
+        // not expected for contact graphs of bounded degree: the rest go to the
+        // last colour, which the solver runs on a single thread in list order
+        if (threadIdx.x == 0) atomicOr(status, ST_COLOUR_OVERFLOW);
+    }
+    // histogram + exclusive scan + placement
+    for (int k = threadIdx.x; k <= MAX_COLOURS; k += blockDim.x) sHist[k] = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+    {
+        int col = cv.colour[i];
+        if (col < 0) { col = MAX_COLOURS - 1; cv.colour[i] = col; }
+        atomicAdd(&sHist[col], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        int acc = 0;
+        for (int k = 0; k < MAX_COLOURS; k++) { cv.start[k] = acc; sCursor[k] = acc; acc += sHist[k]; }
+        cv.start[MAX_COLOURS] = acc;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+    {
+        int pos = atomicAdd(&sCursor[cv.colour[i]], 1);
+        cv.order[pos] = i;
+    }
+    __syncthreads();
+}
+
+struct ColourArgs { ClassView cls[4]; };
+
+__global__ void __launch_bounds__(1024) k_colour(DevCloth c, Buffers b, ColourArgs a)
+{
+    for (int k = 0; k < 4; k++) colour_class(b, a.cls[k], c.status);
+}
+
+// The multi-particle contact classes in the reference's order within one GS
+// iteration: edge, triangle, self vertex-triangle, self edge-edge
+// (Physics/ClothPBD.cpp:349-352). One CTA; one __syncthreads per colour.
+__global__ void __launch_bounds__(1024) k_solve_multi(DevCloth c, SolverParams P, Buffers b, ColourArgs a)
+{
+    if (gs_done(c)) return;
+    __shared__ float sErr[4];
+    if (threadIdx.x < 4) sErr[threadIdx.x] = 0.f;
+    __syncthreads();
+    for (int cls = 0; cls < 4; cls++)
+    {
+        const ClassView& cv = a.cls[cls];
+        const int n = *cv.count;
+        if (n == 0) continue;
+        for (int col = 0; col < MAX_COLOURS; col++)
+        {
+            const int s0 = cv.start[col], s1 = cv.start[col + 1];
+            if (s0 == s1) continue;
+            const bool serial = (col == MAX_COLOURS - 1);
+            for (int j = s0 + (serial ? 0 : threadIdx.x); j < s1; j += (serial ? 1 : blockDim.x))
+            {
+                if (serial && threadIdx.x != 0) break;
+                int i = cv.order[j];
+                float e;
+                if (cls == 0) { EC k = b.ecList[i]; e = solve_edge_contact(c, P, b, k); b.ecList[i] = k; }
+                else if (cls == 1) { TC k = b.tcList[i]; e = solve_tri_contact(c, P, b, k); b.tcList[i] = k; }
+                else if (cls == 2) { SCt k = b.stList[i]; e = solve_self_tri(c, P, k); b.stList[i] = k; }
+                else { SCt k = b.seList[i]; e = solve_self_edge(c, P, k); b.seList[i] = k; }
+                if (e > 0.f) atomicMax((int*)&sErr[cls], __float_as_int(e));
+            }
+            __syncthreads();
+        }
+    }
+    if (threadIdx.x == 0 && !P.fixedIterations)
+    {
+        c.scal[4] = sErr[0]; c.scal[5] = sErr[1]; c.scal[6] = sErr[2]; c.scal[7] = sErr[3];
+    }
+}
+
+// SolveGS exit test (Physics/ClothPBD.cpp:354-361); FEM mode has no link error.
+__global__ void k_gs_exit(DevCloth c, SolverParams P, int iter)
+{
+    if (gs_done(c)) return;
+    c.scal[9] = (float)(iter + 1);
+    if (P.fixedIterations) return;
+    const float eps = 0.01f;
+    float cb = c.scal[2], cv = c.scal[3], ce = c.scal[4], ct = c.scal[5], sct = c.scal[6], see = c.scal[7];
+    if (0.f < 0.05f && cb < 0.005f && see < P.selfThreshold && sct < P.selfThreshold && cv < eps && ce < eps && ct < eps)
+        c.scal[8] = 1.f;
+}
+
+__global__ void k_reset_iter_errors(DevCloth c)
+{
+    // cv is a per-iteration maximum written with atomics; cb persists between
+    // bend iterations (it is only recomputed when bends run)
+    if (threadIdx.x == 0) c.scal[3] = 0.f;
+}
+
+__global__ void k_reset_bend_error(DevCloth c)
+{
+    if (threadIdx.x == 0 && !gs_done(c)) c.scal[2] = 0.f;
+}
+
+// ----------------------------------------------------------------- scans
+constexpr int SCAN_T = 256, SCAN_ITEMS = 4, SCAN_TILE = SCAN_T * SCAN_ITEMS;
+
+__device__ __forceinline__ int block_exclusive_scan(int v, int* sWarp, int& total)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int x = v;
+    for (int o = 1; o < 32; o <<= 1) { int y = __shfl_up_sync(0xffffffffu, x, o); if (lane >= o) x += y; }
+    if (lane == 31) sWarp[warp] = x;
+    __syncthreads();
+    if (warp == 0)
+    {
+        int nw = blockDim.x >> 5;
+        int w = lane < nw ? sWarp[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) { int y = __shfl_up_sync(0xffffffffu, w, o); if (lane >= o) w += y; }
+        if (lane < nw) sWarp[lane] = w;
+    }
+    __syncthreads();
+    int warpPrefix = warp ? sWarp[warp - 1] : 0;
+    total = sWarp[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return warpPrefix + x - v;
+}
+
+__global__ void k_scan_reduce(const int* in, int n, int* blockSums)
+{
+    __shared__ int sWarp[32];
+    int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
+    int s = 0;
+    for (int k = 0; k < SCAN_ITEMS; k++) if (base + k < n) s += in[base + k];
+    int total;
+    block_exclusive_scan(s, sWarp, total);
+    if (threadIdx.x == 0) blockSums[blockIdx.x] = total;
+}
+
+__global__ void k_scan_top(int* blockSums, int nb, int* total)
+{
+    __shared__ int sWarp[32];
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < nb; base += blockDim.x)
+    {
+        int i = base + threadIdx.x;
+        int v = i < nb ? blockSums[i] : 0;
+        int t;
+        int ex = block_exclusive_scan(v, sWarp, t);
+        if (i < nb) blockSums[i] = ex + carry;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += t;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && total) *total = carry;
+}
+
+__global__ void k_scan_down(const int* in, int* out, int n, const int* blockSums)
+{
+    __shared__ int sWarp[32];
+    int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
+    int vals[SCAN_ITEMS];
+    int s = 0;
+    for (int k = 0; k < SCAN_ITEMS; k++) { vals[k] = (base + k < n) ? in[base + k] : 0; s += vals[k]; }
+    int total;
+    int ex = block_exclusive_scan(s, sWarp, total) + blockSums[blockIdx.x];
+    for (int k = 0; k < SCAN_ITEMS; k++) { if (base + k < n) out[base + k] = ex; ex += vals[k]; }
+}
+
+void scan_ints(cudaStream_t s, const int* in, int* out, int n, int* total, int* tmp)
+{
+    int nb = (n + SCAN_TILE - 1) / SCAN_TILE;
+    if (nb < 1) nb = 1;
+    k_scan_reduce<<<nb, SCAN_T, 0, s>>>(in, n, tmp);
+    k_scan_top<<<1, 1024, 0, s>>>(tmp, nb, total);
+    k_scan_down<<<nb, SCAN_T, 0, s>>>(in, out, n, tmp);
+}
+
+// gather items with count[i] records from slots[i*K + k] to dense[base + off[i] + k]
+template <typename R>
+__global__ void k_compact(const int* cnt, const int* off, const R* slots, int K, R* dense, int n, const int* base, int cap, int* status, int ovfBit)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int m = cnt[i];
+    if (m == 0) return;
+    int o = off[i] + (base ? *base : 0);
+    for (int k = 0; k < m; k++)
+    {
+        if (o + k < cap) dense[o + k] = slots[(size_t)i * K + k];
+        else atomicOr(status, ovfBit);
+    }
+}
+
+__global__ void k_add_counts(int* dst, const int* a, const int* b, int cap)
+{
+    if (threadIdx.x == 0) { int v = *a + (b ? *b : 0); *dst = v < cap ? v : cap; }
+}
+
+// ----------------------------------------------------------- LBVH refit
+// Leaf boxes: kind 0 = triangle over prev positions, 1 = edge over prev
+// positions, 2 = swept triangle (prev and pos, extruded by tol), 3 = swept edge.
+// The swept constructions are those of ClothModel::ComputeTree
+// (Physics/ClothCollision.cpp:256-321).
+__device__ __forceinline__ Box leaf_box(const DevCloth& c, int kind, int prim, float tol)
+{
+    Box b = Box::empty();
+    if (kind == 0 || kind == 2)
+    {
+        uint32_t i1 = c.tri[3 * prim], i2 = c.tri[3 * prim + 1], i3 = c.tri[3 * prim + 2];
+        b.add(ld3(c.prev, i1)); b.add(ld3(c.prev, i2)); b.add(ld3(c.prev, i3));
+        if (kind == 2) { b.add(ld3(c.pos, i1)); b.add(ld3(c.pos, i2)); b.add(ld3(c.pos, i3)); b.extrude(tol); }
+    }
+    else
+    {
+        int4 e = c.edge[prim];
+        if (kind == 1) { b.add(ld3(c.prev, e.x)); b.add(ld3(c.prev, e.y)); }
+        else { b.add(ld3(c.pos, e.x)); b.add(ld3(c.pos, e.y)); b.add(ld3(c.prev, e.x)); b.add(ld3(c.prev, e.y)); b.extrude(tol); }
+    }
+    return b;
+}
+
+// Bottom-up refit with one atomic per internal node: the second child to
+// arrive builds the parent's box and continues upwards (no waiting).
+__global__ void k_bvh_refit(DevBVH t, DevCloth c, int kind, float tol)
+{
+    int prim = blockIdx.x * blockDim.x + threadIdx.x;
+    if (prim >= t.numLeaves) return;
+    int node = t.leafNode[prim];
+    Box b = leaf_box(c, kind, prim, tol);
+    t.lo[node] = f4(b.lo, 0.f);
+    t.hi[node] = f4(b.hi, 0.f);
+    __threadfence();
+    int p = t.parent[node];
+    while (p >= 0)
+    {
+        if (atomicAdd(&t.visit[p], 1) == 0) return;
+        __threadfence();
+        int l = p + 1, r = t.child[p];
+        float4 al = __ldcg(&t.lo[l]), ar = __ldcg(&t.lo[r]), bl = __ldcg(&t.hi[l]), br = __ldcg(&t.hi[r]);
+        V3 lo = vmin(mk(al.x, al.y, al.z), mk(ar.x, ar.y, ar.z)), hi = vmax(mk(bl.x, bl.y, bl.z), mk(br.x, br.y, br.z));
+        t.lo[p] = f4(lo, 0.f);
+        t.hi[p] = f4(hi, 0.f);
+        __threadfence();
+        p = t.parent[p];
+    }
+}
+
+__device__ __forceinline__ bool node_overlap(const DevBVH& t, int node, const Box& q)
+{
+    float4 lo = t.lo[node], hi = t.hi[node];
+    return !(hi.x < q.lo.x || hi.y < q.lo.y || hi.z < q.lo.z || q.hi.x < lo.x || q.hi.y < lo.y || q.hi.z < lo.z);
+}
+
+// Stackless preorder traversal with escape indices; calls f(prim) for every
+// leaf whose box overlaps q (AabbOverlap3D on the leaf box itself).
+template <typename F>
+__device__ __forceinline__ void bvh_query(const DevBVH& t, const Box& q, F&& f)
+{
+    int node = 0;
+    while (node < t.numNodes)
+    {
+        if (node_overlap(t, node, q))
+        {
+            int ch = t.child[node];
+            if (ch < 0) { f(~ch); node = t.escape[node]; }
+            else node = node + 1;
+        }
+        else node = t.escape[node];
+    }
+}
+
+// ------------------------------------------------------ self proximity
+// Voronoi-region filters of the live self-collision query
+// (Geometry/VoronoiRegions.cpp:11-113) on the collision mesh (prev positions,
+// normals as of the last mesh update).
+__device__ bool in_vertex_vr(const DevCloth& c, V3 p, int vid)
+{
+    V3 v = ld3(c.prev, vid);
+    float side = 1;
+    if (dot(ld3(c.prevN, vid), p - v) < 0) side = -1;
+    const float eps = 0.1f;
+    for (int k = c.eRingStart[vid]; k < c.eRingStart[vid + 1]; k++)
+    {
+        int4 ed = c.edge[c.eRing[k]];
+        V3 e = normalized(ld3(c.prev, ed.x) - ld3(c.prev, ed.y));
+        if (ed.y != vid) e = -e;
+        float d = dot(e, p - v);
+        if (side > 0 && d < -eps) return false;
+        if (side < 0 && d > eps) return false;
+    }
+    return true;
+}
+
+__device__ bool in_triangle_vr(const DevCloth& c, V3 p, int t)
+{
+    V3 v1 = ld3(c.prev, c.tri[3 * t]), v2 = ld3(c.prev, c.tri[3 * t + 1]), v3 = ld3(c.prev, c.tri[3 * t + 2]);
+    V3 e1 = v2 - v1, e2 = v3 - v2, e3 = v1 - v3;
+    V3 n = ld3(c.prevTriN, t);
+    V3 h1 = cross(e1, n), h2 = cross(e2, n), h3 = cross(e3, n);
+    float d1 = dot(h1, p - v1), d2 = dot(h2, p - v2), d3 = dot(h3, p - v3);
+    bool s1 = signbit(d1), s2 = signbit(d2), s3 = signbit(d3);
+    return (s1 == s2) == s3;   // the reference's chained comparison
+}
+
+__device__ bool in_edge_vr(const DevCloth& c, V3 p, int eid)
+{
+    const float eps = 0.002f;
+    int4 ed = c.edge[eid];
+    V3 a = ld3(c.prev, ed.x), b = ld3(c.prev, ed.y);
+    V3 e = normalized(b - a);
+    float d3 = dot(e, p - a), d4 = dot(e, p - b);
+    if (d3 < 0 || d4 > 0) return false;
+    if (c.edgeSwapped[eid]) e = -e;
+    if (ed.w >= 0)
+    {
+        V3 h1 = normalized(cross(e, ld3(c.prevTriN, ed.z)));
+        V3 h2 = normalized(-cross(e, ld3(c.prevTriN, ed.w)));
+        float d1 = dot(h1, p - a), d2 = dot(h2, p - a);
+        if (d1 < -eps || d2 < -eps) return false;
+    }
+    else
+    {
+        V3 h1 = normalized(cross(e, ld3(c.prevTriN, ed.z)));
+        if (dot(h1, p - a) < -eps) return false;
+    }
+    return true;
+}
+
+__device__ bool adjacent(const DevCloth& c, int a, int b)
+{
+    for (int k = c.vRingStart[a]; k < c.vRingStart[a + 1]; k++) if (c.vRing[k] == b) return true;
+    return false;
+}
+
+// CheckAdjacency (Geometry/ClosestPointsBetweenMeshes.cpp:441-461)
+__device__ bool check_adjacency(const DevCloth& c, int vtx, int t, int region)
+{
+    int i1 = c.tri[3 * t], i2 = c.tri[3 * t + 1], i3 = c.tri[3 * t + 2];
+    if (i1 == vtx || i2 == vtx || i3 == vtx) return true;
+    if (region == TR_VERTEX_A && adjacent(c, vtx, i1)) return true;
+    if (region == TR_VERTEX_B && adjacent(c, vtx, i2)) return true;
+    if (region == TR_VERTEX_C && adjacent(c, vtx, i3)) return true;
+    if (region == TR_EDGE_AB && (adjacent(c, vtx, i1) && adjacent(c, vtx, i2))) return true;
+    if (region == TR_EDGE_BC && (adjacent(c, vtx, i2) && adjacent(c, vtx, i3))) return true;
+    if (region == TR_EDGE_AC && (adjacent(c, vtx, i1) && adjacent(c, vtx, i3))) return true;
+    return false;
+}
+
+// Self vertex-triangle proximity for one vertex: the triangles within radTol
+// come from the BVH (a superset: every triangle at distance <= radTol has a
+// box overlapping the query cube); they are then visited in increasing
+// triangle index, which is the brute-force loop order of
+// ClosestPointsOnMeshToPoint (Geometry/ClosestPointOnMesh.cpp:142-246), so the
+// Voronoi filters and the first-feature dedup decide exactly as there.
+__global__ void __launch_bounds__(128) k_self_vt(DevCloth c, SolverParams P, Buffers b, DevBVH tb)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.N) return;
+    const float radTol = P.thickness + mx(P.tolerance, c.scal[0] * 1.5f);
+    const V3 p = ld3(c.prev, i);
+    const float r = radTol * 1.0001f + 1e-6f;
+    Box q; q.lo = p - mk(r, r, r); q.hi = p + mk(r, r, r);
+    int cand[KCAND];
+    int nc = 0;
+    bool ovf = false;
+    bvh_query(tb, q, [&](int t) { if (nc < KCAND) cand[nc++] = t; else ovf = true; });
+    if (ovf) atomicOr(c.status, ST_SELF_VT_OVERFLOW);
+    for (int a = 1; a < nc; a++)   // insertion sort: small lists
+    {
+        int v = cand[a], j = a - 1;
+        while (j >= 0 && cand[j] > v) { cand[j + 1] = cand[j]; j--; }
+        cand[j + 1] = v;
+    }
+    const bool isBorder = c.vBorder[i] != 0;
+    int resType[KRES], resFeat[KRES];
+    int nres = 0, nout = 0;
+    SCt* out = b.stSlot + (size_t)i * KVT;
+    for (int a = 0; a < nc; a++)
+    {
+        const int t = cand[a];
+        const int i0 = c.tri[3 * t], i1 = c.tri[3 * t + 1], i2 = c.tri[3 * t + 2];
+        V3 va = ld3(c.prev, i0), vb = ld3(c.prev, i1), vc = ld3(c.prev, i2);
+        V3 coords, pt;
+        int region = closest_point_triangle(p, va, vb, vc, pt, coords);
+        V3 delta = p - pt;
+        float dist = len(delta);
+        if (dist > radTol) continue;
+        if (dist == 0) continue;
+        bool inVR = in_vertex_vr(c, pt, i);
+        int rtype = -1, feature = -1;
+        if (region == TR_FACE_INTERIOR)
+        {
+            if (!(inVR || in_triangle_vr(c, p, t))) continue;
+            rtype = 0;
+        }
+        if (region == TR_EDGE_AB || region == TR_EDGE_BC || region == TR_EDGE_AC)
+        {
+            int e = c.triE[3 * t + (region == TR_EDGE_AB ? 0 : (region == TR_EDGE_BC ? 1 : 2))];
+            if (!(c.edge[e].w < 0) && !(inVR || in_edge_vr(c, p, e))) continue;
+            rtype = 1; feature = e;
+        }
+        if (region == TR_VERTEX_A || region == TR_VERTEX_B || region == TR_VERTEX_C)
+        {
+            int vv = region == TR_VERTEX_A ? i0 : (region == TR_VERTEX_B ? i1 : i2);
+            if (!isBorder && !(inVR || in_vertex_vr(c, p, vv))) continue;
+            rtype = 2; feature = vv;
+        }
+        if (feature >= 0)
+        {
+            bool found = false;
+            for (int k = 0; k < nres; k++) if (resType[k] == rtype && resFeat[k] == feature) { found = true; break; }
+            if (found) continue;
+        }
+        if (nres < KRES) { resType[nres] = rtype; resFeat[nres] = feature; nres++; }
+        else { atomicOr(c.status, ST_SELF_VT_OVERFLOW); continue; }
+        // ClosestPoints(self) then MeshCollisions: drop adjacent features,
+        // keep 0 <= dist < radTol (ClosestPointsBetweenMeshes.cpp:553-563,
+        // ClothCollision.cpp:113-131)
+        if (check_adjacency(c, i, t, region)) continue;
+        if (!(dist < radTol && dist >= 0)) continue;
+        SCt rec;
+        rec.idx = make_uint4(i0, i1, i2, i);
+        V3 nrm = (1.f / dist) * delta;
+        rec.normal = f4(nrm, 0.f);
+        rec.side = signed_volume(p, va, vb, vc);
+        rec.w = make_float4(coords.x, coords.y, coords.z, 0.f);
+        rec.lam = make_float2(0.f, 0.f);
+        rec.error = 0.f;
+        if (nout < KVT) out[nout++] = rec;
+        else atomicOr(c.status, ST_SELF_VT_OVERFLOW);
+    }
+    b.stCnt[i] = nout;
+}
+
+__device__ __forceinline__ bool same_triangle(const DevCloth& c, int v, int t)
+{
+    if (t < 0) return false;
+    return v == (int)c.tri[3 * t] || v == (int)c.tri[3 * t + 1] || v == (int)c.tri[3 * t + 2];
+}
+
+// Self edge-edge proximity for one edge: nearest non-adjacent edge of higher
+// index (ties -> lower index, as the strict < of the reference loop), then
+// CheckEdgeAdjacency (Geometry/ClosestPointOnMesh.cpp:499-542,
+// ClosestPointsBetweenMeshes.cpp:474-536,568-591).
+__global__ void __launch_bounds__(128) k_self_ee(DevCloth c, SolverParams P, Buffers b, DevBVH eb)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.E) return;
+    b.seFlag[i] = 0;
+    const float radTol = P.thickness + mx(P.tolerance, c.scal[0] * 1.5f);
+    const int4 e1 = c.edge[i];
+    const V3 p = ld3(c.prev, e1.x), q = ld3(c.prev, e1.y);
+    const float r = radTol * 1.0001f + 1e-6f;
+    Box qb = Box::empty(); qb.add(p); qb.add(q);
+    qb.lo = qb.lo - mk(r, r, r); qb.hi = qb.hi + mk(r, r, r);
+    float best = FLT_MAX;
+    int bestE = -1;
+    bvh_query(eb, qb, [&](int e) {
+        if (e <= i) return;
+        int4 e2 = c.edge[e];
+        if (e2.x == e1.x || e2.x == e1.y || e2.y == e1.x || e2.y == e1.y) return;
+        float ps, pm; V3 cs, cm;
+        closest_segm_segm(p, q, ld3(c.prev, e2.x), ld3(c.prev, e2.y), ps, pm, cs, cm);
+        float dist = len(cs - cm);
+        if (dist != 0 && (dist < best || (dist == best && e < bestE))) { best = dist; bestE = e; }
+    });
+    if (bestE < 0) return;
+    const int4 e2 = c.edge[bestE];
+    const V3 a = ld3(c.prev, e2.x), bb = ld3(c.prev, e2.y);
+    float ps, pm; V3 cs, cm;
+    int region = closest_segm_segm(p, q, a, bb, ps, pm, cs, cm);
+    float dist = len(cs - cm);
+    const float cs0 = 1.0f - ps, cs1 = ps, cm0 = 1.0f - pm, cm1 = pm;
+    const float eps = 1e-5f;
+    if ((region & ER_VERTEX_P1) != 0 || cs0 < eps)
+        if (same_triangle(c, e1.x, e2.z) || same_triangle(c, e1.x, e2.w)) return;
+    if ((region & ER_VERTEX_Q1) != 0 || cs1 < eps)
+        if (same_triangle(c, e1.y, e2.z) || same_triangle(c, e1.y, e2.w)) return;
+    if ((region & ER_VERTEX_P2) != 0 || cm0 < eps)
+        if (same_triangle(c, e2.x, e1.z) || same_triangle(c, e2.x, e1.w)) return;
+    if ((region & ER_VERTEX_Q2) != 0 || cm1 < eps)
+        if (same_triangle(c, e2.y, e1.z) || same_triangle(c, e2.y, e1.w)) return;
+    if (!(dist < radTol && dist >= 0)) return;
+    SCt rec;
+    rec.idx = make_uint4(e1.x, e1.y, e2.x, e2.y);
+    V3 nrm = normalized(cm - cs);
+    rec.normal = f4(nrm, 0.f);
+    rec.side = signed_volume(p, q, a, bb);
+    rec.w = make_float4(cs1, cm1, 0.f, 0.f);
+    rec.lam = make_float2(0.f, 0.f);
+    rec.error = 0.f;
+    b.seSlot[i] = rec;
+    b.seFlag[i] = 1;
+}
+
+// ---------------------------------------------------- continuous collision
+// Broad phase: every (triangle, vertex) and (edge, edge) pair whose swept boxes
+// overlap, with the Midphase's filters (vertex not on the triangle and not
+// pinned; edges sharing no vertex), Physics/SelfCollisionDetector.cpp:60-135,
+// but over all pairs rather than same-leaf pairs only. Per-query candidate
+// lists are sorted so the pair list order is canonical: (vertex, triangle)
+// and (edge, higher edge).
+__global__ void __launch_bounds__(128) k_ccd_broad_vt(DevCloth c, SolverParams P, Buffers b, DevBVH tb, float tol)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.N) return;
+    b.ccdVtCnt[i] = 0;
+    float4 p4 = c.pos[i];
+    if (p4.w == 0.f) return;
+    Box vb = Box::empty(); vb.add(ld3(c.prev, i)); vb.add(mk(p4.x, p4.y, p4.z)); vb.extrude(tol);
+    int* out = b.ccdVtCand + (size_t)i * KCCD;
+    int n = 0;
+    bool ovf = false;
+    bvh_query(tb, vb, [&](int t) {
+        if ((int)c.tri[3 * t] == i || (int)c.tri[3 * t + 1] == i || (int)c.tri[3 * t + 2] == i) return;
+        if (n < KCCD) out[n++] = t; else ovf = true;
+    });
+    if (ovf) atomicOr(c.status, ST_CCD_OVERFLOW);
+    for (int a = 1; a < n; a++) { int v = out[a], j = a - 1; while (j >= 0 && out[j] > v) { out[j + 1] = out[j]; j--; } out[j + 1] = v; }
+    b.ccdVtCnt[i] = n;
+}
+
+__global__ void __launch_bounds__(128) k_ccd_broad_ee(DevCloth c, SolverParams P, Buffers b, DevBVH eb, float tol)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.E) return;
+    const int4 e1 = c.edge[i];
+    Box qb = Box::empty();
+    qb.add(ld3(c.pos, e1.x)); qb.add(ld3(c.pos, e1.y)); qb.add(ld3(c.prev, e1.x)); qb.add(ld3(c.prev, e1.y));
+    qb.extrude(tol);
+    int* out = b.ccdEeCand + (size_t)i * KCCD;
+    int n = 0;
+    bool ovf = false;
+    bvh_query(eb, qb, [&](int e) {
+        if (e <= i) return;
+        int4 e2 = c.edge[e];
+        if (e1.x == e2.x || e1.y == e2.y || e1.x == e2.y || e1.y == e2.x) return;
+        if (n < KCCD) out[n++] = e; else ovf = true;
+    });
+    if (ovf) atomicOr(c.status, ST_CCD_OVERFLOW);
+    for (int a = 1; a < n; a++) { int v = out[a], j = a - 1; while (j >= 0 && out[j] > v) { out[j + 1] = out[j]; j--; } out[j + 1] = v; }
+    b.ccdEeCnt[i] = n;
+}
+
+// expand per-query candidate lists into the dense pair list
+__global__ void k_ccd_pairs(const int* cnt, const int* off, const int* cand, int n, int2* pairs, int cap, int* status)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int m = cnt[i], o = off[i];
+    for (int k = 0; k < m; k++)
+    {
+        if (o + k < cap) pairs[o + k] = make_int2(i, cand[(size_t)i * KCCD + k]);
+        else atomicOr(status, ST_CCD_OVERFLOW);
+    }
+}
+
+// EvaluateFun_Coplanarity (Physics/SelfCollisionDetector.cpp:279-291)
+__device__ __forceinline__ float coplanarity(float t, V3 x1, V3 x2, V3 x3, V3 x4, V3 v1, V3 v2, V3 v3, V3 v4)
+{
+    V3 z1 = x1 + t * v1, z2 = x2 + t * v2, z3 = x3 + t * v3, z4 = x4 + t * v4;
+    V3 n1 = cross(z2 - z1, z3 - z1);
+    return dot(n1, z4 - z1);
+}
+
+// CheckInterval, at most 40 bisections (SelfCollisionDetector.cpp:440-489)
+__device__ bool check_interval(float ta, float tb, V3 x1, V3 x2, V3 x3, V3 x4, V3 v1, V3 v2, V3 v3, V3 v4, float& tx)
+{
+    float tx0 = ta, tx1 = tb;
+    float fx0 = coplanarity(tx0, x1, x2, x3, x4, v1, v2, v3, v4);
+    float fx1 = coplanarity(tx1, x1, x2, x3, x4, v1, v2, v3, v4);
+    if (fx0 * fx1 > 0) return false;
+    tx = tx0;
+    for (int l = 0; l < 40; l++)
+    {
+        float tmid = 0.5f * (tx0 + tx1);
+        float fmid = coplanarity(tmid, x1, x2, x3, x4, v1, v2, v3, v4);
+        if (fabsf(fmid) < 0.01f) { tx = tmid; break; }
+        if (fx0 * fmid < 0) { tx1 = tmid; fx1 = fmid; tx = tx0; }
+        else if (fmid * fx1 < 0) { tx0 = tmid; fx0 = fmid; tx = tmid; }
+        else return false;
+    }
+    return true;
+}
+
+// SolveCubic + FindInflexionPoints + CheckDegenerateCase (SelfCollisionDetector.cpp:293-438)
+__device__ bool solve_cubic(V3 x1, V3 x2, V3 x3, V3 x4, V3 v1, V3 v2, V3 v3, V3 v4, float& toi)
+{
+    float f0 = coplanarity(0.f, x1, x2, x3, x4, v1, v2, v3, v4);
+    if (fabsf(f0) < 0.001f) return false;
+    V3 v10 = v1 - v4, v20 = v2 - v4, v30 = v3 - v4;
+    V3 x10 = x1 - x4, x20 = x2 - x4, x30 = x3 - x4;
+    float a = triple(v10, v20, v30);
+    float b = triple(x10, v20, v30) + triple(v10, x20, v30) + triple(v10, v20, x30);
+    float cc = triple(x10, x20, v30) + triple(x10, v20, x30) + triple(v10, x20, x30);
+    if (fabsf(a) < 0.001f)
+    {
+        if (fabsf(b) < 0.001f) return false;
+        float d = triple(x10, x20, x30);
+        float discr = cc * cc - 4 * b * d;
+        if (discr < 0) return false;
+        if (discr == 0)
+        {
+            float t = -0.5f * cc / b;
+            if (t < 0 || t > 1) return false;
+            toi = t;
+            return true;
+        }
+        float ds = sqrtf(discr);
+        float t1 = 0.5f * (-cc - ds) / b, t2 = 0.5f * (-cc + ds) / b;
+        float t = mn(t1, t2);
+        if (t < 0 || t > 1) return false;
+        toi = t;
+        return true;
+    }
+    float discr = b * b - 3 * a * cc;
+    int num;
+    float ti1 = 0.f, ti2 = 0.f;
+    if (discr < 0) num = 0;
+    else if (discr == 0) { ti1 = ti2 = -b / (3 * a); num = 1; }
+    else
+    {
+        float ds = sqrtf(discr);
+        ti1 = (-b - ds) / (3 * a);
+        ti2 = (-b + ds) / (3 * a);
+        if (ti2 < ti1) { float tmp = ti1; ti1 = ti2; ti2 = tmp; }
+        num = 2;
+    }
+#define CI(ta, tb) check_interval((ta), (tb), x1, x2, x3, x4, v1, v2, v3, v4, toi)
+    bool coplanar = false;
+    if (num == 0) coplanar = CI(0.f, 1.f);
+    else if (num == 1)
+    {
+        if (ti1 < 0 || ti1 > 1) coplanar = CI(0.f, 1.f);
+        else coplanar = CI(0.f, ti1) || CI(ti1, 1.f);
+    }
+    else
+    {
+        if (ti1 > 1 || ti2 < 0 || (ti1 < 0 && ti2 > 1)) coplanar = CI(0.f, 1.f);
+        else if (ti1 < 0 && ti2 < 1) coplanar = CI(0.f, ti2) || CI(ti2, 1.f);
+        else if (ti1 < 1 && ti2 > 1) coplanar = CI(0.f, ti1) || CI(ti1, 1.f);
+        else if (ti1 > 0 && ti2 < 1) coplanar = CI(0.f, ti1) || CI(ti1, ti2) || CI(ti2, 1.f);
+    }
+#undef CI
+    return coplanar;
+}
+
+// VertexTriangleTest + VertexTriangleCCD (SelfCollisionDetector.cpp:171-277)
+__global__ void k_ccd_narrow_vt(DevCloth c, SolverParams P, Buffers b)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    int n = *b.ccdVtPairCount;
+    if (n > b.ccdVtCap) n = b.ccdVtCap;
+    if (k >= n) return;
+    b.ccdVtHit[k] = 0;
+    int2 pr = b.ccdVtPairs[k];
+    const int vtx = pr.x, t = pr.y;
+    const uint32_t i1 = c.tri[3 * t], i2 = c.tri[3 * t + 1], i3 = c.tri[3 * t + 2];
+    V3 x1 = ld3(c.prev, i1), x2 = ld3(c.prev, i2), x3 = ld3(c.prev, i3), x4 = ld3(c.prev, vtx);
+    V3 v1 = ld3(c.pos, i1) - x1, v2 = ld3(c.pos, i2) - x2, v3 = ld3(c.pos, i3) - x3, v4 = ld3(c.pos, vtx) - x4;
+    float toi;
+    if (!solve_cubic(x1, x2, x3, x4, v1, v2, v3, v4, toi)) return;
+    V3 z1 = x1 + toi * v1, z2 = x2 + toi * v2, z3 = x3 + toi * v3, z4 = x4 + toi * v4;
+    V3 coords, p;
+    closest_point_triangle(z4, z1, z2, z3, p, coords);
+    V3 delta = z4 - p;
+    const float eps = 0.1f;
+    if (!(lensq(delta) < eps * eps)) return;
+    V3 triNormal = normalized(cross(x2 - x1, x3 - x1));
+    float side = dot(triNormal, x4 - x1);
+    V3 nn = normalized(cross(z2 - z1, z3 - z1));
+    if (side < 0) nn = -nn;
+    SCt rec;
+    rec.idx = make_uint4(i1, i2, i3, vtx);
+    rec.normal = f4(nn, 0.f);
+    rec.w = make_float4(coords.x, coords.y, coords.z, 0.f);
+    rec.side = signed_volume(x4, x1, x2, x3);
+    rec.lam = make_float2(0.f, 0.f);
+    rec.error = 0.f;
+    b.ccdVtRec[k] = rec;
+    b.ccdVtHit[k] = 1;
+}
+
+// EdgeEdgeTest + EdgeEdgeCCD (SelfCollisionDetector.cpp:491-606)
+__global__ void k_ccd_narrow_ee(DevCloth c, SolverParams P, Buffers b)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    int n = *b.ccdEePairCount;
+    if (n > b.ccdEeCap) n = b.ccdEeCap;
+    if (k >= n) return;
+    b.ccdEeHit[k] = 0;
+    int2 pr = b.ccdEePairs[k];
+    const int4 A = c.edge[pr.x], B = c.edge[pr.y];
+    const int i1 = A.x, i2 = A.y, j1 = B.x, j2 = B.y;
+    if (i1 == j1 || i1 == j2 || i2 == j1 || i2 == j2) return;
+    V3 x1 = ld3(c.prev, i1), x2 = ld3(c.prev, i2), x3 = ld3(c.prev, j1), x4 = ld3(c.prev, j2);
+    V3 v1 = ld3(c.pos, i1) - x1, v2 = ld3(c.pos, i2) - x2, v3 = ld3(c.pos, j1) - x3, v4 = ld3(c.pos, j2) - x4;
+    float toi;
+    if (!solve_cubic(x1, x2, x3, x4, v1, v2, v3, v4, toi)) return;
+    V3 z1 = x1 + toi * v1, z2 = x2 + toi * v2, z3 = x3 + toi * v3, z4 = x4 + toi * v4;
+    V3 c1, c2;
+    float s, t;
+    closest_segm_segm(z1, z2, z3, z4, s, t, c1, c2);
+    float dSqr = lensq(c1 - c2);
+    const float eps = 0.5f * P.thickness;
+    if (!(dSqr <= eps * eps)) return;
+    float s2, t2; V3 d1, d2;
+    closest_segm_segm(x1, x2, x3, x4, s2, t2, d1, d2);
+    SCt rec;
+    rec.idx = make_uint4(i1, i2, j1, j2);
+    rec.normal = f4(normalized(d2 - d1), 0.f);
+    rec.w = make_float4(s, t, 0.f, 0.f);
+    rec.side = signed_volume(x1, x2, x3, x4);
+    rec.lam = make_float2(0.f, 0.f);
+    rec.error = 0.f;
+    b.ccdEeRec[k] = rec;
+    b.ccdEeHit[k] = 1;
+}
+
+// ------------------------------------------------------------- launchers
+void launch_predict(cudaStream_t s, const DevCloth& c, const SolverParams& P)
+{
+    cudaMemsetAsync(c.scal, 0, sizeof(float), s);
+    k_predict<<<blocks_for(c.N), 256, 0, s>>>(c, P);
+}
+
+void launch_velocity(cudaStream_t s, const DevCloth& c, const SolverParams& P)
+{
+    k_velocity<<<blocks_for(c.N), 256, 0, s>>>(c, P);
+}
+
+void launch_fem(cudaStream_t s, const DevCloth& c, const SolverParams& P, int first, int count)
+{
+    if (count > 0) k_fem<<<blocks_for(count), 256, 0, s>>>(c, P, first, count);
+}
+
+void launch_bends(cudaStream_t s, const DevCloth& c, const SolverParams& P, int first, int count, int resetErr)
+{
+    if (resetErr) k_reset_bend_error<<<1, 32, 0, s>>>(c);
+    if (count > 0) k_bends<<<blocks_for(count), 256, 0, s>>>(c, P, first, count);
+}
+
+void launch_normals(cudaStream_t s, const DevCloth& c, bool prevMesh, const float4* verts)
+{
+    float4* triN = prevMesh ? c.prevTriN : c.meshTriN;
+    float4* vn = prevMesh ? c.prevN : c.meshN;
+    k_tri_normals<<<blocks_for(c.T), 256, 0, s>>>(verts, c.tri, c.T, triN, c.triAngles);
+    k_vertex_normals<<<blocks_for(c.N), 256, 0, s>>>(c.N, c.vTriStart, c.vTri, triN, c.triAngles, vn);
+}
+
+void launch_vertex_colliders(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b, const VColl*)
+{
+    if (b.numVColl > 0) k_vertex_colliders<<<blocks_for(c.N, 128), 128, 0, s>>>(c, P, b);
+}
+
+void launch_tri_edge_colliders(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b,
+                               const VColl* hostColl, int numColl, int flags)
+{
+    // per-collider triangle / edge slots: collider slot index = order among
+    // colliders that produce such contacts (world order)
+    int ti = 0, ei = 0;
+    for (int k = 0; k < numColl; k++)
+    {
+        const VColl& g = hostColl[k];
+        if (g.type != 3 && g.type != 4 && g.type != 7) continue;
+        if (flags & CF_EDGES) { k_edge_colliders<<<blocks_for(c.E, 128), 128, 0, s>>>(c, P, b, g, ei); ei++; }
+        if (flags & CF_TRIANGLES) { k_tri_colliders<<<blocks_for(c.T, 128), 128, 0, s>>>(c, P, b, g, ti); ti++; }
+    }
+    // compaction in (collider, item) order
+    if (ti > 0)
+    {
+        int n = ti * c.T;
+        scan_ints(s, b.tcFlag, b.scanOff, n, b.tcCount, b.scanBlock);
+        k_compact<TC><<<blocks_for(n), 256, 0, s>>>(b.tcFlag, b.scanOff, b.tcSlot, 1, b.tcList, n, nullptr, b.tcCap, c.status, ST_CONTACT_OVERFLOW);
+        k_add_counts<<<1, 32, 0, s>>>(b.tcCount, b.tcCount, nullptr, b.tcCap);
+    }
+    else cudaMemsetAsync(b.tcCount, 0, sizeof(int), s);
+    if (ei > 0)
+    {
+        int n = ei * c.E;
+        scan_ints(s, b.ecFlag, b.scanOff, n, b.ecCount, b.scanBlock);
+        k_compact<EC><<<blocks_for(n), 256, 0, s>>>(b.ecFlag, b.scanOff, b.ecSlot, 1, b.ecList, n, nullptr, b.ecCap, c.status, ST_CONTACT_OVERFLOW);
+        k_add_counts<<<1, 32, 0, s>>>(b.ecCount, b.ecCount, nullptr, b.ecCap);
+    }
+    else cudaMemsetAsync(b.ecCount, 0, sizeof(int), s);
+}
+
+void launch_solve_vertex_contacts(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b)
+{
+    k_reset_iter_errors<<<1, 32, 0, s>>>(c);
+    if (b.numVColl > 0) k_solve_vertex_contacts<<<blocks_for(c.N, 128), 128, 0, s>>>(c, P, b);
+}
+
+static ColourArgs colour_args(const Buffers& b)
+{
+    ColourArgs a;
+    a.cls[0] = {0, b.ecCount, b.colour, b.order, b.colourStart};
+    a.cls[1] = {1, b.tcCount, b.colour + b.ecCap, b.order + b.ecCap, b.colourStart + (MAX_COLOURS + 1)};
+    a.cls[2] = {2, b.stCount, b.colour + b.ecCap + b.tcCap, b.order + b.ecCap + b.tcCap, b.colourStart + 2 * (MAX_COLOURS + 1)};
+    a.cls[3] = {3, b.seCount, b.colour + b.ecCap + b.tcCap + b.stCap, b.order + b.ecCap + b.tcCap + b.stCap,
+                b.colourStart + 3 * (MAX_COLOURS + 1)};
+    return a;
+}
+
+void launch_colour_contacts(cudaStream_t s, const DevCloth& c, const Buffers& b)
+{
+    k_colour<<<1, 1024, 0, s>>>(c, b, colour_args(b));
+}
+
+void launch_solve_multi_contacts(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b, int iter)
+{
+    k_solve_multi<<<1, 1024, 0, s>>>(c, P, b, colour_args(b));
+    k_gs_exit<<<1, 32, 0, s>>>(c, P, iter);
+}
+
+void launch_bvh_refit(cudaStream_t s, const DevBVH& t, const DevCloth& c, int kind, float tol)
+{
+    cudaMemsetAsync(t.visit, 0, sizeof(int) * t.numNodes, s);
+    k_bvh_refit<<<blocks_for(t.numLeaves), 256, 0, s>>>(t, c, kind, tol);
+}
+
+void launch_self_proximity(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b,
+                           const DevBVH& triBvh, const DevBVH& edgeBvh)
+{
+    k_self_vt<<<blocks_for(c.N, 128), 128, 0, s>>>(c, P, b, triBvh);
+    k_self_ee<<<blocks_for(c.E, 128), 128, 0, s>>>(c, P, b, edgeBvh);
+}
+
+void launch_compact_self(cudaStream_t s, const DevCloth& c, const Buffers& b, bool ccd)
+{
+    int* off = b.scanOff;
+    scan_ints(s, b.stCnt, off, c.N, b.stCount, b.scanBlock);
+    k_compact<SCt><<<blocks_for(c.N), 256, 0, s>>>(b.stCnt, off, b.stSlot, KVT, b.stList, c.N, nullptr, b.stCap, c.status, ST_SELF_VT_OVERFLOW);
+    scan_ints(s, b.seFlag, off, c.E, b.seCount, b.scanBlock);
+    k_compact<SCt><<<blocks_for(c.E), 256, 0, s>>>(b.seFlag, off, b.seSlot, 1, b.seList, c.E, nullptr, b.seCap, c.status, ST_SELF_EE_OVERFLOW);
+    if (ccd)
+    {
+        // continuous hits go after the proximity contacts, as the detector's
+        // AddSelfTriangle / AddSelfEdge would append them
+        int* tot = b.scanTot;
+        int nvt = b.ccdVtCap, nee = b.ccdEeCap;
+        scan_ints(s, b.ccdVtHit, off, nvt, tot, b.scanBlock);
+        k_compact<SCt><<<blocks_for(nvt), 256, 0, s>>>(b.ccdVtHit, off, b.ccdVtRec, 1, b.stList, nvt, b.stCount, b.stCap, c.status, ST_CCD_OVERFLOW);
+        k_add_counts<<<1, 32, 0, s>>>(b.stCount, b.stCount, tot, b.stCap);
+        scan_ints(s, b.ccdEeHit, off, nee, tot, b.scanBlock);
+        k_compact<SCt><<<blocks_for(nee), 256, 0, s>>>(b.ccdEeHit, off, b.ccdEeRec, 1, b.seList, nee, b.seCount, b.seCap, c.status, ST_CCD_OVERFLOW);
+        k_add_counts<<<1, 32, 0, s>>>(b.seCount, b.seCount, tot, b.seCap);
+    }
+    k_add_counts<<<1, 32, 0, s>>>(b.stCount, b.stCount, nullptr, b.stCap);
+    k_add_counts<<<1, 32, 0, s>>>(b.seCount, b.seCount, nullptr, b.seCap);
+}
+
+void launch_ccd(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b,
+                const DevBVH& triBvh, const DevBVH& edgeBvh)
+{
+    const float tol = P.thickness + P.tolerance * 0.5f;
+    k_ccd_broad_vt<<<blocks_for(c.N, 128), 128, 0, s>>>(c, P, b, triBvh, tol);
+    k_ccd_broad_ee<<<blocks_for(c.E, 128), 128, 0, s>>>(c, P, b, edgeBvh, tol);
+    int* off = b.scanOff;
+    scan_ints(s, b.ccdVtCnt, off, c.N, b.ccdVtPairCount, b.scanBlock);
+    k_ccd_pairs<<<blocks_for(c.N), 256, 0, s>>>(b.ccdVtCnt, off, b.ccdVtCand, c.N, b.ccdVtPairs, b.ccdVtCap, c.status);
+    scan_ints(s, b.ccdEeCnt, off, c.E, b.ccdEePairCount, b.scanBlock);
+    k_ccd_pairs<<<blocks_for(c.E), 256, 0, s>>>(b.ccdEeCnt, off, b.ccdEeCand, c.E, b.ccdEePairs, b.ccdEeCap, c.status);
+    cudaMemsetAsync(b.ccdVtHit, 0, sizeof(int) * b.ccdVtCap, s);
+    cudaMemsetAsync(b.ccdEeHit, 0, sizeof(int) * b.ccdEeCap, s);
+    k_ccd_narrow_vt<<<blocks_for(b.ccdVtCap), 256, 0, s>>>(c, P, b);
+    k_ccd_narrow_ee<<<blocks_for(b.ccdEeCap), 256, 0, s>>>(c, P, b);
+}
+
+void launch_reset_gs(cudaStream_t s, const DevCloth& c)
+{
+    cudaMemsetAsync(c.scal + 1, 0, sizeof(float) * 9, s);
+}
+
+void launch_gs_exit_test(cudaStream_t s, const DevCloth& c, const SolverParams& P, int iter)
+{
+    k_gs_exit<<<1, 32, 0, s>>>(c, P, iter);
+}
+
+} // namespace sc

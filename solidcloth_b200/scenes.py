@@ -232,6 +232,13 @@ def cfg2(seed: int = 2, n: int = 256, level: int = 5) -> Scene:
     p = Params(thickness=0.005, tolerance=0.005, friction=0.3, iterations=20, substeps=8,
                flags=CF_VERTICES | CF_TRIANGLES | CF_EDGES | CF_SELF | CF_WALLS)
     s = make_grid_scene(f"cfg2_{n}x{n}_icosphere_mesh_self", n, 1.5, 0.5 + 0.5, p, seed=seed, frames=300)
+    # Unit masses (inverse mass 1, the reference's own default after Init): the
+    # reference's triangle and edge contact solves divide by the inverse mass
+    # (SolveTriContacts / SolveEdgeContacts, Physics/ClothCollisionHandler.cpp:302,381),
+    # which is only consistent when inverse masses are 1; with ~1 g lumped masses
+    # they move vertices by kilometres. FEM, bends and the other contacts are
+    # invariant to a uniform mass scale.
+    s.masses = np.ones(n * n, dtype=np.float32)
     s.walls = np.array([-20.0, 0.0, -20.0, 20.0, 20.0, 20.0], dtype=np.float32)
     s.meshes.append(icosphere(level, 0.25, (0.0, 0.25, 0.0)))
     return s
@@ -256,3 +263,40 @@ def cfg3_instances(count: int = 512, seed: int = 3, lo: int = 16, hi: int = 128)
 
 
 CONFIGS = {"cfg0": cfg0, "cfg1": cfg1, "cfg2": cfg2}
+
+
+def folded(scene: Scene, gap: float = 0.004, drop_speed: float = 0.0):
+    """A cloth folded in half along its middle row: rows past the middle are
+    mirrored onto the first half, `gap` above it, optionally moving down at
+    `drop_speed` m/s. Returns (pos, prev, vel) float32 arrays (prev == pos)."""
+    n = scene.n
+    pos = scene.positions.copy().reshape(n, n, 3)  # [j (x), i (z), xyz]
+    mid = (n - 1) / 2.0
+    i = np.arange(n)
+    z0 = pos[:, 0, 2].copy()
+    inc = np.float32(scene.inc)
+    top = i > mid
+    zmir = z0[:, None] + (2 * mid - i[None, :]) * inc
+    pos[:, top, 2] = zmir[:, top]
+    pos[:, top, 1] = pos[:, top, 1] + np.float32(gap)
+    pos = pos.reshape(-1, 3).astype(np.float32)
+    vel = np.zeros_like(pos)
+    if drop_speed:
+        vel.reshape(n, n, 3)[:, top, 1] = -drop_speed
+    return pos, pos.copy(), vel.astype(np.float32)
+
+
+def ccd_scene(n: int = 16, seed: int = 5):
+    """Continuous-collision test case in the reference demo's unit scale (the
+    reference's CCD cut-offs are absolute: |f(0)| < 1e-3 and a 0.1 proximity,
+    Physics/SelfCollisionDetector.cpp:257,300, so they only act at that scale):
+    a folded 30-unit cloth whose upper layer falls through the lower one with a
+    deforming (non-rigid) motion. Returns (scene, (pos, prev, vel))."""
+    p = Params(unit=10, thickness=0.5, tolerance=0.4, iterations=2, substeps=1,
+               flags=CF_VERTICES | CF_SELF)
+    sc = make_grid_scene(f"ccd_fold_{n}", n, 30.0, 0.0, p, seed=seed)
+    pos, prev, vel = folded(sc, gap=0.3, drop_speed=40.0)
+    rng = np.random.default_rng(seed + 2)
+    vel = (vel + rng.uniform(-20.0, 20.0, vel.shape)).astype(np.float32)
+    sc.ccd = True
+    return sc, (pos, prev, vel)

@@ -1,0 +1,120 @@
+"""Generate the golden fixtures in this directory from the SolidCloth reference
+itself (oracle/_ref, built from the reference's own C++ sources, single thread).
+
+    python tests/golden/make_golden.py
+
+The fixtures pin the CPU oracle (oracle/cloth_oracle.cpp) on machines where the
+reference build is absent: tests/test_oracle.py replays each case through the
+oracle and requires bit-identical results.
+"""
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE.parent.parent))
+
+from oracle.bridge import RefCloth  # noqa: E402
+from solidcloth_b200 import scenes  # noqa: E402
+
+
+def case_cfg0():
+    sc = scenes.cfg0()
+    r = RefCloth.from_scene(sc)
+    out = {}
+    for f in range(10):
+        r.step(sc.dt)
+        r.update_mesh()
+    pos, prev, vel, w = r.state()
+    idx, rest = r.tris()
+    return dict(pos=pos, prev=prev, vel=vel, invmass=w, tris=idx, rest=rest, bends=r.bends(), edges=r.edges(),
+                normals=r.mesh_normals(False), prev_normals=r.mesh_normals(True))
+
+
+def sdf_scene():
+    sc = scenes.cfg1(n=20)
+    sc.params.substeps = 2
+    sc.params.iterations = 6
+    sc.positions[:, 1] -= np.float32(0.4 - 0.004)
+    return sc
+
+
+def case_sdf():
+    sc = sdf_scene()
+    r = RefCloth.from_scene(sc)
+    for f in range(3):
+        r.step(sc.dt)
+        r.update_mesh()
+    vi, vf = r.contacts(0)
+    pos, prev, vel, _ = r.state()
+    return dict(pos=pos, prev=prev, vel=vel, vc_idx=vi, vc_f=vf)
+
+
+def folded_scene():
+    sc = scenes.cfg1(n=16)
+    sc.sdfs.clear()
+    sc.params.substeps = 1
+    sc.params.iterations = 4
+    return sc, scenes.folded(sc, gap=0.004)
+
+
+def case_self():
+    sc, st = folded_scene()
+    r = RefCloth.from_scene(sc)
+    r.set_state(*st)
+    r.step(sc.dt)
+    ti, tf = r.contacts(3)
+    ei, ef = r.contacts(4)
+    pos, prev, vel, _ = r.state()
+    return dict(pos=pos, vt_idx=ti, vt_f=tf, ee_idx=ei, ee_f=ef)
+
+
+def case_ccd():
+    sc, st = scenes.ccd_scene(16)
+    r = RefCloth.from_scene(sc)
+    r.set_state(*st)
+    r.predict_detect(sc.dt / sc.params.substeps, ccd=False)
+    mid_vt, mid_ee = r.ccd_midphase()
+    boxes_t = r.swept_boxes(0, sc.params.thickness + 0.5 * sc.params.tolerance)
+    r2 = RefCloth.from_scene(sc)
+    r2.set_state(*st)
+    r2.predict_detect(sc.dt / sc.params.substeps, ccd=False)
+    # narrow phase over the midphase candidates (the reference's own pair set)
+    r2.ccd_narrow_on(mid_vt, mid_ee)
+    hi, hf = r2.contacts(3)
+    ei, ef = r2.contacts(4)
+    return dict(mid_vt=mid_vt, mid_ee=mid_ee, boxes_t=boxes_t, hit_vt_idx=hi, hit_vt_f=hf, hit_ee_idx=ei, hit_ee_f=ef)
+
+
+def mesh_scene():
+    sc = scenes.cfg2(n=21, level=3)
+    sc.params.substeps = 2
+    sc.params.iterations = 4
+    sc.positions[:, 1] -= np.float32(0.52)
+    return sc
+
+
+def case_mesh():
+    sc = mesh_scene()
+    r = RefCloth.from_scene(sc)
+    for f in range(2):
+        r.step(sc.dt)
+        r.update_mesh()
+    pos, prev, vel, _ = r.state()
+    out = dict(pos=pos, prev=prev, vel=vel)
+    for k, name in [(0, "vc"), (1, "tc"), (2, "ec")]:
+        a, b = r.contacts(k)
+        out[name + "_idx"], out[name + "_f"] = a, b
+    return out
+
+
+CASES = {"cfg0": case_cfg0, "sdf": case_sdf, "self": case_self, "ccd": case_ccd, "mesh": case_mesh}
+
+
+if __name__ == "__main__":
+    RefCloth.set_threads(1)
+    for name, fn in CASES.items():
+        d = fn()
+        np.savez_compressed(HERE / f"{name}.npz", **d)
+        print(name, {k: v.shape for k, v in d.items()})

@@ -1,0 +1,181 @@
+"""GPU step vs the CPU oracle (the checker), through the C ABI.
+
+Check mode: the oracle runs the reference's sequential Gauss-Seidel sweep in the
+order the coloured GPU sweep realises (constraint colour order from
+scGetConstraintOrder, contacts in the deterministic independent-set colouring),
+so the two agree to FP32 rounding of acosf (CUDA vs glibc) only.
+"""
+import numpy as np
+import pytest
+
+from solidcloth_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5          # metres; per-constraint parity bound of the spec, applied to positions
+
+
+def _pair(sc, ccd=False, state=None):
+    from solidcloth_b200 import api
+    from oracle.bridge import PortCloth
+    w, p = api.load_scene(sc, ccd=ccd)
+    o = PortCloth.from_scene(sc)
+    o._fn("set_ccd")(o.h, int(ccd))
+    if state is not None:
+        p.model.set_state(*state)
+        o.set_state(*state)
+    o.set_tri_order(p.model.constraint_order(0)[0])
+    o.set_bend_order(p.model.constraint_order(1)[0])
+    o.set_contact_order(1)
+    return w, p, o
+
+
+def test_fem_only_bitexact():
+    """FEM projections contain no transcendental: the coloured GPU sweep and the
+    oracle's sequential sweep in the same order agree bit for bit."""
+    sc = scenes.cfg0()
+    sc.params.dihedral = False
+    w, p, o = _pair(sc)
+    for _ in range(5):
+        p.step(sc.dt)
+        o.step(sc.dt)
+    g, c = p.model.positions(), o.positions()
+    assert np.array_equal(g.view(np.uint32), c.view(np.uint32)), float(np.abs(g - c).max())
+    assert p.status() == 0
+
+
+def test_cfg0_check_mode():
+    sc = scenes.cfg0()
+    w, p, o = _pair(sc)
+    worst = 0.0
+    for f in range(20):
+        p.step(sc.dt)
+        o.step(sc.dt)
+        worst = max(worst, float(np.abs(p.model.positions() - o.positions()).max()))
+    assert worst <= TOL, worst
+    assert np.allclose(p.model.velocities(), o.state()[2], atol=1e-3)
+
+
+def test_colouring_is_valid():
+    sc = scenes.cfg0()
+    from solidcloth_b200 import api
+    w, p = api.load_scene(sc)
+    tris = p.model.tris()
+    order, start = p.model.constraint_order(0)
+    assert sorted(order.tolist()) == list(range(len(tris)))
+    for c in range(len(start) - 1):
+        ids = tris[order[start[c]:start[c + 1]]].reshape(-1)
+        assert len(np.unique(ids)) == ids.size, "two triangles of one colour share a particle"
+    bends = p.model.bends()
+    order, start = p.model.constraint_order(1)
+    for c in range(len(start) - 1):
+        ids = bends[order[start[c]:start[c + 1]]].reshape(-1)
+        assert len(np.unique(ids)) == ids.size
+
+
+def test_topology_matches_oracle():
+    from solidcloth_b200 import api
+    from oracle.bridge import PortCloth
+    sc = scenes.cfg0()
+    w, p = api.load_scene(sc)
+    o = PortCloth.from_scene(sc)
+    assert np.array_equal(p.model.tris(), o.tris()[0].astype(np.int32))
+    assert np.array_equal(p.model.bends(), o.bends())
+    assert np.array_equal(p.model.edges(), o.edges())
+
+
+def _sdf_scene(n=20):
+    sc = scenes.cfg1(n=n)
+    sc.params.substeps = 1
+    sc.params.iterations = 6
+    # start just above the sphere so vertex contacts appear in the first substep
+    sc.positions[:, 1] -= np.float32(0.4 - 0.006)
+    sc.offset = sc.offset.copy()
+    return sc
+
+
+def test_sdf_vertex_contacts_match():
+    sc = _sdf_scene()
+    w, p, o = _pair(sc)
+    p.step(sc.dt)
+    o.step(sc.dt)
+    gi, gf = p.model.contacts(0)
+    oi, of = o.contacts(0)
+    assert len(gi) > 0
+    assert np.array_equal(gi, oi)
+    assert np.array_equal(gf[:, :6].view(np.uint32), of[:, :6].view(np.uint32))
+
+
+def test_sdf_check_mode_trajectory():
+    sc = _sdf_scene()
+    sc.params.substeps = 4
+    w, p, o = _pair(sc)
+    worst = 0.0
+    for _ in range(6):
+        p.step(sc.dt)
+        o.step(sc.dt)
+        worst = max(worst, float(np.abs(p.model.positions() - o.positions()).max()))
+    assert worst <= TOL, worst
+
+
+def test_self_contacts_match_folded():
+    sc = scenes.cfg1(n=16)
+    sc.sdfs.clear()
+    sc.params.substeps = 1
+    sc.params.iterations = 4
+    state = scenes.folded(sc, gap=0.004)
+    w, p, o = _pair(sc, state=state)
+    p.step(sc.dt)
+    o.step(sc.dt)
+    for kind in (3, 4):
+        gi, gf = p.model.contacts(kind)
+        oi, of = o.contacts(kind)
+        assert len(oi) > 0, kind
+        assert np.array_equal(gi, oi), (kind, len(gi), len(oi))
+        # normal and side are detection outputs (the solver rewrites w)
+        sel = [0, 1, 2, 6]
+        assert np.array_equal(gf[:, sel].view(np.uint32), of[:, sel].view(np.uint32)), kind
+    assert p.status() == 0
+
+
+def test_self_check_mode_trajectory():
+    sc = scenes.cfg1(n=16)
+    sc.sdfs.clear()
+    sc.params.substeps = 2
+    sc.params.iterations = 5
+    state = scenes.folded(sc, gap=0.004)
+    w, p, o = _pair(sc, state=state)
+    worst = 0.0
+    for _ in range(3):
+        p.step(sc.dt)
+        o.step(sc.dt)
+        worst = max(worst, float(np.abs(p.model.positions() - o.positions()).max()))
+    assert worst <= TOL, worst
+
+
+def test_ccd_broadphase_and_hits_bitexact():
+    sc, state = scenes.ccd_scene(16)
+    w, p, o = _pair(sc, ccd=True, state=state)
+    p.step(sc.dt)
+    # broad phase: all-pairs overlap set of the oracle from the same predicted state
+    o2 = __import__("oracle.bridge", fromlist=["PortCloth"]).PortCloth.from_scene(sc)
+    o2.set_state(*state)
+    o2.predict_detect(sc.dt / sc.params.substeps, ccd=False)
+    tol = sc.params.thickness + 0.5 * sc.params.tolerance
+    ovt = o2.ccd_broadphase(tol, 0)
+    oee = o2.ccd_broadphase(tol, 1)
+    gvt = p.model.ccd_candidates(0)       # (vertex, triangle)
+    gee = p.model.ccd_candidates(1)
+    assert len(ovt) > 0 and len(oee) > 0
+    assert sorted(map(tuple, gvt[:, ::-1].tolist())) == sorted(map(tuple, ovt.tolist()))
+    assert sorted(map(tuple, gee.tolist())) == sorted(map(tuple, oee.tolist()))
+    # narrow phase: the self lists (proximity then continuous hits) match
+    o.step(sc.dt)
+    for kind in (3, 4):
+        gi, gf = p.model.contacts(kind)
+        oi, of = o.contacts(kind)
+        assert len(oi) > 0
+        assert np.array_equal(gi, oi), (kind, len(gi), len(oi))
+        sel = [0, 1, 2, 6]
+        assert np.array_equal(gf[:, sel].view(np.uint32), of[:, sel].view(np.uint32)), kind
+    assert p.status() == 0
