@@ -200,6 +200,10 @@ SCEXP void scGetEdgeContacts(scModel model, int* idx3, float* f8);
 /* continuous-collision broad-phase pairs of the last substep:
    kind 0 -> (vertex, triangle), kind 1 -> (edge, edge); returns the count */
 SCEXP int scGetCCDCandidates(scModel model, int kind, int* pairs, int cap);
+/* contact classes of the last substep (0 edge, 1 triangle, 2 self vertex-triangle,
+   3 self edge-edge): writes the per-colour counts of the independent-set
+   colouring into counts[0..127] (may be NULL) and returns the colours used */
+SCEXP int scGetContactColours(scModel model, int cls, int* counts);
 /* collision-mesh (prev positions) vertex normals as of the last mesh update */
 SCEXP void scGetCollisionMeshNormals(scModel model, float* xyz);
 

@@ -87,6 +87,8 @@ def _load(path: Path, prefix: str):
         sig.update({"set_tri_order": ([C.c_void_p, _i, C.c_int], None),
                     "set_bend_order": ([C.c_void_p, _i, C.c_int], None),
                     "set_contact_order": ([C.c_void_p, C.c_int], None),
+                    "set_portable_math": ([C.c_int], None),
+                    "portable_acos": ([C.c_float], C.c_float),
                     "self_contact_colours": ([C.c_void_p, C.c_int, _i], None),
                     "ccd_broadphase": ([C.c_void_p, C.c_float, C.c_int, _i, C.c_int], C.c_int)})
     for name, (args, res) in sig.items():
@@ -262,6 +264,16 @@ class PortCloth(CpuCloth):
 
     def __init__(self):
         super().__init__(PORT_LIB, "orc_")
+
+    @staticmethod
+    def set_portable_math(on: bool):
+        """True: bends and normal weights use the library's portable arc cosine
+        (check mode against the GPU); False: libm acosf (as the reference)."""
+        _load(PORT_LIB, "orc_").orc_set_portable_math(int(on))
+
+    @staticmethod
+    def portable_acos(x: float) -> float:
+        return _load(PORT_LIB, "orc_").orc_portable_acos(float(x))
 
     def set_tri_order(self, order):
         if order is None:

@@ -26,6 +26,8 @@
 using namespace orc;
 typedef uint32_t u32;
 
+namespace orc { bool g_portable_math = false; }
+
 namespace {
 
 const V3 kGravity = {0.f, -9.8f, 0.f}; /* Physics/Common.h:18 */
@@ -70,9 +72,9 @@ struct Topo
             V3 e1 = normalized(b - a), e2 = normalized(c - b), e3 = normalized(a - c);
             float c1 = -dot(e1, e3), c2 = -dot(e1, e2), c3 = -dot(e2, e3);
             float s1 = len(cross(e1, -e3)), s2 = len(cross(e2, -e1)), s3 = len(cross(e3, -e1));
-            float t1 = std::fabs(c1) > 1 ? (float)std::fabs(std::atan2((double)s1, (double)c1)) : acosf(c1);
-            float t2 = std::fabs(c2) > 1 ? (float)std::fabs(std::atan2((double)s2, (double)c2)) : acosf(c2);
-            float t3 = std::fabs(c3) > 1 ? (float)std::fabs(std::atan2((double)s3, (double)c3)) : acosf(c3);
+            float t1 = std::fabs(c1) > 1 ? (float)std::fabs(std::atan2((double)s1, (double)c1)) : step_acos(c1);
+            float t2 = std::fabs(c2) > 1 ? (float)std::fabs(std::atan2((double)s2, (double)c2)) : step_acos(c2);
+            float t3 = std::fabs(c3) > 1 ? (float)std::fabs(std::atan2((double)s3, (double)c3)) : step_acos(c3);
             normals[i1] += t1 * nt;
             normals[i2] += t2 * nt;
             normals[i3] += t3 * nt;
@@ -1216,7 +1218,7 @@ struct Cloth
             float il1 = 1.f / l1, il2 = 1.f / l2;
             cosine = dot(il1 * n1, il2 * n2);
             cosine = std::min(1.f, std::max(-1.f, cosine));
-            theta = acosf(cosine);
+            theta = step_acos(cosine);
         }
         if (std::fabs(cosine) >= 1 - 0.001f) return -1;
         /* EvaluateGradient (recomputes the same quantities) */
@@ -1464,8 +1466,11 @@ struct Cloth
         std::vector<int> colour(n, -1);
         std::vector<uint64_t> key(n), minKey(N);
         for (int i = 0; i < n; i++) key[i] = ((uint64_t)contact_hash((u32)i) << 32) | (u32)i;
+        /* at most MAX_ROUNDS rounds; what is left takes the last colour and is
+           solved in list order (as the GPU's single-thread fallback does) */
+        const int MAX_ROUNDS = 127;
         int remaining = n, round = 0;
-        while (remaining > 0)
+        while (remaining > 0 && round < MAX_ROUNDS)
         {
             std::fill(minKey.begin(), minKey.end(), ~0ull);
             for (int i = 0; i < n; i++)
@@ -1485,6 +1490,7 @@ struct Cloth
             for (int i = 0; i < n; i++) if (colour[i] == round) remaining--;
             round++;
         }
+        for (int i = 0; i < n; i++) if (colour[i] < 0) colour[i] = MAX_ROUNDS;
         std::vector<int> order(n);
         for (int i = 0; i < n; i++) order[i] = i;
         std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return colour[a] < colour[b]; });
@@ -1952,6 +1958,11 @@ void orc_set_bend_order(void* h, const int* o, int n)
 }
 
 void orc_set_contact_order(void* h, int mode) { ((Cloth*)h)->contactOrder = mode; }
+
+/* 0: libm acosf as the reference; 1: the library's portable arc cosine (check mode).
+   Process-wide, since the initial normals are computed when a grid is built. */
+void orc_set_portable_math(int on) { g_portable_math = on != 0; }
+float orc_portable_acos(float x) { return portable_acos(x); }
 
 /* ClothPatch::Step (Physics/ClothPatch.cpp:323-335) */
 void orc_step(void* h, float dt)

@@ -41,6 +41,8 @@ void orc_set_bend_order(void* h, const int* order, int n);
 /* Check mode for multi-vertex contacts: 0 = list order (reference), 1 = the
    GPU's deterministic independent-set colouring order (colour, then list index). */
 void orc_set_contact_order(void* h, int mode);
+void orc_set_portable_math(int on);
+float orc_portable_acos(float x);
 void orc_step(void* h, float dt);
 void orc_update_mesh(void* h);
 void orc_predict_detect(void* h, float hh, int runCCD);

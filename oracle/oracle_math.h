@@ -207,3 +207,31 @@ static inline bool overlap(const Box& a, const Box& b)
 }
 
 } // namespace orc
+
+namespace orc {
+/* The library's portable arc cosine (same algorithm and operation order as
+   solidcloth_b200/csrc/scmath.cuh: Moshier's Cephes asinf polynomial), used by
+   the oracle's check mode so bends and normal weights match the GPU bit for bit. */
+static inline float asin_core(float a)
+{
+    const float z = a * a;
+    float p = 4.2163199048E-2f;
+    p = p * z + 2.4181311049E-2f;
+    p = p * z + 4.5470025998E-2f;
+    p = p * z + 7.4953002686E-2f;
+    p = p * z + 1.6666752422E-1f;
+    return p * z * a + a;
+}
+
+static inline float portable_acos(float x)
+{
+    const float PIO2 = 1.5707963267948966192f, PI_F = 3.14159265358979323846f;
+    if (x < -0.5f) return PI_F - 2.0f * asin_core(std::sqrt(0.5f * (1.0f + x)));
+    if (x > 0.5f) return 2.0f * asin_core(std::sqrt(0.5f * (1.0f - x)));
+    return PIO2 - asin_core(x);
+}
+
+/* acos used by the step: libm's acosf (as the reference) or the portable one */
+extern bool g_portable_math;
+static inline float step_acos(float x) { return g_portable_math ? portable_acos(x) : acosf(x); }
+} // namespace orc

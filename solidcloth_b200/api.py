@@ -137,6 +137,7 @@ SIGNATURES = {
     "scGetEdgeContacts": ([scModel, _i, _f], None),
     "scGetCCDCandidates": ([scModel, C.c_int, _i, C.c_int], C.c_int),
     "scGetCollisionMeshNormals": ([scModel, _f], None),
+    "scGetContactColours": ([scModel, C.c_int, _i], C.c_int),
     "scGetLastError": ([], C.c_int),
     "scGetLastErrorString": ([], C.c_char_p),
     "scGetStatus": ([scClothPatch], C.c_int),
@@ -340,6 +341,11 @@ class ClothModel:
 
     def solver_iterations(self):
         return lib().scGetSolverIterations(self.h)
+
+    def contact_colours(self, cls):
+        counts = np.zeros(128, np.int32)
+        used = lib().scGetContactColours(self.h, int(cls), counts.ctypes.data_as(_i))
+        return counts[:used].copy()
 
 
 class ClothPatch:

@@ -532,6 +532,22 @@ int scGetCCDCandidates(scModel m, int kind, int* pairs, int cap)
     return n;
 }
 
+int scGetContactColours(scModel m, int cls, int* counts)
+{
+    ClothModel* c = M(m);
+    if (!c || !c->buf.colourStart || cls < 0 || cls > 3) return 0;
+    host_sync(c);
+    std::vector<int> st = dl(c->buf.colourStart + cls * (MAX_COLOURS + 1), MAX_COLOURS + 1);
+    int used = 0;
+    for (int k = 0; k < MAX_COLOURS; k++)
+    {
+        int n = st[k + 1] - st[k];
+        if (counts) counts[k] = n;
+        if (n > 0) used = k + 1;
+    }
+    return used;
+}
+
 void scGetCollisionMeshNormals(scModel m, float* xyz)
 {
     ClothModel* c = M(m);

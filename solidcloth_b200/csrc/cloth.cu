@@ -49,9 +49,9 @@ void HMesh::compute_normals()
         V3 e1 = normalized(b - a), e2 = normalized(c - b), e3 = normalized(a - c);
         float c1 = -dot(e1, e3), c2 = -dot(e1, e2), c3 = -dot(e2, e3);
         float s1 = len(cross(e1, -e3)), s2 = len(cross(e2, -e1)), s3 = len(cross(e3, -e1));
-        float t1 = std::fabs(c1) > 1 ? (float)std::fabs(std::atan2((double)s1, (double)c1)) : acosf(c1);
-        float t2 = std::fabs(c2) > 1 ? (float)std::fabs(std::atan2((double)s2, (double)c2)) : acosf(c2);
-        float t3 = std::fabs(c3) > 1 ? (float)std::fabs(std::atan2((double)s3, (double)c3)) : acosf(c3);
+        float t1 = std::fabs(c1) > 1 ? (float)std::fabs(std::atan2((double)s1, (double)c1)) : portable_acos(c1);
+        float t2 = std::fabs(c2) > 1 ? (float)std::fabs(std::atan2((double)s2, (double)c2)) : portable_acos(c2);
+        float t3 = std::fabs(c3) > 1 ? (float)std::fabs(std::atan2((double)s3, (double)c3)) : portable_acos(c3);
         normals[i1] += t1 * nt;
         normals[i2] += t2 * nt;
         normals[i3] += t3 * nt;
@@ -934,7 +934,10 @@ void ClothPatch::record_substep(float h)
     launch_colour_contacts(s, c, b);
     // ClothModelPBD::SolveGS (Physics/ClothPBD.cpp:324-369)
     launch_reset_gs(s, c);
-    for (int k = 0; k < m.prm.iterations; k++)
+    // the reference's loop tests its exit conditions after the body, so it always
+    // runs at least one iteration (Physics/ClothPBD.cpp:335-362)
+    const int iterations = m.prm.iterations > 1 ? m.prm.iterations : 1;
+    for (int k = 0; k < iterations; k++)
     {
         if (m.prm.fem)
             for (size_t col = 0; col + 1 < m.triColourStart.size(); col++)

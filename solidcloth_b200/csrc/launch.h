@@ -4,11 +4,11 @@
 
 namespace sc {
 
-constexpr int KVT = 16;        // self vertex-triangle contact slots per vertex
-constexpr int KCAND = 192;     // BVH candidates kept per proximity query
-constexpr int KRES = 48;       // distinct features tracked per vertex for the dedup
+constexpr int KVT = 48;        // self vertex-triangle contact slots per vertex
+constexpr int KCAND = 256;     // BVH candidates kept per proximity query
+constexpr int KRES = 96;       // distinct features tracked per vertex for the dedup
 constexpr int KCCD = 64;       // continuous-collision candidates per query
-constexpr int MAX_COLOURS = 64;// independent-set colouring rounds per contact class
+constexpr int MAX_COLOURS = 128; // independent-set colouring rounds per contact class
 constexpr int WALL_SLOTS = 5;
 
 // Vertex contact slot (walls, sphere, SDF, mesh vertex contacts).

@@ -160,6 +160,40 @@ SC_HD bool overlap(const Box& a, const Box& b)
     return true;
 }
 
+// Arc cosine evaluated identically on the host and the GPU (plain float
+// operations, no fused multiply-add), after Moshier's Cephes single-precision
+// asinf/acosf: acos(x) = pi/2 - asin(x) for |x| <= 0.5 and
+// acos(x) = 2 asin(sqrt((1 - |x|)/2)) (reflected for x < 0) otherwise, with
+// asin(a) = a + a z P(z), z = a^2, P the Cephes degree-4 polynomial. About one
+// ulp from the correctly rounded value; used for bend angles and normal
+// weights so the library and the oracle's check mode agree bit for bit.
+SC_HD float asin_core(float a)
+{
+    const float z = a * a;
+    float p = 4.2163199048E-2f;
+    p = p * z + 2.4181311049E-2f;
+    p = p * z + 4.5470025998E-2f;
+    p = p * z + 7.4953002686E-2f;
+    p = p * z + 1.6666752422E-1f;
+    return p * z * a + a;
+}
+
+SC_HD float portable_acos(float x)
+{
+    const float PIO2 = 1.5707963267948966192f, PI_F = 3.14159265358979323846f;
+    if (x < -0.5f)
+    {
+        const float s = sqrtf(0.5f * (1.0f + x));
+        return PI_F - 2.0f * asin_core(s);
+    }
+    if (x > 0.5f)
+    {
+        const float s = sqrtf(0.5f * (1.0f - x));
+        return 2.0f * asin_core(s);
+    }
+    return PIO2 - asin_core(x);
+}
+
 // Integer finaliser used to give contacts pseudo-random colouring priorities
 // ("lowbias32", C. Wellons, public domain).
 SC_HD uint32_t mix32(uint32_t x)

@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(256) k_bends(DevCloth c, SolverParams P, int f
         float il1 = 1.f / l1, il2 = 1.f / l2;
         cosine = dot(il1 * n1, il2 * n2);
         cosine = mn(1.f, mx(-1.f, cosine));
-        theta = acosf(cosine);
+        theta = portable_acos(cosine);
     }
     if (fabsf(cosine) >= 1 - 0.001f) return;
     float h1 = l1 / l, h2 = l2 / l;
@@ -183,9 +183,9 @@ __global__ void k_tri_normals(const float4* verts, const uint32_t* tri, int T, f
     V3 e1 = normalized(b - a), e2 = normalized(cc - b), e3 = normalized(a - cc);
     float c1 = -dot(e1, e3), c2 = -dot(e1, e2), c3 = -dot(e2, e3);
     float s1 = len(cross(e1, -e3)), s2 = len(cross(e2, -e1)), s3 = len(cross(e3, -e1));
-    float t1 = fabsf(c1) > 1 ? fabsf((float)atan2((double)s1, (double)c1)) : acosf(c1);
-    float t2 = fabsf(c2) > 1 ? fabsf((float)atan2((double)s2, (double)c2)) : acosf(c2);
-    float t3 = fabsf(c3) > 1 ? fabsf((float)atan2((double)s3, (double)c3)) : acosf(c3);
+    float t1 = fabsf(c1) > 1 ? fabsf((float)atan2((double)s1, (double)c1)) : portable_acos(c1);
+    float t2 = fabsf(c2) > 1 ? fabsf((float)atan2((double)s2, (double)c2)) : portable_acos(c2);
+    float t3 = fabsf(c3) > 1 ? fabsf((float)atan2((double)s3, (double)c3)) : portable_acos(c3);
     ang[t] = make_float4(t1, t2, t3, 0.f);
 }
 
@@ -1073,11 +1073,15 @@ __global__ void __launch_bounds__(1024) k_solve_multi(DevCloth c, SolverParams P
         {
             const int s0 = cv.start[col], s1 = cv.start[col + 1];
             if (s0 == s1) continue;
+            // the last colour holds contacts left after the colouring rounds; one
+            // thread solves them in list order (deterministic, as the oracle does)
             const bool serial = (col == MAX_COLOURS - 1);
-            for (int j = s0 + (serial ? 0 : threadIdx.x); j < s1; j += (serial ? 1 : blockDim.x))
+            const int jEnd = serial ? n : s1;
+            for (int j = serial ? 0 : s0 + threadIdx.x; j < jEnd; j += (serial ? 1 : blockDim.x))
             {
                 if (serial && threadIdx.x != 0) break;
-                int i = cv.order[j];
+                if (serial && cv.colour[j] != MAX_COLOURS - 1) continue;
+                int i = serial ? j : cv.order[j];
                 float e;
                 if (cls == 0) { EC k = b.ecList[i]; e = solve_edge_contact(c, P, b, k); b.ecList[i] = k; }
                 else if (cls == 1) { TC k = b.tcList[i]; e = solve_tri_contact(c, P, b, k); b.tcList[i] = k; }
@@ -1430,8 +1434,12 @@ __global__ void __launch_bounds__(128) k_self_vt(DevCloth c, SolverParams P, Buf
             for (int k = 0; k < nres; k++) if (resType[k] == rtype && resFeat[k] == feature) { found = true; break; }
             if (found) continue;
         }
-        if (nres < KRES) { resType[nres] = rtype; resFeat[nres] = feature; nres++; }
-        else { atomicOr(c.status, ST_SELF_VT_OVERFLOW); continue; }
+        // only edge and vertex features take part in the dedup (faces carry -1)
+        if (feature >= 0)
+        {
+            if (nres < KRES) { resType[nres] = rtype; resFeat[nres] = feature; nres++; }
+            else { atomicOr(c.status, ST_SELF_VT_OVERFLOW); continue; }
+        }
         // ClosestPoints(self) then MeshCollisions: drop adjacent features,
         // keep 0 <= dist < radTol (ClosestPointsBetweenMeshes.cpp:553-563,
         // ClothCollision.cpp:113-131)

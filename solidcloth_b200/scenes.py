@@ -219,19 +219,36 @@ def cfg0(seed: int = 0) -> Scene:
     return make_grid_scene("cfg0_32x32_pinned", 32, 1.0, 0.0, p, pinned_corners=(1, 3), seed=seed, frames=120)
 
 
-def cfg1(seed: int = 1, n: int = 128, ccd: bool = False) -> Scene:
+def _self_flags(self_mode: str):
+    """Self-collision mapping. "ccd": the continuous detector the benchmark
+    configurations name (Physics/SelfCollisionDetector.cpp), CF_SELF off.
+    "proximity": the reference's live CF_SELF path (brute-force closest features,
+    Geometry/ClosestPointsBetweenMeshes.cpp:538-592). "both": the two together.
+    At the configurations' scale (5 mm thickness + 5 mm tolerance on a 7.9 mm
+    grid) the live path finds coplanar non-adjacent neighbours within radTol and
+    its solve treats them as penetrating (it tests the triangle-normal component,
+    ClothCollisionHandler.cpp:400-412), so the reference itself crumples the
+    cloth; the continuous detector does not."""
+    return {"ccd": (0, True), "proximity": (CF_SELF, False), "both": (CF_SELF, True)}[self_mode]
+
+
+def cfg1(seed: int = 1, n: int = 128, ccd: bool = True, self_mode: str | None = None) -> Scene:
+    mode = self_mode or ("ccd" if ccd else "proximity")
+    sf, use_ccd = _self_flags(mode)
     p = Params(thickness=0.005, tolerance=0.005, friction=0.3, iterations=15, substeps=8,
-               flags=CF_VERTICES | CF_SELF)
-    s = make_grid_scene(f"cfg1_{n}x{n}_sphere_sdf_self", n, 1.0, 0.3 + 0.4, p, seed=seed, frames=300)
+               flags=CF_VERTICES | sf)
+    s = make_grid_scene(f"cfg1_{n}x{n}_sphere_sdf_self_{mode}", n, 1.0, 0.3 + 0.4, p, seed=seed, frames=300)
     s.sdfs.append(sphere_sdf((0.0, 0.0, 0.0), 0.3, 63, 0.1))
-    s.ccd = ccd
+    s.ccd = use_ccd
     return s
 
 
-def cfg2(seed: int = 2, n: int = 256, level: int = 5) -> Scene:
+def cfg2(seed: int = 2, n: int = 256, level: int = 5, self_mode: str = "ccd") -> Scene:
+    sf, use_ccd = _self_flags(self_mode)
     p = Params(thickness=0.005, tolerance=0.005, friction=0.3, iterations=20, substeps=8,
-               flags=CF_VERTICES | CF_TRIANGLES | CF_EDGES | CF_SELF | CF_WALLS)
-    s = make_grid_scene(f"cfg2_{n}x{n}_icosphere_mesh_self", n, 1.5, 0.5 + 0.5, p, seed=seed, frames=300)
+               flags=CF_VERTICES | CF_TRIANGLES | CF_EDGES | CF_WALLS | sf)
+    s = make_grid_scene(f"cfg2_{n}x{n}_icosphere_mesh_self_{self_mode}", n, 1.5, 0.5 + 0.5, p, seed=seed, frames=300)
+    s.ccd = use_ccd
     # Unit masses (inverse mass 1, the reference's own default after Init): the
     # reference's triangle and edge contact solves divide by the inverse mass
     # (SolveTriContacts / SolveEdgeContacts, Physics/ClothCollisionHandler.cpp:302,381),
@@ -254,10 +271,11 @@ def cfg3_instances(count: int = 512, seed: int = 3, lo: int = 16, hi: int = 128)
         npins = int(rng.integers(1, 5))
         corners = tuple(sorted(rng.choice(4, size=npins, replace=False).tolist()))
         p = Params(thickness=0.005, tolerance=0.005, friction=0.3, iterations=15, substeps=8,
-                   flags=CF_VERTICES | CF_SELF)
+                   flags=CF_VERTICES)
         s = make_grid_scene(f"cfg3_inst{k}_{n}", n, 1.0, r + 0.4, p, pinned_corners=corners,
                             seed=seed * 100003 + k, frames=200)
         s.sdfs.append(sphere_sdf((0.0, 0.0, 0.0), r, 31, 0.1))
+        s.ccd = True
         scenes.append(s)
     return scenes
 

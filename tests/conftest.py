@@ -19,6 +19,18 @@ def cuda_available() -> bool:
         return False
 
 
+@pytest.fixture(autouse=True)
+def libm_math_by_default():
+    """The oracle's arc cosine is process-wide: libm (as the reference) unless a
+    test asks for the library's portable one (GPU check mode)."""
+    from oracle.bridge import PortCloth, available
+    if available("port"):
+        PortCloth.set_portable_math(False)
+    yield
+    if available("port"):
+        PortCloth.set_portable_math(False)
+
+
 @pytest.fixture(scope="session")
 def ref_threads():
     from oracle.bridge import RefCloth, available

@@ -33,7 +33,7 @@ def case_cfg0():
 
 
 def sdf_scene():
-    sc = scenes.cfg1(n=20)
+    sc = scenes.cfg1(n=20, self_mode="proximity")
     sc.params.substeps = 2
     sc.params.iterations = 6
     sc.positions[:, 1] -= np.float32(0.4 - 0.004)
@@ -52,7 +52,7 @@ def case_sdf():
 
 
 def folded_scene():
-    sc = scenes.cfg1(n=16)
+    sc = scenes.cfg1(n=16, self_mode="proximity")
     sc.sdfs.clear()
     sc.params.substeps = 1
     sc.params.iterations = 4

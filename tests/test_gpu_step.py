@@ -18,6 +18,7 @@ TOL = 1e-5          # metres; per-constraint parity bound of the spec, applied t
 def _pair(sc, ccd=False, state=None):
     from solidcloth_b200 import api
     from oracle.bridge import PortCloth
+    PortCloth.set_portable_math(True)
     w, p = api.load_scene(sc, ccd=ccd)
     o = PortCloth.from_scene(sc)
     o._fn("set_ccd")(o.h, int(ccd))
@@ -44,15 +45,20 @@ def test_fem_only_bitexact():
     assert p.status() == 0
 
 
+def _same(g, c):
+    return np.array_equal(np.ascontiguousarray(g, np.float32).view(np.uint32),
+                          np.ascontiguousarray(c, np.float32).view(np.uint32))
+
+
 def test_cfg0_check_mode():
+    """FEM + bends: the coloured GPU sweep equals the oracle's sequential sweep in
+    the same order bit for bit (both use the library's portable arc cosine)."""
     sc = scenes.cfg0()
     w, p, o = _pair(sc)
-    worst = 0.0
     for f in range(20):
         p.step(sc.dt)
         o.step(sc.dt)
-        worst = max(worst, float(np.abs(p.model.positions() - o.positions()).max()))
-    assert worst <= TOL, worst
+        assert _same(p.model.positions(), o.positions()), (f, float(np.abs(p.model.positions() - o.positions()).max()))
     assert np.allclose(p.model.velocities(), o.state()[2], atol=1e-3)
 
 
@@ -110,16 +116,16 @@ def test_sdf_check_mode_trajectory():
     sc = _sdf_scene()
     sc.params.substeps = 4
     w, p, o = _pair(sc)
-    worst = 0.0
-    for _ in range(6):
+    for f in range(6):
         p.step(sc.dt)
         o.step(sc.dt)
-        worst = max(worst, float(np.abs(p.model.positions() - o.positions()).max()))
-    assert worst <= TOL, worst
+        p.update_mesh()
+        o.update_mesh()
+        assert _same(p.model.positions(), o.positions()), (f, float(np.abs(p.model.positions() - o.positions()).max()))
 
 
 def test_self_contacts_match_folded():
-    sc = scenes.cfg1(n=16)
+    sc = scenes.cfg1(n=16, self_mode="proximity")
     sc.sdfs.clear()
     sc.params.substeps = 1
     sc.params.iterations = 4
@@ -135,22 +141,24 @@ def test_self_contacts_match_folded():
         # normal and side are detection outputs (the solver rewrites w)
         sel = [0, 1, 2, 6]
         assert np.array_equal(gf[:, sel].view(np.uint32), of[:, sel].view(np.uint32)), kind
-    assert p.status() == 0
+    # this stress case needs more colouring rounds than the parallel schedule
+    # keeps (bit 16): the rest is solved serially in list order, as the oracle does
+    assert p.status() & ~16 == 0
 
 
 def test_self_check_mode_trajectory():
-    sc = scenes.cfg1(n=16)
+    sc = scenes.cfg1(n=16, self_mode="proximity")
     sc.sdfs.clear()
     sc.params.substeps = 2
     sc.params.iterations = 5
     state = scenes.folded(sc, gap=0.004)
     w, p, o = _pair(sc, state=state)
-    worst = 0.0
-    for _ in range(3):
+    for f in range(3):
         p.step(sc.dt)
         o.step(sc.dt)
-        worst = max(worst, float(np.abs(p.model.positions() - o.positions()).max()))
-    assert worst <= TOL, worst
+        p.update_mesh()
+        o.update_mesh()
+        assert _same(p.model.positions(), o.positions()), (f, float(np.abs(p.model.positions() - o.positions()).max()))
 
 
 def test_ccd_broadphase_and_hits_bitexact():
@@ -178,4 +186,6 @@ def test_ccd_broadphase_and_hits_bitexact():
         assert np.array_equal(gi, oi), (kind, len(gi), len(oi))
         sel = [0, 1, 2, 6]
         assert np.array_equal(gf[:, sel].view(np.uint32), of[:, sel].view(np.uint32)), kind
-    assert p.status() == 0
+    # this stress case needs more colouring rounds than the parallel schedule
+    # keeps (bit 16): the rest is solved serially in list order, as the oracle does
+    assert p.status() & ~16 == 0

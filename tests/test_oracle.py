@@ -145,7 +145,7 @@ def test_golden_mesh_collider():
 @pytest.mark.parametrize("n", [12, 20])
 def test_port_matches_reference_sdf_self(n, ref_threads):
     R, P = ref(), port()
-    sc = scenes.cfg1(n=n)
+    sc = scenes.cfg1(n=n, self_mode="proximity")
     sc.params.substeps = 2
     sc.params.iterations = 5
     sc.positions[:, 1] -= np.float32(0.4 - 0.003)
