@@ -226,6 +226,26 @@ SCEXP int scGetGraphKernelCount(scClothPatch patch);
    Particle positions are modified. */
 SCEXP float scProfileSweep(scClothPatch patch, int kind, int reps);
 
+/* ---- addition with no counterpart in the reference: normals without allocation ----
+   For callers that cannot call cudaMalloc (engines that reserve all GPU memory up
+   front and forbid allocation in their frame loop, code running inside another
+   library's memory pool, real-time threads where an allocation would stall the
+   frame). Computes the angle-weighted vertex normals of a triangle mesh — the
+   normals scUpdateClothMesh computes — from caller-owned DEVICE buffers:
+   vertices and normals are numVertices packed xyz floats, indices 3*numTriangles.
+   Its only scratch is a fixed file-scope device array of SC_NOALLOC_MAX_VERTICES
+   float4 accumulators (1 MiB, resident on every GPU that loads the library until
+   the process exits); meshes with more vertices are rejected (SC_ERR_ARG = 2).
+   Every call shares that scratch and leaves its contents behind; a call clears
+   what it uses first, but calls that overlap on the GPU race and must be
+   serialised by the caller. The first call on a device looks the scratch's
+   device address up, so make it before any stream capture that includes later
+   calls. Work is enqueued on `stream` (a cudaStream_t, NULL = legacy default).
+   Returns 0 or an error code (details from scGetLastErrorString). */
+#define SC_NOALLOC_MAX_VERTICES 65536
+SCEXP int scComputeVertexNormalsNoAlloc(const float* vertices, int numVertices, const unsigned* indices,
+                                        int numTriangles, float* normals, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -138,6 +138,7 @@ SIGNATURES = {
     "scGetCCDCandidates": ([scModel, C.c_int, _i, C.c_int], C.c_int),
     "scGetCollisionMeshNormals": ([scModel, _f], None),
     "scGetContactColours": ([scModel, C.c_int, _i], C.c_int),
+    "scComputeVertexNormalsNoAlloc": ([C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p], C.c_int),
     "scGetLastError": ([], C.c_int),
     "scGetLastErrorString": ([], C.c_char_p),
     "scGetStatus": ([scClothPatch], C.c_int),
