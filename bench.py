@@ -42,7 +42,9 @@ UNIT = "vertex-substeps/s"
 def _args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--self", dest="self_mode", default="ccd", choices=["ccd", "proximity", "both"],
+                    help="self-collision: the continuous detector (default), the live proximity path, or both")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="cfg1", choices=["cfg0", "cfg1", "cfg2"])
@@ -51,9 +53,9 @@ def _args():
     return ap.parse_args()
 
 
-def _scene(name):
+def _scene(name, self_mode="ccd"):
     from solidcloth_b200 import scenes
-    return scenes.CONFIGS[name]()
+    return scenes.CONFIGS[name]() if name == "cfg0" else scenes.CONFIGS[name](self_mode=self_mode)
 
 
 def _workload(sc):
@@ -90,7 +92,7 @@ class Clocks:
                  "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -161,7 +163,7 @@ def run_reference(args):
     ws, rank, _ = _dist()
     if rank != 0:
         return
-    sc = _scene(args.config)
+    sc = _scene(args.config, args.self_mode)
     from oracle.bridge import available
     if not available("ref"):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libscref.so not built (reference sources absent at build time)"}))
@@ -204,7 +206,7 @@ def run_ours(args):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
     from solidcloth_b200 import api
-    sc = _scene(args.config)
+    sc = _scene(args.config, args.self_mode)
     w, p = api.load_scene(sc)
     stream = torch.cuda.ExternalStream(p.cuda_stream(), device=torch.device("cuda", local))
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")

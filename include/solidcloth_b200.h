@@ -178,6 +178,14 @@ SCEXP void scSetFixedIterations(scModel model, bool val);
    (Physics/SelfCollisionDetector.cpp), appended to the self contacts each substep. */
 SCEXP void scSetSelfCCD(scModel model, bool val);
 SCEXP int scGetSolverIterations(scModel model);
+/* true (default): the Gauss-Seidel loop of a substep runs as one thread-block
+   cluster with the particles in distributed shared memory, when the cloth fits
+   (up to 131,072 particles); false: one kernel per colour. Same results. */
+SCEXP void scSetClusterSolver(scModel model, bool val);
+/* true (default): the cluster solver copies each CTA's FEM and bend records to
+   shared memory once per substep when they fit; false: read them from global
+   memory in every sweep. Same results. */
+SCEXP void scSetClusterStaging(scModel model, bool val);
 
 /* ---- additions: inspection for parity checks ---- */
 /* kind 0: FEM triangles, 1: bends. Writes the solve order (a permutation) and

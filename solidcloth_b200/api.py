@@ -124,6 +124,8 @@ SIGNATURES = {
     "scSetParticleState": ([scModel, _f, _f, _f], None),
     "scSetFixedIterations": ([scModel, C.c_bool], None),
     "scSetSelfCCD": ([scModel, C.c_bool], None),
+    "scSetClusterSolver": ([scModel, C.c_bool], None),
+    "scSetClusterStaging": ([scModel, C.c_bool], None),
     "scGetSolverIterations": ([scModel], C.c_int),
     "scGetConstraintOrder": ([scModel, C.c_int, _i, _i], C.c_int),
     "scGetNumBends": ([scModel], C.c_int),
@@ -288,6 +290,12 @@ class ClothModel:
 
     def set_ccd(self, on: bool):
         lib().scSetSelfCCD(self.h, bool(on))
+
+    def set_cluster_solver(self, on: bool):
+        lib().scSetClusterSolver(self.h, bool(on))
+
+    def set_cluster_staging(self, on: bool):
+        lib().scSetClusterStaging(self.h, bool(on))
 
     def constraint_order(self, kind):
         n = lib().scGetNumTris(self.h) if kind == 0 else lib().scGetNumBends(self.h)

@@ -398,6 +398,8 @@ void scGetParticleVelocities(scModel m, float* xyz) { get3(m, xyz, 1); }
 void scGetParticlePrevPositions(scModel m, float* xyz) { get3(m, xyz, 2); }
 void scSetFixedIterations(scModel m, bool v) { if (M(m)) { M(m)->prm.fixedIterations = v; M(m)->touch(); } }
 void scSetSelfCCD(scModel m, bool v) { if (M(m)) { M(m)->prm.ccd = v; M(m)->touch(); } }
+void scSetClusterSolver(scModel m, bool v) { if (M(m)) { M(m)->prm.clusterSolver = v; M(m)->touch(); } }
+void scSetClusterStaging(scModel m, bool v) { if (M(m)) { M(m)->prm.stageRecords = v; M(m)->touch(); } }
 int scGetSolverIterations(scModel m)
 {
     if (!M(m) || !M(m)->dc.scal) return 0;

@@ -937,6 +937,44 @@ void ClothPatch::record_substep(float h)
     // the reference's loop tests its exit conditions after the body, so it always
     // runs at least one iteration (Physics/ClothPBD.cpp:335-362)
     const int iterations = m.prm.iterations > 1 ? m.prm.iterations : 1;
+    int shift = 0;
+    size_t smem = 0;
+    const int cluster = m.prm.clusterSolver ? gs_cluster_size(m.N, shift, smem) : 0;
+    if (cluster > 0 && m.triColourStart.size() <= 65 && m.bendColourStart.size() <= 65)
+    {
+        GsPlan plan = {};
+        plan.iterations = iterations;
+        plan.shift = shift;
+        plan.nFemCol = (int)m.triColourStart.size() - 1;
+        plan.nBendCol = (int)m.bendColourStart.size() - 1;
+        for (size_t k = 0; k < m.triColourStart.size(); k++) plan.femStart[k] = m.triColourStart[k];
+        for (size_t k = 0; k < m.bendColourStart.size(); k++) plan.bendStart[k] = m.bendColourStart[k];
+        // records each CTA handles: per colour a contiguous chunk of ceil(count / cluster)
+        auto perCta = [&](const std::vector<int>& start) {
+            int most = 0;
+            for (int r = 0; r < cluster; r++)
+            {
+                int sum = 0;
+                for (size_t k = 0; k + 1 < start.size(); k++)
+                {
+                    const int cnt = start[k + 1] - start[k], chunk = (cnt + cluster - 1) / cluster;
+                    sum += std::max(0, std::min(chunk, cnt - r * chunk));
+                }
+                most = std::max(most, sum);
+            }
+            return most;
+        };
+        plan.femStage = perCta(m.triColourStart);
+        plan.bendStage = perCta(m.bendColourStart);
+        const size_t staged = smem + (size_t)plan.femStage * 3 * sizeof(float4) + (size_t)plan.bendStage * sizeof(uint4);
+        if (m.prm.stageRecords && staged <= (size_t)GS_SMEM_MAX)
+        {
+            plan.stage = 1;
+            smem = staged;
+        }
+        launch_gs_cluster(s, c, P, b, plan, cluster, smem);   // includes the velocity update
+        return;
+    }
     for (int k = 0; k < iterations; k++)
     {
         if (m.prm.fem)

@@ -96,6 +96,8 @@ struct HostParams
     float selfThreshold = 0.003f;
     int iterations = 50, flags = 0, bendFreq = 2;
     bool fem = false, dihedral = true, fixedIterations = false, ccd = false;
+    bool clusterSolver = true;   // cluster-resident solver when the cloth fits
+    bool stageRecords = true;    // cluster solver: constraint records in shared memory
 };
 
 struct FemHost { uint32_t i1, i2, i3; float du1, du2, dv1, dv2, det, invDet, lu0, lv0, su, sv, lu2, lv2, area; };

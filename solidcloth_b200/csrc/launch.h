@@ -79,6 +79,23 @@ void launch_compact_self(cudaStream_t s, const DevCloth& c, const Buffers& b, bo
 void launch_reset_gs(cudaStream_t s, const DevCloth& c);
 void launch_gs_exit_test(cudaStream_t s, const DevCloth& c, const SolverParams& P, int iter);
 
+// cluster-resident Gauss-Seidel solver (one cluster per cloth, one launch per substep)
+constexpr int GS_THREADS = 512;
+constexpr int GS_SMEM_MAX = 200 * 1024; // dynamic shared memory per CTA: particles + staged records
+struct GsPlan
+{
+    int iterations, shift, nFemCol, nBendCol;
+    int stage;               // 1: each CTA copies its constraint records to shared memory first
+    int femStage, bendStage; // records per CTA when staged (max over the cluster's CTAs)
+    int femStart[65];
+    int bendStart[65];
+};
+// cluster size usable for N particles (0: too large or unsupported); sets the
+// log2 particles-per-CTA and the dynamic shared memory per CTA
+int gs_cluster_size(int N, int& shift, size_t& smem);
+void launch_gs_cluster(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b, GsPlan plan,
+                       int clusterSize, size_t smem);
+
 // exclusive scan of n ints (out may alias nothing); total written to *total if not null
 void scan_ints(cudaStream_t s, const int* in, int* out, int n, int* total, int* tmp);
 

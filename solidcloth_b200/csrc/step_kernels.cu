@@ -13,7 +13,10 @@
 // the reference decides them. acosf/atan2f are CUDA's and may differ from glibc's
 // by a few ulp (bend angles, angle-weighted normals).
 #include "launch.h"
+#include <cooperative_groups.h>
 #include <cstdio>
+
+namespace cg = cooperative_groups;
 
 namespace sc {
 
@@ -28,6 +31,15 @@ __device__ __forceinline__ void atomic_max_pos(float* addr, float v)
     atomicMax((int*)addr, __float_as_int(v));
 }
 __device__ __forceinline__ bool gs_done(const DevCloth& c) { return c.scal[8] != 0.f; }
+
+// Particle positions as the projections see them: plain global memory here;
+// the cluster solver (gs_cluster.cu) substitutes distributed shared memory.
+struct GlobalPos
+{
+    float4* p;
+    __device__ __forceinline__ float4 ld(uint32_t v) const { return p[v]; }
+    __device__ __forceinline__ void st(uint32_t v, float4 x) const { p[v] = x; }
+};
 
 static inline int blocks_for(int n, int t = 256) { int b = (n + t - 1) / t; return b < 1 ? 1 : b; }
 
@@ -68,16 +80,13 @@ __global__ void k_velocity(DevCloth c, SolverParams P)
 // ------------------------------------------------------------ FEM sweep
 // ClothModelPBD::SolveTriangles for the triangles of one colour
 // (Physics/ClothPBD.cpp:52-108): warp and weft hard, shear compliant.
-__global__ void __launch_bounds__(256) k_fem(DevCloth c, SolverParams P, int first, int count)
+template <class PA>
+__device__ __forceinline__ void fem_project(const PA& pa, float4 r0, float4 r1, float4 r2, const SolverParams& P)
 {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= count || gs_done(c)) return;
-    k += first;
-    const float4 r0 = c.fem[3 * k], r1 = c.fem[3 * k + 1], r2 = c.fem[3 * k + 2];
     const uint32_t i1 = __float_as_uint(r0.x), i2 = __float_as_uint(r0.y), i3 = __float_as_uint(r0.z);
     const float du1 = r0.w, du2 = r1.x, dv1 = r1.y, dv2 = r1.z, invDet = r1.w;
     const float lu2 = r2.x, lv2 = r2.y, lu0lv0 = r2.z, area = r2.w;
-    float4 a = c.pos[i1], b = c.pos[i2], d = c.pos[i3];
+    float4 a = pa.ld(i1), b = pa.ld(i2), d = pa.ld(i3);
     V3 x1 = mk(a.x, a.y, a.z), x2 = mk(b.x, b.y, b.z), x3 = mk(d.x, d.y, d.z);
     const float w1 = a.w, w2 = b.w, w3 = d.w;
     V3 dx1 = x2 - x1, dx2 = x3 - x1;
@@ -110,22 +119,29 @@ __global__ void __launch_bounds__(256) k_fem(DevCloth c, SolverParams P, int fir
     float s = 1.f / (1.f + lu0lv0 * P.epsUV / (diag * P.h2 * area));
     lambda = -s * err / diag;
     x1 += (w1 * lambda) * q1; x2 += (w2 * lambda) * q2; x3 += (w3 * lambda) * q3;
-    c.pos[i1] = make_float4(x1.x, x1.y, x1.z, w1);
-    c.pos[i2] = make_float4(x2.x, x2.y, x2.z, w2);
-    c.pos[i3] = make_float4(x3.x, x3.y, x3.z, w3);
+    pa.st(i1, make_float4(x1.x, x1.y, x1.z, w1));
+    pa.st(i2, make_float4(x2.x, x2.y, x2.z, w2));
+    pa.st(i3, make_float4(x3.x, x3.y, x3.z, w3));
+}
+
+__global__ void __launch_bounds__(256) k_fem(DevCloth c, SolverParams P, int first, int count)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count || gs_done(c)) return;
+    k += first;
+    fem_project(GlobalPos{c.pos}, c.fem[3 * k], c.fem[3 * k + 1], c.fem[3 * k + 2], P);
 }
 
 // ---------------------------------------------------------- bend sweep
 // SolveBends + EvaluateAngle + EvaluateGradient for one colour
 // (Physics/ClothPBD.cpp:110-224).
-__global__ void __launch_bounds__(256) k_bends(DevCloth c, SolverParams P, int first, int count)
+// returns |error| of the projection, or -1 when the bend is skipped
+template <class PA>
+__device__ __forceinline__ float bend_project(const PA& pa, uint4 bc, const SolverParams& P)
 {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= count || gs_done(c)) return;
-    const uint4 bc = c.bend[first + k];
-    float4 a = c.pos[bc.x], b = c.pos[bc.y], d = c.pos[bc.z], e = c.pos[bc.w];
+    float4 a = pa.ld(bc.x), b = pa.ld(bc.y), d = pa.ld(bc.z), e = pa.ld(bc.w);
     const float m1 = a.w, m2 = b.w, m3 = d.w, m4 = e.w;
-    if (m1 + m2 + m3 + m4 == 0) return;
+    if (m1 + m2 + m3 + m4 == 0) return -1.f;
     V3 x1 = mk(a.x, a.y, a.z), x2 = mk(b.x, b.y, b.z), x3 = mk(d.x, d.y, d.z), x4 = mk(e.x, e.y, e.z);
     V3 x12 = x2 - x1;
     float l = len(x12);
@@ -144,7 +160,7 @@ __global__ void __launch_bounds__(256) k_bends(DevCloth c, SolverParams P, int f
         cosine = mn(1.f, mx(-1.f, cosine));
         theta = portable_acos(cosine);
     }
-    if (fabsf(cosine) >= 1 - 0.001f) return;
+    if (fabsf(cosine) >= 1 - 0.001f) return -1.f;
     float h1 = l1 / l, h2 = l2 / l;
     float he = 0.5f * (h1 + h2);
     float il1 = 1.f / l1, il2 = 1.f / l2;
@@ -157,16 +173,24 @@ __global__ void __launch_bounds__(256) k_bends(DevCloth c, SolverParams P, int f
     V3 q2 = (-il1 / sine / he) * cross(x13, n2p) + (il2 / sine / he) * cross(x14, n1p);
     V3 q1 = -q2 - q3 - q4;
     float diag = m1 * lensq(q1) + m2 * lensq(q2) + m3 * lensq(q3) + m4 * lensq(q4);
-    if (diag == 0) return;
+    if (diag == 0) return -1.f;
     float s = 0.0005f * P.bend;
     float errv = fabsf(s * theta);
     float lambda = -s * theta / he / diag;
     x1 += (lambda * m1) * q1; x2 += (lambda * m2) * q2; x3 += (lambda * m3) * q3; x4 += (lambda * m4) * q4;
-    c.pos[bc.x] = make_float4(x1.x, x1.y, x1.z, m1);
-    c.pos[bc.y] = make_float4(x2.x, x2.y, x2.z, m2);
-    c.pos[bc.z] = make_float4(x3.x, x3.y, x3.z, m3);
-    c.pos[bc.w] = make_float4(x4.x, x4.y, x4.z, m4);
-    if (!P.fixedIterations) atomic_max_pos(&c.scal[2], errv);
+    pa.st(bc.x, make_float4(x1.x, x1.y, x1.z, m1));
+    pa.st(bc.y, make_float4(x2.x, x2.y, x2.z, m2));
+    pa.st(bc.z, make_float4(x3.x, x3.y, x3.z, m3));
+    pa.st(bc.w, make_float4(x4.x, x4.y, x4.z, m4));
+    return errv;
+}
+
+__global__ void __launch_bounds__(256) k_bends(DevCloth c, SolverParams P, int first, int count)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count || gs_done(c)) return;
+    float errv = bend_project(GlobalPos{c.pos}, c.bend[first + k], P);
+    if (!P.fixedIterations && errv >= 0.f) atomic_max_pos(&c.scal[2], errv);
 }
 
 // ----------------------------------------------------------- normals
@@ -698,12 +722,11 @@ __device__ __forceinline__ V3 blended_normal(const DevMesh& m, int t, V3 w)
 // per particle processes that particle's contacts in list order (collider, slot),
 // which equals the reference's sequential order because every vertex contact
 // moves a single particle.
-__global__ void k_solve_vertex_contacts(DevCloth c, SolverParams P, Buffers b)
+template <class PA>
+__device__ __forceinline__ float vertex_contacts_one(const PA& pa, const DevCloth& c, const SolverParams& P, const Buffers& b, int i)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= c.N || gs_done(c)) return;
     float err = 0.f;
-    float4 p4 = c.pos[i];
+    float4 p4 = pa.ld(i);
     V3 p = mk(p4.x, p4.y, p4.z);
     const V3 q = ld3(c.prev, i);
     bool touched = false;
@@ -758,14 +781,23 @@ __global__ void k_solve_vertex_contacts(DevCloth c, SolverParams P, Buffers b)
             slot[k] = v;
         }
     }
-    if (touched) c.pos[i] = make_float4(p.x, p.y, p.z, p4.w);
+    if (touched) pa.st(i, make_float4(p.x, p.y, p.z, p4.w));
+    return err;
+}
+
+__global__ void k_solve_vertex_contacts(DevCloth c, SolverParams P, Buffers b)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.N || gs_done(c)) return;
+    float err = vertex_contacts_one(GlobalPos{c.pos}, c, P, b, i);
     if (!P.fixedIterations && err > 0.f) atomic_max_pos(&c.scal[3], err);
 }
 
 // SolveEdgeContacts for one contact (Physics/ClothCollisionHandler.cpp:289-362)
-__device__ float solve_edge_contact(const DevCloth& c, const SolverParams& P, const Buffers& b, EC& k)
+template <class PA>
+__device__ float solve_edge_contact(const PA& pa, const DevCloth& c, const SolverParams& P, const Buffers& b, EC& k)
 {
-    float4 a4 = c.pos[k.idx.x], b4 = c.pos[k.idx.y];
+    float4 a4 = pa.ld(k.idx.x), b4 = pa.ld(k.idx.y);
     V3 x1 = mk(a4.x, a4.y, a4.z), x2 = mk(b4.x, b4.y, b4.z);
     const float m1 = a4.w, m2 = b4.w;
     float w1 = k.w.x, w2 = k.w.y;
@@ -809,15 +841,16 @@ __device__ float solve_edge_contact(const DevCloth& c, const SolverParams& P, co
         }
     }
     x1 += disp * (w1 * m1); x2 += disp * (w2 * m2);
-    c.pos[k.idx.x] = make_float4(x1.x, x1.y, x1.z, m1);
-    c.pos[k.idx.y] = make_float4(x2.x, x2.y, x2.z, m2);
+    pa.st(k.idx.x, make_float4(x1.x, x1.y, x1.z, m1));
+    pa.st(k.idx.y, make_float4(x2.x, x2.y, x2.z, m2));
     return depth;
 }
 
 // SolveTriContacts for one contact (Physics/ClothCollisionHandler.cpp:204-287)
-__device__ float solve_tri_contact(const DevCloth& c, const SolverParams& P, const Buffers& b, TC& k)
+template <class PA>
+__device__ float solve_tri_contact(const PA& pa, const DevCloth& c, const SolverParams& P, const Buffers& b, TC& k)
 {
-    float4 a4 = c.pos[k.idx.x], b4 = c.pos[k.idx.y], c4 = c.pos[k.idx.z];
+    float4 a4 = pa.ld(k.idx.x), b4 = pa.ld(k.idx.y), c4 = pa.ld(k.idx.z);
     V3 x1 = mk(a4.x, a4.y, a4.z), x2 = mk(b4.x, b4.y, b4.z), x3 = mk(c4.x, c4.y, c4.z);
     const float m1 = a4.w, m2 = b4.w, m3 = c4.w;
     V3 point = mk(k.point.x, k.point.y, k.point.z);
@@ -861,18 +894,19 @@ __device__ float solve_tri_contact(const DevCloth& c, const SolverParams& P, con
         }
     }
     x1 += disp * (w1 * m1); x2 += disp * (w2 * m2); x3 += disp * (w3 * m3);
-    c.pos[k.idx.x] = make_float4(x1.x, x1.y, x1.z, m1);
-    c.pos[k.idx.y] = make_float4(x2.x, x2.y, x2.z, m2);
-    c.pos[k.idx.z] = make_float4(x3.x, x3.y, x3.z, m3);
+    pa.st(k.idx.x, make_float4(x1.x, x1.y, x1.z, m1));
+    pa.st(k.idx.y, make_float4(x2.x, x2.y, x2.z, m2));
+    pa.st(k.idx.z, make_float4(x3.x, x3.y, x3.z, m3));
     return depth;
 }
 
 // SolveSelfTrisPosition for one contact (Physics/ClothCollisionHandler.cpp:364-450)
-__device__ float solve_self_tri(const DevCloth& c, const SolverParams& P, SCt& k)
+template <class PA>
+__device__ float solve_self_tri(const PA& pa, const DevCloth& c, const SolverParams& P, SCt& k)
 {
     const float soften = .9f;
     float len0 = P.thickness * P.selfShrink;
-    float4 a4 = c.pos[k.idx.x], b4 = c.pos[k.idx.y], c4 = c.pos[k.idx.z], d4 = c.pos[k.idx.w];
+    float4 a4 = pa.ld(k.idx.x), b4 = pa.ld(k.idx.y), c4 = pa.ld(k.idx.z), d4 = pa.ld(k.idx.w);
     V3 x1 = mk(a4.x, a4.y, a4.z), x2 = mk(b4.x, b4.y, b4.z), x3 = mk(c4.x, c4.y, c4.z), x4 = mk(d4.x, d4.y, d4.z);
     const float m1 = a4.w, m2 = b4.w, m3 = c4.w, m4 = d4.w;
     V3 p, coords;
@@ -898,19 +932,20 @@ __device__ float solve_self_tri(const DevCloth& c, const SolverParams& P, SCt& k
     x2 += disp * (w2 * m2);
     x3 += disp * (w3 * m3);
     x4 -= disp * m4;
-    c.pos[k.idx.x] = make_float4(x1.x, x1.y, x1.z, m1);
-    c.pos[k.idx.y] = make_float4(x2.x, x2.y, x2.z, m2);
-    c.pos[k.idx.z] = make_float4(x3.x, x3.y, x3.z, m3);
-    c.pos[k.idx.w] = make_float4(x4.x, x4.y, x4.z, m4);
+    pa.st(k.idx.x, make_float4(x1.x, x1.y, x1.z, m1));
+    pa.st(k.idx.y, make_float4(x2.x, x2.y, x2.z, m2));
+    pa.st(k.idx.z, make_float4(x3.x, x3.y, x3.z, m3));
+    pa.st(k.idx.w, make_float4(x4.x, x4.y, x4.z, m4));
     return absErr;
 }
 
 // SolveSelfEdgesPosition for one contact (Physics/ClothCollisionHandler.cpp:453-542)
-__device__ float solve_self_edge(const DevCloth& c, const SolverParams& P, SCt& k)
+template <class PA>
+__device__ float solve_self_edge(const PA& pa, const DevCloth& c, const SolverParams& P, SCt& k)
 {
     float thick = P.thickness * P.selfShrink;
     const float soften = 0.9f;
-    float4 a4 = c.pos[k.idx.x], b4 = c.pos[k.idx.y], c4 = c.pos[k.idx.z], d4 = c.pos[k.idx.w];
+    float4 a4 = pa.ld(k.idx.x), b4 = pa.ld(k.idx.y), c4 = pa.ld(k.idx.z), d4 = pa.ld(k.idx.w);
     V3 x1 = mk(a4.x, a4.y, a4.z), x2 = mk(b4.x, b4.y, b4.z), x3 = mk(c4.x, c4.y, c4.z), x4 = mk(d4.x, d4.y, d4.z);
     const float m1 = a4.w, m2 = b4.w, m3 = c4.w, m4 = d4.w;
     float side = signed_volume(x1, x2, x3, x4);
@@ -938,10 +973,10 @@ __device__ float solve_self_edge(const DevCloth& c, const SolverParams& P, SCt& 
     x2 -= disp * (w1 * m2);
     x3 += disp * (omw2 * m3);
     x4 += disp * (w2 * m4);
-    c.pos[k.idx.x] = make_float4(x1.x, x1.y, x1.z, m1);
-    c.pos[k.idx.y] = make_float4(x2.x, x2.y, x2.z, m2);
-    c.pos[k.idx.z] = make_float4(x3.x, x3.y, x3.z, m3);
-    c.pos[k.idx.w] = make_float4(x4.x, x4.y, x4.z, m4);
+    pa.st(k.idx.x, make_float4(x1.x, x1.y, x1.z, m1));
+    pa.st(k.idx.y, make_float4(x2.x, x2.y, x2.z, m2));
+    pa.st(k.idx.z, make_float4(x3.x, x3.y, x3.z, m3));
+    pa.st(k.idx.w, make_float4(x4.x, x4.y, x4.z, m4));
     return absErr;
 }
 
@@ -1055,6 +1090,18 @@ __global__ void __launch_bounds__(1024) k_colour(DevCloth c, Buffers b, ColourAr
     for (int k = 0; k < 4; k++) colour_class(b, a.cls[k], c.status);
 }
 
+// one contact of class cls (0 edge, 1 triangle, 2 self VT, 3 self EE)
+template <class PA>
+__device__ __forceinline__ float solve_contact(const PA& pa, const DevCloth& c, const SolverParams& P, const Buffers& b, int cls, int i)
+{
+    float e;
+    if (cls == 0) { EC k = b.ecList[i]; e = solve_edge_contact(pa, c, P, b, k); b.ecList[i] = k; }
+    else if (cls == 1) { TC k = b.tcList[i]; e = solve_tri_contact(pa, c, P, b, k); b.tcList[i] = k; }
+    else if (cls == 2) { SCt k = b.stList[i]; e = solve_self_tri(pa, c, P, k); b.stList[i] = k; }
+    else { SCt k = b.seList[i]; e = solve_self_edge(pa, c, P, k); b.seList[i] = k; }
+    return e;
+}
+
 // The multi-particle contact classes in the reference's order within one GS
 // iteration: edge, triangle, self vertex-triangle, self edge-edge
 // (Physics/ClothPBD.cpp:349-352). One CTA; one __syncthreads per colour.
@@ -1082,11 +1129,7 @@ __global__ void __launch_bounds__(1024) k_solve_multi(DevCloth c, SolverParams P
                 if (serial && threadIdx.x != 0) break;
                 if (serial && cv.colour[j] != MAX_COLOURS - 1) continue;
                 int i = serial ? j : cv.order[j];
-                float e;
-                if (cls == 0) { EC k = b.ecList[i]; e = solve_edge_contact(c, P, b, k); b.ecList[i] = k; }
-                else if (cls == 1) { TC k = b.tcList[i]; e = solve_tri_contact(c, P, b, k); b.tcList[i] = k; }
-                else if (cls == 2) { SCt k = b.stList[i]; e = solve_self_tri(c, P, k); b.stList[i] = k; }
-                else { SCt k = b.seList[i]; e = solve_self_edge(c, P, k); b.seList[i] = k; }
+                float e = solve_contact(GlobalPos{c.pos}, c, P, b, cls, i);
                 if (e > 0.f) atomicMax((int*)&sErr[cls], __float_as_int(e));
             }
             __syncthreads();
@@ -1742,6 +1785,258 @@ __global__ void k_ccd_narrow_ee(DevCloth c, SolverParams P, Buffers b)
     rec.error = 0.f;
     b.ccdEeRec[k] = rec;
     b.ccdEeHit[k] = 1;
+}
+
+// ------------------------------------------------- cluster-resident solver
+// The whole Gauss-Seidel loop of one substep (SolveGS, Physics/ClothPBD.cpp:324-369)
+// plus the velocity update in ONE launch of ONE thread-block cluster. Every CTA
+// owns a power-of-two block of particles and keeps their positions in its shared
+// memory for the whole solve; a projection reaches any particle through the
+// cluster's distributed shared memory (mapa + ld/st.shared::cluster). Colours
+// are separated by hardware cluster barriers instead of kernel boundaries.
+// Constraint records stream from global memory (L2-resident at these sizes).
+// The phase structure is identical to the per-colour kernels, so results are
+// bit-identical to them.
+static ColourArgs colour_args(const Buffers& b);
+
+struct ClusterPos
+{
+    float4* local;
+    uint32_t shift, mask;
+    __device__ __forceinline__ float4* addr(uint32_t v) const
+    {
+        return cg::this_cluster().map_shared_rank(local + (v & mask), v >> shift);
+    }
+    __device__ __forceinline__ float4 ld(uint32_t v) const { return *addr(v); }
+    __device__ __forceinline__ void st(uint32_t v, float4 x) const { *addr(v) = x; }
+};
+
+__global__ void __launch_bounds__(GS_THREADS) k_gs_cluster(DevCloth c, SolverParams P, Buffers b, ColourArgs ca, GsPlan plan)
+{
+    extern __shared__ float4 sPos[];
+    __shared__ float sErr[8];
+    cg::cluster_group cl = cg::this_cluster();
+    const int rank = (int)cl.block_rank();
+    const int nRank = (int)cl.num_blocks();
+    const uint32_t vpc = 1u << plan.shift;
+    const int v0 = rank * (int)vpc;
+    for (uint32_t v = threadIdx.x; v < vpc; v += blockDim.x)
+    {
+        int g = v0 + (int)v;
+        if (g < c.N) sPos[v] = c.pos[g];
+    }
+    if (threadIdx.x < 8) sErr[threadIdx.x] = 0.f;
+    // split [s0, s1) into nRank contiguous chunks (contiguous constraints are
+    // spatially close, so most particle accesses stay in the CTA's own block)
+    auto range = [&](int s0, int s1, int& a, int& e) {
+        const int chunk = (s1 - s0 + nRank - 1) / nRank;
+        a = s0 + rank * chunk;
+        e = min(s1, a + chunk);
+    };
+    // staged records: this CTA's chunks of every colour, copied once per substep
+    // (layout after the particle block: FEM records, then bends)
+    __shared__ int sFemOff[65], sBendOff[65];
+    float4* sFem = sPos + vpc;
+    uint4* sBend = reinterpret_cast<uint4*>(sFem + 3 * plan.femStage);
+    if (threadIdx.x == 0)
+    {
+        int acc = 0;
+        for (int col = 0; col < plan.nFemCol; col++)
+        {
+            int a, e;
+            range(plan.femStart[col], plan.femStart[col + 1], a, e);
+            sFemOff[col] = acc;
+            acc += max(0, e - a);
+        }
+        acc = 0;
+        for (int col = 0; col < plan.nBendCol; col++)
+        {
+            int a, e;
+            range(plan.bendStart[col], plan.bendStart[col + 1], a, e);
+            sBendOff[col] = acc;
+            acc += max(0, e - a);
+        }
+    }
+    __syncthreads();
+    if (plan.stage)
+    {
+        for (int col = 0; col < plan.nFemCol; col++)
+        {
+            int a, e;
+            range(plan.femStart[col], plan.femStart[col + 1], a, e);
+            for (int j = a * 3 + threadIdx.x; j < e * 3; j += blockDim.x) sFem[3 * sFemOff[col] + (j - 3 * a)] = c.fem[j];
+        }
+        for (int col = 0; col < plan.nBendCol; col++)
+        {
+            int a, e;
+            range(plan.bendStart[col], plan.bendStart[col + 1], a, e);
+            for (int j = a + threadIdx.x; j < e; j += blockDim.x) sBend[sBendOff[col] + (j - a)] = c.bend[j];
+        }
+    }
+    cl.sync();
+    const ClusterPos pa{sPos, (uint32_t)plan.shift, vpc - 1};
+    const bool track = !P.fixedIterations;
+    for (int k = 0; k < plan.iterations; k++)
+    {
+        if (P.fem)
+            for (int col = 0; col < plan.nFemCol; col++)
+            {
+                int a, e;
+                range(plan.femStart[col], plan.femStart[col + 1], a, e);
+                for (int j = a + threadIdx.x; j < e; j += blockDim.x)
+                {
+                    if (plan.stage)
+                    {
+                        const float4* r = sFem + 3 * (sFemOff[col] + (j - a));
+                        fem_project(pa, r[0], r[1], r[2], P);
+                    }
+                    else
+                        fem_project(pa, c.fem[3 * j], c.fem[3 * j + 1], c.fem[3 * j + 2], P);
+                }
+                cl.sync();
+            }
+        if (P.dihedral && k % P.bendFreq == 0)
+            for (int col = 0; col < plan.nBendCol; col++)
+            {
+                int a, e;
+                range(plan.bendStart[col], plan.bendStart[col + 1], a, e);
+                for (int j = a + threadIdx.x; j < e; j += blockDim.x)
+                {
+                    float errv = bend_project(pa, plan.stage ? sBend[sBendOff[col] + (j - a)] : c.bend[j], P);
+                    if (track && errv > 0.f) atomicMax((int*)&sErr[2], __float_as_int(errv));
+                }
+                cl.sync();
+            }
+        if (b.numVColl > 0)
+        {
+            // each CTA solves the vertex contacts of its own particles
+            for (uint32_t v = threadIdx.x; v < vpc; v += blockDim.x)
+            {
+                const int g = v0 + (int)v;
+                if (g >= c.N) continue;
+                float err = vertex_contacts_one(pa, c, P, b, g);
+                if (track && err > 0.f) atomicMax((int*)&sErr[3], __float_as_int(err));
+            }
+            cl.sync();
+        }
+        for (int cls = 0; cls < 4; cls++)
+        {
+            const ClassView& cv = ca.cls[cls];
+            const int n = *cv.count;
+            if (n == 0) continue;
+            for (int col = 0; col < MAX_COLOURS; col++)
+            {
+                const int s0 = cv.start[col], s1 = cv.start[col + 1];
+                if (s0 == s1) continue;
+                if (col == MAX_COLOURS - 1)
+                {
+                    // colours exhausted: one thread, list order (as the oracle)
+                    if (rank == 0 && threadIdx.x == 0)
+                        for (int i = 0; i < n; i++)
+                            if (cv.colour[i] == MAX_COLOURS - 1)
+                            {
+                                float e = solve_contact(pa, c, P, b, cls, i);
+                                if (track && e > 0.f) atomicMax((int*)&sErr[4 + cls], __float_as_int(e));
+                            }
+                }
+                else
+                {
+                    int a, e;
+                    range(s0, s1, a, e);
+                    for (int j = a + threadIdx.x; j < e; j += blockDim.x)
+                    {
+                        float err = solve_contact(pa, c, P, b, cls, cv.order[j]);
+                        if (track && err > 0.f) atomicMax((int*)&sErr[4 + cls], __float_as_int(err));
+                    }
+                }
+                cl.sync();
+            }
+        }
+        if (threadIdx.x == 0 && rank == 0) c.scal[9] = (float)(k + 1);
+        if (track)
+        {
+            // SolveGS exit test (Physics/ClothPBD.cpp:354-361) on cluster-wide maxima
+            if (threadIdx.x < 8 && threadIdx.x >= 2 && sErr[threadIdx.x] > 0.f)
+                atomic_max_pos(&c.scal[threadIdx.x], sErr[threadIdx.x]);
+            cl.sync();
+            if (rank == 0 && threadIdx.x == 0)
+            {
+                const float eps = 0.01f;
+                float cb = c.scal[2], cv = c.scal[3], ce = c.scal[4], ct = c.scal[5], sct = c.scal[6], see = c.scal[7];
+                if (cb < 0.005f && see < P.selfThreshold && sct < P.selfThreshold && cv < eps && ce < eps && ct < eps)
+                    c.scal[8] = 1.f;
+                for (int s = 3; s < 8; s++) c.scal[s] = 0.f;          // per-iteration maxima
+                if ((k + 1) % P.bendFreq == 0) c.scal[2] = 0.f;       // recomputed by the next bend sweep
+            }
+            if (threadIdx.x < 8) sErr[threadIdx.x] = 0.f;
+            cl.sync();
+            if (__ldcg(&c.scal[8]) != 0.f) break;
+        }
+    }
+    // write back own particles and update their velocities (ClothPBD.cpp:314-321)
+    for (uint32_t v = threadIdx.x; v < vpc; v += blockDim.x)
+    {
+        const int g = v0 + (int)v;
+        if (g >= c.N) continue;
+        const float4 p = sPos[v];
+        c.pos[g] = p;
+        if (p.w == 0.f) continue;
+        const float4 q = c.prev[g];
+        V3 vel = P.invH * (mk(p.x, p.y, p.z) - mk(q.x, q.y, q.z));
+        c.vel[g] = make_float4(vel.x, vel.y, vel.z, 0.f);
+    }
+}
+
+int gs_cluster_size(int N, int& shift, size_t& smem)
+{
+    static int supported = -1;
+    if (supported < 0)
+    {
+        supported = 0;
+        cudaFuncSetAttribute(k_gs_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        cudaFuncSetAttribute(k_gs_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, GS_SMEM_MAX);
+        for (int cs : {16, 8})
+        {
+            cudaLaunchConfig_t cfg = {};
+            cfg.gridDim = dim3(cs);
+            cfg.blockDim = dim3(GS_THREADS);
+            cfg.dynamicSmemBytes = GS_SMEM_MAX;
+            cudaLaunchAttribute at;
+            at.id = cudaLaunchAttributeClusterDimension;
+            at.val.clusterDim.x = cs; at.val.clusterDim.y = 1; at.val.clusterDim.z = 1;
+            cfg.attrs = &at; cfg.numAttrs = 1;
+            int clusters = 0;
+            if (cudaOccupancyMaxActiveClusters(&clusters, k_gs_cluster, &cfg) == cudaSuccess && clusters > 0)
+            {
+                supported = cs;
+                break;
+            }
+        }
+        cudaGetLastError();
+    }
+    if (supported == 0) return 0;
+    const int cs = supported;
+    int vpc = 1, sh = 0;
+    while (vpc * cs < N) { vpc <<= 1; sh++; }
+    if ((size_t)vpc * sizeof(float4) > 128 * 1024) return 0;
+    shift = sh;
+    smem = (size_t)vpc * sizeof(float4);
+    return cs;
+}
+
+void launch_gs_cluster(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b, GsPlan plan,
+                       int clusterSize, size_t smem)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(clusterSize);
+    cfg.blockDim = dim3(GS_THREADS);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at;
+    at.id = cudaLaunchAttributeClusterDimension;
+    at.val.clusterDim.x = clusterSize; at.val.clusterDim.y = 1; at.val.clusterDim.z = 1;
+    cfg.attrs = &at; cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_gs_cluster, c, P, b, colour_args(b), plan);
 }
 
 // ------------------------------------------------------------- launchers

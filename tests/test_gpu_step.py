@@ -189,3 +189,54 @@ def test_ccd_broadphase_and_hits_bitexact():
     # this stress case needs more colouring rounds than the parallel schedule
     # keeps (bit 16): the rest is solved serially in list order, as the oracle does
     assert p.status() & ~16 == 0
+
+
+@pytest.mark.parametrize("scene", ["cfg0", "sdf", "fold", "ccd"])
+def test_cluster_solver_equals_per_colour_kernels(scene):
+    """The cluster-resident solver (one launch per substep, particles in
+    distributed shared memory, records staged in shared memory or read from
+    global memory) and the one-kernel-per-colour path are the same algorithm in
+    the same order: bit-identical trajectories."""
+    from solidcloth_b200 import api
+    state = None
+    if scene == "cfg0":
+        sc = scenes.cfg0()
+    elif scene == "sdf":
+        sc = _sdf_scene()
+        sc.params.substeps = 4
+    elif scene == "fold":
+        sc = scenes.cfg1(n=16, self_mode="proximity")
+        sc.sdfs.clear()
+        sc.params.substeps = 2
+        state = scenes.folded(sc, gap=0.004)
+    else:
+        sc, state = scenes.ccd_scene(16)
+    out = []
+    for cluster, staged in ((True, True), (True, False), (False, False)):
+        w, p = api.load_scene(sc)
+        p.model.set_cluster_solver(cluster)
+        p.model.set_cluster_staging(staged)
+        if state is not None:
+            p.model.set_state(*state)
+        for _ in range(4):
+            p.step(sc.dt)
+            p.update_mesh()
+        out.append((p.model.positions(), p.model.velocities(), p.status() & ~16))
+        p.free()
+    for o in out:
+        assert o[2] == 0
+    for o in out[1:]:
+        assert _same(out[0][0], o[0]) and _same(out[0][1], o[1])
+
+
+def test_early_exit_mode_matches_oracle():
+    """Without fixed iterations the reference's exit test (Physics/ClothPBD.cpp:357)
+    decides the iteration count; FEM without contacts exits after one iteration."""
+    sc = scenes.cfg0()
+    sc.params.fixed_iterations = False
+    w, p, o = _pair(sc)
+    for f in range(5):
+        p.step(sc.dt)
+        o.step(sc.dt)
+        assert _same(p.model.positions(), o.positions()), f
+    assert p.model.solver_iterations() >= 1
