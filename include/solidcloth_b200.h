@@ -206,7 +206,8 @@ SCEXP void scGetTriContacts(scModel model, int* idx4, float* f9);
 /* edge contacts: idx3 = i1 i2 feature; f8 = point normal w1 w2 */
 SCEXP void scGetEdgeContacts(scModel model, int* idx3, float* f8);
 /* continuous-collision broad-phase pairs of the last substep:
-   kind 0 -> (vertex, triangle), kind 1 -> (edge, edge); returns the count */
+   kind 0 -> (vertex, triangle), kind 1 -> (edge, edge), sorted; returns the number
+   of pairs held (a list longer than the pair store sets status bit 4) */
 SCEXP int scGetCCDCandidates(scModel model, int kind, int* pairs, int cap);
 /* contact classes of the last substep (0 edge, 1 triangle, 2 self vertex-triangle,
    3 self edge-edge): writes the per-colour counts of the independent-set

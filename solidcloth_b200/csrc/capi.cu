@@ -3,6 +3,7 @@
 #include "cloth.h"
 #include "../../include/solidcloth_b200.h"
 #include <cstring>
+#include <algorithm>
 #include <cmath>
 
 using namespace sc;
@@ -528,9 +529,14 @@ int scGetCCDCandidates(scModel m, int kind, int* pairs, int cap)
     host_sync(c);
     int n = dcount(kind == 0 ? c->buf.ccdVtPairCount : c->buf.ccdEePairCount);
     int lim = kind == 0 ? c->buf.ccdVtCap : c->buf.ccdEeCap;
-    int k = std::min(std::min(n, lim), cap);
-    if (pairs && k > 0)
-        cudaMemcpy(pairs, kind == 0 ? c->buf.ccdVtPairs : c->buf.ccdEePairs, sizeof(int2) * k, cudaMemcpyDeviceToHost);
+    n = std::min(n, lim);
+    if (pairs && n > 0 && cap > 0)
+    {
+        // the device keeps each query's candidates in traversal order; report them sorted
+        std::vector<int2> all = dl(kind == 0 ? c->buf.ccdVtPairs : c->buf.ccdEePairs, n);
+        std::sort(all.begin(), all.end(), [](int2 a, int2 b) { return a.x < b.x || (a.x == b.x && a.y < b.y); });
+        memcpy(pairs, all.data(), sizeof(int2) * std::min(n, cap));
+    }
     return n;
 }
 

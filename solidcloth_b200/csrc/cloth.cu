@@ -349,13 +349,12 @@ static uint32_t expand_bits(uint32_t v)
 // splits (balanced), nodes emitted in depth-first preorder so traversal needs
 // no stack (escape index = first node after the subtree). The topology is
 // built once from the rest shape; every substep only refits the boxes.
-void LBVHHost::build(const std::vector<V3>& cen)
+// primitives sorted by the 30-bit Morton code of their centroid in the set's bounds
+static std::vector<int> morton_order(const std::vector<V3>& cen)
 {
     const int n = (int)cen.size();
-    numLeaves = n;
-    numNodes = n > 0 ? 2 * n - 1 : 0;
-    child.assign(numNodes, 0); escape.assign(numNodes, 0); parent.assign(numNodes, -1); leafNode.assign(n, 0);
-    if (n == 0) return;
+    std::vector<int> out(n);
+    if (n == 0) return out;
     V3 lo = cen[0], hi = cen[0];
     for (const V3& c : cen) { lo = vmin(lo, c); hi = vmax(hi, c); }
     std::vector<std::pair<uint32_t, int>> key(n);
@@ -371,6 +370,20 @@ void LBVHHost::build(const std::vector<V3>& cen)
         key[i] = {m, i};
     }
     std::sort(key.begin(), key.end());
+    for (int i = 0; i < n; i++) out[i] = key[i].second;
+    return out;
+}
+
+void LBVHHost::build(const std::vector<V3>& cen)
+{
+    const int n = (int)cen.size();
+    numLeaves = n;
+    numNodes = n > 0 ? 2 * n - 1 : 0;
+    child.assign(numNodes, 0); escape.assign(numNodes, 0); parent.assign(numNodes, -1); leafNode.assign(n, 0);
+    if (n == 0) return;
+    const std::vector<int> order = morton_order(cen);
+    std::vector<std::pair<uint32_t, int>> key(n);
+    for (int i = 0; i < n; i++) key[i] = {0u, order[i]};
     int next = 0;
     // iterative preorder build over (range, parent, is-right-child) jobs
     struct Job { int lo, hi, par; bool right; };
@@ -394,6 +407,10 @@ void LBVHHost::build(const std::vector<V3>& cen)
         jobs.push_back({mid, j.hi, node, true});
         jobs.push_back({j.lo, mid, node, false});
     }
+    // children follow their parent in preorder, so a reverse sweep sees them first
+    maxPrim.assign(numNodes, -1);
+    for (int k = numNodes - 1; k >= 0; k--)
+        maxPrim[k] = child[k] < 0 ? ~child[k] : std::max(maxPrim[k + 1], maxPrim[child[k]]);
 }
 
 // ------------------------------------------------------------------ model
@@ -560,6 +577,17 @@ bool ClothModel::upload_topology(const HMesh& mesh)
     uint8_t* dborder = (uint8_t*)dalloc(N);
     SC_CUDA(cudaMemcpy(dborder, border.data(), N, cudaMemcpyHostToDevice));
     dc.vBorder = dborder;
+    {
+        // query orders for the warp-packet traversals: spatially adjacent queries
+        // share a warp (vertices by Morton code; edges in the edge tree's leaf order)
+        std::vector<V3> ec(E);
+        for (int e = 0; e < E; e++) ec[e] = 0.5f * (hpos[mesh.edges[e].i1] + hpos[mesh.edges[e].i2]);
+        std::vector<int> vq = morton_order(hpos), eq = morton_order(ec);
+        int* d = (int*)dalloc(sizeof(int) * ((size_t)N + E + 2));
+        SC_CUDA(cudaMemcpy(d, vq.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
+        if (E) SC_CUDA(cudaMemcpy(d + N, eq.data(), sizeof(int) * E, cudaMemcpyHostToDevice));
+        dc.vQuery = d; dc.eQuery = d + N;
+    }
     dc.prevN = (float4*)dalloc(sizeof(float4) * N);
     dc.prevTriN = (float4*)dalloc(sizeof(float4) * T);
     dc.meshN = (float4*)dalloc(sizeof(float4) * N);
@@ -585,19 +613,31 @@ bool ClothModel::upload_topology(const HMesh& mesh)
         out.numLeaves = h.numLeaves; out.numNodes = h.numNodes;
         if (shareTopo)
         {
-            out.child = shareTopo->child; out.escape = shareTopo->escape; out.parent = shareTopo->parent; out.leafNode = shareTopo->leafNode;
+            out.child = shareTopo->child; out.escape = shareTopo->escape; out.parent = shareTopo->parent;
+            out.leafNode = shareTopo->leafNode; out.maxPrim = shareTopo->maxPrim;
         }
         else
         {
-            int* d = (int*)dalloc(sizeof(int) * (3 * (size_t)h.numNodes + h.numLeaves + 4));
+            int* d = (int*)dalloc(sizeof(int) * (4 * (size_t)h.numNodes + h.numLeaves + 4));
             SC_CUDA(cudaMemcpy(d, h.child.data(), sizeof(int) * h.numNodes, cudaMemcpyHostToDevice));
             SC_CUDA(cudaMemcpy(d + h.numNodes, h.escape.data(), sizeof(int) * h.numNodes, cudaMemcpyHostToDevice));
             SC_CUDA(cudaMemcpy(d + 2 * h.numNodes, h.parent.data(), sizeof(int) * h.numNodes, cudaMemcpyHostToDevice));
-            SC_CUDA(cudaMemcpy(d + 3 * h.numNodes, h.leafNode.data(), sizeof(int) * h.numLeaves, cudaMemcpyHostToDevice));
-            out.child = d; out.escape = d + h.numNodes; out.parent = d + 2 * h.numNodes; out.leafNode = d + 3 * h.numNodes;
+            SC_CUDA(cudaMemcpy(d + 3 * h.numNodes, h.maxPrim.data(), sizeof(int) * h.numNodes, cudaMemcpyHostToDevice));
+            SC_CUDA(cudaMemcpy(d + 4 * h.numNodes, h.leafNode.data(), sizeof(int) * h.numLeaves, cudaMemcpyHostToDevice));
+            out.child = d; out.escape = d + h.numNodes; out.parent = d + 2 * h.numNodes;
+            out.maxPrim = d + 3 * h.numNodes; out.leafNode = d + 4 * h.numNodes;
+        }
+        // traversal reads a node's links from the w components of its box
+        std::vector<float4> lo(h.numNodes), hi(h.numNodes);
+        for (int k = 0; k < h.numNodes; k++)
+        {
+            lo[k] = make_float4(0.f, 0.f, 0.f, bits_f((uint32_t)h.child[k]));
+            hi[k] = make_float4(0.f, 0.f, 0.f, bits_f((uint32_t)h.escape[k]));
         }
         out.lo = (float4*)dalloc(sizeof(float4) * h.numNodes);
         out.hi = (float4*)dalloc(sizeof(float4) * h.numNodes);
+        SC_CUDA(cudaMemcpy(out.lo, lo.data(), sizeof(float4) * h.numNodes, cudaMemcpyHostToDevice));
+        SC_CUDA(cudaMemcpy(out.hi, hi.data(), sizeof(float4) * h.numNodes, cudaMemcpyHostToDevice));
         out.visit = (int*)dalloc(sizeof(int) * h.numNodes);
         return true;
     };
@@ -728,10 +768,10 @@ bool ClothModel::ensure_buffers(const CollisionWorld& world, cudaStream_t s)
     buf.ccdVtPairCount = counts + 4; buf.ccdEePairCount = counts + 5; buf.scanTot = counts + 8;
     // self contacts
     const bool self = (prm.flags & CF_SELF) != 0;
-    buf.ccdVtCap = ccd ? std::max(1, N * KCCD) : 1;
-    buf.ccdEeCap = ccd ? std::max(1, E * KCCD) : 1;
-    buf.stCap = (self ? N * KVT : 1) + (ccd ? buf.ccdVtCap : 0);
-    buf.seCap = (self ? E : 1) + (ccd ? buf.ccdEeCap : 0);
+    buf.ccdVtCap = ccd ? std::max(1, N * CCD_VT_PAIRS) : 1;
+    buf.ccdEeCap = ccd ? std::max(1, E * CCD_EE_PAIRS) : 1;
+    buf.stCap = (self ? N * KVT : 1) + (ccd ? N * CCD_VT_HITS : 0);
+    buf.seCap = (self ? E : 1) + (ccd ? E * CCD_EE_HITS : 0);
     buf.stCnt = (int*)dalloc(sizeof(int) * N, true);
     buf.stSlot = (SCt*)dalloc(sizeof(SCt) * (size_t)(self ? N * KVT : 1), true);
     buf.stList = (SCt*)dalloc(sizeof(SCt) * (size_t)buf.stCap, true);
@@ -744,10 +784,17 @@ bool ClothModel::ensure_buffers(const CollisionWorld& world, cudaStream_t s)
     buf.ccdEeCand = (int*)dalloc(sizeof(int) * (size_t)(ccd ? E * KCCD : 1), true);
     buf.ccdVtPairs = (int2*)dalloc(sizeof(int2) * (size_t)buf.ccdVtCap, true);
     buf.ccdEePairs = (int2*)dalloc(sizeof(int2) * (size_t)buf.ccdEeCap, true);
-    buf.ccdVtHit = (int*)dalloc(sizeof(int) * (size_t)buf.ccdVtCap, true);
-    buf.ccdEeHit = (int*)dalloc(sizeof(int) * (size_t)buf.ccdEeCap, true);
-    buf.ccdVtRec = (SCt*)dalloc(sizeof(SCt) * (size_t)buf.ccdVtCap, true);
-    buf.ccdEeRec = (SCt*)dalloc(sizeof(SCt) * (size_t)buf.ccdEeCap, true);
+    buf.ccdVtHit = (uint8_t*)dalloc((size_t)buf.ccdVtCap, true);
+    buf.ccdEeHit = (uint8_t*)dalloc((size_t)buf.ccdEeCap, true);
+    buf.ccdVtOff = (int*)dalloc(sizeof(int) * N, true);
+    buf.ccdEeOff = (int*)dalloc(sizeof(int) * E, true);
+    buf.ccdVtHitCnt = (int*)dalloc(sizeof(int) * N, true);
+    buf.ccdEeHitCnt = (int*)dalloc(sizeof(int) * E, true);
+    buf.ccdVtPoolOff = (int*)dalloc(sizeof(int) * N, true);
+    buf.ccdEePoolOff = (int*)dalloc(sizeof(int) * E, true);
+    buf.ccdPoolCap = ccd ? std::max(N, E) * KCCD / 2 : 1;
+    buf.ccdPool = (int*)dalloc(sizeof(int) * (size_t)buf.ccdPoolCap, true);
+    buf.ccdPoolUsed = counts + 6;
     // colouring
     buf.vmin = (unsigned long long*)dalloc(sizeof(unsigned long long) * N, true);
     SC_CUDA(cudaMemset(buf.vmin, 0xff, sizeof(unsigned long long) * N));
@@ -756,8 +803,7 @@ bool ClothModel::ensure_buffers(const CollisionWorld& world, cudaStream_t s)
     buf.order = (int*)dalloc(sizeof(int) * (size_t)buf.colourCap, true);
     buf.colourStart = (int*)dalloc(sizeof(int) * 4 * (MAX_COLOURS + 1), true);
     // scans
-    size_t maxScan = std::max<size_t>({(size_t)N, (size_t)E, (size_t)buf.tcCap, (size_t)buf.ecCap,
-                                       (size_t)buf.ccdVtCap, (size_t)buf.ccdEeCap});
+    size_t maxScan = std::max<size_t>({(size_t)N, (size_t)E, (size_t)buf.tcCap, (size_t)buf.ecCap});
     buf.scanOff = (int*)dalloc(sizeof(int) * (maxScan + 1), true);
     buf.scanBlock = (int*)dalloc(sizeof(int) * (maxScan / 1024 + 8), true);
     bufWorldVersion = world.version;
@@ -929,7 +975,7 @@ void ClothPatch::record_substep(float h)
         launch_bvh_refit(s, m.sweptEdgeBvh, c, 3, tol);
         launch_ccd(s, c, P, b, m.sweptTriBvh, m.sweptEdgeBvh);
     }
-    if (self || ccd) launch_compact_self(s, c, b, ccd);
+    if (self || ccd) launch_compact_self(s, c, P, b, ccd);
     else cudaMemsetAsync(b.stCount, 0, 2 * sizeof(int), s);
     launch_colour_contacts(s, c, b);
     // ClothModelPBD::SolveGS (Physics/ClothPBD.cpp:324-369)

@@ -104,7 +104,7 @@ struct FemHost { uint32_t i1, i2, i3; float du1, du2, dv1, dv2, det, invDet, lu0
 
 struct LBVHHost
 {
-    std::vector<int> child, escape, parent, leafNode;
+    std::vector<int> child, escape, parent, leafNode, maxPrim;
     int numLeaves = 0, numNodes = 0;
     void build(const std::vector<V3>& centroids);
 };

@@ -7,7 +7,9 @@ namespace sc {
 constexpr int KVT = 48;        // self vertex-triangle contact slots per vertex
 constexpr int KCAND = 256;     // BVH candidates kept per proximity query
 constexpr int KRES = 96;       // distinct features tracked per vertex for the dedup
-constexpr int KCCD = 64;       // continuous-collision candidates per query
+constexpr int KCCD = 128;      // continuous-collision candidates kept in a query's own slots
+constexpr int CCD_VT_PAIRS = 128, CCD_EE_PAIRS = 96; // pair store per vertex / edge
+constexpr int CCD_VT_HITS = 32, CCD_EE_HITS = 16;   // continuous contacts per vertex / edge
 constexpr int MAX_COLOURS = 128; // independent-set colouring rounds per contact class
 constexpr int WALL_SLOTS = 5;
 
@@ -49,7 +51,11 @@ struct Buffers
     // continuous collision
     int* ccdVtCnt; int* ccdVtCand; int* ccdEeCnt; int* ccdEeCand;
     int2* ccdVtPairs; int2* ccdEePairs; int* ccdVtPairCount; int* ccdEePairCount; int ccdVtCap, ccdEeCap;
-    int* ccdVtHit; SCt* ccdVtRec; int* ccdEeHit; SCt* ccdEeRec;
+    uint8_t* ccdVtHit; uint8_t* ccdEeHit;  // per pair: 1 if the narrow phase reports a contact
+    int* ccdVtOff; int* ccdEeOff;          // first pair of each query
+    int* ccdVtHitCnt; int* ccdEeHitCnt;    // hits per query
+    int* ccdPool; int ccdPoolCap; int* ccdPoolUsed;  // candidate lists longer than KCCD
+    int* ccdVtPoolOff; int* ccdEePoolOff;
     // colouring scratch
     unsigned long long* vmin;  // N, kept at ~0
     int* colour; int* order; int* colourStart; int colourCap;
@@ -75,7 +81,7 @@ void launch_self_proximity(cudaStream_t s, const DevCloth& c, const SolverParams
                            const DevBVH& triBvh, const DevBVH& edgeBvh);
 void launch_ccd(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b,
                 const DevBVH& triBvh, const DevBVH& edgeBvh);
-void launch_compact_self(cudaStream_t s, const DevCloth& c, const Buffers& b, bool ccd);
+void launch_compact_self(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b, bool ccd);
 void launch_reset_gs(cudaStream_t s, const DevCloth& c);
 void launch_gs_exit_test(cudaStream_t s, const DevCloth& c, const SolverParams& P, int iter);
 

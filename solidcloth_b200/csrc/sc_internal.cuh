@@ -57,6 +57,8 @@ struct DevCloth
     const int* vTriStart;       // N+1, incident (triangle, corner) sorted by triangle
     const int2* vTri;
     const uint8_t* vBorder;     // N, Mesh::IsBorderVertex
+    const int* vQuery;          // N: vertices in spatial (Morton, rest shape) order, for warp packets
+    const int* eQuery;          // E: edges in the edge tree's leaf order
     float4* prevN;              // collision mesh vertex normals (refreshed per frame)
     float4* prevTriN;           // collision mesh triangle normals
     float4* meshN;              // render mesh normals
@@ -74,8 +76,9 @@ struct DevBVH
     const int* escape;      // numNodes: preorder index after the subtree
     const int* parent;      // numNodes (root -1)
     const int* leafNode;    // numLeaves: primitive -> node index
-    float4* lo;             // numNodes (box min)
-    float4* hi;             // numNodes (box max)
+    const int* maxPrim;     // numNodes: largest primitive index in the subtree
+    float4* lo;             // numNodes: box min; w = child[] as int bits
+    float4* hi;             // numNodes: box max; w = escape[] as int bits
     int* visit;             // numNodes refit counters
 };
 

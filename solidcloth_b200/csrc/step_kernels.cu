@@ -15,6 +15,7 @@
 #include "launch.h"
 #include <cooperative_groups.h>
 #include <cstdio>
+#include <climits>
 
 namespace cg = cooperative_groups;
 
@@ -1293,8 +1294,8 @@ __global__ void k_bvh_refit(DevBVH t, DevCloth c, int kind, float tol)
     if (prim >= t.numLeaves) return;
     int node = t.leafNode[prim];
     Box b = leaf_box(c, kind, prim, tol);
-    t.lo[node] = f4(b.lo, 0.f);
-    t.hi[node] = f4(b.hi, 0.f);
+    t.lo[node] = f4(b.lo, __int_as_float(~prim));
+    t.hi[node] = f4(b.hi, __int_as_float(node + 1));
     __threadfence();
     int p = t.parent[node];
     while (p >= 0)
@@ -1304,34 +1305,59 @@ __global__ void k_bvh_refit(DevBVH t, DevCloth c, int kind, float tol)
         int l = p + 1, r = t.child[p];
         float4 al = __ldcg(&t.lo[l]), ar = __ldcg(&t.lo[r]), bl = __ldcg(&t.hi[l]), br = __ldcg(&t.hi[r]);
         V3 lo = vmin(mk(al.x, al.y, al.z), mk(ar.x, ar.y, ar.z)), hi = vmax(mk(bl.x, bl.y, bl.z), mk(br.x, br.y, br.z));
-        t.lo[p] = f4(lo, 0.f);
-        t.hi[p] = f4(hi, 0.f);
+        t.lo[p] = f4(lo, __int_as_float(r));
+        t.hi[p] = f4(hi, __int_as_float(t.escape[p]));
         __threadfence();
         p = t.parent[p];
     }
 }
 
-__device__ __forceinline__ bool node_overlap(const DevBVH& t, int node, const Box& q)
-{
-    float4 lo = t.lo[node], hi = t.hi[node];
-    return !(hi.x < q.lo.x || hi.y < q.lo.y || hi.z < q.lo.z || q.hi.x < lo.x || q.hi.y < lo.y || q.hi.z < lo.z);
-}
 
 // Stackless preorder traversal with escape indices; calls f(prim) for every
-// leaf whose box overlaps q (AabbOverlap3D on the leaf box itself).
+// leaf whose box overlaps q (AabbOverlap3D on the leaf box itself). A node is
+// one round trip: two 16-byte loads carry its box and its links. With above >= 0
+// subtrees holding only primitives <= above are skipped (the callers reject them).
 template <typename F>
-__device__ __forceinline__ void bvh_query(const DevBVH& t, const Box& q, F&& f)
+__device__ __forceinline__ void bvh_query(const DevBVH& t, const Box& q, F&& f, int above = -1)
 {
     int node = 0;
     while (node < t.numNodes)
     {
-        if (node_overlap(t, node, q))
+        const float4 lo = __ldg(&t.lo[node]), hi = __ldg(&t.hi[node]);
+        const int ch = __float_as_int(lo.w), esc = __float_as_int(hi.w);
+        bool hit = !(hi.x < q.lo.x || hi.y < q.lo.y || hi.z < q.lo.z || q.hi.x < lo.x || q.hi.y < lo.y || q.hi.z < lo.z);
+        if (above >= 0 && hit) hit = __ldg(&t.maxPrim[node]) > above;
+        if (hit)
         {
-            int ch = t.child[node];
-            if (ch < 0) { f(~ch); node = t.escape[node]; }
+            if (ch < 0) { f(~ch); node = esc; }
             else node = node + 1;
         }
-        else node = t.escape[node];
+        else node = esc;
+    }
+}
+
+// Warp-packet form of bvh_query: the 32 lanes hold spatially adjacent queries and
+// walk the tree together. A node is entered when any lane's box overlaps it
+// (ballot), so every step is one broadcast load and no lane diverges; each lane
+// still reports exactly the leaves its own box overlaps. Must be called by all
+// lanes of a warp (inactive lanes pass active = false).
+template <typename F>
+__device__ __forceinline__ void bvh_query_warp(const DevBVH& t, const Box& q, bool active, F&& f, int above = -1)
+{
+    int node = 0;
+    if (!__any_sync(0xffffffffu, active)) return;
+    while (node < t.numNodes)
+    {
+        const float4 lo = __ldg(&t.lo[node]), hi = __ldg(&t.hi[node]);
+        const int ch = __float_as_int(lo.w), esc = __float_as_int(hi.w);
+        bool hit = active && !(hi.x < q.lo.x || hi.y < q.lo.y || hi.z < q.lo.z || q.hi.x < lo.x || q.hi.y < lo.y || q.hi.z < lo.z);
+        if (above >= 0 && hit) hit = __ldg(&t.maxPrim[node]) > above;
+        if (__any_sync(0xffffffffu, hit))
+        {
+            if (ch < 0) { if (hit) f(~ch); node = esc; }
+            else node = node + 1;
+        }
+        else node = esc;
     }
 }
 
@@ -1533,7 +1559,7 @@ __global__ void __launch_bounds__(128) k_self_ee(DevCloth c, SolverParams P, Buf
         closest_segm_segm(p, q, ld3(c.prev, e2.x), ld3(c.prev, e2.y), ps, pm, cs, cm);
         float dist = len(cs - cm);
         if (dist != 0 && (dist < best || (dist == best && e < bestE))) { best = dist; bestE = e; }
-    });
+    }, i);
     if (bestE < 0) return;
     const int4 e2 = c.edge[bestE];
     const V3 a = ld3(c.prev, e2.x), bb = ld3(c.prev, e2.y);
@@ -1570,57 +1596,92 @@ __global__ void __launch_bounds__(128) k_self_ee(DevCloth c, SolverParams P, Buf
 // but over all pairs rather than same-leaf pairs only. Per-query candidate
 // lists are sorted so the pair list order is canonical: (vertex, triangle)
 // and (edge, higher edge).
-__global__ void __launch_bounds__(128) k_ccd_broad_vt(DevCloth c, SolverParams P, Buffers b, DevBVH tb, float tol)
+// Two passes, both through these kernels: the first keeps up to KCCD candidates
+// in the query's own slots and counts all of them; the second (pool = true) runs
+// only the queries that had more, storing their full lists in a shared pool.
+// Lists stay in traversal order: only the (rare) hits are put in candidate order.
+__device__ __forceinline__ int* ccd_pool_alloc(const Buffers& b, int m, int* poolOff, int* status)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= c.N) return;
-    b.ccdVtCnt[i] = 0;
+    const int base = atomicAdd(b.ccdPoolUsed, m);
+    if (base + m > b.ccdPoolCap)
+    {
+        atomicOr(status, ST_CCD_OVERFLOW);
+        *poolOff = -1;
+        return nullptr;
+    }
+    *poolOff = base;
+    return b.ccdPool + base;
+}
+
+__global__ void __launch_bounds__(128) k_ccd_broad_vt(DevCloth c, SolverParams P, Buffers b, DevBVH tb, float tol, bool pool)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g - (int)(threadIdx.x & 31) >= c.N) return;          // whole warp past the end
+    const int i = g < c.N ? c.vQuery[g] : 0;
+    bool active = g < c.N;
+    if (active && !pool) b.ccdVtCnt[i] = 0;
+    if (active && pool && b.ccdVtCnt[i] <= KCCD) active = false;
     float4 p4 = c.pos[i];
-    if (p4.w == 0.f) return;
+    if (p4.w == 0.f) active = false;
     Box vb = Box::empty(); vb.add(ld3(c.prev, i)); vb.add(mk(p4.x, p4.y, p4.z)); vb.extrude(tol);
     int* out = b.ccdVtCand + (size_t)i * KCCD;
     int n = 0;
-    bool ovf = false;
-    bvh_query(tb, vb, [&](int t) {
+    if (active && pool)
+    {
+        // second pass for a query with more than KCCD candidates: all of them into the pool
+        out = ccd_pool_alloc(b, b.ccdVtCnt[i], b.ccdVtPoolOff + i, c.status);
+        if (!out) { b.ccdVtCnt[i] = 0; active = false; }
+    }
+    bvh_query_warp(tb, vb, active, [&](int t) {
         if ((int)c.tri[3 * t] == i || (int)c.tri[3 * t + 1] == i || (int)c.tri[3 * t + 2] == i) return;
-        if (n < KCCD) out[n++] = t; else ovf = true;
+        if (pool || n < KCCD) out[n] = t;
+        n++;
     });
-    if (ovf) atomicOr(c.status, ST_CCD_OVERFLOW);
-    for (int a = 1; a < n; a++) { int v = out[a], j = a - 1; while (j >= 0 && out[j] > v) { out[j + 1] = out[j]; j--; } out[j + 1] = v; }
+    if (!active) return;
     b.ccdVtCnt[i] = n;
 }
 
-__global__ void __launch_bounds__(128) k_ccd_broad_ee(DevCloth c, SolverParams P, Buffers b, DevBVH eb, float tol)
+__global__ void __launch_bounds__(128) k_ccd_broad_ee(DevCloth c, SolverParams P, Buffers b, DevBVH eb, float tol, bool pool)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= c.E) return;
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g - (int)(threadIdx.x & 31) >= c.E) return;
+    const int i = g < c.E ? c.eQuery[g] : 0;
+    bool active = g < c.E;
+    if (active && pool && b.ccdEeCnt[i] <= KCCD) active = false;
+    int* out = b.ccdEeCand + (size_t)i * KCCD;
+    if (active && pool)
+    {
+        out = ccd_pool_alloc(b, b.ccdEeCnt[i], b.ccdEePoolOff + i, c.status);
+        if (!out) { b.ccdEeCnt[i] = 0; active = false; }
+    }
     const int4 e1 = c.edge[i];
     Box qb = Box::empty();
     qb.add(ld3(c.pos, e1.x)); qb.add(ld3(c.pos, e1.y)); qb.add(ld3(c.prev, e1.x)); qb.add(ld3(c.prev, e1.y));
     qb.extrude(tol);
-    int* out = b.ccdEeCand + (size_t)i * KCCD;
     int n = 0;
-    bool ovf = false;
-    bvh_query(eb, qb, [&](int e) {
+    bvh_query_warp(eb, qb, active, [&](int e) {
         if (e <= i) return;
         int4 e2 = c.edge[e];
         if (e1.x == e2.x || e1.y == e2.y || e1.x == e2.y || e1.y == e2.x) return;
-        if (n < KCCD) out[n++] = e; else ovf = true;
-    });
-    if (ovf) atomicOr(c.status, ST_CCD_OVERFLOW);
-    for (int a = 1; a < n; a++) { int v = out[a], j = a - 1; while (j >= 0 && out[j] > v) { out[j + 1] = out[j]; j--; } out[j + 1] = v; }
+        if (pool || n < KCCD) out[n] = e;
+        n++;
+    }, i);
+    if (!active) return;
     b.ccdEeCnt[i] = n;
 }
 
-// expand per-query candidate lists into the dense pair list
-__global__ void k_ccd_pairs(const int* cnt, const int* off, const int* cand, int n, int2* pairs, int cap, int* status)
+// expand per-query candidate lists (own slots, or the pool for long lists)
+// into the dense pair list; one warp per query, coalesced copies
+__global__ void k_ccd_pairs(const int* cnt, const int* off, const int* cand, const int* pool, const int* poolOff,
+                            int n, int2* pairs, int cap, int* status)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (i >= n) return;
-    int m = cnt[i], o = off[i];
-    for (int k = 0; k < m; k++)
+    const int m = cnt[i], o = off[i];
+    const int* src = m > KCCD ? pool + poolOff[i] : cand + (size_t)i * KCCD;
+    for (int k = lane; k < m; k += 32)
     {
-        if (o + k < cap) pairs[o + k] = make_int2(i, cand[(size_t)i * KCCD + k]);
+        if (o + k < cap) pairs[o + k] = make_int2(i, src[k]);
         else atomicOr(status, ST_CCD_OVERFLOW);
     }
 }
@@ -1715,76 +1776,140 @@ __device__ bool solve_cubic(V3 x1, V3 x2, V3 x3, V3 x4, V3 v1, V3 v2, V3 v3, V3 
     return coplanar;
 }
 
-// VertexTriangleTest + VertexTriangleCCD (SelfCollisionDetector.cpp:171-277)
-__global__ void k_ccd_narrow_vt(DevCloth c, SolverParams P, Buffers b)
+// VertexTriangleTest + VertexTriangleCCD (SelfCollisionDetector.cpp:171-277) for
+// pair k: 1 and the contact record on a hit, else 0
+__device__ int ccd_vt_test(const DevCloth& c, const SolverParams& P, const Buffers& b, int k, SCt& rec)
 {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    int n = *b.ccdVtPairCount;
-    if (n > b.ccdVtCap) n = b.ccdVtCap;
-    if (k >= n) return;
-    b.ccdVtHit[k] = 0;
     int2 pr = b.ccdVtPairs[k];
     const int vtx = pr.x, t = pr.y;
     const uint32_t i1 = c.tri[3 * t], i2 = c.tri[3 * t + 1], i3 = c.tri[3 * t + 2];
     V3 x1 = ld3(c.prev, i1), x2 = ld3(c.prev, i2), x3 = ld3(c.prev, i3), x4 = ld3(c.prev, vtx);
     V3 v1 = ld3(c.pos, i1) - x1, v2 = ld3(c.pos, i2) - x2, v3 = ld3(c.pos, i3) - x3, v4 = ld3(c.pos, vtx) - x4;
     float toi;
-    if (!solve_cubic(x1, x2, x3, x4, v1, v2, v3, v4, toi)) return;
+    if (!solve_cubic(x1, x2, x3, x4, v1, v2, v3, v4, toi)) return 0;
     V3 z1 = x1 + toi * v1, z2 = x2 + toi * v2, z3 = x3 + toi * v3, z4 = x4 + toi * v4;
     V3 coords, p;
     closest_point_triangle(z4, z1, z2, z3, p, coords);
     V3 delta = z4 - p;
     const float eps = 0.1f;
-    if (!(lensq(delta) < eps * eps)) return;
+    if (!(lensq(delta) < eps * eps)) return 0;
     V3 triNormal = normalized(cross(x2 - x1, x3 - x1));
     float side = dot(triNormal, x4 - x1);
     V3 nn = normalized(cross(z2 - z1, z3 - z1));
     if (side < 0) nn = -nn;
-    SCt rec;
     rec.idx = make_uint4(i1, i2, i3, vtx);
     rec.normal = f4(nn, 0.f);
     rec.w = make_float4(coords.x, coords.y, coords.z, 0.f);
     rec.side = signed_volume(x4, x1, x2, x3);
     rec.lam = make_float2(0.f, 0.f);
     rec.error = 0.f;
-    b.ccdVtRec[k] = rec;
-    b.ccdVtHit[k] = 1;
+    return 1;
 }
 
-// EdgeEdgeTest + EdgeEdgeCCD (SelfCollisionDetector.cpp:491-606)
-__global__ void k_ccd_narrow_ee(DevCloth c, SolverParams P, Buffers b)
+// EdgeEdgeTest + EdgeEdgeCCD (SelfCollisionDetector.cpp:491-606) for pair k
+__device__ int ccd_ee_test(const DevCloth& c, const SolverParams& P, const Buffers& b, int k, SCt& rec)
 {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    int n = *b.ccdEePairCount;
-    if (n > b.ccdEeCap) n = b.ccdEeCap;
-    if (k >= n) return;
-    b.ccdEeHit[k] = 0;
     int2 pr = b.ccdEePairs[k];
     const int4 A = c.edge[pr.x], B = c.edge[pr.y];
     const int i1 = A.x, i2 = A.y, j1 = B.x, j2 = B.y;
-    if (i1 == j1 || i1 == j2 || i2 == j1 || i2 == j2) return;
+    if (i1 == j1 || i1 == j2 || i2 == j1 || i2 == j2) return 0;
     V3 x1 = ld3(c.prev, i1), x2 = ld3(c.prev, i2), x3 = ld3(c.prev, j1), x4 = ld3(c.prev, j2);
     V3 v1 = ld3(c.pos, i1) - x1, v2 = ld3(c.pos, i2) - x2, v3 = ld3(c.pos, j1) - x3, v4 = ld3(c.pos, j2) - x4;
     float toi;
-    if (!solve_cubic(x1, x2, x3, x4, v1, v2, v3, v4, toi)) return;
+    if (!solve_cubic(x1, x2, x3, x4, v1, v2, v3, v4, toi)) return 0;
     V3 z1 = x1 + toi * v1, z2 = x2 + toi * v2, z3 = x3 + toi * v3, z4 = x4 + toi * v4;
     V3 c1, c2;
     float s, t;
     closest_segm_segm(z1, z2, z3, z4, s, t, c1, c2);
     float dSqr = lensq(c1 - c2);
     const float eps = 0.5f * P.thickness;
-    if (!(dSqr <= eps * eps)) return;
+    if (!(dSqr <= eps * eps)) return 0;
     float s2, t2; V3 d1, d2;
     closest_segm_segm(x1, x2, x3, x4, s2, t2, d1, d2);
-    SCt rec;
     rec.idx = make_uint4(i1, i2, j1, j2);
     rec.normal = f4(normalized(d2 - d1), 0.f);
     rec.w = make_float4(s, t, 0.f, 0.f);
     rec.side = signed_volume(x1, x2, x3, x4);
     rec.lam = make_float2(0.f, 0.f);
     rec.error = 0.f;
-    b.ccdEeRec[k] = rec;
-    b.ccdEeHit[k] = 1;
+    return 1;
+}
+
+// narrow phase over the device-counted pair lists (grid-stride; every pair
+// gets its hit flag, so no clearing is needed)
+__global__ void k_ccd_narrow_vt(DevCloth c, SolverParams P, Buffers b)
+{
+    int n = *b.ccdVtPairCount;
+    if (n > b.ccdVtCap) n = b.ccdVtCap;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+    {
+        SCt rec;
+        b.ccdVtHit[k] = (uint8_t)ccd_vt_test(c, P, b, k, rec);
+    }
+}
+
+__global__ void k_ccd_narrow_ee(DevCloth c, SolverParams P, Buffers b)
+{
+    int n = *b.ccdEePairCount;
+    if (n > b.ccdEeCap) n = b.ccdEeCap;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+    {
+        SCt rec;
+        b.ccdEeHit[k] = (uint8_t)ccd_ee_test(c, P, b, k, rec);
+    }
+}
+
+// hits per query (its pairs are contiguous from off[i]); one warp per query
+__global__ void k_ccd_hit_count(const int* cnt, const int* off, const uint8_t* hit, int n, int cap, int* hcnt)
+{
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (i >= n) return;
+    const int o = off[i], e = min(cap, o + cnt[i]);
+    int h = 0;
+    for (int k = o + lane; k < e; k += 32) h += hit[k];
+    h = __reduce_add_sync(0xffffffffu, h);
+    if (lane == 0) hcnt[i] = h;
+}
+
+// append the hit records after the list's current count, per query in ascending
+// candidate order (the order of an all-pairs sweep); one warp per query picks its
+// hits smallest candidate first. A hit's record is recomputed by the same
+// deterministic test rather than stored per pair.
+template <bool VT>
+__global__ void k_ccd_gather(DevCloth c, SolverParams P, Buffers b, const int* hoff, SCt* list, const int* listCount, int listCap)
+{
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    const int n = VT ? c.N : c.E;
+    if (i >= n) return;
+    const int h = (VT ? b.ccdVtHitCnt : b.ccdEeHitCnt)[i];
+    if (h == 0) return;
+    const int* cnt = VT ? b.ccdVtCnt : b.ccdEeCnt;
+    const int* off = VT ? b.ccdVtOff : b.ccdEeOff;
+    const uint8_t* hit = VT ? b.ccdVtHit : b.ccdEeHit;
+    const int2* pairs = VT ? b.ccdVtPairs : b.ccdEePairs;
+    const int cap = VT ? b.ccdVtCap : b.ccdEeCap;
+    const int o = off[i], e = min(cap, o + cnt[i]);
+    const int d0 = *listCount + hoff[i];
+    int last = -1;
+    for (int r = 0; r < h; r++)
+    {
+        int best = INT_MAX, bestK = -1;
+        for (int k = o + lane; k < e; k += 32)
+            if (hit[k])
+            {
+                const int id = pairs[k].y;
+                if (id > last && id < best) { best = id; bestK = k; }
+            }
+        const int m = __reduce_min_sync(0xffffffffu, best);
+        if (best == m && bestK >= 0)
+        {
+            SCt rec;
+            if (VT) ccd_vt_test(c, P, b, bestK, rec); else ccd_ee_test(c, P, b, bestK, rec);
+            if (d0 + r < listCap) list[d0 + r] = rec;
+            else atomicOr(c.status, ST_CCD_OVERFLOW);
+        }
+        last = m;
+    }
 }
 
 // ------------------------------------------------- cluster-resident solver
@@ -2148,7 +2273,7 @@ void launch_self_proximity(cudaStream_t s, const DevCloth& c, const SolverParams
     k_self_ee<<<blocks_for(c.E, 128), 128, 0, s>>>(c, P, b, edgeBvh);
 }
 
-void launch_compact_self(cudaStream_t s, const DevCloth& c, const Buffers& b, bool ccd)
+void launch_compact_self(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b, bool ccd)
 {
     int* off = b.scanOff;
     scan_ints(s, b.stCnt, off, c.N, b.stCount, b.scanBlock);
@@ -2158,14 +2283,15 @@ void launch_compact_self(cudaStream_t s, const DevCloth& c, const Buffers& b, bo
     if (ccd)
     {
         // continuous hits go after the proximity contacts, as the detector's
-        // AddSelfTriangle / AddSelfEdge would append them
+        // AddSelfTriangle / AddSelfEdge would append them (in pair order)
         int* tot = b.scanTot;
-        int nvt = b.ccdVtCap, nee = b.ccdEeCap;
-        scan_ints(s, b.ccdVtHit, off, nvt, tot, b.scanBlock);
-        k_compact<SCt><<<blocks_for(nvt), 256, 0, s>>>(b.ccdVtHit, off, b.ccdVtRec, 1, b.stList, nvt, b.stCount, b.stCap, c.status, ST_CCD_OVERFLOW);
+        k_ccd_hit_count<<<blocks_for(32 * c.N), 256, 0, s>>>(b.ccdVtCnt, b.ccdVtOff, b.ccdVtHit, c.N, b.ccdVtCap, b.ccdVtHitCnt);
+        scan_ints(s, b.ccdVtHitCnt, off, c.N, tot, b.scanBlock);
+        k_ccd_gather<true><<<blocks_for(32 * c.N), 256, 0, s>>>(c, P, b, off, b.stList, b.stCount, b.stCap);
         k_add_counts<<<1, 32, 0, s>>>(b.stCount, b.stCount, tot, b.stCap);
-        scan_ints(s, b.ccdEeHit, off, nee, tot, b.scanBlock);
-        k_compact<SCt><<<blocks_for(nee), 256, 0, s>>>(b.ccdEeHit, off, b.ccdEeRec, 1, b.seList, nee, b.seCount, b.seCap, c.status, ST_CCD_OVERFLOW);
+        k_ccd_hit_count<<<blocks_for(32 * c.E), 256, 0, s>>>(b.ccdEeCnt, b.ccdEeOff, b.ccdEeHit, c.E, b.ccdEeCap, b.ccdEeHitCnt);
+        scan_ints(s, b.ccdEeHitCnt, off, c.E, tot, b.scanBlock);
+        k_ccd_gather<false><<<blocks_for(32 * c.E), 256, 0, s>>>(c, P, b, off, b.seList, b.seCount, b.seCap);
         k_add_counts<<<1, 32, 0, s>>>(b.seCount, b.seCount, tot, b.seCap);
     }
     k_add_counts<<<1, 32, 0, s>>>(b.stCount, b.stCount, nullptr, b.stCap);
@@ -2176,17 +2302,21 @@ void launch_ccd(cudaStream_t s, const DevCloth& c, const SolverParams& P, const 
                 const DevBVH& triBvh, const DevBVH& edgeBvh)
 {
     const float tol = P.thickness + P.tolerance * 0.5f;
-    k_ccd_broad_vt<<<blocks_for(c.N, 128), 128, 0, s>>>(c, P, b, triBvh, tol);
-    k_ccd_broad_ee<<<blocks_for(c.E, 128), 128, 0, s>>>(c, P, b, edgeBvh, tol);
-    int* off = b.scanOff;
-    scan_ints(s, b.ccdVtCnt, off, c.N, b.ccdVtPairCount, b.scanBlock);
-    k_ccd_pairs<<<blocks_for(c.N), 256, 0, s>>>(b.ccdVtCnt, off, b.ccdVtCand, c.N, b.ccdVtPairs, b.ccdVtCap, c.status);
-    scan_ints(s, b.ccdEeCnt, off, c.E, b.ccdEePairCount, b.scanBlock);
-    k_ccd_pairs<<<blocks_for(c.E), 256, 0, s>>>(b.ccdEeCnt, off, b.ccdEeCand, c.E, b.ccdEePairs, b.ccdEeCap, c.status);
-    cudaMemsetAsync(b.ccdVtHit, 0, sizeof(int) * b.ccdVtCap, s);
-    cudaMemsetAsync(b.ccdEeHit, 0, sizeof(int) * b.ccdEeCap, s);
-    k_ccd_narrow_vt<<<blocks_for(b.ccdVtCap), 256, 0, s>>>(c, P, b);
-    k_ccd_narrow_ee<<<blocks_for(b.ccdEeCap), 256, 0, s>>>(c, P, b);
+    cudaMemsetAsync(b.ccdPoolUsed, 0, sizeof(int), s);
+    for (bool pool : {false, true})
+    {
+        k_ccd_broad_vt<<<blocks_for(c.N, 128), 128, 0, s>>>(c, P, b, triBvh, tol, pool);
+        k_ccd_broad_ee<<<blocks_for(c.E, 128), 128, 0, s>>>(c, P, b, edgeBvh, tol, pool);
+    }
+    scan_ints(s, b.ccdVtCnt, b.ccdVtOff, c.N, b.ccdVtPairCount, b.scanBlock);
+    k_ccd_pairs<<<blocks_for(32 * c.N), 256, 0, s>>>(b.ccdVtCnt, b.ccdVtOff, b.ccdVtCand, b.ccdPool, b.ccdVtPoolOff, c.N,
+                                                b.ccdVtPairs, b.ccdVtCap, c.status);
+    scan_ints(s, b.ccdEeCnt, b.ccdEeOff, c.E, b.ccdEePairCount, b.scanBlock);
+    k_ccd_pairs<<<blocks_for(32 * c.E), 256, 0, s>>>(b.ccdEeCnt, b.ccdEeOff, b.ccdEeCand, b.ccdPool, b.ccdEePoolOff, c.E,
+                                                b.ccdEePairs, b.ccdEeCap, c.status);
+    // narrow phase: a fixed grid strides over the device-side pair counts
+    k_ccd_narrow_vt<<<8 * 148, 128, 0, s>>>(c, P, b);
+    k_ccd_narrow_ee<<<8 * 148, 128, 0, s>>>(c, P, b);
 }
 
 void launch_reset_gs(cudaStream_t s, const DevCloth& c)

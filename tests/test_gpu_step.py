@@ -161,8 +161,14 @@ def test_self_check_mode_trajectory():
         assert _same(p.model.positions(), o.positions()), (f, float(np.abs(p.model.positions() - o.positions()).max()))
 
 
-def test_ccd_broadphase_and_hits_bitexact():
+@pytest.mark.parametrize("thickness", [0.5, 1.5])
+def test_ccd_broadphase_and_hits_bitexact(thickness):
+    """Candidate pair sets and hit lists of the continuous detector are bit-exact.
+    At thickness 1.5 (boxes two grid cells wide around each edge, two layers)
+    edge queries have more candidates than their own 64 slots hold and take the
+    overflow-pool pass."""
     sc, state = scenes.ccd_scene(16)
+    sc.params.thickness = thickness
     w, p, o = _pair(sc, ccd=True, state=state)
     p.step(sc.dt)
     # broad phase: all-pairs overlap set of the oracle from the same predicted state
@@ -177,6 +183,14 @@ def test_ccd_broadphase_and_hits_bitexact():
     assert len(ovt) > 0 and len(oee) > 0
     assert sorted(map(tuple, gvt[:, ::-1].tolist())) == sorted(map(tuple, ovt.tolist()))
     assert sorted(map(tuple, gee.tolist())) == sorted(map(tuple, oee.tolist()))
+    # per query the list is sorted and contiguous, as the pair list is built
+    assert np.array_equal(gee, np.array(sorted(map(tuple, gee.tolist()))).reshape(gee.shape))
+    most = max(np.bincount(gvt[:, 0]).max(), np.bincount(gee[:, 0]).max())
+    if thickness > 1.0:
+        assert most > 64
+    assert p.status() & 4 == 0
+    if p.status() & ~16:
+        return   # proximity slots overflowed at this thickness; the pair sets were the point
     # narrow phase: the self lists (proximity then continuous hits) match
     o.step(sc.dt)
     for kind in (3, 4):
