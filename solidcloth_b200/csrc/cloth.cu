@@ -578,8 +578,9 @@ bool ClothModel::upload_topology(const HMesh& mesh)
     SC_CUDA(cudaMemcpy(dborder, border.data(), N, cudaMemcpyHostToDevice));
     dc.vBorder = dborder;
     {
-        // query orders for the warp-packet traversals: spatially adjacent queries
-        // share a warp (vertices by Morton code; edges in the edge tree's leaf order)
+        // query orders for the tree traversals: spatially adjacent queries share a
+        // warp, so its lanes walk the same subtrees (vertices and edge centroids by
+        // Morton code of the rest shape)
         std::vector<V3> ec(E);
         for (int e = 0; e < E; e++) ec[e] = 0.5f * (hpos[mesh.edges[e].i1] + hpos[mesh.edges[e].i2]);
         std::vector<int> vq = morton_order(hpos), eq = morton_order(ec);
@@ -806,6 +807,7 @@ bool ClothModel::ensure_buffers(const CollisionWorld& world, cudaStream_t s)
     size_t maxScan = std::max<size_t>({(size_t)N, (size_t)E, (size_t)buf.tcCap, (size_t)buf.ecCap});
     buf.scanOff = (int*)dalloc(sizeof(int) * (maxScan + 1), true);
     buf.scanBlock = (int*)dalloc(sizeof(int) * (maxScan / 1024 + 8), true);
+    buf.scanBlock2 = (int*)dalloc(sizeof(int) * (maxScan / 1024 + 8), true);
     bufWorldVersion = world.version;
     bufFlags = prm.flags;
     bufCcd = ccd;
@@ -817,12 +819,18 @@ bool ClothModel::ensure_buffers(const CollisionWorld& world, cudaStream_t s)
 ClothPatch::ClothPatch(CollisionWorld& w) : world(w), model(this)
 {
     cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking);
+    cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking);
+    cudaEventCreateWithFlags(&evFork, cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&evJoin, cudaEventDisableTiming);
 }
 
 ClothPatch::~ClothPatch()
 {
     if (graph) cudaGraphExecDestroy(graph);
     if (stream) { cudaStreamSynchronize(stream); cudaStreamDestroy(stream); }
+    if (side) { cudaStreamSynchronize(side); cudaStreamDestroy(side); }
+    if (evFork) cudaEventDestroy(evFork);
+    if (evJoin) cudaEventDestroy(evJoin);
 }
 
 // ClothModel::AddTriangle: FEM rest data from the uv parameterisation
@@ -970,10 +978,7 @@ void ClothPatch::record_substep(float h)
     }
     if (ccd)
     {
-        const float tol = m.prm.thickness + m.prm.tolerance * 0.5f;
-        launch_bvh_refit(s, m.sweptTriBvh, c, 2, tol);
-        launch_bvh_refit(s, m.sweptEdgeBvh, c, 3, tol);
-        launch_ccd(s, c, P, b, m.sweptTriBvh, m.sweptEdgeBvh);
+        launch_ccd(s, side, evFork, evJoin, c, P, b, m.sweptTriBvh, m.sweptEdgeBvh);
     }
     if (self || ccd) launch_compact_self(s, c, P, b, ccd);
     else cudaMemsetAsync(b.stCount, 0, 2 * sizeof(int), s);

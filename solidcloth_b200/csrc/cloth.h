@@ -170,6 +170,8 @@ public:
     int numSteps = 1;
     bool isQuadMesh = true;
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;               // second branch of the captured frame graph
+    cudaEvent_t evFork = nullptr, evJoin = nullptr;
 
     // cached CUDA graph of one frame
     cudaGraphExec_t graph = nullptr;

@@ -7,6 +7,7 @@ namespace sc {
 constexpr int KVT = 48;        // self vertex-triangle contact slots per vertex
 constexpr int KCAND = 256;     // BVH candidates kept per proximity query
 constexpr int KRES = 96;       // distinct features tracked per vertex for the dedup
+constexpr int KADJ = 16;       // adjacent primitives held in registers by a broad-phase query
 constexpr int KCCD = 128;      // continuous-collision candidates kept in a query's own slots
 constexpr int CCD_VT_PAIRS = 128, CCD_EE_PAIRS = 96; // pair store per vertex / edge
 constexpr int CCD_VT_HITS = 32, CCD_EE_HITS = 16;   // continuous contacts per vertex / edge
@@ -61,6 +62,7 @@ struct Buffers
     int* colour; int* order; int* colourStart; int colourCap;
     // scan scratch: block sums, per-item offsets, totals
     int* scanBlock; int* scanOff; int* scanTot;
+    int* scanBlock2;           // second block-sum scratch for scans on the side stream
     const DevMesh* meshes;     // device array
     int numMeshes;
 };
@@ -79,8 +81,10 @@ void launch_colour_contacts(cudaStream_t s, const DevCloth& c, const Buffers& b)
 void launch_bvh_refit(cudaStream_t s, const DevBVH& bvh, const DevCloth& c, int kind, float tol);
 void launch_self_proximity(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b,
                            const DevBVH& triBvh, const DevBVH& edgeBvh);
-void launch_ccd(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b,
-                const DevBVH& triBvh, const DevBVH& edgeBvh);
+// swept-tree refits + continuous-collision broad and narrow phases; the
+// vertex-triangle half runs on `side` (forked from / joined to s by the events)
+void launch_ccd(cudaStream_t s, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join, const DevCloth& c,
+                const SolverParams& P, const Buffers& b, const DevBVH& triBvh, const DevBVH& edgeBvh);
 void launch_compact_self(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b, bool ccd);
 void launch_reset_gs(cudaStream_t s, const DevCloth& c);
 void launch_gs_exit_test(cudaStream_t s, const DevCloth& c, const SolverParams& P, int iter);

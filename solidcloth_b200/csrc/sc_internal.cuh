@@ -57,8 +57,8 @@ struct DevCloth
     const int* vTriStart;       // N+1, incident (triangle, corner) sorted by triangle
     const int2* vTri;
     const uint8_t* vBorder;     // N, Mesh::IsBorderVertex
-    const int* vQuery;          // N: vertices in spatial (Morton, rest shape) order, for warp packets
-    const int* eQuery;          // E: edges in the edge tree's leaf order
+    const int* vQuery;          // N: vertices in spatial (Morton, rest shape) order: neighbouring
+    const int* eQuery;          // E: edges likewise; queries of one warp walk the same subtrees
     float4* prevN;              // collision mesh vertex normals (refreshed per frame)
     float4* prevTriN;           // collision mesh triangle normals
     float4* meshN;              // render mesh normals
