@@ -210,9 +210,13 @@ def run_ours(args):
     w, p = api.load_scene(sc)
     stream = torch.cuda.ExternalStream(p.cuda_stream(), device=torch.device("cuda", local))
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    # CUDA events inside the frame graph bracket the solve and the broad phases of
+    # every timed substep (fresh events per frame: no host sync in the timed loop)
+    p.set_kernel_timing(args.steps)
     for _ in range(args.warmup):
         p.step(sc.dt)
     p.synchronize()
+    p.kernel_timing()                      # drop the warm-up frames' records
     st = p.status()
     kernels_per_frame = p.graph_kernel_count()
 
@@ -234,6 +238,8 @@ def run_ours(args):
         barrier()
     ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     tot_ms = float(sum(ms))
+    sections, timed_frames = p.kernel_timing()
+    p.set_kernel_timing(0)
     if ws > 1:
         t = torch.tensor([tot_ms], device="cuda")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -270,26 +276,45 @@ def run_ours(args):
                "d2h_bytes_per_step": 3 * 16 * sc.num_vertices,
                "path": "scSetParticleState -> scStepCloth -> scGetParticlePositions/Prev/Velocities"}
 
-    # roofline of the dominant constraint sweep (FEM), timed alone with events
-    T = len(p.model.tris())
-    fem_ms = p.profile_sweep(0, reps=50)
-    bend_ms = p.profile_sweep(1, reps=50)
-    B = len(p.model.bends())
+    # roofline of the dominant kernel, from the in-graph events of the timed frames
+    T, B, E, N = p.model.num_tris(), p.model.num_bends(), p.model.num_edges(), sc.num_vertices
+    it = max(1, sc.params.iterations)
     peak, peak_kind = _peaks()
-    fem_bytes = 144 * T
-    achieved = fem_bytes / (fem_ms * 1e-3) / 1e9
+    ee_pairs = len(p.model.ccd_candidates(1)) if sc.ccd else 0
+    algo = {
+        # iterations x 144 B per FEM projection + bend iterations x 144 B per bend + velocity 48 B per vertex
+        "gs_solve": it * 144 * T + ((it + 1) // 2) * 144 * B + 48 * N,
+        # per query: 2 endpoints x (pos, prev) 64 B + edge 16 B + count 4 B; 4 B per pair; tree read once
+        "ccd_broad_ee": E * 84 + 4 * ee_pairs + 32 * (2 * E - 1),
+    }
+    kernel_names = {"gs_solve": "k_gs_cluster (one substep's Gauss-Seidel loop + velocity, one cluster launch)",
+                    "ccd_broad_ee": "k_ccd_broad_ee (edge-edge swept-box LBVH query, both passes)"}
+    per = {}
+    for k in algo:
+        tot, cnt = sections.get(k, (0.0, 0))
+        if cnt:
+            avg = tot / cnt
+            per[k] = {"ms_per_launch": avg, "launches": cnt, "algorithmic_bytes_per_launch": algo[k],
+                      "achieved_gbs": algo[k] / (avg * 1e-3) / 1e9, "share_of_frame": tot / tot_ms}
+    dom = max(per, key=lambda k: per[k]["ms_per_launch"] * per[k]["launches"]) if per else None
     traffic = None
     tj = ROOT / "profiles" / "traffic.json"
-    if tj.exists():
+    if dom and tj.exists():
         try:
-            traffic = json.loads(tj.read_text()).get(f"{args.config}_fem_sweep_bytes")
+            traffic = json.loads(tj.read_text()).get(f"{args.config}_{dom}_bytes_per_launch")
         except Exception:
             traffic = None
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "kernel": "k_fem (one FEM sweep = all colours of one iteration)",
-                "algorithmic_bytes_per_launch": fem_bytes, "ms_per_sweep": fem_ms,
-                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                "bend_sweep": {"ms": bend_ms, "achieved_gbs": 144 * B / (bend_ms * 1e-3) / 1e9}}
+    roofline = None
+    if dom:
+        d = per[dom]
+        roofline = {"bound": "hbm", "achieved": d["achieved_gbs"], "peak": peak, "unit": "GB/s",
+                    "frac": d["achieved_gbs"] / peak, "traffic": traffic, "kernel": kernel_names[dom],
+                    "algorithmic_bytes_per_launch": d["algorithmic_bytes_per_launch"],
+                    "ms_per_launch": d["ms_per_launch"], "launches_timed": d["launches"],
+                    "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, burst copy)",
+                    "sections": per,
+                    "ccd_broad_vt_ms_per_launch": (sections["ccd_broad_vt"][0] / sections["ccd_broad_vt"][1]
+                                                   if sections.get("ccd_broad_vt", (0, 0))[1] else None)}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:

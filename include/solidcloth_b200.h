@@ -178,6 +178,11 @@ SCEXP void scSetFixedIterations(scModel model, bool val);
    (Physics/SelfCollisionDetector.cpp), appended to the self contacts each substep. */
 SCEXP void scSetSelfCCD(scModel model, bool val);
 SCEXP int scGetSolverIterations(scModel model);
+/* addition (no reference counterpart): constraint residual of the current
+   positions, max |C| over every triangle's warp, weft and shear constraint (the
+   quantities Physics/ClothPBD.cpp:66-99 projects); bends are excluded because a
+   draped cloth holds them away from zero. -1 before the first step. */
+SCEXP float scGetResidual(scModel model);
 /* true (default): the Gauss-Seidel loop of a substep runs as one thread-block
    cluster with the particles in distributed shared memory, when the cloth fits
    (up to 131,072 particles); false: one kernel per colour. Same results. */
@@ -234,6 +239,15 @@ SCEXP int scGetGraphKernelCount(scClothPatch patch);
    the patch stream; returns milliseconds per sweep, or a negative value on error.
    Particle positions are modified. */
 SCEXP float scProfileSweep(scClothPatch patch, int kind, int reps);
+/* Section timing inside the frame graph (additions, no reference counterpart):
+   frames > 0 brackets, in every substep, the Gauss-Seidel solve (section 0), the
+   edge-edge (1) and vertex-triangle (2) continuous-collision broad phases with
+   CUDA events, fresh ones for each of the next `frames` frames, so no host
+   synchronisation enters a timed run; 0 turns it off. Re-captures the graph. */
+SCEXP bool scSetKernelTiming(scClothPatch patch, int frames);
+/* Synchronises; ms[3] = summed event time per section, counts[3] = timed
+   instances, over the frames since the last read; returns those frames. */
+SCEXP int scGetKernelTiming(scClothPatch patch, float* ms, int* counts);
 
 /* ---- addition with no counterpart in the reference: normals without allocation ----
    For callers that cannot call cudaMalloc (engines that reserve all GPU memory up

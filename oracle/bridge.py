@@ -90,7 +90,8 @@ def _load(path: Path, prefix: str):
                     "set_portable_math": ([C.c_int], None),
                     "portable_acos": ([C.c_float], C.c_float),
                     "self_contact_colours": ([C.c_void_p, C.c_int, _i], None),
-                    "ccd_broadphase": ([C.c_void_p, C.c_float, C.c_int, _i, C.c_int], C.c_int)})
+                    "ccd_broadphase": ([C.c_void_p, C.c_float, C.c_int, _i, C.c_int], C.c_int),
+                    "residual": ([C.c_void_p], C.c_float)})
     for name, (args, res) in sig.items():
         fn = getattr(lib, P + name)
         fn.argtypes = args
@@ -297,6 +298,10 @@ class PortCloth(CpuCloth):
         c = np.zeros(n, np.int32)
         self._fn("self_contact_colours")(self.h, kind, _ip(c))
         return c
+
+    def residual(self) -> float:
+        """max |C| over the warp, weft and shear constraints at the current positions"""
+        return float(self._fn("residual")(self.h))
 
     def ccd_broadphase(self, tol, kind, cap=1 << 24):
         out = np.zeros((cap, 2), np.int32)

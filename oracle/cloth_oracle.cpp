@@ -1900,6 +1900,27 @@ void orc_set_masses(void* h, const float* m)
 
 void orc_set_inv_mass(void* h, int i, float w) { ((Cloth*)h)->invMass[i] = w; }
 
+/* Constraint residual: max |C| over every triangle's warp, weft and shear
+   constraints at the current positions (the C values SolveTriangles computes,
+   Physics/ClothPBD.cpp:66-67,76,87,99). Bends are left out: with a flat rest
+   angle a draped cloth holds them away from zero at equilibrium. */
+float orc_residual(void* h)
+{
+    Cloth* c = (Cloth*)h;
+    float r = 0.f;
+    for (const Tri& t : c->tris)
+    {
+        V3 dx1 = c->pos[t.i2] - c->pos[t.i1], dx2 = c->pos[t.i3] - c->pos[t.i1];
+        V3 wu = t.invDet * (t.dv2 * dx1 - t.dv1 * dx2);
+        V3 wv = t.invDet * (-t.du2 * dx1 + t.du1 * dx2);
+        float cu = std::fabs(0.5f * (dot(wu, wu) - t.lu2));
+        float cv = std::fabs(0.5f * (dot(wv, wv) - t.lv2));
+        float cs = std::fabs(dot(wu, wv));
+        r = std::max(r, std::max(cu, std::max(cv, cs)));
+    }
+    return r;
+}
+
 void orc_get_state(void* h, float* p, float* q, float* v, float* w)
 {
     Cloth* c = (Cloth*)h;

@@ -31,6 +31,7 @@ void orc_set_state(void* h, const float* pos, const float* prev, const float* ve
 void orc_set_masses(void* h, const float* masses);
 void orc_set_inv_mass(void* h, int i, float w);
 void orc_get_state(void* h, float* pos, float* prev, float* vel, float* invMass);
+float orc_residual(void* h);
 void orc_get_tris(void* h, unsigned* idx, float* rest10);
 void orc_get_bends(void* h, unsigned* idx);
 void orc_get_edges(void* h, int* e4);

@@ -127,6 +127,7 @@ SIGNATURES = {
     "scSetClusterSolver": ([scModel, C.c_bool], None),
     "scSetClusterStaging": ([scModel, C.c_bool], None),
     "scGetSolverIterations": ([scModel], C.c_int),
+    "scGetResidual": ([scModel], C.c_float),
     "scGetConstraintOrder": ([scModel, C.c_int, _i, _i], C.c_int),
     "scGetNumBends": ([scModel], C.c_int),
     "scGetBends": ([scModel, _u], None),
@@ -148,6 +149,8 @@ SIGNATURES = {
     "scGetCudaStream": ([scClothPatch], C.c_void_p),
     "scGetGraphKernelCount": ([scClothPatch], C.c_int),
     "scProfileSweep": ([scClothPatch, C.c_int, C.c_int], C.c_float),
+    "scSetKernelTiming": ([scClothPatch, C.c_int], C.c_bool),
+    "scGetKernelTiming": ([scClothPatch, _f, _i], C.c_int),
 }
 
 _lib = None
@@ -319,6 +322,15 @@ class ClothModel:
         lib().scGetBends(self.h, out.ctypes.data_as(_u))
         return out
 
+    def num_edges(self) -> int:
+        return int(lib().scGetNumEdges(self.h))
+
+    def num_tris(self) -> int:
+        return int(lib().scGetNumTris(self.h))
+
+    def num_bends(self) -> int:
+        return int(lib().scGetNumBends(self.h))
+
     def edges(self):
         n = lib().scGetNumEdges(self.h)
         out = np.zeros((n, 4), np.int32)
@@ -347,6 +359,10 @@ class ClothModel:
         out = np.zeros((cap, 2), np.int32)
         n = lib().scGetCCDCandidates(self.h, kind, out.ctypes.data_as(_i), cap)
         return out[:min(n, cap)].copy()
+
+    def residual(self) -> float:
+        """max |C| over the warp, weft and shear constraints at the current positions"""
+        return float(lib().scGetResidual(self.h))
 
     def solver_iterations(self):
         return lib().scGetSolverIterations(self.h)
@@ -397,6 +413,20 @@ class ClothPatch:
         ms = lib().scProfileSweep(self.h, int(kind), int(reps))
         _check("scProfileSweep")
         return float(ms)
+
+    def set_kernel_timing(self, frames: int):
+        """bracket the solve and broad phases of the next `frames` frames with CUDA events"""
+        ok = lib().scSetKernelTiming(self.h, int(frames))
+        _check("scSetKernelTiming")
+        return bool(ok)
+
+    def kernel_timing(self):
+        """{section: (total ms, instances)} since the last read, and the frames covered"""
+        ms = np.zeros(3, np.float32)
+        cnt = np.zeros(3, np.int32)
+        frames = lib().scGetKernelTiming(self.h, ms.ctypes.data_as(_f), cnt.ctypes.data_as(_i))
+        names = ("gs_solve", "ccd_broad_ee", "ccd_broad_vt")
+        return {n: (float(ms[k]), int(cnt[k])) for k, n in enumerate(names)}, int(frames)
 
     def mesh_buffers(self):
         L = lib()

@@ -401,6 +401,21 @@ void scSetFixedIterations(scModel m, bool v) { if (M(m)) { M(m)->prm.fixedIterat
 void scSetSelfCCD(scModel m, bool v) { if (M(m)) { M(m)->prm.ccd = v; M(m)->touch(); } }
 void scSetClusterSolver(scModel m, bool v) { if (M(m)) { M(m)->prm.clusterSolver = v; M(m)->touch(); } }
 void scSetClusterStaging(scModel m, bool v) { if (M(m)) { M(m)->prm.stageRecords = v; M(m)->touch(); } }
+float scGetResidual(scModel m)
+{
+    ClothModel* c = M(m);
+    if (!c || !c->dc.scal || !c->dc.fem) return -1.f;
+    host_sync(c);
+    unsigned* word = reinterpret_cast<unsigned*>(c->dc.scal + 12);
+    launch_residual(c->owner->stream, c->dc, word);
+    unsigned u = 0;
+    cudaMemcpyAsync(&u, word, sizeof(unsigned), cudaMemcpyDeviceToHost, c->owner->stream);
+    cudaStreamSynchronize(c->owner->stream);
+    float r;
+    memcpy(&r, &u, sizeof(r));
+    return r;
+}
+
 int scGetSolverIterations(scModel m)
 {
     if (!M(m) || !M(m)->dc.scal) return 0;
@@ -591,6 +606,20 @@ int scGetGraphKernelCount(scClothPatch p)
 {
     if (!P(p) || !P(p)->graph) return 0;
     return P(p)->graphKernelCount;
+}
+
+bool scSetKernelTiming(scClothPatch p, int frames)
+{
+    ClothPatch* cp = P(p);
+    if (!cp || frames < 0) { set_error(SC_ERR_ARG, "bad timing request"); return false; }
+    return cp->set_timing(frames);
+}
+
+int scGetKernelTiming(scClothPatch p, float* ms, int* counts)
+{
+    ClothPatch* cp = P(p);
+    if (!cp) return 0;
+    return cp->read_timing(ms, counts);
 }
 
 float scProfileSweep(scClothPatch p, int kind, int reps)

@@ -827,6 +827,7 @@ ClothPatch::ClothPatch(CollisionWorld& w) : world(w), model(this)
 ClothPatch::~ClothPatch()
 {
     if (graph) cudaGraphExecDestroy(graph);
+    if (graphDef) cudaGraphDestroy(graphDef);
     if (stream) { cudaStreamSynchronize(stream); cudaStreamDestroy(stream); }
     if (side) { cudaStreamSynchronize(side); cudaStreamDestroy(side); }
     if (evFork) cudaEventDestroy(evFork);
@@ -978,7 +979,17 @@ void ClothPatch::record_substep(float h)
     }
     if (ccd)
     {
-        launch_ccd(s, side, evFork, evJoin, c, P, b, m.sweptTriBvh, m.sweptEdgeBvh);
+        cudaEvent_t marks[4] = {nullptr, nullptr, nullptr, nullptr};
+        if (timingFrames)
+        {
+            const size_t k = (size_t)recordingSubstep * NSEC * 2;
+            if (k + 2 * NSEC <= timingCapture.size())
+            {
+                marks[0] = timingCapture[k + 2 * SEC_BROAD_EE]; marks[1] = timingCapture[k + 2 * SEC_BROAD_EE + 1];
+                marks[2] = timingCapture[k + 2 * SEC_BROAD_VT]; marks[3] = timingCapture[k + 2 * SEC_BROAD_VT + 1];
+            }
+        }
+        launch_ccd(s, side, evFork, evJoin, c, P, b, m.sweptTriBvh, m.sweptEdgeBvh, marks);
     }
     if (self || ccd) launch_compact_self(s, c, P, b, ccd);
     else cudaMemsetAsync(b.stCount, 0, 2 * sizeof(int), s);
@@ -990,6 +1001,7 @@ void ClothPatch::record_substep(float h)
     const int iterations = m.prm.iterations > 1 ? m.prm.iterations : 1;
     int shift = 0;
     size_t smem = 0;
+    timing_mark(SEC_GS, false, s);
     const int cluster = m.prm.clusterSolver ? gs_cluster_size(m.N, shift, smem) : 0;
     if (cluster > 0 && m.triColourStart.size() <= 65 && m.bendColourStart.size() <= 65)
     {
@@ -1024,6 +1036,8 @@ void ClothPatch::record_substep(float h)
             smem = staged;
         }
         launch_gs_cluster(s, c, P, b, plan, cluster, smem);   // includes the velocity update
+        timing_mark(SEC_GS, true, s);
+        recordingSubstep++;
         return;
     }
     for (int k = 0; k < iterations; k++)
@@ -1038,6 +1052,57 @@ void ClothPatch::record_substep(float h)
         launch_solve_multi_contacts(s, c, P, b, k);
     }
     launch_velocity(s, c, P);
+    timing_mark(SEC_GS, true, s);
+    recordingSubstep++;
+}
+
+void ClothPatch::timing_mark(int section, bool end, cudaStream_t s)
+{
+    if (!timingFrames) return;
+    const size_t k = ((size_t)recordingSubstep * NSEC + section) * 2 + (end ? 1 : 0);
+    // external: captured as an event-record node (a plain record only orders streams)
+    if (k < timingCapture.size()) cudaEventRecordWithFlags(timingCapture[k], s, cudaEventRecordExternal);
+}
+
+bool ClothPatch::set_timing(int frames)
+{
+    sync();
+    for (cudaEvent_t e : timingCapture) cudaEventDestroy(e);
+    for (cudaEvent_t e : timingPool) cudaEventDestroy(e);
+    timingCapture.clear(); timingPool.clear(); timingNodes.clear();
+    timingFrames = std::max(0, frames);
+    timingUsed = 0;
+    if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }   // re-capture with (or without) the marks
+    if (!timingFrames) return true;
+    const size_t per = (size_t)std::max(1, numSteps) * NSEC * 2;
+    timingCapture.resize(per);
+    timingPool.resize(per * timingFrames);
+    for (auto& e : timingCapture) SC_CUDA(cudaEventCreate(&e));
+    for (auto& e : timingPool) SC_CUDA(cudaEventCreate(&e));
+    return true;
+}
+
+int ClothPatch::read_timing(float* ms, int* count)
+{
+    sync();
+    const size_t per = timingCapture.size();
+    for (int sct = 0; sct < NSEC; sct++) { if (ms) ms[sct] = 0.f; if (count) count[sct] = 0; }
+    for (int f = 0; f < timingUsed; f++)
+        for (size_t k = 0; k + 1 < per; k += 2)
+        {
+            const size_t i = (size_t)f * per + k;
+            float t = 0.f;
+            if (timingNodes[k] && timingNodes[k + 1] && cudaEventElapsedTime(&t, timingPool[i], timingPool[i + 1]) == cudaSuccess)
+            {
+                const int sct = (int)((k / 2) % NSEC);
+                if (ms) ms[sct] += t;
+                if (count) count[sct]++;
+            }
+        }
+    cudaGetLastError();
+    const int used = timingUsed;
+    timingUsed = 0;
+    return used;
 }
 
 // ClothPatch::Step (Physics/ClothPatch.cpp:323-335): numSteps substeps of dt/n,
@@ -1059,6 +1124,8 @@ bool ClothPatch::step(float dt)
     {
         if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
         cudaGraph_t g;
+        if (timingFrames && timingCapture.size() != (size_t)n * NSEC * 2) set_timing(timingFrames);
+        recordingSubstep = 0;
         SC_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
         for (int i = 0; i < n; i++) record_substep(h);
         SC_CUDA(cudaStreamEndCapture(stream, &g));
@@ -1067,15 +1134,34 @@ bool ClothPatch::step(float dt)
         std::vector<cudaGraphNode_t> nodes(numNodes);
         if (numNodes) cudaGraphGetNodes(g, nodes.data(), &numNodes);
         graphKernelCount = 0;
+        timingNodes.assign(timingCapture.size(), nullptr);
         for (size_t k = 0; k < numNodes; k++)
         {
             cudaGraphNodeType t;
-            if (cudaGraphNodeGetType(nodes[k], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) graphKernelCount++;
+            if (cudaGraphNodeGetType(nodes[k], &t) != cudaSuccess) continue;
+            if (t == cudaGraphNodeTypeKernel) graphKernelCount++;
+            if (t == cudaGraphNodeTypeEventRecord && !timingCapture.empty())
+            {
+                cudaEvent_t ev;
+                if (cudaGraphEventRecordNodeGetEvent(nodes[k], &ev) != cudaSuccess) continue;
+                for (size_t j = 0; j < timingCapture.size(); j++)
+                    if (timingCapture[j] == ev) { timingNodes[j] = nodes[k]; break; }
+            }
         }
         cudaError_t e = cudaGraphInstantiate(&graph, g, 0);
-        cudaGraphDestroy(g);
+        // the definition outlives the instantiation: the timing nodes' handles
+        // (used to retarget their events per replay) belong to it
+        if (graphDef) cudaGraphDestroy(graphDef);
+        graphDef = g;
         if (e != cudaSuccess) { set_error(SC_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e)); graph = nullptr; return false; }
         graphDt = dt; graphSteps = n; graphParamVersion = m.paramVersion; graphWorldVersion = world.version;
+    }
+    if (timingFrames && timingUsed < timingFrames)
+    {
+        const size_t per = timingCapture.size();
+        for (size_t k = 0; k < per; k++)
+            if (timingNodes[k]) SC_CUDA(cudaGraphExecEventRecordNodeSetEvent(graph, timingNodes[k], timingPool[(size_t)timingUsed * per + k]));
+        timingUsed++;
     }
     SC_CUDA(cudaGraphLaunch(graph, stream));
     hostStateDirty = true;

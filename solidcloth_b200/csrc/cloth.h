@@ -175,11 +175,27 @@ public:
 
     // cached CUDA graph of one frame
     cudaGraphExec_t graph = nullptr;
+    cudaGraph_t graphDef = nullptr;            // the captured definition of `graph`
     float graphDt = -1.f;
     int graphSteps = -1;
     uint64_t graphParamVersion = 0, graphWorldVersion = ~0ull;
     bool hostStateDirty = false;   // host copies older than the device state
     int graphKernelCount = 0;
+
+    // In-graph section timing: event-record nodes bracket the Gauss-Seidel solve
+    // and the two broad phases of every substep; before each replay they are
+    // pointed at fresh events (cudaGraphExecEventRecordNodeSetEvent affects only
+    // later launches), so a run of frames is timed with no host synchronisation.
+    enum { SEC_GS = 0, SEC_BROAD_EE = 1, SEC_BROAD_VT = 2, NSEC = 3 };
+    int timingFrames = 0;                       // frames the pool can hold (0: off)
+    int timingUsed = 0;                         // frames recorded since the last read
+    std::vector<cudaEvent_t> timingCapture;     // events named at capture: [substep][section][start/end]
+    std::vector<cudaGraphNode_t> timingNodes;   // their record nodes in the instantiated graph
+    std::vector<cudaEvent_t> timingPool;        // [frame][substep][section][start/end]
+    int recordingSubstep = 0;
+    void timing_mark(int section, bool end, cudaStream_t s);
+    bool set_timing(int frames);
+    int read_timing(float* msPerSection, int* countPerSection);
 
     bool init_grid(int divX, int divY, float inc, V3 offset, bool horizontal, bool attached);
     bool step(float dt);

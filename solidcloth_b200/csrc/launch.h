@@ -82,11 +82,16 @@ void launch_bvh_refit(cudaStream_t s, const DevBVH& bvh, const DevCloth& c, int 
 void launch_self_proximity(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b,
                            const DevBVH& triBvh, const DevBVH& edgeBvh);
 // swept-tree refits + continuous-collision broad and narrow phases; the
-// vertex-triangle half runs on `side` (forked from / joined to s by the events)
+// vertex-triangle half runs on `side` (forked from / joined to s by the events);
+// marks (optional, entries may be null): records around the edge-edge and the
+// vertex-triangle broad phases {ee start, ee end, vt start, vt end}
 void launch_ccd(cudaStream_t s, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join, const DevCloth& c,
-                const SolverParams& P, const Buffers& b, const DevBVH& triBvh, const DevBVH& edgeBvh);
+                const SolverParams& P, const Buffers& b, const DevBVH& triBvh, const DevBVH& edgeBvh,
+                const cudaEvent_t* marks = nullptr);
 void launch_compact_self(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b, bool ccd);
 void launch_reset_gs(cudaStream_t s, const DevCloth& c);
+// max |C| over warp / weft / shear constraints, as float bits into *out
+void launch_residual(cudaStream_t s, const DevCloth& c, unsigned* out);
 void launch_gs_exit_test(cudaStream_t s, const DevCloth& c, const SolverParams& P, int iter);
 
 // cluster-resident Gauss-Seidel solver (one cluster per cloth, one launch per substep)

@@ -1965,6 +1965,36 @@ __global__ void k_ccd_gather(DevCloth c, SolverParams P, Buffers b, const int* h
     }
 }
 
+// Constraint residual: max |C| over the warp, weft and shear constraints of every
+// triangle (the C values of SolveTriangles, Physics/ClothPBD.cpp:66-67,76,87,99)
+// at the current positions; same operation order as the oracle's, so bit-equal.
+template <typename PA>
+__device__ __forceinline__ float fem_residual(const PA& pa, float4 r0, float4 r1, float4 r2)
+{
+    const uint32_t i1 = __float_as_uint(r0.x), i2 = __float_as_uint(r0.y), i3 = __float_as_uint(r0.z);
+    const float du1 = r0.w, du2 = r1.x, dv1 = r1.y, dv2 = r1.z, invDet = r1.w;
+    const float4 a = pa.ld(i1), b = pa.ld(i2), d = pa.ld(i3);
+    const V3 x1 = mk(a.x, a.y, a.z), x2 = mk(b.x, b.y, b.z), x3 = mk(d.x, d.y, d.z);
+    const V3 dx1 = x2 - x1, dx2 = x3 - x1;
+    const V3 wu = invDet * (dv2 * dx1 - dv1 * dx2);
+    const V3 wv = invDet * (-du2 * dx1 + du1 * dx2);
+    const float cu = fabsf(0.5f * (dot(wu, wu) - r2.x));
+    const float cv = fabsf(0.5f * (dot(wv, wv) - r2.y));
+    const float cs = fabsf(dot(wu, wv));
+    return fmaxf(cu, fmaxf(cv, cs));
+}
+
+// max over the triangles into *out (float bits; |C| >= 0 orders like its bits)
+__global__ void k_residual(DevCloth c, unsigned* out)
+{
+    const GlobalPos pa{c.pos};
+    float r = 0.f;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < c.T; j += gridDim.x * blockDim.x)
+        r = fmaxf(r, fem_residual(pa, c.fem[3 * j], c.fem[3 * j + 1], c.fem[3 * j + 2]));
+    const unsigned u = __reduce_max_sync(0xffffffffu, __float_as_uint(r));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, u);
+}
+
 // ------------------------------------------------- cluster-resident solver
 // The whole Gauss-Seidel loop of one substep (SolveGS, Physics/ClothPBD.cpp:324-369)
 // plus the velocity update in ONE launch of ONE thread-block cluster. Every CTA
@@ -2352,8 +2382,12 @@ void launch_compact_self(cudaStream_t s, const DevCloth& c, const SolverParams& 
 }
 
 void launch_ccd(cudaStream_t s, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join, const DevCloth& c,
-                const SolverParams& P, const Buffers& b, const DevBVH& triBvh, const DevBVH& edgeBvh)
+                const SolverParams& P, const Buffers& b, const DevBVH& triBvh, const DevBVH& edgeBvh,
+                const cudaEvent_t* marks)
 {
+    auto mark = [&](int k, cudaStream_t st) {
+        if (marks && marks[k]) cudaEventRecordWithFlags(marks[k], st, cudaEventRecordExternal);
+    };
     // The vertex-triangle chain (refit, broad phase, pairs, narrow phase) runs on
     // the side stream beside the edge-edge chain; each is latency bound and fills
     // only part of the GPU. They share nothing but the pool counter (atomic).
@@ -2362,8 +2396,10 @@ void launch_ccd(cudaStream_t s, cudaStream_t side, cudaEvent_t fork, cudaEvent_t
     cudaEventRecord(fork, s);
     cudaStreamWaitEvent(side, fork, 0);
     launch_bvh_refit(side, triBvh, c, 2, tol);
+    mark(2, side);
     for (bool pool : {false, true})
         k_ccd_broad_vt<<<blocks_for(c.N, 128), 128, 0, side>>>(c, P, b, triBvh, tol, pool);
+    mark(3, side);
     scan_ints(side, b.ccdVtCnt, b.ccdVtOff, c.N, b.ccdVtPairCount, b.scanBlock2);
     k_ccd_pairs<<<blocks_for(32 * c.N), 256, 0, side>>>(b.ccdVtCnt, b.ccdVtOff, b.ccdVtCand, b.ccdPool, b.ccdVtPoolOff, c.N,
                                                    b.ccdVtPairs, b.ccdVtCap, c.status);
@@ -2371,14 +2407,22 @@ void launch_ccd(cudaStream_t s, cudaStream_t side, cudaEvent_t fork, cudaEvent_t
     cudaEventRecord(join, side);
 
     launch_bvh_refit(s, edgeBvh, c, 3, tol);
+    mark(0, s);
     for (bool pool : {false, true})
         k_ccd_broad_ee<<<blocks_for(c.E, 128), 128, 0, s>>>(c, P, b, edgeBvh, tol, pool);
+    mark(1, s);
     scan_ints(s, b.ccdEeCnt, b.ccdEeOff, c.E, b.ccdEePairCount, b.scanBlock);
     k_ccd_pairs<<<blocks_for(32 * c.E), 256, 0, s>>>(b.ccdEeCnt, b.ccdEeOff, b.ccdEeCand, b.ccdPool, b.ccdEePoolOff, c.E,
                                                 b.ccdEePairs, b.ccdEeCap, c.status);
     // narrow phase: a fixed grid strides over the device-side pair counts
     k_ccd_narrow_ee<<<8 * 148, 128, 0, s>>>(c, P, b);
     cudaStreamWaitEvent(s, join, 0);
+}
+
+void launch_residual(cudaStream_t s, const DevCloth& c, unsigned* out)
+{
+    cudaMemsetAsync(out, 0, sizeof(unsigned), s);
+    k_residual<<<2 * 148, 256, 0, s>>>(c, out);
 }
 
 void launch_reset_gs(cudaStream_t s, const DevCloth& c)
