@@ -187,6 +187,21 @@ SCEXP float scGetResidual(scModel model);
    cluster with the particles in distributed shared memory, when the cloth fits
    (up to 131,072 particles); false: one kernel per colour. Same results. */
 SCEXP void scSetClusterSolver(scModel model, bool val);
+/* Solver for the Gauss-Seidel loop (additions, no reference counterpart; all
+   give the same results): 0 = autotuned at the first step (default: the fastest
+   of the cluster kernel, the grid-resident cooperative kernel's variants and the
+   per-colour kernels, timed on this cloth), 1 = cluster kernel (clothes up to
+   131,072 particles), 2 = grid kernel (tuned variant), 3 = per-colour kernels.
+   scSetClusterSolver(true/false) is mode 1 / 3. */
+SCEXP void scSetSolverMode(scModel model, int mode);
+/* force grid variant `variant` (0 .. scGetGridVariants()-1) with blocksPerSm CTAs per SM */
+SCEXP void scSetGridSolver(scModel model, int variant, int blocksPerSm);
+/* out4 = {kind, grid variant, CTAs per SM, threads per CTA} of the solver in use;
+   tuneMs (4 floats per candidate: kind, variant, CTAs per SM, ms per substep)
+   gets up to cap candidates of the last tuning; returns the candidate count */
+SCEXP int scGetSolverChoice(scModel model, int* out4, float* tuneMs, int cap);
+/* info3 = {threads per CTA, FEM constraints per thread, bends per thread} per variant */
+SCEXP int scGetGridVariants(int* info3, int cap);
 /* true (default): the cluster solver copies each CTA's FEM and bend records to
    shared memory once per substep when they fit; false: read them from global
    memory in every sweep. Same results. */

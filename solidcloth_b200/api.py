@@ -126,6 +126,10 @@ SIGNATURES = {
     "scSetSelfCCD": ([scModel, C.c_bool], None),
     "scSetClusterSolver": ([scModel, C.c_bool], None),
     "scSetClusterStaging": ([scModel, C.c_bool], None),
+    "scSetSolverMode": ([scModel, C.c_int], None),
+    "scSetGridSolver": ([scModel, C.c_int, C.c_int], None),
+    "scGetSolverChoice": ([scModel, _i, _f, C.c_int], C.c_int),
+    "scGetGridVariants": ([_i, C.c_int], C.c_int),
     "scGetSolverIterations": ([scModel], C.c_int),
     "scGetResidual": ([scModel], C.c_float),
     "scGetConstraintOrder": ([scModel, C.c_int, _i, _i], C.c_int),
@@ -297,6 +301,22 @@ class ClothModel:
     def set_cluster_solver(self, on: bool):
         lib().scSetClusterSolver(self.h, bool(on))
 
+    def set_solver_mode(self, mode: int):
+        """0 autotuned, 1 cluster kernel, 2 grid kernel, 3 per-colour kernels"""
+        lib().scSetSolverMode(self.h, int(mode))
+        _check("scSetSolverMode")
+
+    def set_grid_solver(self, variant: int, blocks_per_sm: int):
+        lib().scSetGridSolver(self.h, int(variant), int(blocks_per_sm))
+        _check("scSetGridSolver")
+
+    def solver_choice(self):
+        """(kind, variant, CTAs per SM, threads) in use, and the last tuning's candidates"""
+        out = np.zeros(4, np.int32)
+        log = np.zeros((64, 4), np.float32)
+        n = lib().scGetSolverChoice(self.h, out.ctypes.data_as(_i), log.ctypes.data_as(_f), 64)
+        return tuple(int(x) for x in out), log[:min(n, 64)].copy()
+
     def set_cluster_staging(self, on: bool):
         lib().scSetClusterStaging(self.h, bool(on))
 
@@ -442,6 +462,13 @@ class ClothPatch:
         if self.h is not None:
             lib().scFreeClothPatch(self.h)
             self.h = None
+
+
+def grid_variants():
+    """(threads per CTA, FEM constraints per thread, bends per thread) per grid-solver variant"""
+    info = np.zeros((64, 3), np.int32)
+    n = lib().scGetGridVariants(info.ctypes.data_as(_i), 64)
+    return [tuple(int(x) for x in info[k]) for k in range(n)]
 
 
 def load_scene(scene: Scene, ccd: bool | None = None):

@@ -399,7 +399,48 @@ void scGetParticleVelocities(scModel m, float* xyz) { get3(m, xyz, 1); }
 void scGetParticlePrevPositions(scModel m, float* xyz) { get3(m, xyz, 2); }
 void scSetFixedIterations(scModel m, bool v) { if (M(m)) { M(m)->prm.fixedIterations = v; M(m)->touch(); } }
 void scSetSelfCCD(scModel m, bool v) { if (M(m)) { M(m)->prm.ccd = v; M(m)->touch(); } }
-void scSetClusterSolver(scModel m, bool v) { if (M(m)) { M(m)->prm.clusterSolver = v; M(m)->touch(); } }
+void scSetClusterSolver(scModel m, bool v) { scSetSolverMode(m, v ? SOLVE_CLUSTER : SOLVE_KERNELS); }
+void scSetSolverMode(scModel m, int mode)
+{
+    if (!M(m) || mode < SOLVE_AUTO || mode > SOLVE_KERNELS) { set_error(SC_ERR_ARG, "solver mode must be 0..3"); return; }
+    M(m)->solverMode = mode;
+    M(m)->tuned = false;
+    M(m)->touch();
+}
+void scSetGridSolver(scModel m, int variant, int blocksPerSm)
+{
+    if (!M(m) || variant < 0 || variant >= gs_grid_variants() || blocksPerSm < 1) { set_error(SC_ERR_ARG, "bad grid solver variant"); return; }
+    M(m)->solverMode = SOLVE_GRID;
+    M(m)->choice = {SOLVE_GRID, variant, blocksPerSm, 0.f};
+    M(m)->tuned = true;
+    M(m)->touch();
+    M(m)->tunedVersion = M(m)->paramVersion;
+}
+int scGetSolverChoice(scModel m, int* out4, float* tuneMs, int cap)
+{
+    if (!M(m)) return 0;
+    const SolverChoice& ch = M(m)->choice;
+    if (out4)
+    {
+        int th = 0, ft = 0, bt = 0;
+        if (ch.kind == SOLVE_GRID) gs_grid_variant_info(ch.variant, th, ft, bt);
+        out4[0] = ch.kind; out4[1] = ch.variant; out4[2] = ch.blocksPerSm; out4[3] = th;
+    }
+    const auto& log = M(m)->tuneLog;
+    if (tuneMs)
+        for (int k = 0; k < cap && k < (int)log.size(); k++)
+        {
+            tuneMs[4 * k] = (float)log[k].kind; tuneMs[4 * k + 1] = (float)log[k].variant;
+            tuneMs[4 * k + 2] = (float)log[k].blocksPerSm; tuneMs[4 * k + 3] = log[k].ms;
+        }
+    return (int)log.size();
+}
+int scGetGridVariants(int* info3, int cap)
+{
+    const int n = gs_grid_variants();
+    for (int v = 0; info3 && v < n && v < cap; v++) gs_grid_variant_info(v, info3[3 * v], info3[3 * v + 1], info3[3 * v + 2]);
+    return n;
+}
 void scSetClusterStaging(scModel m, bool v) { if (M(m)) { M(m)->prm.stageRecords = v; M(m)->touch(); } }
 float scGetResidual(scModel m)
 {

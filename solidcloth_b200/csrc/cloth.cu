@@ -996,22 +996,40 @@ void ClothPatch::record_substep(float h)
     launch_colour_contacts(s, c, b);
     // ClothModelPBD::SolveGS (Physics/ClothPBD.cpp:324-369)
     launch_reset_gs(s, c);
+    timing_mark(SEC_GS, false, s);
+    record_solve(s, P, m.choice);
+    timing_mark(SEC_GS, true, s);
+    recordingSubstep++;
+}
+
+// One substep's Gauss-Seidel loop and velocity update, by the chosen solver:
+// the cluster-resident kernel, the grid-resident cooperative kernel (a tuned
+// variant), or one kernel per colour. The three are the same algorithm in the
+// same order (bit-identical results).
+bool ClothPatch::record_solve(cudaStream_t s, const SolverParams& P, const SolverChoice& ch)
+{
+    ClothModel& m = model;
+    const DevCloth& c = m.dc;
+    Buffers& b = m.buf;
     // the reference's loop tests its exit conditions after the body, so it always
     // runs at least one iteration (Physics/ClothPBD.cpp:335-362)
     const int iterations = m.prm.iterations > 1 ? m.prm.iterations : 1;
-    int shift = 0;
-    size_t smem = 0;
-    timing_mark(SEC_GS, false, s);
-    const int cluster = m.prm.clusterSolver ? gs_cluster_size(m.N, shift, smem) : 0;
-    if (cluster > 0 && m.triColourStart.size() <= 65 && m.bendColourStart.size() <= 65)
+    const bool planFits = m.triColourStart.size() <= 65 && m.bendColourStart.size() <= 65;
+    GsPlan plan = {};
+    plan.iterations = iterations;
+    plan.nFemCol = (int)m.triColourStart.size() - 1;
+    plan.nBendCol = (int)m.bendColourStart.size() - 1;
+    if (planFits)
     {
-        GsPlan plan = {};
-        plan.iterations = iterations;
-        plan.shift = shift;
-        plan.nFemCol = (int)m.triColourStart.size() - 1;
-        plan.nBendCol = (int)m.bendColourStart.size() - 1;
         for (size_t k = 0; k < m.triColourStart.size(); k++) plan.femStart[k] = m.triColourStart[k];
         for (size_t k = 0; k < m.bendColourStart.size(); k++) plan.bendStart[k] = m.bendColourStart[k];
+    }
+    int shift = 0;
+    size_t smem = 0;
+    const int cluster = (ch.kind == SOLVE_CLUSTER && planFits) ? gs_cluster_size(m.N, shift, smem) : 0;
+    if (cluster > 0)
+    {
+        plan.shift = shift;
         // records each CTA handles: per colour a contiguous chunk of ceil(count / cluster)
         auto perCta = [&](const std::vector<int>& start) {
             int most = 0;
@@ -1036,10 +1054,10 @@ void ClothPatch::record_substep(float h)
             smem = staged;
         }
         launch_gs_cluster(s, c, P, b, plan, cluster, smem);   // includes the velocity update
-        timing_mark(SEC_GS, true, s);
-        recordingSubstep++;
-        return;
+        return true;
     }
+    if (ch.kind == SOLVE_GRID && planFits && launch_gs_grid(s, c, P, b, plan, ch.variant, ch.blocksPerSm))
+        return true;
     for (int k = 0; k < iterations; k++)
     {
         if (m.prm.fem)
@@ -1052,8 +1070,98 @@ void ClothPatch::record_substep(float h)
         launch_solve_multi_contacts(s, c, P, b, k);
     }
     launch_velocity(s, c, P);
-    timing_mark(SEC_GS, true, s);
-    recordingSubstep++;
+    return true;
+}
+
+// Autotuner: time one substep's solve (reset + Gauss-Seidel + velocity) for
+// every candidate — the cluster kernel when the cloth fits, each grid variant
+// (threads per CTA x constraints per thread) at 1, 2 and the most resident CTAs
+// per SM, and the per-colour kernels — each captured as a graph and replayed
+// with CUDA events; positions and velocities are restored after each. The
+// fastest is kept per problem shape for the process.
+static std::mutex g_tuneMutex;
+static std::vector<std::pair<std::vector<int>, SolverChoice>> g_tuneCache;
+
+bool ClothPatch::autotune(float h)
+{
+    ClothModel& m = model;
+    const SolverParams P = m.solver_params(h);
+    std::vector<int> key = {m.N, m.dc.T, m.dc.B, m.prm.iterations, m.prm.dihedral, m.prm.fem, m.prm.fixedIterations,
+                            (int)m.buf.numVColl, m.prm.bendFreq, (int)m.prm.stageRecords, m.solverMode};
+    key.insert(key.end(), m.triColourStart.begin(), m.triColourStart.end());
+    key.insert(key.end(), m.bendColourStart.begin(), m.bendColourStart.end());
+    {
+        std::lock_guard<std::mutex> lk(g_tuneMutex);
+        for (auto& kv : g_tuneCache)
+            if (kv.first == key) { m.choice = kv.second; m.tuned = true; return true; }
+    }
+    std::vector<SolverChoice> cand;
+    int shift = 0; size_t smem = 0;
+    const bool fits = m.triColourStart.size() <= 65 && m.bendColourStart.size() <= 65;
+    if (fits && m.solverMode != SOLVE_GRID && gs_cluster_size(m.N, shift, smem) > 0) cand.push_back({SOLVE_CLUSTER, 0, 0, 0.f});
+    if (fits && m.solverMode != SOLVE_CLUSTER)
+        for (int v = 0; v < gs_grid_variants(); v++)
+        {
+            const int mb = gs_grid_max_blocks_per_sm(v);
+            for (int bps : {1, 2, mb})
+                if (bps >= 1 && bps <= mb)
+                {
+                    bool dup = false;
+                    for (auto& c : cand) dup |= c.kind == SOLVE_GRID && c.variant == v && c.blocksPerSm == bps;
+                    if (!dup) cand.push_back({SOLVE_GRID, v, bps, 0.f});
+                }
+        }
+    if (m.solverMode == SOLVE_AUTO) cand.push_back({SOLVE_KERNELS, 0, 0, 0.f});
+    if (cand.empty()) cand.push_back({SOLVE_KERNELS, 0, 0, 0.f});
+    const size_t bytes = sizeof(float4) * (size_t)m.N;
+    float4* backup = nullptr;
+    SC_CUDA(cudaMalloc(&backup, 2 * bytes));
+    SC_CUDA(cudaMemcpyAsync(backup, m.dc.pos, bytes, cudaMemcpyDeviceToDevice, stream));
+    SC_CUDA(cudaMemcpyAsync(backup + m.N, m.dc.vel, bytes, cudaMemcpyDeviceToDevice, stream));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0); cudaEventCreate(&e1);
+    SolverChoice best = cand.back();
+    best.ms = 1e30f;
+    for (SolverChoice& ch : cand)
+    {
+        cudaGraph_t g = nullptr;
+        cudaGraphExec_t ge = nullptr;
+        if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) continue;
+        launch_reset_gs(stream, m.dc);
+        record_solve(stream, P, ch);
+        if (cudaStreamEndCapture(stream, &g) != cudaSuccess || cudaGraphInstantiate(&ge, g, 0) != cudaSuccess)
+        {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            continue;
+        }
+        cudaGraphDestroy(g);
+        const int reps = 3;
+        cudaGraphLaunch(ge, stream);                  // warm-up
+        cudaEventRecord(e0, stream);
+        for (int r = 0; r < reps; r++) cudaGraphLaunch(ge, stream);
+        cudaEventRecord(e1, stream);
+        cudaError_t err = cudaEventSynchronize(e1);
+        float ms = 0.f;
+        if (err == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
+        {
+            ch.ms = ms / reps;
+            if (ch.ms < best.ms) best = ch;
+        }
+        cudaGetLastError();
+        cudaGraphExecDestroy(ge);
+        cudaMemcpyAsync(m.dc.pos, backup, bytes, cudaMemcpyDeviceToDevice, stream);
+        cudaMemcpyAsync(m.dc.vel, backup + m.N, bytes, cudaMemcpyDeviceToDevice, stream);
+    }
+    cudaStreamSynchronize(stream);
+    cudaEventDestroy(e0); cudaEventDestroy(e1);
+    cudaFree(backup);
+    m.tuneLog = cand;
+    m.choice = best;
+    m.tuned = true;
+    std::lock_guard<std::mutex> lk(g_tuneMutex);
+    g_tuneCache.push_back({key, best});
+    return true;
 }
 
 void ClothPatch::timing_mark(int section, bool end, cudaStream_t s)
@@ -1123,6 +1231,12 @@ bool ClothPatch::step(float dt)
     if (!graph || graphDt != dt || graphSteps != n || graphParamVersion != m.paramVersion || graphWorldVersion != world.version)
     {
         if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
+        if (m.solverMode == SOLVE_KERNELS) m.choice = {SOLVE_KERNELS, 0, 0, 0.f};
+        else if (!m.tuned || m.tunedVersion != m.paramVersion)
+        {
+            if (!autotune(h)) return false;
+            m.tunedVersion = m.paramVersion;
+        }
         cudaGraph_t g;
         if (timingFrames && timingCapture.size() != (size_t)n * NSEC * 2) set_timing(timingFrames);
         recordingSubstep = 0;

@@ -96,9 +96,12 @@ struct HostParams
     float selfThreshold = 0.003f;
     int iterations = 50, flags = 0, bendFreq = 2;
     bool fem = false, dihedral = true, fixedIterations = false, ccd = false;
-    bool clusterSolver = true;   // cluster-resident solver when the cloth fits
     bool stageRecords = true;    // cluster solver: constraint records in shared memory
 };
+
+// solver selection (autotuned unless forced)
+enum SolverKind { SOLVE_AUTO = 0, SOLVE_CLUSTER = 1, SOLVE_GRID = 2, SOLVE_KERNELS = 3 };
+struct SolverChoice { int kind, variant, blocksPerSm; float ms; };
 
 struct FemHost { uint32_t i1, i2, i3; float du1, du2, dv1, dv2, det, invDet, lu0, lv0, su, sv, lu2, lv2, area; };
 
@@ -154,6 +157,11 @@ public:
     void download_state(cudaStream_t s);
     void upload_state(cudaStream_t s);
     SolverParams solver_params(float h) const;
+    int solverMode = SOLVE_AUTO;                // forced solver, or the tuner's choice
+    SolverChoice choice{SOLVE_CLUSTER, 0, 0, 0.f};
+    bool tuned = false;
+    uint64_t tunedVersion = 0;
+    std::vector<SolverChoice> tuneLog;          // candidates and their times of the last tuning
     void colour_constraints();
     void touch() { paramVersion++; }
 };
@@ -201,6 +209,8 @@ public:
     bool step(float dt);
     void update_mesh();
     void record_substep(float h);
+    bool record_solve(cudaStream_t s, const SolverParams& P, const SolverChoice& ch);
+    bool autotune(float h);
     void sync();
 };
 

@@ -111,6 +111,14 @@ int gs_cluster_size(int N, int& shift, size_t& smem);
 void launch_gs_cluster(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b, GsPlan plan,
                        int clusterSize, size_t smem);
 
+// grid-resident solver (cooperative launch, any cloth or batch size); variants
+// differ in threads per CTA and in constraints per thread (tiles)
+int gs_grid_variants();
+void gs_grid_variant_info(int variant, int& threads, int& femTile, int& bendTile);
+int gs_grid_max_blocks_per_sm(int variant);
+bool launch_gs_grid(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b, GsPlan plan,
+                    int variant, int blocksPerSm);
+
 // exclusive scan of n ints (out may alias nothing); total written to *total if not null
 void scan_ints(cudaStream_t s, const int* in, int* out, int n, int* total, int* tmp);
 

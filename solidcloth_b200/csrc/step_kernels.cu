@@ -2195,6 +2195,249 @@ __global__ void __launch_bounds__(GS_THREADS) k_gs_cluster(DevCloth c, SolverPar
     }
 }
 
+// ---------------------------------------------------- grid-resident solver
+// The same Gauss-Seidel loop as k_gs_cluster for clothes (and batches of
+// clothes) too large for one cluster: one cooperative launch per substep, every
+// CTA of the grid resident, particles in global memory (L2-resident: 16 B per
+// particle), grid-wide barriers between colours. Each thread takes TILE
+// consecutive constraints of a colour and issues all their loads before any
+// projection (the constraints of a colour share no particle), so TILE
+// projections' memory latencies overlap. Same phases and order as the
+// per-colour kernels: bit-identical results.
+
+// particle accessor over a tile entry's own registers (the projection functions
+// load their particles first and store them last)
+struct RegPos
+{
+    uint32_t id[4];
+    mutable float4 v[4];
+    __device__ __forceinline__ float4 ld(uint32_t q) const
+    {
+        return q == id[0] ? v[0] : q == id[1] ? v[1] : q == id[2] ? v[2] : v[3];
+    }
+    __device__ __forceinline__ void st(uint32_t q, float4 x) const
+    {
+        if (q == id[0]) v[0] = x;
+        else if (q == id[1]) v[1] = x;
+        else if (q == id[2]) v[2] = x;
+        else v[3] = x;
+    }
+};
+
+template <int TILE>
+__device__ __forceinline__ void fem_tiles(const DevCloth& c, const SolverParams& P, int s0, int s1, int tid, int nth)
+{
+    for (int base = s0 + tid * TILE; base < s1; base += nth * TILE)
+    {
+        float4 r0[TILE], r1[TILE], r2[TILE];
+        RegPos rp[TILE];
+#pragma unroll
+        for (int u = 0; u < TILE; u++)
+        {
+            const int j = min(base + u, s1 - 1);
+            r0[u] = c.fem[3 * j]; r1[u] = c.fem[3 * j + 1]; r2[u] = c.fem[3 * j + 2];
+        }
+#pragma unroll
+        for (int u = 0; u < TILE; u++)
+        {
+            rp[u].id[0] = __float_as_uint(r0[u].x); rp[u].id[1] = __float_as_uint(r0[u].y);
+            rp[u].id[2] = __float_as_uint(r0[u].z); rp[u].id[3] = 0xffffffffu;
+            rp[u].v[0] = c.pos[rp[u].id[0]]; rp[u].v[1] = c.pos[rp[u].id[1]]; rp[u].v[2] = c.pos[rp[u].id[2]];
+        }
+#pragma unroll
+        for (int u = 0; u < TILE; u++)
+            if (base + u < s1) fem_project(rp[u], r0[u], r1[u], r2[u], P);
+#pragma unroll
+        for (int u = 0; u < TILE; u++)
+            if (base + u < s1)
+            {
+                c.pos[rp[u].id[0]] = rp[u].v[0]; c.pos[rp[u].id[1]] = rp[u].v[1]; c.pos[rp[u].id[2]] = rp[u].v[2];
+            }
+    }
+}
+
+template <int TILE>
+__device__ __forceinline__ float bend_tiles(const DevCloth& c, const SolverParams& P, int s0, int s1, int tid, int nth)
+{
+    float err = 0.f;
+    for (int base = s0 + tid * TILE; base < s1; base += nth * TILE)
+    {
+        uint4 bc[TILE];
+        RegPos rp[TILE];
+#pragma unroll
+        for (int u = 0; u < TILE; u++) bc[u] = c.bend[min(base + u, s1 - 1)];
+#pragma unroll
+        for (int u = 0; u < TILE; u++)
+        {
+            rp[u].id[0] = bc[u].x; rp[u].id[1] = bc[u].y; rp[u].id[2] = bc[u].z; rp[u].id[3] = bc[u].w;
+            rp[u].v[0] = c.pos[bc[u].x]; rp[u].v[1] = c.pos[bc[u].y]; rp[u].v[2] = c.pos[bc[u].z]; rp[u].v[3] = c.pos[bc[u].w];
+        }
+        bool moved[TILE];
+#pragma unroll
+        for (int u = 0; u < TILE; u++)
+        {
+            moved[u] = false;
+            if (base + u < s1)
+            {
+                const float e = bend_project(rp[u], bc[u], P);
+                moved[u] = e >= 0.f;
+                err = fmaxf(err, e);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < TILE; u++)
+            if (moved[u])
+            {
+                c.pos[bc[u].x] = rp[u].v[0]; c.pos[bc[u].y] = rp[u].v[1]; c.pos[bc[u].z] = rp[u].v[2]; c.pos[bc[u].w] = rp[u].v[3];
+            }
+    }
+    return err;
+}
+
+template <int NT, int FT, int BT>
+__global__ void __launch_bounds__(NT) k_gs_grid(DevCloth c, SolverParams P, Buffers b, ColourArgs ca, GsPlan plan)
+{
+    cg::grid_group grid = cg::this_grid();
+    __shared__ float sErr[8];
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+    const GlobalPos pa{c.pos};
+    const bool track = !P.fixedIterations;
+    if (threadIdx.x < 8) sErr[threadIdx.x] = 0.f;
+    __syncthreads();
+    for (int k = 0; k < plan.iterations; k++)
+    {
+        if (P.fem)
+            for (int col = 0; col < plan.nFemCol; col++)
+            {
+                fem_tiles<FT>(c, P, plan.femStart[col], plan.femStart[col + 1], tid, nth);
+                grid.sync();
+            }
+        if (P.dihedral && k % P.bendFreq == 0)
+            for (int col = 0; col < plan.nBendCol; col++)
+            {
+                const float e = bend_tiles<BT>(c, P, plan.bendStart[col], plan.bendStart[col + 1], tid, nth);
+                if (track && e > 0.f) atomicMax((int*)&sErr[2], __float_as_int(e));
+                grid.sync();
+            }
+        if (b.numVColl > 0)
+        {
+            for (int i = tid; i < c.N; i += nth)
+            {
+                const float e = vertex_contacts_one(pa, c, P, b, i);
+                if (track && e > 0.f) atomicMax((int*)&sErr[3], __float_as_int(e));
+            }
+            grid.sync();
+        }
+        for (int cls = 0; cls < 4; cls++)
+        {
+            const ClassView& cv = ca.cls[cls];
+            const int n = *cv.count;
+            if (n == 0) continue;
+            for (int col = 0; col < MAX_COLOURS; col++)
+            {
+                const int s0 = cv.start[col], s1 = cv.start[col + 1];
+                if (s0 == s1) continue;
+                if (col == MAX_COLOURS - 1)
+                {
+                    // colours exhausted: one thread, list order (as the oracle)
+                    if (tid == 0)
+                        for (int i = 0; i < n; i++)
+                            if (cv.colour[i] == MAX_COLOURS - 1)
+                            {
+                                const float e = solve_contact(pa, c, P, b, cls, i);
+                                if (track && e > 0.f) atomicMax((int*)&sErr[4 + cls], __float_as_int(e));
+                            }
+                }
+                else
+                    for (int j = s0 + tid; j < s1; j += nth)
+                    {
+                        const float e = solve_contact(pa, c, P, b, cls, cv.order[j]);
+                        if (track && e > 0.f) atomicMax((int*)&sErr[4 + cls], __float_as_int(e));
+                    }
+                grid.sync();
+            }
+        }
+        if (tid == 0) c.scal[9] = (float)(k + 1);
+        if (track)
+        {
+            // SolveGS exit test (Physics/ClothPBD.cpp:354-361) on grid-wide maxima
+            __syncthreads();
+            if (threadIdx.x < 8 && threadIdx.x >= 2 && sErr[threadIdx.x] > 0.f)
+                atomic_max_pos(&c.scal[threadIdx.x], sErr[threadIdx.x]);
+            grid.sync();
+            if (tid == 0)
+            {
+                const float eps = 0.01f;
+                float cb = c.scal[2], cv = c.scal[3], ce = c.scal[4], ct = c.scal[5], sct = c.scal[6], see = c.scal[7];
+                if (cb < 0.005f && see < P.selfThreshold && sct < P.selfThreshold && cv < eps && ce < eps && ct < eps)
+                    c.scal[8] = 1.f;
+                for (int s2 = 3; s2 < 8; s2++) c.scal[s2] = 0.f;
+                if ((k + 1) % P.bendFreq == 0) c.scal[2] = 0.f;
+            }
+            if (threadIdx.x < 8) sErr[threadIdx.x] = 0.f;
+            grid.sync();
+            if (__ldcg(&c.scal[8]) != 0.f) break;
+        }
+    }
+    // velocity update (ClothPBD.cpp:314-321)
+    for (int g = tid; g < c.N; g += nth)
+    {
+        const float4 p = c.pos[g];
+        if (p.w == 0.f) continue;
+        const float4 q = c.prev[g];
+        V3 vel = P.invH * (mk(p.x, p.y, p.z) - mk(q.x, q.y, q.z));
+        c.vel[g] = make_float4(vel.x, vel.y, vel.z, 0.f);
+    }
+}
+
+// variants the tuner chooses among: (threads per CTA, FEM tile, bend tile)
+using GridKernel = void (*)(DevCloth, SolverParams, Buffers, ColourArgs, GsPlan);
+static const GridKernel kGridVariants[] = {
+    k_gs_grid<256, 1, 1>, k_gs_grid<256, 2, 1>, k_gs_grid<256, 2, 2>, k_gs_grid<256, 4, 2>,
+    k_gs_grid<512, 1, 1>, k_gs_grid<512, 2, 1>, k_gs_grid<512, 2, 2>, k_gs_grid<512, 4, 2>,
+};
+static const int kGridThreads[] = {256, 256, 256, 256, 512, 512, 512, 512};
+static const int kGridFemTile[] = {1, 2, 2, 4, 1, 2, 2, 4};
+static const int kGridBendTile[] = {1, 1, 2, 2, 1, 1, 2, 2};
+
+int gs_grid_variants() { return (int)(sizeof(kGridThreads) / sizeof(int)); }
+
+void gs_grid_variant_info(int v, int& threads, int& femTile, int& bendTile)
+{
+    threads = kGridThreads[v]; femTile = kGridFemTile[v]; bendTile = kGridBendTile[v];
+}
+
+// resident CTAs per SM for variant v (0 if it cannot launch cooperatively)
+int gs_grid_max_blocks_per_sm(int v)
+{
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kGridVariants[v], kGridThreads[v], 0) != cudaSuccess) n = 0;
+    cudaGetLastError();
+    return n;
+}
+
+bool launch_gs_grid(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b, GsPlan plan,
+                    int variant, int blocksPerSm)
+{
+    int dev = 0, sms = 0, coop = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+    const int maxB = gs_grid_max_blocks_per_sm(variant);
+    if (!coop || maxB < 1) return false;
+    const int bps = blocksPerSm < 1 ? 1 : (blocksPerSm > maxB ? maxB : blocksPerSm);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(sms * bps);
+    cfg.blockDim = dim3(kGridThreads[variant]);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute at;
+    at.id = cudaLaunchAttributeCooperative;
+    at.val.cooperative = 1;
+    cfg.attrs = &at; cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kGridVariants[variant], c, P, b, colour_args(b), plan) == cudaSuccess;
+}
+
 int gs_cluster_size(int N, int& shift, size_t& smem)
 {
     static int supported = -1;

@@ -208,11 +208,12 @@ def test_ccd_broadphase_and_hits_bitexact(thickness):
 
 
 @pytest.mark.parametrize("scene", ["cfg0", "sdf", "fold", "ccd"])
-def test_cluster_solver_equals_per_colour_kernels(scene):
+def test_solvers_are_bit_identical(scene):
     """The cluster-resident solver (one launch per substep, particles in
     distributed shared memory, records staged in shared memory or read from
-    global memory) and the one-kernel-per-colour path are the same algorithm in
-    the same order: bit-identical trajectories."""
+    global memory), every variant of the grid-resident cooperative solver, the
+    one-kernel-per-colour path and the autotuner's choice are the same algorithm
+    in the same order: bit-identical trajectories."""
     from solidcloth_b200 import api
     state = None
     if scene == "cfg0":
@@ -228,10 +229,17 @@ def test_cluster_solver_equals_per_colour_kernels(scene):
     else:
         sc, state = scenes.ccd_scene(16)
     out = []
-    for cluster, staged in ((True, True), (True, False), (False, False)):
+    modes = [("cluster", True), ("cluster", False), ("kernels", False)]
+    modes += [("grid", (v, 1)) for v in range(len(api.grid_variants()))] + [("grid", (0, 2)), ("auto", None)]
+    for mode, arg in modes:
         w, p = api.load_scene(sc)
-        p.model.set_cluster_solver(cluster)
-        p.model.set_cluster_staging(staged)
+        if mode == "cluster":
+            p.model.set_cluster_solver(True)
+            p.model.set_cluster_staging(arg)
+        elif mode == "kernels":
+            p.model.set_cluster_solver(False)
+        elif mode == "grid":
+            p.model.set_grid_solver(*arg)
         if state is not None:
             p.model.set_state(*state)
         for _ in range(4):
@@ -239,10 +247,10 @@ def test_cluster_solver_equals_per_colour_kernels(scene):
             p.update_mesh()
         out.append((p.model.positions(), p.model.velocities(), p.status() & ~16))
         p.free()
-    for o in out:
-        assert o[2] == 0
-    for o in out[1:]:
-        assert _same(out[0][0], o[0]) and _same(out[0][1], o[1])
+    for o, m in zip(out, modes):
+        assert o[2] == 0, m
+    for o, m in zip(out[1:], modes[1:]):
+        assert _same(out[0][0], o[0]) and _same(out[0][1], o[1]), m
 
 
 def test_early_exit_mode_matches_oracle():
