@@ -97,6 +97,17 @@ SCEXP void scGetCapsuleInfo(scHandle capsule, float* radius, float* halfHeight, 
 /* ---- cloth patch (Demo/ClothAPI.h:91-99) ---- */
 SCEXP scClothPatch scCreateClothPatch(scCollisionWorld collWorld);
 SCEXP void scFreeClothPatch(scClothPatch patch);
+/* Batches (additions, no reference counterpart): one patch that steps `count`
+   initialised patches as independent instances in one CUDA graph per frame and
+   one solver launch per substep. The parts must share every solver parameter and
+   the substep count; each keeps the colliders of its own world (vertex, wall and
+   self collisions; triangle / edge collider contacts are not supported). The
+   parts' state is copied: they may be freed afterwards. The batch is an ordinary
+   patch for scStepCloth and the getters; instance k owns particles
+   [first, first + num) of its model. */
+SCEXP scClothPatch scCreateClothBatch(scCollisionWorld world, const scClothPatch* parts, int count);
+SCEXP int scGetBatchSize(scClothPatch batch);
+SCEXP void scGetBatchInstance(scClothPatch batch, int k, int* firstParticle, int* numParticles);
 SCEXP scModel scGetClothModel(scClothPatch patch);
 SCEXP scMesh scGetClothMesh(scClothPatch patch);
 SCEXP void scInitCloth(scClothPatch patch, int divX, int divY, float inc, scVector3 offset, bool horizontal, bool attached);

@@ -1456,16 +1456,22 @@ struct Cloth
 
     /* Deterministic independent-set colouring used by the GPU for contacts that
        touch several particles: a contact joins the current colour when its key
-       (hash of its list index, then the index) is the smallest among the still
-       uncoloured contacts on each of its particles. Returns the solve order
-       (colour, then list index). */
+       (a hash of its particle indices, then its list index) is the smallest among
+       the still uncoloured contacts on each of its particles. Returns the solve
+       order (colour, then list index). */
     template <typename C, typename F>
     std::vector<int> colour_order(const std::vector<C>& list, F verts, std::vector<int>* colOut = nullptr) const
     {
         const int n = (int)list.size();
         std::vector<int> colour(n, -1);
         std::vector<uint64_t> key(n), minKey(N);
-        for (int i = 0; i < n; i++) key[i] = ((uint64_t)contact_hash((u32)i) << 32) | (u32)i;
+        for (int i = 0; i < n; i++)
+        {
+            u32 vs[4]; int nv = verts(list[i], vs);
+            u32 hsh = 0x9e3779b9U;
+            for (int k = 0; k < nv; k++) hsh = contact_hash(hsh ^ vs[k]);
+            key[i] = ((uint64_t)hsh << 32) | (u32)i;
+        }
         /* at most MAX_ROUNDS rounds; what is left takes the last colour and is
            solved in list order (as the GPU's single-thread fallback does) */
         const int MAX_ROUNDS = 127;

@@ -126,6 +126,9 @@ SIGNATURES = {
     "scSetSelfCCD": ([scModel, C.c_bool], None),
     "scSetClusterSolver": ([scModel, C.c_bool], None),
     "scSetClusterStaging": ([scModel, C.c_bool], None),
+    "scCreateClothBatch": ([scCollisionWorld, C.POINTER(scClothPatch), C.c_int], scClothPatch),
+    "scGetBatchSize": ([scClothPatch], C.c_int),
+    "scGetBatchInstance": ([scClothPatch, C.c_int, _i, _i], None),
     "scSetSolverMode": ([scModel, C.c_int], None),
     "scSetGridSolver": ([scModel, C.c_int, C.c_int], None),
     "scGetSolverChoice": ([scModel, _i, _f, C.c_int], C.c_int),
@@ -462,6 +465,40 @@ class ClothPatch:
         if self.h is not None:
             lib().scFreeClothPatch(self.h)
             self.h = None
+
+
+class ClothBatch(ClothPatch):
+    """Independent clothes stepped as one patch (scCreateClothBatch)."""
+
+    def __init__(self, parts):
+        self.world = CollisionWorld()
+        arr = (scClothPatch * len(parts))(*[p.h for p in parts])
+        self.h = lib().scCreateClothBatch(self.world.h, arr, len(parts))
+        _check("scCreateClothBatch")
+        if not self.h.ptr:
+            raise RuntimeError("scCreateClothBatch failed")
+        self.model = ClothModel(lib().scGetClothModel(self.h), self)
+
+    def size(self) -> int:
+        return int(lib().scGetBatchSize(self.h))
+
+    def instance(self, k: int):
+        """(first particle, particle count) of instance k"""
+        a, n = C.c_int(), C.c_int()
+        lib().scGetBatchInstance(self.h, int(k), C.byref(a), C.byref(n))
+        _check("scGetBatchInstance")
+        return a.value, n.value
+
+
+def load_batch(scenes_, ccd: bool | None = None):
+    """One batch patch over a list of scenes.Scene (each with its own colliders);
+    the per-scene patches are built, merged and freed."""
+    parts = [load_scene(s, ccd) for s in scenes_]
+    b = ClothBatch([p for _, p in parts])
+    for w, p in parts:
+        p.free()
+        w.free()
+    return b
 
 
 def grid_variants():

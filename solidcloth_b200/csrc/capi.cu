@@ -160,6 +160,39 @@ scClothPatch scCreateClothPatch(scCollisionWorld w)
     return p;
 }
 void scFreeClothPatch(scClothPatch p) { delete P(p); }
+
+scClothPatch scCreateClothBatch(scCollisionWorld w, const scClothPatch* parts, int count)
+{
+    scClothPatch p; p.ptr = nullptr;
+    if (!W(w) || !parts || count < 1) { set_error(SC_ERR_ARG, "batch needs a world and at least one patch"); return p; }
+    std::vector<ClothPatch*> v;
+    for (int k = 0; k < count; k++) v.push_back(P(parts[k]));
+    ClothPatch* b = new ClothPatch(*W(w));
+    if (!b->init_batch(v)) { delete b; return p; }
+    p.ptr = b;
+    return p;
+}
+
+int scGetBatchSize(scClothPatch p)
+{
+    if (!P(p)) return 0;
+    const auto& iv = P(p)->model.instV;
+    return iv.empty() ? 1 : (int)iv.size() - 1;
+}
+
+void scGetBatchInstance(scClothPatch p, int k, int* firstParticle, int* numParticles)
+{
+    if (!P(p)) return;
+    const auto& iv = P(p)->model.instV;
+    int a = 0, n = P(p)->model.N;
+    if (!iv.empty())
+    {
+        if (k < 0 || k + 1 >= (int)iv.size()) { set_error(SC_ERR_ARG, "instance out of range"); return; }
+        a = iv[k]; n = iv[k + 1] - iv[k];
+    }
+    if (firstParticle) *firstParticle = a;
+    if (numParticles) *numParticles = n;
+}
 scModel scGetClothModel(scClothPatch p) { scModel m; m.ptr = P(p) ? &P(p)->model : nullptr; return m; }
 scMesh scGetClothMesh(scClothPatch p) { scMesh m; m.ptr = P(p) ? &P(p)->mesh : nullptr; return m; }
 
@@ -251,17 +284,21 @@ static std::vector<VC> vertex_contacts(ClothModel* m, std::vector<int>* owner)
     std::vector<VC> out;
     if (!m->buf.vc || m->buf.numVColl == 0) return out;
     host_sync(m);
-    std::vector<uint8_t> cnt = dl(m->buf.vcCount, (size_t)m->buf.numVColl * m->N);
-    size_t total = 0;
-    for (auto& g : m->vcollHost) total += (size_t)g.kmax * m->N;
+    size_t total = 0, counts = 0;
+    for (auto& g : m->vcollHost)
+    {
+        total = std::max(total, (size_t)g.slotBase + (size_t)g.kmax * g.vCount);
+        counts = std::max(counts, (size_t)g.countBase + g.vCount);
+    }
+    std::vector<uint8_t> cnt = dl(m->buf.vcCount, counts);
     std::vector<VC> slots = dl(m->buf.vc, total);
     for (int ci = 0; ci < m->buf.numVColl; ci++)
     {
         const VColl& g = m->vcollHost[ci];
-        for (int i = 0; i < m->N; i++)
-            for (int k = 0; k < cnt[(size_t)ci * m->N + i]; k++)
+        for (int i = g.vBegin; i < g.vBegin + g.vCount; i++)
+            for (int k = 0; k < cnt[(size_t)g.countBase + (i - g.vBegin)]; k++)
             {
-                out.push_back(slots[g.slotBase + (size_t)i * g.kmax + k]);
+                out.push_back(slots[g.slotBase + (size_t)(i - g.vBegin) * g.kmax + k]);
                 if (owner) owner->push_back(i);
             }
     }

@@ -583,7 +583,27 @@ bool ClothModel::upload_topology(const HMesh& mesh)
         // Morton code of the rest shape)
         std::vector<V3> ec(E);
         for (int e = 0; e < E; e++) ec[e] = 0.5f * (hpos[mesh.edges[e].i1] + hpos[mesh.edges[e].i2]);
-        std::vector<int> vq = morton_order(hpos), eq = morton_order(ec);
+        std::vector<int> vq, eq;
+        if (instV.empty()) { vq = morton_order(hpos); eq = morton_order(ec); }
+        else
+        {
+            // a batch: instance after instance, Morton order inside each
+            for (size_t k = 0; k + 1 < instV.size(); k++)
+            {
+                for (int v : morton_order(std::vector<V3>(hpos.begin() + instV[k], hpos.begin() + instV[k + 1])))
+                    vq.push_back(v + instV[k]);
+                for (int e : morton_order(std::vector<V3>(ec.begin() + instE[k], ec.begin() + instE[k + 1])))
+                    eq.push_back(e + instE[k]);
+            }
+            std::vector<int> vi(N);
+            for (size_t k = 0; k + 1 < instV.size(); k++)
+                for (int v = instV[k]; v < instV[k + 1]; v++) vi[v] = (int)k;
+            int* dv = (int*)dalloc(sizeof(int) * ((size_t)N + instV.size()));
+            SC_CUDA(cudaMemcpy(dv, vi.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
+            SC_CUDA(cudaMemcpy(dv + N, instV.data(), sizeof(int) * instV.size(), cudaMemcpyHostToDevice));
+            dc.vInst = dv;
+            dc.instStart = dv + N;
+        }
         int* d = (int*)dalloc(sizeof(int) * ((size_t)N + E + 2));
         SC_CUDA(cudaMemcpy(d, vq.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
         if (E) SC_CUDA(cudaMemcpy(d + N, eq.data(), sizeof(int) * E, cudaMemcpyHostToDevice));
@@ -608,27 +628,24 @@ bool ClothModel::upload_topology(const HMesh& mesh)
         SC_CUDA(cudaMemcpy(dc.meshTriN, t4.data(), sizeof(float4) * T, cudaMemcpyHostToDevice));
     }
     // BVH topologies from the rest shape
-    auto mkbvh = [&](const std::vector<V3>& cen, DevBVH& out, DevBVH* shareTopo) -> bool {
-        LBVHHost h;
-        h.build(cen);
+    // upload a built topology (h) with its node boxes' link words
+    auto upload_bvh = [&](LBVHHost& h, DevBVH& out, const std::vector<int>* roots) -> bool {
         out.numLeaves = h.numLeaves; out.numNodes = h.numNodes;
-        if (shareTopo)
+        int* d = (int*)dalloc(sizeof(int) * (4 * (size_t)h.numNodes + h.numLeaves + 4));
+        SC_CUDA(cudaMemcpy(d, h.child.data(), sizeof(int) * h.numNodes, cudaMemcpyHostToDevice));
+        SC_CUDA(cudaMemcpy(d + h.numNodes, h.escape.data(), sizeof(int) * h.numNodes, cudaMemcpyHostToDevice));
+        SC_CUDA(cudaMemcpy(d + 2 * h.numNodes, h.parent.data(), sizeof(int) * h.numNodes, cudaMemcpyHostToDevice));
+        SC_CUDA(cudaMemcpy(d + 3 * h.numNodes, h.maxPrim.data(), sizeof(int) * h.numNodes, cudaMemcpyHostToDevice));
+        SC_CUDA(cudaMemcpy(d + 4 * h.numNodes, h.leafNode.data(), sizeof(int) * h.numLeaves, cudaMemcpyHostToDevice));
+        out.child = d; out.escape = d + h.numNodes; out.parent = d + 2 * h.numNodes;
+        out.maxPrim = d + 3 * h.numNodes; out.leafNode = d + 4 * h.numNodes;
+        out.instRoot = nullptr;
+        if (roots)
         {
-            out.child = shareTopo->child; out.escape = shareTopo->escape; out.parent = shareTopo->parent;
-            out.leafNode = shareTopo->leafNode; out.maxPrim = shareTopo->maxPrim;
+            int* r = (int*)dalloc(sizeof(int) * roots->size());
+            SC_CUDA(cudaMemcpy(r, roots->data(), sizeof(int) * roots->size(), cudaMemcpyHostToDevice));
+            out.instRoot = r;
         }
-        else
-        {
-            int* d = (int*)dalloc(sizeof(int) * (4 * (size_t)h.numNodes + h.numLeaves + 4));
-            SC_CUDA(cudaMemcpy(d, h.child.data(), sizeof(int) * h.numNodes, cudaMemcpyHostToDevice));
-            SC_CUDA(cudaMemcpy(d + h.numNodes, h.escape.data(), sizeof(int) * h.numNodes, cudaMemcpyHostToDevice));
-            SC_CUDA(cudaMemcpy(d + 2 * h.numNodes, h.parent.data(), sizeof(int) * h.numNodes, cudaMemcpyHostToDevice));
-            SC_CUDA(cudaMemcpy(d + 3 * h.numNodes, h.maxPrim.data(), sizeof(int) * h.numNodes, cudaMemcpyHostToDevice));
-            SC_CUDA(cudaMemcpy(d + 4 * h.numNodes, h.leafNode.data(), sizeof(int) * h.numLeaves, cudaMemcpyHostToDevice));
-            out.child = d; out.escape = d + h.numNodes; out.parent = d + 2 * h.numNodes;
-            out.maxPrim = d + 3 * h.numNodes; out.leafNode = d + 4 * h.numNodes;
-        }
-        // traversal reads a node's links from the w components of its box
         std::vector<float4> lo(h.numNodes), hi(h.numNodes);
         for (int k = 0; k < h.numNodes; k++)
         {
@@ -642,12 +659,66 @@ bool ClothModel::upload_topology(const HMesh& mesh)
         out.visit = (int*)dalloc(sizeof(int) * h.numNodes);
         return true;
     };
+    // batch: one tree per instance over its own primitives [start[k], start[k+1]),
+    // concatenated (node and primitive indices offset); queries start at their
+    // instance's root, so instances never see each other
+    auto mkforest = [&](const std::vector<V3>& cen, const std::vector<int>& start, DevBVH& out) -> bool {
+        LBVHHost all;
+        std::vector<int> roots;
+        for (size_t k = 0; k + 1 < start.size(); k++)
+        {
+            const int p0 = start[k], np = start[k + 1] - start[k];
+            const int o = all.numNodes;
+            roots.push_back(o);
+            if (np == 0) continue;
+            LBVHHost h;
+            h.build(std::vector<V3>(cen.begin() + p0, cen.begin() + p0 + np));
+            for (int j = 0; j < h.numNodes; j++)
+            {
+                all.child.push_back(h.child[j] < 0 ? ~(~h.child[j] + p0) : h.child[j] + o);
+                all.escape.push_back(h.escape[j] + o);
+                all.parent.push_back(h.parent[j] < 0 ? -1 : h.parent[j] + o);
+                all.maxPrim.push_back(h.maxPrim[j] + p0);
+            }
+            for (int j = 0; j < np; j++) all.leafNode.push_back(h.leafNode[j] + o);
+            all.numNodes += h.numNodes;
+            all.numLeaves += h.numLeaves;
+        }
+        return upload_bvh(all, out, &roots);
+    };
+    // a tree over cen, or (shareTopo) a second set of boxes over another tree's topology
+    auto mkbvh = [&](const std::vector<V3>& cen, DevBVH& out, DevBVH* shareTopo) -> bool {
+        if (!shareTopo)
+        {
+            LBVHHost h;
+            h.build(cen);
+            return upload_bvh(h, out, nullptr);
+        }
+        out = *shareTopo;
+        std::vector<float4> lo(out.numNodes), hi(out.numNodes);
+        SC_CUDA(cudaMemcpy(lo.data(), shareTopo->lo, sizeof(float4) * out.numNodes, cudaMemcpyDeviceToHost));
+        SC_CUDA(cudaMemcpy(hi.data(), shareTopo->hi, sizeof(float4) * out.numNodes, cudaMemcpyDeviceToHost));
+        out.lo = (float4*)dalloc(sizeof(float4) * out.numNodes);
+        out.hi = (float4*)dalloc(sizeof(float4) * out.numNodes);
+        SC_CUDA(cudaMemcpy(out.lo, lo.data(), sizeof(float4) * out.numNodes, cudaMemcpyHostToDevice));
+        SC_CUDA(cudaMemcpy(out.hi, hi.data(), sizeof(float4) * out.numNodes, cudaMemcpyHostToDevice));
+        out.visit = (int*)dalloc(sizeof(int) * out.numNodes);
+        return true;
+    };
     std::vector<V3> tc(T), ec(E);
     for (int t = 0; t < T; t++)
         tc[t] = (1.f / 3.f) * (hpos[mesh.idx[3 * t]] + hpos[mesh.idx[3 * t + 1]] + hpos[mesh.idx[3 * t + 2]]);
     for (int e = 0; e < E; e++) ec[e] = 0.5f * (hpos[mesh.edges[e].i1] + hpos[mesh.edges[e].i2]);
-    if (!mkbvh(tc, triBvh, nullptr)) return false;
-    if (!mkbvh(ec, edgeBvh, nullptr)) return false;
+    if (instV.empty())
+    {
+        if (!mkbvh(tc, triBvh, nullptr)) return false;
+        if (!mkbvh(ec, edgeBvh, nullptr)) return false;
+    }
+    else
+    {
+        if (!mkforest(tc, instT, triBvh)) return false;
+        if (!mkforest(ec, instE, edgeBvh)) return false;
+    }
     if (!mkbvh(tc, sweptTriBvh, &triBvh)) return false;
     if (!mkbvh(ec, sweptEdgeBvh, &edgeBvh)) return false;
     bufWorldVersion = ~0ull;
@@ -694,12 +765,20 @@ bool ClothModel::ensure_buffers(const CollisionWorld& world, cudaStream_t s)
     const int T = dc.T, E = dc.E;
     vcollHost.clear();
     std::vector<DevMesh> meshes;
-    int slotBase = 0;
-    for (auto& cp : world.list)
+    int slotBase = 0, countBase = 0;
+    // (collider, first particle, particles): the world's colliders act on the whole
+    // cloth; a batch's on their own instance
+    std::vector<BatchColl> entries = batchColl;
+    if (instV.empty())
+        for (auto& cp : world.list) entries.push_back({cp, 0, N, 0});
+    std::vector<int2> instColl(instV.empty() ? 0 : instV.size() - 1, make_int2(0, 0));
+    for (auto& en : entries)
     {
-        Collidable* c = cp.get();
+        Collidable* c = en.coll.get();
         VColl g = {};
         g.type = c->type;
+        g.vBegin = en.vBegin;
+        g.vCount = en.vCount;
         if (c->type == CT_WALLS)
         {
             WallsC* w = (WallsC*)c;
@@ -738,14 +817,29 @@ bool ClothModel::ensure_buffers(const CollisionWorld& world, cudaStream_t s)
             continue;
         }
         g.slotBase = slotBase;
-        slotBase += g.kmax * N;
+        slotBase += g.kmax * g.vCount;
+        g.countBase = countBase;
+        countBase += g.vCount;
+        if (!instColl.empty())
+        {
+            int2& r = instColl[en.inst];
+            if (r.y == 0) r.x = (int)vcollHost.size();
+            r.y++;
+        }
         vcollHost.push_back(g);
     }
     const int nv = (int)vcollHost.size();
+    buf.instColl = nullptr;
+    if (!instColl.empty())
+    {
+        int2* d = (int2*)dalloc(sizeof(int2) * instColl.size(), true);
+        SC_CUDA(cudaMemcpy(d, instColl.data(), sizeof(int2) * instColl.size(), cudaMemcpyHostToDevice));
+        buf.instColl = d;
+    }
     int nTE = 0;
     for (auto& g : vcollHost) if (g.type == CT_SPHERE || g.type == CT_SDF || g.type == CT_MESH) nTE++;
     buf.numVColl = nv;
-    buf.vcCount = (uint8_t*)dalloc((size_t)std::max(1, nv) * N, true);
+    buf.vcCount = (uint8_t*)dalloc((size_t)std::max(1, countBase), true);
     buf.vc = (VC*)dalloc(sizeof(VC) * (size_t)std::max(1, slotBase), true);
     VColl* dcoll = (VColl*)dalloc(sizeof(VColl) * std::max(1, nv), true);
     if (nv) SC_CUDA(cudaMemcpy(dcoll, vcollHost.data(), sizeof(VColl) * nv, cudaMemcpyHostToDevice));
@@ -943,6 +1037,101 @@ bool ClothPatch::init_grid(int divX, int divY, float inc, V3 offset, bool horizo
     }
     prevMesh = mesh;
     if (!m.upload_topology(mesh)) return false;
+    m.upload_state(stream);
+    hostStateDirty = false;
+    return true;
+}
+
+// A batch: independent clothes stepped as one model. The parts' particles,
+// triangles (with their rest data), bends, edges and rings are concatenated with
+// index offsets, each part keeps the colliders of its own world, and every
+// spatial query is confined to its instance (one tree per instance). Per-part
+// colouring is the greedy colouring of the part alone, so a colour of the batch
+// is the union of the parts' colours: each instance runs the same projections in
+// the same order as it would alone.
+bool ClothPatch::init_batch(const std::vector<ClothPatch*>& parts)
+{
+    if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
+    if (parts.empty()) { set_error(SC_ERR_ARG, "empty batch"); return false; }
+    ClothModel& m = model;
+    const ClothModel& m0 = parts[0]->model;
+    for (ClothPatch* q : parts)
+    {
+        if (!q || q->model.N == 0) { set_error(SC_ERR_ARG, "batch part not initialised"); return false; }
+        if (!q->model.instV.empty()) { set_error(SC_ERR_ARG, "a batch cannot contain a batch"); return false; }
+        q->sync();
+        const HostParams& a = q->model.prm;
+        const HostParams& b = m0.prm;
+        const bool same = a.unit == b.unit && a.thickness == b.thickness && a.tolerance == b.tolerance && a.shear == b.shear &&
+                          a.bend == b.bend && a.stretch == b.stretch && a.poisson == b.poisson && a.friction == b.friction &&
+                          a.drag == b.drag && a.iterations == b.iterations && a.flags == b.flags && a.fem == b.fem &&
+                          a.dihedral == b.dihedral && a.fixedIterations == b.fixedIterations && a.ccd == b.ccd &&
+                          a.bendFreq == b.bendFreq && a.area == b.area && q->numSteps == parts[0]->numSteps;
+        if (!same) { set_error(SC_ERR_ARG, "batch parts must share every solver parameter and the substep count"); return false; }
+    }
+    if (m0.prm.flags & (CF_TRIANGLES | CF_EDGES))
+    {
+        set_error(SC_ERR_UNSUPPORTED, "batches support vertex, wall and self collisions (not triangle / edge collider contacts)");
+        return false;
+    }
+    m.prm = m0.prm;
+    numSteps = parts[0]->numSteps;
+    m.N = 0;
+    m.hpos.clear(); m.hprev.clear(); m.hvel.clear(); m.invMass.clear(); m.uvx.clear(); m.uvy.clear();
+    m.tris.clear(); m.bends.clear(); m.links.clear(); m.quads.clear();
+    m.instV = {0}; m.instT = {0}; m.instE = {0}; m.instB = {0};
+    m.batchColl.clear();
+    mesh = HMesh();
+    for (size_t k = 0; k < parts.size(); k++)
+    {
+        const ClothModel& q = parts[k]->model;
+        const HMesh& qm = parts[k]->mesh;
+        const uint32_t vo = (uint32_t)m.N, to = (uint32_t)m.tris.size(), eo = (uint32_t)mesh.edges.size();
+        m.hpos.insert(m.hpos.end(), q.hpos.begin(), q.hpos.end());
+        m.hprev.insert(m.hprev.end(), q.hprev.begin(), q.hprev.end());
+        m.hvel.insert(m.hvel.end(), q.hvel.begin(), q.hvel.end());
+        m.invMass.insert(m.invMass.end(), q.invMass.begin(), q.invMass.end());
+        m.uvx.insert(m.uvx.end(), q.uvx.begin(), q.uvx.end());
+        m.uvy.insert(m.uvy.end(), q.uvy.begin(), q.uvy.end());
+        for (FemHost t : q.tris) { t.i1 += vo; t.i2 += vo; t.i3 += vo; m.tris.push_back(t); }
+        for (uint4 b : q.bends) m.bends.push_back(make_uint4(b.x + vo, b.y + vo, b.z + vo, b.w + vo));
+        for (uint2 l : q.links) m.links.push_back(make_uint2(l.x + vo, l.y + vo));
+        for (uint4 d : q.quads) m.quads.push_back(make_uint4(d.x + vo, d.y + vo, d.z + vo, d.w + vo));
+        mesh.verts.insert(mesh.verts.end(), qm.verts.begin(), qm.verts.end());
+        mesh.normals.insert(mesh.normals.end(), qm.normals.begin(), qm.normals.end());
+        mesh.triN.insert(mesh.triN.end(), qm.triN.begin(), qm.triN.end());
+        for (uint32_t i : qm.idx) mesh.idx.push_back(i + vo);
+        for (uint32_t e : qm.triE) mesh.triE.push_back(e + eo);
+        for (HEdge e : qm.edges)
+        {
+            e.i1 += vo; e.i2 += vo;
+            if (e.t1 >= 0) e.t1 += (int)to;
+            if (e.t2 >= 0) e.t2 += (int)to;
+            mesh.edges.push_back(e);
+        }
+        for (const auto& r : qm.vtxRing)
+        {
+            mesh.vtxRing.emplace_back();
+            for (int v : r) mesh.vtxRing.back().push_back(v + (int)vo);
+        }
+        for (const auto& r : qm.edgeRing)
+        {
+            mesh.edgeRing.emplace_back();
+            for (int e : r) mesh.edgeRing.back().push_back(e + (int)eo);
+        }
+        for (auto& cp : parts[k]->world.list) m.batchColl.push_back({cp, (int)vo, q.N, (int)k});
+        m.N += q.N;
+        m.instV.push_back(m.N);
+        m.instT.push_back((int)m.tris.size());
+        m.instE.push_back((int)mesh.edges.size());
+        m.instB.push_back((int)m.bends.size());
+    }
+    isQuadMesh = true;
+    prevMesh = mesh;
+    m.tuned = false;
+    m.touch();
+    if (!m.upload_topology(mesh)) return false;
+    m.bufWorldVersion = ~0ull;
     m.upload_state(stream);
     hostStateDirty = false;
     return true;

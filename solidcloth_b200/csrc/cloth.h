@@ -99,6 +99,9 @@ struct HostParams
     bool stageRecords = true;    // cluster solver: constraint records in shared memory
 };
 
+// a collider acting on the particles [vBegin, vBegin + vCount) of batch instance `inst`
+struct BatchColl { std::shared_ptr<Collidable> coll; int vBegin, vCount, inst; };
+
 // solver selection (autotuned unless forced)
 enum SolverKind { SOLVE_AUTO = 0, SOLVE_CLUSTER = 1, SOLVE_GRID = 2, SOLVE_KERNELS = 3 };
 struct SolverChoice { int kind, variant, blocksPerSm; float ms; };
@@ -157,6 +160,10 @@ public:
     void download_state(cudaStream_t s);
     void upload_state(cudaStream_t s);
     SolverParams solver_params(float h) const;
+    // batch of independent clothes (empty: one cloth): first particle / triangle /
+    // edge / bend of each instance (+ end), and each instance's colliders
+    std::vector<int> instV, instT, instE, instB;
+    std::vector<BatchColl> batchColl;
     int solverMode = SOLVE_AUTO;                // forced solver, or the tuner's choice
     SolverChoice choice{SOLVE_CLUSTER, 0, 0, 0.f};
     bool tuned = false;
@@ -206,6 +213,7 @@ public:
     int read_timing(float* msPerSection, int* countPerSection);
 
     bool init_grid(int divX, int divY, float inc, V3 offset, bool horizontal, bool attached);
+    bool init_batch(const std::vector<ClothPatch*>& parts);
     bool step(float dt);
     void update_mesh();
     void record_substep(float h);

@@ -29,6 +29,8 @@ struct VColl
     int type;        // 1 walls, 3 sphere, 7 sdf, 4 mesh
     int slotBase;    // first slot of this collider in the vertex-contact slot array
     int kmax;        // slots per vertex
+    int vBegin, vCount; // particles it acts on (a batch instance's range; else all)
+    int countBase;   // first of its vCount per-particle slot counts
     int mesh;        // mesh collider index for type 4
     float4 a, b;     // walls: lo, hi; sphere: centre (a.xyz), radius (a.w)
     cudaTextureObject_t val, grad; // sdf
@@ -43,6 +45,7 @@ struct Buffers
     VC* vc;
     int numVColl;
     const VColl* vcoll;       // device copy
+    const int2* instColl;     // batch: (first collider, count) per instance; null: all colliders act on all
     // triangle / edge contacts: per-collider slot arrays, flags, dense lists
     TC* tcSlot; int* tcFlag; TC* tcList; int* tcCount; int tcCap;
     EC* ecSlot; int* ecFlag; EC* ecList; int* ecCount; int ecCap;

@@ -57,6 +57,8 @@ struct DevCloth
     const int* vTriStart;       // N+1, incident (triangle, corner) sorted by triangle
     const int2* vTri;
     const uint8_t* vBorder;     // N, Mesh::IsBorderVertex
+    const int* vInst;           // N: instance of each particle in a batch (null: one cloth)
+    const int* instStart;       // batch: first particle of each instance (+ end)
     const int* vQuery;          // N: vertices in spatial (Morton, rest shape) order: neighbouring
     const int* eQuery;          // E: edges likewise; queries of one warp walk the same subtrees
     float4* prevN;              // collision mesh vertex normals (refreshed per frame)
@@ -77,6 +79,7 @@ struct DevBVH
     const int* parent;      // numNodes (root -1)
     const int* leafNode;    // numLeaves: primitive -> node index
     const int* maxPrim;     // numNodes: largest primitive index in the subtree
+    const int* instRoot;    // batch: root node of each instance's tree (a forest); null: one tree at 0
     float4* lo;             // numNodes: box min; w = child[] as int bits
     float4* hi;             // numNodes: box max; w = escape[] as int bits
     int* visit;             // numNodes refit counters

@@ -35,6 +35,13 @@ __device__ __forceinline__ bool gs_done(const DevCloth& c) { return c.scal[8] !=
 
 // Particle positions as the projections see them: plain global memory here;
 // the cluster solver (gs_cluster.cu) substitutes distributed shared memory.
+// the vertex colliders acting on particle i: all of them for one cloth, the
+// instance's own for a batch
+__device__ __forceinline__ int2 colliders_of(const DevCloth& c, const Buffers& b, int i)
+{
+    return b.instColl ? b.instColl[c.vInst[i]] : make_int2(0, b.numVColl);
+}
+
 struct GlobalPos
 {
     float4* p;
@@ -515,10 +522,11 @@ __global__ void k_vertex_colliders(DevCloth c, SolverParams P, Buffers b)
     const V3 pos = ld3(c.pos, i), prev = ld3(c.prev, i);
     const float maxTv = c.scal[0];
     const float radTolMesh = P.thickness + mx(P.tolerance, maxTv * 1.5f);
-    for (int ci = 0; ci < b.numVColl; ci++)
+    const int2 cr = colliders_of(c, b, i);
+    for (int ci = cr.x; ci < cr.x + cr.y; ci++)
     {
         const VColl& g = b.vcoll[ci];
-        VC* slot = b.vc + g.slotBase + (size_t)i * g.kmax;
+        VC* slot = b.vc + g.slotBase + (size_t)(i - g.vBegin) * g.kmax;
         int n = 0;
         auto add = [&](V3 p, V3 nn, int feature, int mesh) {
             VC v;
@@ -557,7 +565,7 @@ __global__ void k_vertex_colliders(DevCloth c, SolverParams P, Buffers b)
                 if (h.dist < radTolMesh && h.dist >= 0) add(h.cp, h.normal, h.tri, g.mesh);
             }
         }
-        b.vcCount[(size_t)ci * c.N + i] = (uint8_t)n;
+        b.vcCount[(size_t)g.countBase + (i - g.vBegin)] = (uint8_t)n;
     }
 }
 
@@ -731,11 +739,12 @@ __device__ __forceinline__ float vertex_contacts_one(const PA& pa, const DevClot
     V3 p = mk(p4.x, p4.y, p4.z);
     const V3 q = ld3(c.prev, i);
     bool touched = false;
-    for (int ci = 0; ci < b.numVColl; ci++)
+    const int2 cr = colliders_of(c, b, i);
+    for (int ci = cr.x; ci < cr.x + cr.y; ci++)
     {
         const VColl& g = b.vcoll[ci];
-        const int n = b.vcCount[(size_t)ci * c.N + i];
-        VC* slot = b.vc + g.slotBase + (size_t)i * g.kmax;
+        const int n = b.vcCount[(size_t)g.countBase + (i - g.vBegin)];
+        VC* slot = b.vc + g.slotBase + (size_t)(i - g.vBegin) * g.kmax;
         for (int k = 0; k < n; k++)
         {
             VC v = slot[k];
@@ -1005,7 +1014,19 @@ __device__ __forceinline__ int contact_verts(const Buffers& b, int kind, int i, 
     v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w; return 4;
 }
 
-__device__ void colour_class(const Buffers& b, const ClassView& cv, int* status)
+// colouring priority of contact i: a hash of its particle indices (relative to
+// its instance's first particle in a batch), then the list index — so an
+// instance's contacts get the same colours in a batch as alone (a batch list
+// keeps each instance's contacts in their own relative order)
+__device__ __forceinline__ unsigned long long contact_key(const DevCloth& c, const uint32_t* v, int nv, int i)
+{
+    const uint32_t base = c.vInst ? (uint32_t)c.instStart[c.vInst[v[0]]] : 0u;
+    uint32_t h = 0x9e3779b9u;
+    for (int k = 0; k < nv; k++) h = mix32(h ^ (v[k] - base));
+    return ((unsigned long long)h << 32) | (uint32_t)i;
+}
+
+__device__ void colour_class(const DevCloth& c, const Buffers& b, const ClassView& cv, int* status)
 {
     __shared__ int sHist[MAX_COLOURS + 1];
     __shared__ int sCursor[MAX_COLOURS + 1];
@@ -1020,8 +1041,8 @@ __device__ void colour_class(const Buffers& b, const ClassView& cv, int* status)
         for (int i = threadIdx.x; i < n; i += blockDim.x)
         {
             if (cv.colour[i] >= 0) continue;
-            unsigned long long key = ((unsigned long long)mix32((uint32_t)i) << 32) | (uint32_t)i;
             uint32_t v[4]; int nv = contact_verts(b, cv.kind, i, v);
+            const unsigned long long key = contact_key(c, v, nv, i);
             for (int k = 0; k < nv; k++) atomicMin(&b.vmin[v[k]], key);
         }
         __syncthreads();
@@ -1029,8 +1050,8 @@ __device__ void colour_class(const Buffers& b, const ClassView& cv, int* status)
         for (int i = threadIdx.x; i < n; i += blockDim.x)
         {
             if (cv.colour[i] >= 0) continue;
-            unsigned long long key = ((unsigned long long)mix32((uint32_t)i) << 32) | (uint32_t)i;
             uint32_t v[4]; int nv = contact_verts(b, cv.kind, i, v);
+            const unsigned long long key = contact_key(c, v, nv, i);
             bool ok = true;
             for (int k = 0; k < nv; k++) ok = ok && (b.vmin[v[k]] == key);
             if (ok) { cv.colour[i] = MAX_COLOURS + round; mine++; }   // tentative mark
@@ -1088,7 +1109,7 @@ struct ColourArgs { ClassView cls[4]; };
 
 __global__ void __launch_bounds__(1024) k_colour(DevCloth c, Buffers b, ColourArgs a)
 {
-    for (int k = 0; k < 4; k++) colour_class(b, a.cls[k], c.status);
+    for (int k = 0; k < 4; k++) colour_class(c, b, a.cls[k], c.status);
 }
 
 // one contact of class cls (0 edge, 1 triangle, 2 self VT, 3 self EE)
@@ -1318,10 +1339,11 @@ __global__ void k_bvh_refit(DevBVH t, DevCloth c, int kind, float tol)
 // one round trip: two 16-byte loads carry its box and its links. With above >= 0
 // subtrees holding only primitives <= above are skipped (the callers reject them).
 template <typename F>
-__device__ __forceinline__ void bvh_query(const DevBVH& t, const Box& q, F&& f, int above = -1)
+__device__ __forceinline__ void bvh_query(const DevBVH& t, const Box& q, F&& f, int above = -1, int root = 0)
 {
-    int node = 0;
-    while (node < t.numNodes)
+    int node = root;
+    const int end = t.instRoot ? __float_as_int(__ldg(&t.hi[root]).w) : t.numNodes;   // the root's escape
+    while (node < end)
     {
         const float4 lo = __ldg(&t.lo[node]), hi = __ldg(&t.hi[node]);
         const int ch = __float_as_int(lo.w), esc = __float_as_int(hi.w);
@@ -1343,18 +1365,18 @@ __device__ __forceinline__ void bvh_query(const DevBVH& t, const Box& q, F&& f, 
 // different order. A median-split tree over n < 2^31 leaves is at most 31 deep,
 // so the 32-entry stack cannot overflow.
 template <typename F>
-__device__ __forceinline__ void bvh_query2(const DevBVH& t, const Box& q, bool active, F&& f, int above = -1)
+__device__ __forceinline__ void bvh_query2(const DevBVH& t, const Box& q, bool active, F&& f, int above = -1, int root = 0)
 {
     if (!active || t.numNodes == 0) return;
     auto over = [&](const float4& lo, const float4& hi) {
         return !(hi.x < q.lo.x || hi.y < q.lo.y || hi.z < q.lo.z || q.hi.x < lo.x || q.hi.y < lo.y || q.hi.z < lo.z);
     };
-    const float4 rlo = __ldg(&t.lo[0]), rhi = __ldg(&t.hi[0]);
-    if (!over(rlo, rhi) || (above >= 0 && __ldg(&t.maxPrim[0]) <= above)) return;
+    const float4 rlo = __ldg(&t.lo[root]), rhi = __ldg(&t.hi[root]);
+    if (!over(rlo, rhi) || (above >= 0 && __ldg(&t.maxPrim[root]) <= above)) return;
     if (__float_as_int(rlo.w) < 0) { f(~__float_as_int(rlo.w)); return; }
     int stack[32];
     int sp = 0;
-    int node = 0, ch = __float_as_int(rlo.w);
+    int node = root, ch = __float_as_int(rlo.w);
     while (true)
     {
         const int L = node + 1, R = ch;
@@ -1382,6 +1404,12 @@ __device__ __forceinline__ void bvh_query2(const DevBVH& t, const Box& q, bool a
             ch = __float_as_int(__ldg(&t.lo[node]).w);
         }
     }
+}
+
+// tree root for a query on particle v: its instance's tree in a batch
+__device__ __forceinline__ int tree_root(const DevCloth& c, const DevBVH& t, int v)
+{
+    return t.instRoot ? t.instRoot[c.vInst[v]] : 0;
 }
 
 // ------------------------------------------------------ self proximity
@@ -1478,7 +1506,7 @@ __global__ void __launch_bounds__(128) k_self_vt(DevCloth c, SolverParams P, Buf
     int cand[KCAND];
     int nc = 0;
     bool ovf = false;
-    bvh_query(tb, q, [&](int t) { if (nc < KCAND) cand[nc++] = t; else ovf = true; });
+    bvh_query(tb, q, [&](int t) { if (nc < KCAND) cand[nc++] = t; else ovf = true; }, -1, tree_root(c, tb, i));
     if (ovf) atomicOr(c.status, ST_SELF_VT_OVERFLOW);
     for (int a = 1; a < nc; a++)   // insertion sort: small lists
     {
@@ -1582,7 +1610,7 @@ __global__ void __launch_bounds__(128) k_self_ee(DevCloth c, SolverParams P, Buf
         closest_segm_segm(p, q, ld3(c.prev, e2.x), ld3(c.prev, e2.y), ps, pm, cs, cm);
         float dist = len(cs - cm);
         if (dist != 0 && (dist < best || (dist == best && e < bestE))) { best = dist; bestE = e; }
-    }, i);
+    }, i, tree_root(c, eb, e1.x));
     if (bestE < 0) return;
     const int4 e2 = c.edge[bestE];
     const V3 a = ld3(c.prev, e2.x), bb = ld3(c.prev, e2.y);
@@ -1671,7 +1699,7 @@ __global__ void __launch_bounds__(128) k_ccd_broad_vt(DevCloth c, SolverParams P
         else if ((int)c.tri[3 * t] == i || (int)c.tri[3 * t + 1] == i || (int)c.tri[3 * t + 2] == i) return;
         if (pool || n < KCCD) out[n] = t;
         n++;
-    });
+    }, -1, tree_root(c, tb, i));
     if (!active) return;
     b.ccdVtCnt[i] = n;
 }
@@ -1718,7 +1746,7 @@ __global__ void __launch_bounds__(128) k_ccd_broad_ee(DevCloth c, SolverParams P
         }
         if (pool || n < KCCD) out[n] = e;
         n++;
-    }, i);
+    }, i, tree_root(c, eb, e1.x));
     if (!active) return;
     b.ccdEeCnt[i] = n;
 }
