@@ -194,6 +194,40 @@ SCEXP int scGetSolverIterations(scModel model);
    quantities Physics/ClothPBD.cpp:66-99 projects); bends are excluded because a
    draped cloth holds them away from zero. -1 before the first step. */
 SCEXP float scGetResidual(scModel model);
+/* addition: tol > 0 makes every substep's Gauss-Seidel loop run until its update
+   residual — the largest particle displacement of the last iteration divided by
+   the mean rest edge length — is <= tol, at most maxIterations iterations (the
+   reference's own exit test is then off); tol = 0 restores iteration counting.
+   (The constraint residual above does not vanish at convergence: the shear
+   constraint is compliant and contacts hold the cloth strained.) */
+SCEXP void scSetResidualTarget(scModel model, float tol, int maxIterations);
+/* addition: Gauss-Seidel iterations run by all substeps since the last call */
+SCEXP int scGetIterationTotal(scModel model);
+
+/* ---- additions: learned warm start (no reference counterpart) ----
+   A per-particle MLP 12 -> 64 -> 64 -> 64 -> 3 (GELU; BF16 weights and
+   activations on the tensor cores, FP32 accumulation) maps a particle's features
+   after the substep's prediction to a position correction that is applied before
+   the Gauss-Seidel loop. Features: predicted minus previous position (3),
+   velocity (3), mean strain of the incident edges (1), collision-mesh normal (3),
+   distance to the first sphere / SDF collider (1, clamped to +-1), free = 1 /
+   pinned = 0 (1). params: scMlpParamCount() FP32 values, W[out][in] row-major per
+   layer then the layer's bias; norm: feature mean (12), 1 / feature std (12),
+   output scale (3). params = NULL turns the warm start off. */
+SCEXP bool scSetWarmStart(scModel model, const float* params, const float* norm);
+/* Record every substep of the next frames: features (numSteps x N x 12) after the
+   prediction and targets (numSteps x N x 3) = solved minus predicted positions,
+   into caller-owned DEVICE buffers; NULL stops recording. */
+SCEXP bool scSetSampleBuffers(scModel model, float* features, float* targets);
+SCEXP int scMlpParamCount(void);
+/* Device-pointer training and inference on `stream` (a cudaStream_t, 0 = legacy):
+   Y = MLP(X) * output scale for S rows; gradients of mean((MLP(X) - T / scale)^2)
+   (grad and loss are overwritten); one Adam step (beta 0.9 / 0.999, eps 1e-8).
+   Return 0 or an error code. */
+SCEXP int scMlpForward(const float* X, int S, const float* params, const float* norm, float* Y, void* stream);
+SCEXP int scMlpGradients(const float* X, const float* T, int S, const float* params, const float* norm,
+                         float* grad, float* loss, void* stream);
+SCEXP int scMlpAdamStep(float* params, const float* grad, float* m, float* v, int step, float lr, void* stream);
 /* true (default): the Gauss-Seidel loop of a substep runs as one thread-block
    cluster with the particles in distributed shared memory, when the cloth fits
    (up to 131,072 particles); false: one kernel per colour. Same results. */

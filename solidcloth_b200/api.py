@@ -135,6 +135,14 @@ SIGNATURES = {
     "scGetGridVariants": ([_i, C.c_int], C.c_int),
     "scGetSolverIterations": ([scModel], C.c_int),
     "scGetResidual": ([scModel], C.c_float),
+    "scSetResidualTarget": ([scModel, C.c_float, C.c_int], None),
+    "scGetIterationTotal": ([scModel], C.c_int),
+    "scSetWarmStart": ([scModel, _f, _f], C.c_bool),
+    "scSetSampleBuffers": ([scModel, C.c_void_p, C.c_void_p], C.c_bool),
+    "scMlpParamCount": ([], C.c_int),
+    "scMlpForward": ([C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "scMlpGradients": ([C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "scMlpAdamStep": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_float, C.c_void_p], C.c_int),
     "scGetConstraintOrder": ([scModel, C.c_int, _i, _i], C.c_int),
     "scGetNumBends": ([scModel], C.c_int),
     "scGetBends": ([scModel, _u], None),
@@ -386,6 +394,32 @@ class ClothModel:
     def residual(self) -> float:
         """max |C| over the warp, weft and shear constraints at the current positions"""
         return float(lib().scGetResidual(self.h))
+
+    def set_residual_target(self, tol: float, max_iterations: int):
+        """iterate each substep until the residual <= tol (at most max_iterations)"""
+        lib().scSetResidualTarget(self.h, float(tol), int(max_iterations))
+        _check("scSetResidualTarget")
+
+    def set_warm_start(self, params, norm):
+        """params (9347 FP32) and norm (27 FP32) host arrays; None turns it off"""
+        if params is None:
+            ok = lib().scSetWarmStart(self.h, None, None)
+        else:
+            p = np.ascontiguousarray(params, np.float32)
+            n = np.ascontiguousarray(norm, np.float32)
+            ok = lib().scSetWarmStart(self.h, p.ctypes.data_as(_f), n.ctypes.data_as(_f))
+        _check("scSetWarmStart")
+        return bool(ok)
+
+    def set_sample_buffers(self, features_ptr, targets_ptr):
+        """device pointers (numSteps x N x 12, numSteps x N x 3) or 0 to stop"""
+        ok = lib().scSetSampleBuffers(self.h, C.c_void_p(features_ptr or None), C.c_void_p(targets_ptr or None))
+        _check("scSetSampleBuffers")
+        return bool(ok)
+
+    def iteration_total(self) -> int:
+        """Gauss-Seidel iterations of all substeps since the last call"""
+        return int(lib().scGetIterationTotal(self.h))
 
     def solver_iterations(self):
         return lib().scGetSolverIterations(self.h)

@@ -479,6 +479,93 @@ int scGetGridVariants(int* info3, int cap)
     return n;
 }
 void scSetClusterStaging(scModel m, bool v) { if (M(m)) { M(m)->prm.stageRecords = v; M(m)->touch(); } }
+void scSetResidualTarget(scModel m, float tol, int maxIterations)
+{
+    ClothModel* c = M(m);
+    if (!c || tol < 0.f || maxIterations < 1) { set_error(SC_ERR_ARG, "residual target needs tol >= 0 and maxIterations >= 1"); return; }
+    c->prm.resTol = tol;
+    if (tol > 0.f)
+    {
+        c->prm.iterations = maxIterations;
+        c->prm.fixedIterations = true;     // the residual decides, not the reference's exit test
+    }
+    c->tuned = false;
+    c->touch();
+}
+
+int scGetIterationTotal(scModel m)
+{
+    ClothModel* c = M(m);
+    if (!c || !c->dc.scal) return 0;
+    host_sync(c);
+    float v = 0.f;
+    cudaMemcpy(&v, c->dc.scal + 10, sizeof(float), cudaMemcpyDeviceToHost);
+    cudaMemset(c->dc.scal + 10, 0, sizeof(float));
+    return (int)v;
+}
+
+bool scSetWarmStart(scModel m, const float* params, const float* norm)
+{
+    ClothModel* c = M(m);
+    if (!c) { set_error(SC_ERR_ARG, "null model"); return false; }
+    host_sync(c);
+    if (!params) { c->warmStart = false; c->touch(); return true; }
+    if (!norm) { set_error(SC_ERR_ARG, "warm start needs its 27 normalisation values"); return false; }
+    if (!c->mlpPrm && cudaMalloc(&c->mlpPrm, sizeof(float) * (MLP_NPARAM + MLP_NNORM)) != cudaSuccess)
+    {
+        c->mlpPrm = nullptr;
+        set_error(SC_ERR_CUDA, "cudaMalloc failed");
+        return false;
+    }
+    cudaMemcpy(c->mlpPrm, params, sizeof(float) * MLP_NPARAM, cudaMemcpyHostToDevice);
+    cudaMemcpy(c->mlpPrm + MLP_NPARAM, norm, sizeof(float) * MLP_NNORM, cudaMemcpyHostToDevice);
+    c->warmStart = true;
+    c->tuned = false;
+    c->touch();
+    return true;
+}
+
+bool scSetSampleBuffers(scModel m, float* features, float* targets)
+{
+    ClothModel* c = M(m);
+    if (!c || c->N == 0) { set_error(SC_ERR_ARG, "model not initialised"); return false; }
+    host_sync(c);
+    if (!features || !targets) { c->sampleFeat = c->sampleTarget = nullptr; c->touch(); return true; }
+    if (!c->xpred && cudaMalloc(&c->xpred, sizeof(float4) * (size_t)c->N) != cudaSuccess)
+    {
+        c->xpred = nullptr;
+        set_error(SC_ERR_CUDA, "cudaMalloc failed");
+        return false;
+    }
+    c->sampleFeat = features;
+    c->sampleTarget = targets;
+    c->touch();
+    return true;
+}
+
+int scMlpParamCount(void) { return MLP_NPARAM; }
+
+int scMlpForward(const float* X, int S, const float* params, const float* norm, float* Y, void* stream)
+{
+    if (!X || !params || !norm || !Y || S < 0) return SC_ERR_ARG;
+    launch_mlp_forward((cudaStream_t)stream, X, S, params, norm, Y);
+    return cudaGetLastError() == cudaSuccess ? SC_OK : SC_ERR_CUDA;
+}
+
+int scMlpGradients(const float* X, const float* T, int S, const float* params, const float* norm, float* grad,
+                   float* loss, void* stream)
+{
+    if (!X || !T || !params || !norm || !grad || !loss || S < 1) return SC_ERR_ARG;
+    return launch_mlp_grad((cudaStream_t)stream, X, T, S, params, norm, grad, loss) ? SC_OK : SC_ERR_CUDA;
+}
+
+int scMlpAdamStep(float* params, const float* grad, float* m, float* v, int step, float lr, void* stream)
+{
+    if (!params || !grad || !m || !v || step < 1) return SC_ERR_ARG;
+    launch_adam((cudaStream_t)stream, params, grad, m, v, step, lr);
+    return cudaGetLastError() == cudaSuccess ? SC_OK : SC_ERR_CUDA;
+}
+
 float scGetResidual(scModel m)
 {
     ClothModel* c = M(m);

@@ -414,7 +414,12 @@ void LBVHHost::build(const std::vector<V3>& cen)
 }
 
 // ------------------------------------------------------------------ model
-ClothModel::~ClothModel() { release_device(); }
+ClothModel::~ClothModel()
+{
+    release_device();
+    if (mlpPrm) cudaFree(mlpPrm);
+    if (xpred) cudaFree(xpred);
+}
 
 void* ClothModel::dalloc(size_t bytes, bool contact)
 {
@@ -457,6 +462,8 @@ SolverParams ClothModel::solver_params(float h) const
     P.epsUV = 2 * (1 + prm.poisson) / (std::max(prm.shear, 0.1f) * prm.unit * prm.unit);
     P.iterations = prm.iterations; P.flags = prm.flags; P.fem = prm.fem; P.dihedral = prm.dihedral;
     P.fixedIterations = prm.fixedIterations; P.bendFreq = prm.bendFreq;
+    P.resTol = prm.resTol;
+    P.resScale = resScale;
     P.selfThreshold = prm.selfThreshold;
     return P;
 }
@@ -608,6 +615,24 @@ bool ClothModel::upload_topology(const HMesh& mesh)
         SC_CUDA(cudaMemcpy(d, vq.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
         if (E) SC_CUDA(cudaMemcpy(d + N, eq.data(), sizeof(int) * E, cudaMemcpyHostToDevice));
         dc.vQuery = d; dc.eQuery = d + N;
+    }
+    {
+        // rest length of every edge from the uv layout (warm-start strain feature)
+        std::vector<float> rest(std::max(1, E), 1.f);
+        for (int e = 0; e < E; e++)
+        {
+            const int a = mesh.edges[e].i1, b2 = mesh.edges[e].i2;
+            const float du = uvx[b2] - uvx[a], dv = uvy[b2] - uvy[a];
+            const float l = std::sqrt(du * du + dv * dv);
+            rest[e] = l > 0.f ? l : 1.f;
+        }
+        float* dr = (float*)dalloc(sizeof(float) * rest.size());
+        SC_CUDA(cudaMemcpy(dr, rest.data(), sizeof(float) * rest.size(), cudaMemcpyHostToDevice));
+        dc.edgeRest = dr;
+        double sum = 0;
+        for (int e = 0; e < E; e++) sum += rest[e];
+        resScale = E > 0 ? (float)(E / sum) : 1.f;
+        dc.xsnap = (float4*)dalloc(sizeof(float4) * (size_t)N);
     }
     dc.prevN = (float4*)dalloc(sizeof(float4) * N);
     dc.prevTriN = (float4*)dalloc(sizeof(float4) * T);
@@ -1183,11 +1208,17 @@ void ClothPatch::record_substep(float h)
     if (self || ccd) launch_compact_self(s, c, P, b, ccd);
     else cudaMemsetAsync(b.stCount, 0, 2 * sizeof(int), s);
     launch_colour_contacts(s, c, b);
+    // learned warm start (no reference counterpart): record the features and the
+    // predicted positions, and / or move the particles by the network's correction
+    const size_t sub = (size_t)recordingSubstep;
+    if (m.sampleFeat && m.xpred) launch_mlp_features(s, c, b, m.sampleFeat + sub * m.N * MLP_IN, m.xpred);
+    if (m.warmStart && m.mlpPrm) launch_mlp_warm(s, c, b, m.mlpPrm, m.mlpPrm + MLP_NPARAM);
     // ClothModelPBD::SolveGS (Physics/ClothPBD.cpp:324-369)
     launch_reset_gs(s, c);
     timing_mark(SEC_GS, false, s);
     record_solve(s, P, m.choice);
     timing_mark(SEC_GS, true, s);
+    if (m.sampleTarget && m.xpred) launch_mlp_targets(s, c, m.xpred, m.sampleTarget + sub * m.N * MLP_OUT);
     recordingSubstep++;
 }
 
@@ -1247,6 +1278,7 @@ bool ClothPatch::record_solve(cudaStream_t s, const SolverParams& P, const Solve
     }
     if (ch.kind == SOLVE_GRID && planFits && launch_gs_grid(s, c, P, b, plan, ch.variant, ch.blocksPerSm))
         return true;
+    if (P.resTol > 0.f) launch_residual_exit(s, c, P, -1);
     for (int k = 0; k < iterations; k++)
     {
         if (m.prm.fem)
@@ -1257,7 +1289,9 @@ bool ClothPatch::record_solve(cudaStream_t s, const SolverParams& P, const Solve
                 launch_bends(s, c, P, m.bendColourStart[col], m.bendColourStart[col + 1] - m.bendColourStart[col], col == 0);
         launch_solve_vertex_contacts(s, c, P, b);
         launch_solve_multi_contacts(s, c, P, b, k);
+        if (P.resTol > 0.f) launch_residual_exit(s, c, P, k);
     }
+    launch_iteration_total(s, c);
     launch_velocity(s, c, P);
     return true;
 }

@@ -97,6 +97,7 @@ struct HostParams
     int iterations = 50, flags = 0, bendFreq = 2;
     bool fem = false, dihedral = true, fixedIterations = false, ccd = false;
     bool stageRecords = true;    // cluster solver: constraint records in shared memory
+    float resTol = 0.f;          // > 0: Gauss-Seidel runs until the residual is <= resTol (iterations = cap)
 };
 
 // a collider acting on the particles [vBegin, vBegin + vCount) of batch instance `inst`
@@ -164,6 +165,14 @@ public:
     // edge / bend of each instance (+ end), and each instance's colliders
     std::vector<int> instV, instT, instE, instB;
     std::vector<BatchColl> batchColl;
+    // learned warm start: FP32 parameters + normalisation on the device (owned),
+    // and optional per-substep sample recording into caller-owned device buffers
+    float resScale = 1.f;                       // 1 / mean rest edge length
+    float* mlpPrm = nullptr;
+    bool warmStart = false;
+    float* sampleFeat = nullptr;
+    float* sampleTarget = nullptr;
+    float4* xpred = nullptr;
     int solverMode = SOLVE_AUTO;                // forced solver, or the tuner's choice
     SolverChoice choice{SOLVE_CLUSTER, 0, 0, 0.f};
     bool tuned = false;

@@ -95,6 +95,9 @@ void launch_compact_self(cudaStream_t s, const DevCloth& c, const SolverParams& 
 void launch_reset_gs(cudaStream_t s, const DevCloth& c);
 // max |C| over warp / weft / shear constraints, as float bits into *out
 void launch_residual(cudaStream_t s, const DevCloth& c, unsigned* out);
+// residual-target mode for the per-colour path: residual + exit flag after an iteration
+void launch_residual_exit(cudaStream_t s, const DevCloth& c, const SolverParams& P, int iter);
+void launch_iteration_total(cudaStream_t s, const DevCloth& c);
 void launch_gs_exit_test(cudaStream_t s, const DevCloth& c, const SolverParams& P, int iter);
 
 // cluster-resident Gauss-Seidel solver (one cluster per cloth, one launch per substep)
@@ -121,6 +124,16 @@ void gs_grid_variant_info(int variant, int& threads, int& femTile, int& bendTile
 int gs_grid_max_blocks_per_sm(int variant);
 bool launch_gs_grid(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b, GsPlan plan,
                     int variant, int blocksPerSm);
+
+// learned warm start (mlp_kernels.cuh): 9347 FP32 parameters, 27 normalisation values
+constexpr int MLP_NPARAM = 9347, MLP_NNORM = 27, MLP_IN = 12, MLP_OUT = 3;
+void launch_mlp_warm(cudaStream_t s, const DevCloth& c, const Buffers& b, const float* prm, const float* norm);
+void launch_mlp_features(cudaStream_t s, const DevCloth& c, const Buffers& b, float* feat, float4* xpred);
+void launch_mlp_targets(cudaStream_t s, const DevCloth& c, const float4* xpred, float* target);
+void launch_mlp_forward(cudaStream_t s, const float* X, int S, const float* prm, const float* norm, float* Y);
+bool launch_mlp_grad(cudaStream_t s, const float* X, const float* T, int S, const float* prm, const float* norm,
+                     float* grad, float* loss);
+void launch_adam(cudaStream_t s, float* prm, const float* grad, float* m, float* v, int step, float lr);
 
 // exclusive scan of n ints (out may alias nothing); total written to *total if not null
 void scan_ints(cudaStream_t s, const int* in, int* out, int n, int* total, int* tmp);

@@ -35,6 +35,8 @@ struct SolverParams
     float h, h2, invH, epsUV;
     int iterations, flags, fem, dihedral, fixedIterations, bendFreq;
     float selfThreshold;
+    float resTol;            // > 0: iterate until the update residual <= resTol
+    float resScale;          // 1 / mean rest edge length (the update residual's unit)
 };
 
 // Device view of one cloth patch (plain pointers, passed by value).
@@ -59,6 +61,8 @@ struct DevCloth
     const uint8_t* vBorder;     // N, Mesh::IsBorderVertex
     const int* vInst;           // N: instance of each particle in a batch (null: one cloth)
     const int* instStart;       // batch: first particle of each instance (+ end)
+    const float* edgeRest;      // E: rest length of each edge (from the uv layout)
+    float4* xsnap;              // N: positions at the start of the current iteration (update residual)
     const int* vQuery;          // N: vertices in spatial (Morton, rest shape) order: neighbouring
     const int* eQuery;          // E: edges likewise; queries of one warp walk the same subtrees
     float4* prevN;              // collision mesh vertex normals (refreshed per frame)

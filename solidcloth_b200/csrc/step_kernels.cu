@@ -1175,6 +1175,22 @@ __global__ void k_gs_exit(DevCloth c, SolverParams P, int iter)
         c.scal[8] = 1.f;
 }
 
+// residual-target mode, per-colour path: after iteration `iter` the residual
+// word (float bits in scal[11]) decides whether the loop is done
+__global__ void k_residual_exit(DevCloth c, SolverParams P, int iter)
+{
+    unsigned* word = reinterpret_cast<unsigned*>(c.scal + 11);
+    const float res = __uint_as_float(*word);
+    *word = 0u;
+    if (!gs_done(c) && res <= P.resTol) c.scal[8] = 1.f;
+}
+
+// total iterations of the substeps since the last read (scal[10])
+__global__ void k_iteration_total(DevCloth c)
+{
+    c.scal[10] += c.scal[9];
+}
+
 __global__ void k_reset_iter_errors(DevCloth c)
 {
     // cv is a per-iteration maximum written with atomics; cb persists between
@@ -2112,6 +2128,12 @@ __global__ void __launch_bounds__(GS_THREADS) k_gs_cluster(DevCloth c, SolverPar
     cl.sync();
     const ClusterPos pa{sPos, (uint32_t)plan.shift, vpc - 1};
     const bool track = !P.fixedIterations;
+    if (P.resTol > 0.f)
+    {
+        for (uint32_t v = threadIdx.x; v < vpc; v += blockDim.x)
+            if (v0 + (int)v < c.N) c.xsnap[v0 + v] = sPos[v];
+        cl.sync();     // no CTA writes a particle before its snapshot is taken
+    }
     for (int k = 0; k < plan.iterations; k++)
     {
         if (P.fem)
@@ -2189,6 +2211,29 @@ __global__ void __launch_bounds__(GS_THREADS) k_gs_cluster(DevCloth c, SolverPar
             }
         }
         if (threadIdx.x == 0 && rank == 0) c.scal[9] = (float)(k + 1);
+        if (P.resTol > 0.f)
+        {
+            // residual-target mode: the largest displacement of this iteration (own
+            // particles, against the snapshot), cluster-wide; then the next snapshot
+            float r = 0.f;
+            for (uint32_t v = threadIdx.x; v < vpc; v += blockDim.x)
+            {
+                const int g = v0 + (int)v;
+                if (g >= c.N) continue;
+                const float4 x = sPos[v], x0 = c.xsnap[g];
+                const float dx = x.x - x0.x, dy = x.y - x0.y, dz = x.z - x0.z;
+                r = fmaxf(r, sqrtf(dx * dx + dy * dy + dz * dz) * P.resScale);
+                c.xsnap[g] = x;
+            }
+            const unsigned u = __reduce_max_sync(0xffffffffu, __float_as_uint(r));
+            unsigned* word = reinterpret_cast<unsigned*>(c.scal + 11);
+            if ((threadIdx.x & 31) == 0 && u) atomicMax(word, u);
+            cl.sync();
+            const float res = __uint_as_float(__ldcg(word));
+            cl.sync();
+            if (rank == 0 && threadIdx.x == 0) *word = 0u;
+            if (res <= P.resTol) break;
+        }
         if (track)
         {
             // SolveGS exit test (Physics/ClothPBD.cpp:354-361) on cluster-wide maxima
@@ -2209,6 +2254,7 @@ __global__ void __launch_bounds__(GS_THREADS) k_gs_cluster(DevCloth c, SolverPar
             if (__ldcg(&c.scal[8]) != 0.f) break;
         }
     }
+    if (rank == 0 && threadIdx.x == 0) c.scal[10] += c.scal[9];
     // write back own particles and update their velocities (ClothPBD.cpp:314-321)
     for (uint32_t v = threadIdx.x; v < vpc; v += blockDim.x)
     {
@@ -2331,6 +2377,11 @@ __global__ void __launch_bounds__(NT) k_gs_grid(DevCloth c, SolverParams P, Buff
     const GlobalPos pa{c.pos};
     const bool track = !P.fixedIterations;
     if (threadIdx.x < 8) sErr[threadIdx.x] = 0.f;
+    if (P.resTol > 0.f)
+    {
+        for (int g = tid; g < c.N; g += nth) c.xsnap[g] = c.pos[g];
+        grid.sync();
+    }
     __syncthreads();
     for (int k = 0; k < plan.iterations; k++)
     {
@@ -2386,6 +2437,27 @@ __global__ void __launch_bounds__(NT) k_gs_grid(DevCloth c, SolverParams P, Buff
             }
         }
         if (tid == 0) c.scal[9] = (float)(k + 1);
+        if (P.resTol > 0.f)
+        {
+            // residual-target mode: the largest displacement of this iteration,
+            // grid-wide; then the next snapshot (each thread its own particles)
+            float r = 0.f;
+            for (int g = tid; g < c.N; g += nth)
+            {
+                const float4 x = c.pos[g], x0 = c.xsnap[g];
+                const float dx = x.x - x0.x, dy = x.y - x0.y, dz = x.z - x0.z;
+                r = fmaxf(r, sqrtf(dx * dx + dy * dy + dz * dz) * P.resScale);
+                c.xsnap[g] = x;
+            }
+            const unsigned u = __reduce_max_sync(0xffffffffu, __float_as_uint(r));
+            unsigned* word = reinterpret_cast<unsigned*>(c.scal + 11);
+            if ((threadIdx.x & 31) == 0 && u) atomicMax(word, u);
+            grid.sync();
+            const float res = __uint_as_float(__ldcg(word));
+            grid.sync();
+            if (tid == 0) *word = 0u;
+            if (res <= P.resTol) break;
+        }
         if (track)
         {
             // SolveGS exit test (Physics/ClothPBD.cpp:354-361) on grid-wide maxima
@@ -2407,6 +2479,7 @@ __global__ void __launch_bounds__(NT) k_gs_grid(DevCloth c, SolverParams P, Buff
             if (__ldcg(&c.scal[8]) != 0.f) break;
         }
     }
+    if (tid == 0) c.scal[10] += c.scal[9];
     // velocity update (ClothPBD.cpp:314-321)
     for (int g = tid; g < c.N; g += nth)
     {
@@ -2690,6 +2763,41 @@ void launch_ccd(cudaStream_t s, cudaStream_t side, cudaEvent_t fork, cudaEvent_t
     cudaStreamWaitEvent(s, join, 0);
 }
 
+// largest displacement since the snapshot (scaled), into scal[11]; new snapshot
+__global__ void k_update_residual(DevCloth c, SolverParams P, bool measure)
+{
+    float r = 0.f;
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < c.N; g += gridDim.x * blockDim.x)
+    {
+        const float4 x = c.pos[g];
+        if (measure)
+        {
+            const float4 x0 = c.xsnap[g];
+            const float dx = x.x - x0.x, dy = x.y - x0.y, dz = x.z - x0.z;
+            r = fmaxf(r, sqrtf(dx * dx + dy * dy + dz * dz) * P.resScale);
+        }
+        c.xsnap[g] = x;
+    }
+    const unsigned u = __reduce_max_sync(0xffffffffu, __float_as_uint(r));
+    if (measure && (threadIdx.x & 31) == 0 && u) atomicMax(reinterpret_cast<unsigned*>(c.scal + 11), u);
+}
+
+void launch_residual_exit(cudaStream_t s, const DevCloth& c, const SolverParams& P, int iter)
+{
+    if (iter < 0)
+    {
+        k_update_residual<<<2 * 148, 256, 0, s>>>(c, P, false);     // the first snapshot
+        return;
+    }
+    k_update_residual<<<2 * 148, 256, 0, s>>>(c, P, true);
+    k_residual_exit<<<1, 1, 0, s>>>(c, P, iter);
+}
+
+void launch_iteration_total(cudaStream_t s, const DevCloth& c)
+{
+    k_iteration_total<<<1, 1, 0, s>>>(c);
+}
+
 void launch_residual(cudaStream_t s, const DevCloth& c, unsigned* out)
 {
     cudaMemsetAsync(out, 0, sizeof(unsigned), s);
@@ -2704,6 +2812,58 @@ void launch_reset_gs(cudaStream_t s, const DevCloth& c)
 void launch_gs_exit_test(cudaStream_t s, const DevCloth& c, const SolverParams& P, int iter)
 {
     k_gs_exit<<<1, 32, 0, s>>>(c, P, iter);
+}
+
+} // namespace sc
+
+// ----------------------------------------------------- learned warm start
+#include "mlp_kernels.cuh"
+
+namespace sc {
+
+static_assert(MLP_NPARAM == ML_NPARAM && MLP_NNORM == ML_NNORM, "MLP layout");
+
+void launch_mlp_warm(cudaStream_t s, const DevCloth& c, const Buffers& b, const float* prm, const float* norm)
+{
+    k_mlp_warm<<<(c.N + 127) / 128, 128, 0, s>>>(c, b, MlpArgs{prm, norm});
+}
+
+void launch_mlp_features(cudaStream_t s, const DevCloth& c, const Buffers& b, float* feat, float4* xpred)
+{
+    k_mlp_features<<<blocks_for(c.N), 256, 0, s>>>(c, b, feat, xpred);
+}
+
+void launch_mlp_targets(cudaStream_t s, const DevCloth& c, const float4* xpred, float* target)
+{
+    k_mlp_targets<<<blocks_for(c.N), 256, 0, s>>>(c, xpred, target);
+}
+
+void launch_mlp_forward(cudaStream_t s, const float* X, int S, const float* prm, const float* norm, float* Y)
+{
+    k_mlp_forward<<<(S + 127) / 128, 128, 0, s>>>(X, S, MlpArgs{prm, norm}, Y);
+}
+
+size_t mlp_grad_smem() { return ((sizeof(MlpSmem) + 15) / 16) * 16 + sizeof(MlpTrainSmem); }
+
+bool launch_mlp_grad(cudaStream_t s, const float* X, const float* T, int S, const float* prm, const float* norm,
+                     float* grad, float* loss)
+{
+    static bool attr = false;
+    const size_t smem = mlp_grad_smem();
+    if (!attr)
+    {
+        if (cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return false;
+        attr = true;
+    }
+    cudaMemsetAsync(grad, 0, sizeof(float) * ML_NPARAM, s);
+    cudaMemsetAsync(loss, 0, sizeof(float), s);
+    k_mlp_grad<<<(S + ML_ROWS - 1) / ML_ROWS, 128, smem, s>>>(X, T, S, MlpArgs{prm, norm}, grad, loss);
+    return cudaGetLastError() == cudaSuccess;
+}
+
+void launch_adam(cudaStream_t s, float* prm, const float* grad, float* m, float* v, int step, float lr)
+{
+    k_adam<<<(ML_NPARAM + 255) / 256, 256, 0, s>>>(prm, grad, m, v, step, lr, 0.9f, 0.999f, 1e-8f);
 }
 
 } // namespace sc

@@ -1,0 +1,189 @@
+"""Learned warm start: data generation with the GPU solver, training with the
+library's own kernels, and the plain-versus-learned comparison.
+
+The network (12 -> 64 -> 64 -> 64 -> 3, GELU, BF16 weights on the tensor cores)
+predicts, per particle, the correction the Gauss-Seidel loop will apply in a
+substep (solved minus predicted position) from features available right after
+the prediction. The library applies it before the loop; plain iterations then
+continue until the residual target, so the plain solver remains both fallback
+and judge. Everything runs on the GPU: samples come from the solver through
+scSetSampleBuffers, gradients from scMlpGradients, updates from scMlpAdamStep.
+"""
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import api, scenes
+
+NPARAM = 9347
+NNORM = 27
+IN, OUT = 12, 3
+
+
+def init_params(seed: int = 0) -> np.ndarray:
+    """He-style weights, zero biases, zero output layer (no correction at start)."""
+    rng = np.random.default_rng(seed)
+    shapes = [(64, 12), (64,), (64, 64), (64,), (64, 64), (64,), (3, 64), (3,)]
+    parts = []
+    for k, shp in enumerate(shapes):
+        if len(shp) == 1 or k == 6:
+            parts.append(np.zeros(shp, np.float32))
+        else:
+            parts.append((rng.standard_normal(shp) * np.sqrt(2.0 / shp[1])).astype(np.float32))
+    return np.concatenate([q.ravel() for q in parts]).astype(np.float32)
+
+
+def drape_scene(seed: int, n: int = 64, side: float = 1.0, ccd: bool = True) -> scenes.Scene:
+    """A random drape: sphere SDF (centre within 0.15 m of the cloth's axis, radius
+    0.2-0.4 m, 64^3 samples) under a flat cloth rotated about the vertical by a
+    random angle and released 3 cm above the sphere's top; no pins."""
+    rng = np.random.default_rng(seed)
+    r = float(rng.uniform(0.2, 0.4))
+    cx, cz = (float(v) for v in rng.uniform(-0.15, 0.15, 2))
+    angle = float(rng.uniform(0.0, np.pi))
+    p = scenes.Params(thickness=0.005, tolerance=0.005, friction=0.3, iterations=20, substeps=8,
+                      flags=scenes.CF_VERTICES)
+    height = r + 0.03
+    s = scenes.make_grid_scene(f"drape_{n}_s{seed}", n, side, height, p, seed=seed, frames=60)
+    c, sn = np.cos(angle), np.sin(angle)
+    rot = np.array([[c, 0, -sn], [0, 1, 0], [sn, 0, c]], np.float32)
+    centre = s.positions.mean(0)
+    s.positions = ((s.positions - centre) @ rot.T + centre).astype(np.float32)
+    s.sdfs.append(scenes.sphere_sdf((cx, 0.0, cz), r, 63, 0.1))
+    s.ccd = ccd
+    return s
+
+
+@dataclass
+class Dataset:
+    X: "object"       # torch float32 (S, 12) on the GPU
+    T: "object"       # torch float32 (S, 3)
+    drapes: int
+    seconds: float
+
+
+def generate(num_drapes: int, n: int = 64, per_batch: int = 250, skip_frames: int = 4, record_frames: int = 3,
+             keep_every: int = 8, tol: float = 1e-4, max_iter: int = 200, seed0: int = 0) -> Dataset:
+    """Simulate `num_drapes` drapes with the plain solver (residual target `tol`,
+    at most `max_iter` iterations a substep) in batches, and keep every
+    `keep_every`-th particle's (features, correction) of every substep of the
+    recorded frames."""
+    import torch
+    t0 = time.time()
+    xs, ts = [], []
+    for b0 in range(0, num_drapes, per_batch):
+        ds = [drape_scene(seed0 + k, n) for k in range(b0, min(num_drapes, b0 + per_batch))]
+        b = api.load_batch(ds)
+        b.model.set_residual_target(tol, max_iter)
+        N = sum(d.num_vertices for d in ds)
+        sub = ds[0].params.substeps
+        for _ in range(skip_frames):
+            b.step(ds[0].dt)
+        F = torch.zeros((sub, N, IN), device="cuda")
+        Tg = torch.zeros((sub, N, OUT), device="cuda")
+        b.model.set_sample_buffers(F.data_ptr(), Tg.data_ptr())
+        for f in range(record_frames):
+            b.step(ds[0].dt)
+            b.synchronize()
+            sel = torch.arange((f * 7) % keep_every, N, keep_every, device="cuda")
+            xs.append(F[:, sel].reshape(-1, IN).clone())
+            ts.append(Tg[:, sel].reshape(-1, OUT).clone())
+        b.model.set_sample_buffers(0, 0)
+        b.free()
+    torch.cuda.synchronize()
+    return Dataset(torch.cat(xs), torch.cat(ts), num_drapes, time.time() - t0)
+
+
+def fit_norm(X, T) -> np.ndarray:
+    """feature mean and 1/std (std floored), output scale = target std per axis"""
+    mean = X.mean(0).cpu().numpy()
+    std = X.std(0).cpu().numpy()
+    std = np.where(std > 1e-6, std, 1.0)
+    tstd = T.std(0).cpu().numpy()
+    tstd = np.where(tstd > 1e-9, tstd, 1e-6)
+    return np.concatenate([mean, 1.0 / std, tstd]).astype(np.float32)
+
+
+def train(X, T, norm: np.ndarray, epochs: int = 20, batch: int = 65536, lr: float = 2e-3, seed: int = 0,
+          params: np.ndarray | None = None, log=None):
+    """Adam on mean((MLP(X) - T / scale)^2) with the library's kernels; returns
+    (params, per-epoch mean losses)."""
+    import torch
+    lib = api.lib()
+    p = torch.from_numpy(params if params is not None else init_params(seed)).cuda()
+    m = torch.zeros(NPARAM, device="cuda")
+    v = torch.zeros(NPARAM, device="cuda")
+    g = torch.zeros(NPARAM, device="cuda")
+    loss = torch.zeros(1, device="cuda")
+    dn = torch.from_numpy(norm).cuda()
+    S = X.shape[0]
+    gen = torch.Generator(device="cuda").manual_seed(seed)
+    step = 0
+    history = []
+    for ep in range(epochs):
+        perm = torch.randperm(S, device="cuda", generator=gen)
+        tot, cnt = 0.0, 0
+        losses = []
+        for k in range(0, S, batch):
+            idx = perm[k:k + batch]
+            xb, tb = X[idx].contiguous(), T[idx].contiguous()
+            rc = lib.scMlpGradients(xb.data_ptr(), tb.data_ptr(), xb.shape[0], p.data_ptr(), dn.data_ptr(),
+                                    g.data_ptr(), loss.data_ptr(), None)
+            if rc != 0:
+                raise RuntimeError(f"scMlpGradients: {rc}")
+            step += 1
+            lib.scMlpAdamStep(p.data_ptr(), g.data_ptr(), m.data_ptr(), v.data_ptr(), step, lr, None)
+            losses.append(loss.clone())
+        ep_loss = float(torch.stack(losses).mean().item())
+        history.append(ep_loss)
+        if log:
+            log(f"epoch {ep}: loss {ep_loss:.4f}")
+    return p.cpu().numpy(), history
+
+
+def predict(X, params: np.ndarray, norm: np.ndarray):
+    import torch
+    Y = torch.zeros((X.shape[0], OUT), device="cuda")
+    dp, dn = torch.from_numpy(params).cuda(), torch.from_numpy(norm).cuda()   # alive until the kernel ran
+    rc = api.lib().scMlpForward(X.data_ptr(), X.shape[0], dp.data_ptr(), dn.data_ptr(), Y.data_ptr(), None)
+    torch.cuda.synchronize()
+    if rc != 0:
+        raise RuntimeError(f"scMlpForward: {rc}")
+    return Y
+
+
+def compare(drapes, params: np.ndarray | None, norm: np.ndarray | None, frames: int = 6, skip: int = 4,
+            tol: float = 1e-4, max_iter: int = 200):
+    """Plain versus learned on the same drapes (a batch): Gauss-Seidel iterations a
+    substep to reach the residual target, and device-timed vertex-substeps/s over
+    the measured frames (after `skip` untimed frames)."""
+    import torch
+    out = {}
+    for label, warm in (("plain", False), ("learned", True)):
+        b = api.load_batch(drapes) if len(drapes) > 1 else api.load_scene(drapes[0])[1]
+        b.model.set_residual_target(tol, max_iter)
+        if warm:
+            b.model.set_warm_start(params, norm)
+        dt = drapes[0].dt
+        for _ in range(skip):
+            b.step(dt)
+        b.synchronize()
+        b.model.iteration_total()
+        st = torch.cuda.ExternalStream(b.cuda_stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(frames):
+            b.step(dt)
+        e1.record(st)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        its = b.model.iteration_total()
+        sub = drapes[0].params.substeps * frames
+        N = sum(d.num_vertices for d in drapes)
+        out[label] = {"iterations_per_substep": its / sub, "vertex_substeps_per_s": N * sub / (ms * 1e-3),
+                      "ms_per_frame": ms / frames, "residual_after": b.model.residual(), "status": b.status()}
+        b.free()
+    return out
