@@ -210,8 +210,8 @@ SCEXP int scGetIterationTotal(scModel model);
    after the substep's prediction to a position correction that is applied before
    the Gauss-Seidel loop. Features: predicted minus previous position (3),
    velocity (3), mean strain of the incident edges (1), collision-mesh normal (3),
-   distance to the first sphere / SDF collider (1, clamped to +-1), free = 1 /
-   pinned = 0 (1). params: scMlpParamCount() FP32 values, W[out][in] row-major per
+   distance to the first sphere / SDF collider (1, clamped to +-1), the previous
+   substep's solver correction along that normal (1). params: scMlpParamCount() FP32 values, W[out][in] row-major per
    layer then the layer's bias; norm: feature mean (12), 1 / feature std (12),
    output scale (3). params = NULL turns the warm start off. */
 SCEXP bool scSetWarmStart(scModel model, const float* params, const float* norm);

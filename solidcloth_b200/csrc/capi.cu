@@ -531,12 +531,6 @@ bool scSetSampleBuffers(scModel m, float* features, float* targets)
     if (!c || c->N == 0) { set_error(SC_ERR_ARG, "model not initialised"); return false; }
     host_sync(c);
     if (!features || !targets) { c->sampleFeat = c->sampleTarget = nullptr; c->touch(); return true; }
-    if (!c->xpred && cudaMalloc(&c->xpred, sizeof(float4) * (size_t)c->N) != cudaSuccess)
-    {
-        c->xpred = nullptr;
-        set_error(SC_ERR_CUDA, "cudaMalloc failed");
-        return false;
-    }
     c->sampleFeat = features;
     c->sampleTarget = targets;
     c->touch();

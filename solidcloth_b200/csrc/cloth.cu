@@ -418,7 +418,6 @@ ClothModel::~ClothModel()
 {
     release_device();
     if (mlpPrm) cudaFree(mlpPrm);
-    if (xpred) cudaFree(xpred);
 }
 
 void* ClothModel::dalloc(size_t bytes, bool contact)
@@ -633,6 +632,8 @@ bool ClothModel::upload_topology(const HMesh& mesh)
         for (int e = 0; e < E; e++) sum += rest[e];
         resScale = E > 0 ? (float)(E / sum) : 1.f;
         dc.xsnap = (float4*)dalloc(sizeof(float4) * (size_t)N);
+        dc.xpred = (float4*)dalloc(sizeof(float4) * (size_t)N);
+        dc.lastCorr = (float*)dalloc(sizeof(float) * (size_t)N);
     }
     dc.prevN = (float4*)dalloc(sizeof(float4) * N);
     dc.prevTriN = (float4*)dalloc(sizeof(float4) * T);
@@ -888,8 +889,16 @@ bool ClothModel::ensure_buffers(const CollisionWorld& world, cudaStream_t s)
     buf.ccdVtPairCount = counts + 4; buf.ccdEePairCount = counts + 5; buf.scanTot = counts + 8;
     // self contacts
     const bool self = (prm.flags & CF_SELF) != 0;
-    buf.ccdVtCap = ccd ? std::max(1, N * CCD_VT_PAIRS) : 1;
-    buf.ccdEeCap = ccd ? std::max(1, E * CCD_EE_PAIRS) : 1;
+    // Candidate pairs grow with (swept-box width / edge length)^2: a box of half
+    // width r = thickness + tolerance / 2 around a primitive meets about
+    // (2 r / l + 1)^2 primitives per layer of cloth; the stores hold four layers'
+    // worth, and at least the per-query constants.
+    const float r = prm.thickness + 0.5f * prm.tolerance, l = resScale > 0.f ? 1.f / resScale : 1.f;
+    const double per = 4.0 * 3.0 * (2.0 * r / l + 1.0) * (2.0 * r / l + 1.0);
+    const size_t vtPer = (size_t)std::max<double>(CCD_VT_PAIRS, per), eePer = (size_t)std::max<double>(CCD_EE_PAIRS, per);
+    const size_t cap32 = (size_t)1 << 30;
+    buf.ccdVtCap = ccd ? (int)std::max<size_t>(1, std::min(cap32, (size_t)N * vtPer)) : 1;
+    buf.ccdEeCap = ccd ? (int)std::max<size_t>(1, std::min(cap32, (size_t)E * eePer)) : 1;
     buf.stCap = (self ? N * KVT : 1) + (ccd ? N * CCD_VT_HITS : 0);
     buf.seCap = (self ? E : 1) + (ccd ? E * CCD_EE_HITS : 0);
     buf.stCnt = (int*)dalloc(sizeof(int) * N, true);
@@ -912,7 +921,7 @@ bool ClothModel::ensure_buffers(const CollisionWorld& world, cudaStream_t s)
     buf.ccdEeHitCnt = (int*)dalloc(sizeof(int) * E, true);
     buf.ccdVtPoolOff = (int*)dalloc(sizeof(int) * N, true);
     buf.ccdEePoolOff = (int*)dalloc(sizeof(int) * E, true);
-    buf.ccdPoolCap = ccd ? std::max(N, E) * KCCD / 2 : 1;
+    buf.ccdPoolCap = ccd ? std::max(buf.ccdEeCap, std::max(N, E) * KCCD / 2) : 1;
     buf.ccdPool = (int*)dalloc(sizeof(int) * (size_t)buf.ccdPoolCap, true);
     buf.ccdPoolUsed = counts + 6;
     // colouring
@@ -1211,14 +1220,15 @@ void ClothPatch::record_substep(float h)
     // learned warm start (no reference counterpart): record the features and the
     // predicted positions, and / or move the particles by the network's correction
     const size_t sub = (size_t)recordingSubstep;
-    if (m.sampleFeat && m.xpred) launch_mlp_features(s, c, b, m.sampleFeat + sub * m.N * MLP_IN, m.xpred);
+    const bool learn = (m.warmStart && m.mlpPrm) || m.sampleFeat;
+    if (learn) launch_mlp_features(s, c, b, m.sampleFeat ? m.sampleFeat + sub * m.N * MLP_IN : nullptr);
     if (m.warmStart && m.mlpPrm) launch_mlp_warm(s, c, b, m.mlpPrm, m.mlpPrm + MLP_NPARAM);
     // ClothModelPBD::SolveGS (Physics/ClothPBD.cpp:324-369)
     launch_reset_gs(s, c);
     timing_mark(SEC_GS, false, s);
     record_solve(s, P, m.choice);
     timing_mark(SEC_GS, true, s);
-    if (m.sampleTarget && m.xpred) launch_mlp_targets(s, c, m.xpred, m.sampleTarget + sub * m.N * MLP_OUT);
+    if (learn) launch_mlp_targets(s, c, m.sampleTarget ? m.sampleTarget + sub * m.N * MLP_OUT : nullptr);
     recordingSubstep++;
 }
 

@@ -172,7 +172,6 @@ public:
     bool warmStart = false;
     float* sampleFeat = nullptr;
     float* sampleTarget = nullptr;
-    float4* xpred = nullptr;
     int solverMode = SOLVE_AUTO;                // forced solver, or the tuner's choice
     SolverChoice choice{SOLVE_CLUSTER, 0, 0, 0.f};
     bool tuned = false;

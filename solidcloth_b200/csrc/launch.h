@@ -128,8 +128,8 @@ bool launch_gs_grid(cudaStream_t s, const DevCloth& c, const SolverParams& P, co
 // learned warm start (mlp_kernels.cuh): 9347 FP32 parameters, 27 normalisation values
 constexpr int MLP_NPARAM = 9347, MLP_NNORM = 27, MLP_IN = 12, MLP_OUT = 3;
 void launch_mlp_warm(cudaStream_t s, const DevCloth& c, const Buffers& b, const float* prm, const float* norm);
-void launch_mlp_features(cudaStream_t s, const DevCloth& c, const Buffers& b, float* feat, float4* xpred);
-void launch_mlp_targets(cudaStream_t s, const DevCloth& c, const float4* xpred, float* target);
+void launch_mlp_features(cudaStream_t s, const DevCloth& c, const Buffers& b, float* feat);
+void launch_mlp_targets(cudaStream_t s, const DevCloth& c, float* target);
 void launch_mlp_forward(cudaStream_t s, const float* X, int S, const float* prm, const float* norm, float* Y);
 bool launch_mlp_grad(cudaStream_t s, const float* X, const float* T, int S, const float* prm, const float* norm,
                      float* grad, float* loss);

@@ -173,7 +173,9 @@ __device__ __forceinline__ void mlp_forward_tile(const MlpSmem& s, const float* 
 // The 12 inputs of particle i after the substep's prediction: predicted minus
 // previous position (3), velocity (3), mean strain of its incident edges (1),
 // collision-mesh normal (3), signed distance to its first sphere / SDF collider
-// (1, clamped to +-1 m), and 1 for a free particle, 0 for a pinned one (1).
+// (1, clamped to +-1 m), and — the twelfth, chosen here — the previous
+// substep's solver correction along that normal (1): corrections are coherent
+// in time, and the normal component carries the contact response.
 __device__ __forceinline__ void ml_features(const DevCloth& c, const Buffers& b, int i, float* f)
 {
     const float4 p = c.pos[i], q = c.prev[i], v = c.vel[i];
@@ -204,7 +206,7 @@ __device__ __forceinline__ void ml_features(const DevCloth& c, const Buffers& b,
         break;
     }
     f[10] = fminf(1.f, fmaxf(-1.f, dist));
-    f[11] = p.w > 0.f ? 1.f : 0.f;
+    f[11] = c.lastCorr[i];
 }
 
 struct MlpArgs
@@ -251,24 +253,30 @@ __global__ void __launch_bounds__(128) k_mlp_warm(DevCloth c, Buffers b, MlpArgs
     }
 }
 
-// raw features of every particle (sample recording) and the predicted positions
-__global__ void k_mlp_features(DevCloth c, Buffers b, float* feat, float4* xpred)
+// the predicted positions, and (sample recording) every particle's raw features
+__global__ void k_mlp_features(DevCloth c, Buffers b, float* feat)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.N) return;
-    float f[ML_IN];
-    ml_features(c, b, i, f);
-    for (int k = 0; k < ML_IN; k++) feat[(size_t)i * ML_IN + k] = f[k];
-    xpred[i] = c.pos[i];
+    if (feat)
+    {
+        float f[ML_IN];
+        ml_features(c, b, i, f);
+        for (int k = 0; k < ML_IN; k++) feat[(size_t)i * ML_IN + k] = f[k];
+    }
+    c.xpred[i] = c.pos[i];
 }
 
-// the substep's correction: converged minus predicted positions
-__global__ void k_mlp_targets(DevCloth c, const float4* xpred, float* target)
+// the substep's correction (solved minus predicted positions): its normal
+// component for the next substep's features, and (sample recording) the target
+__global__ void k_mlp_targets(DevCloth c, float* target)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.N) return;
-    const float4 p = c.pos[i], q = xpred[i];
-    target[3 * (size_t)i] = p.x - q.x; target[3 * (size_t)i + 1] = p.y - q.y; target[3 * (size_t)i + 2] = p.z - q.z;
+    const float4 p = c.pos[i], q = c.xpred[i], n = c.prevN[i];
+    const float dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
+    c.lastCorr[i] = dx * n.x + dy * n.y + dz * n.z;
+    if (target) { target[3 * (size_t)i] = dx; target[3 * (size_t)i + 1] = dy; target[3 * (size_t)i + 2] = dz; }
 }
 
 // forward over raw feature rows (S x 12) -> outputs (S x 3, output scale applied)

@@ -63,6 +63,8 @@ struct DevCloth
     const int* instStart;       // batch: first particle of each instance (+ end)
     const float* edgeRest;      // E: rest length of each edge (from the uv layout)
     float4* xsnap;              // N: positions at the start of the current iteration (update residual)
+    float4* xpred;              // N: positions after the substep's prediction (warm start / samples)
+    float* lastCorr;            // N: last substep's solver correction along the collision normal
     const int* vQuery;          // N: vertices in spatial (Morton, rest shape) order: neighbouring
     const int* eQuery;          // E: edges likewise; queries of one warp walk the same subtrees
     float4* prevN;              // collision mesh vertex normals (refreshed per frame)

@@ -2828,14 +2828,14 @@ void launch_mlp_warm(cudaStream_t s, const DevCloth& c, const Buffers& b, const 
     k_mlp_warm<<<(c.N + 127) / 128, 128, 0, s>>>(c, b, MlpArgs{prm, norm});
 }
 
-void launch_mlp_features(cudaStream_t s, const DevCloth& c, const Buffers& b, float* feat, float4* xpred)
+void launch_mlp_features(cudaStream_t s, const DevCloth& c, const Buffers& b, float* feat)
 {
-    k_mlp_features<<<blocks_for(c.N), 256, 0, s>>>(c, b, feat, xpred);
+    k_mlp_features<<<blocks_for(c.N), 256, 0, s>>>(c, b, feat);
 }
 
-void launch_mlp_targets(cudaStream_t s, const DevCloth& c, const float4* xpred, float* target)
+void launch_mlp_targets(cudaStream_t s, const DevCloth& c, float* target)
 {
-    k_mlp_targets<<<blocks_for(c.N), 256, 0, s>>>(c, xpred, target);
+    k_mlp_targets<<<blocks_for(c.N), 256, 0, s>>>(c, target);
 }
 
 void launch_mlp_forward(cudaStream_t s, const float* X, int S, const float* prm, const float* norm, float* Y)

@@ -187,3 +187,60 @@ def compare(drapes, params: np.ndarray | None, norm: np.ndarray | None, frames: 
                       "ms_per_frame": ms / frames, "residual_after": b.model.residual(), "status": b.status()}
         b.free()
     return out
+
+
+def scaled(norm: np.ndarray, alpha: float) -> np.ndarray:
+    """the same network with its correction multiplied by alpha"""
+    out = norm.copy()
+    out[2 * IN:] *= alpha
+    return out
+
+
+def main(argv=None):
+    """Generate, train, evaluate; writes the parameters (npz) and a JSON report.
+
+    python -m solidcloth_b200.learned --drapes 2000 --out solidcloth_b200/data/warmstart.npz
+    """
+    import argparse
+    import json
+    import torch
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--drapes", type=int, default=2000)
+    ap.add_argument("--n", type=int, default=64)
+    ap.add_argument("--per-batch", type=int, default=250)
+    ap.add_argument("--epochs", type=int, default=20)
+    ap.add_argument("--tol", type=float, default=1e-4)
+    ap.add_argument("--max-iter", type=int, default=400)
+    ap.add_argument("--eval", type=int, default=4, help="held-out drapes per evaluation size")
+    ap.add_argument("--eval-n", type=int, nargs="*", default=[64, 256])
+    ap.add_argument("--out", default="solidcloth_b200/data/warmstart.npz")
+    ap.add_argument("--report", default=None)
+    a = ap.parse_args(argv)
+    torch.cuda.init()
+    ds = generate(a.drapes, n=a.n, per_batch=a.per_batch, tol=a.tol, max_iter=a.max_iter)
+    print(f"samples {ds.X.shape[0]} from {ds.drapes} drapes in {ds.seconds:.1f} s", flush=True)
+    norm = fit_norm(ds.X, ds.T)
+    t0 = time.time()
+    params, hist = train(ds.X, ds.T, norm, epochs=a.epochs, log=lambda m: print(m, flush=True))
+    train_s = time.time() - t0
+    np.savez(a.out, params=params, norm=norm, drapes=a.drapes, n=a.n, tol=a.tol, loss=np.array(hist))
+    report = {"drapes": a.drapes, "n_train": a.n, "samples": int(ds.X.shape[0]), "generate_s": ds.seconds,
+              "train_s": train_s, "loss_per_epoch": hist, "tol": a.tol, "max_iter": a.max_iter, "eval": {}}
+    for n in a.eval_n:
+        rows = []
+        for k in range(a.eval):
+            d = drape_scene(10_000_000 + 1000 * n + k, n)
+            r = compare([d], params, norm, frames=3, skip=4, tol=a.tol, max_iter=a.max_iter)
+            r["learned_alpha_0.5"] = compare([d], params, scaled(norm, 0.5), frames=3, skip=4, tol=a.tol,
+                                             max_iter=a.max_iter)["learned"]
+            rows.append(r)
+            print(n, k, json.dumps(r), flush=True)
+        report["eval"][str(n)] = rows
+    if a.report:
+        with open(a.report, "w") as f:
+            json.dump(report, f, indent=1)
+    return report
+
+
+if __name__ == "__main__":
+    main()

@@ -147,7 +147,11 @@ def test_recorded_features_match_numpy():
     assert np.allclose(f[:, 6], strain / cnt, atol=1e-5)
     d = np.linalg.norm(xp, axis=1) - 0.2
     assert np.allclose(f[:, 10], np.clip(d, -1, 1), atol=2e-3)     # 32^3 SDF sampling
-    assert np.all(f[:, 11] == 1.0)
+    assert np.all(f[:, 11] == 0.0)                                  # no earlier substep
+    # substep 1's twelfth feature: substep 0's correction along the normal
+    f1 = F.cpu().numpy()[1]
+    t0 = Tg.cpu().numpy()[0]
+    assert np.allclose(f1[:, 11], np.sum(t0 * f[:, 7:10], axis=1), atol=1e-8)
     nrm = np.linalg.norm(f[:, 7:10], axis=1)
     assert np.allclose(nrm, 1.0, atol=1e-5)
     p.free()
