@@ -7,7 +7,14 @@ Workload (default): the 128x128 drape onto a 64^3 sphere SDF with self-collision
 i.e. one scStepCloth(1/60) call = 8 substeps. Multi-GPU (torchrun, one process
 per GPU) runs independent replicas (a single cloth does not shard): scaling is
 weak and `value` is the sum over ranks of the device-timed throughput, using the
-max time over ranks.
+max time over ranks. --config cfg3 steps the 512 uneven instances as one batch
+patch; under torchrun the instances are partitioned over the ranks (no
+collective on the data path, strong scaling) and `value` is all instances'
+vertex-substeps over the slowest rank's time.
+
+The line's `learned` object compares the plain solver with the learned warm
+start (solidcloth_b200/data/warmstart.npz) on held-out drapes: Gauss-Seidel
+iterations a substep to the residual target and vertex-substeps/s.
 
 Timing: W untimed frames, then K frames each bracketed by CUDA events on the
 patch's stream; L2 is flushed (a 256 MiB write) before every timed frame,
@@ -47,9 +54,10 @@ def _args():
                     help="self-collision: the continuous detector (default), the live proximity path, or both")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="cfg1", choices=["cfg0", "cfg1", "cfg2"])
+    ap.add_argument("--config", default="cfg1", choices=["cfg0", "cfg1", "cfg2", "cfg3"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the plain-vs-learned warm-start comparison")
     return ap.parse_args()
 
 
@@ -58,7 +66,33 @@ def _scene(name, self_mode="ccd"):
     return scenes.CONFIGS[name]() if name == "cfg0" else scenes.CONFIGS[name](self_mode=self_mode)
 
 
+class _Batch:
+    """cfg3: the rank's share of the 512 uneven instances, as one batch patch"""
+
+    def __init__(self, insts, rank, ws):
+        from solidcloth_b200.shard import shard
+        self.all = insts
+        self.mine = shard(insts, rank, ws)
+        s0 = self.mine[0]
+        self.name = f"cfg3_512_uneven_instances_rank{rank}of{ws}"
+        self.n = 0
+        self.params = s0.params
+        self.dt = s0.dt
+        self.ccd = s0.ccd
+        self.num_vertices = sum(s.num_vertices for s in self.mine)
+        self.sdfs, self.meshes, self.walls = s0.sdfs, s0.meshes, None
+
+
 def _workload(sc):
+    if isinstance(sc, _Batch):
+        return {"workload": f"cfg3: {len(sc.all)} independent cloths, sides log-uniform in [16, 128] "
+                            f"({sum(s.num_vertices for s in sc.all)} vertices in all, {sc.num_vertices} on this rank, "
+                            f"{len(sc.mine)} instances), own 32^3 sphere SDF each, 1-4 pinned corners, continuous "
+                            f"self-collision, {sc.params.substeps} substeps x {sc.params.iterations} iterations per frame, "
+                            f"one batch patch (one graph per frame, one solver launch per substep)",
+                "flags": sc.params.flags, "iterations": "fixed",
+                "l2": "flushed (256 MiB write) before every timed frame; the batch state (~30 MB/1M vertices) exceeds L2 anyway",
+                "step": "one frame = one scStepCloth call on the batch"}
     return {"workload": f"{sc.name}: {sc.n}x{sc.n} grid ({sc.num_vertices} vertices), "
                         f"{sc.params.substeps} substeps x {sc.params.iterations} iterations per frame, dt 1/60",
             "flags": sc.params.flags, "colliders": {"sdf": len(sc.sdfs), "mesh": len(sc.meshes),
@@ -163,38 +197,78 @@ def run_reference(args):
     ws, rank, _ = _dist()
     if rank != 0:
         return
-    sc = _scene(args.config, args.self_mode)
     from oracle.bridge import available
     if not available("ref"):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libscref.so not built (reference sources absent at build time)"}))
         return
     from oracle.bridge import RefCloth, _load, REF_LIB
+    import ctypes as C
     lib = _load(REF_LIB, "ref_")
     cores = lib.ref_max_threads()
-    r = RefCloth.from_scene(sc)
-    import ctypes as C
-    h = sc.dt / sc.params.substeps
-    pa = sc.params.as_array().copy()
-    pa[9] = 1
-    r._fn("set_params")(r.h, pa.ctypes.data_as(C.POINTER(C.c_float)), pa.size)
+    if args.config == "cfg3":
+        # a bounded sample of the batch: 8 instances spread over the list, one substep each per step
+        from solidcloth_b200 import scenes
+        insts = scenes.cfg3_instances()
+        sample = insts[::len(insts) // 8][:8]
+        work = _Batch(insts, 0, 1)
+        label = f"{len(sample)} of the {len(insts)} cfg3 instances ({sum(x.num_vertices for x in sample)} vertices)"
+    else:
+        sample = [_scene(args.config, args.self_mode)]
+        work = sample[0]
+        label = sample[0].name
+    clothes = []
+    for sc in sample:
+        r = RefCloth.from_scene(sc)
+        pa = sc.params.as_array().copy()
+        pa[9] = 1
+        r._fn("set_params")(r.h, pa.ctypes.data_as(C.POINTER(C.c_float)), pa.size)
+        clothes.append((r, sc.dt / sc.params.substeps))
     for _ in range(args.warmup):
-        r.step(h)
+        for r, h in clothes:
+            r.step(h)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        r.step(h)
+        for r, h in clothes:
+            r.step(h)
         times.append(time.perf_counter() - t0)
     tot = sum(times)
-    value = sc.num_vertices * args.steps / tot
+    value = sum(sc.num_vertices for sc in sample) * args.steps / tot
     line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
-            "data": "synthetic", "config": dict(_workload(sc), step="one substep (reference CPU)"),
+            "higher_is_better": True, "scaling": "strong" if args.config == "cfg3" else "weak", "vs_baseline": None,
+            "dtype": "fp32", "data": "synthetic", "config": dict(_workload(work), step="one substep (reference CPU)"),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
-                             "sample": f"{args.steps} substeps of {sc.name} after {args.warmup} warm-up substeps, "
+                             "sample": f"{args.steps} substeps of {label} after {args.warmup} warm-up substeps, "
                                        f"OpenMP threads = {cores}"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
+
+
+def _learned_ab(drapes: int = 2, n: int = 64):
+    """iterations a substep to the residual target (update residual <= 1e-4, cap
+    400) and device-timed vertex-substeps/s, plain versus learned warm start, on
+    held-out drapes (seeds the training never saw)"""
+    from solidcloth_b200 import learned
+    path = ROOT / "solidcloth_b200" / "data" / "warmstart.npz"
+    if not path.exists():
+        return {"unavailable": "no trained weights (python -m solidcloth_b200.learned)"}
+    z = np.load(path)
+    params, norm = z["params"].astype(np.float32), z["norm"].astype(np.float32)
+    rows = [learned.compare([learned.drape_scene(20_000_000 + k, n)], params, norm, frames=3, skip=4,
+                            tol=1e-4, max_iter=400)
+            for k in range(drapes)]
+    plain_it = float(np.mean([r["plain"]["iterations_per_substep"] for r in rows]))
+    learn_it = float(np.mean([r["learned"]["iterations_per_substep"] for r in rows]))
+    plain_v = float(np.mean([r["plain"]["vertex_substeps_per_s"] for r in rows]))
+    learn_v = float(np.mean([r["learned"]["vertex_substeps_per_s"] for r in rows]))
+    return {"workload": f"{drapes} held-out {n}x{n} drapes over a sphere SDF, 8 substeps, continuous self-collision; "
+                        f"trained on {int(z['drapes'])} drapes at {int(z['n'])}x{int(z['n'])}",
+            "residual": "update residual (largest displacement of an iteration / mean rest edge) <= 1e-4, cap 400",
+            "plain_iterations_per_substep": plain_it, "learned_iterations_per_substep": learn_it,
+            "iteration_ratio": plain_it / learn_it if learn_it else None,
+            "plain_vertex_substeps_per_s": plain_v, "learned_vertex_substeps_per_s": learn_v,
+            "throughput_ratio": learn_v / plain_v if plain_v else None}
 
 
 def run_ours(args):
@@ -205,9 +279,14 @@ def run_ours(args):
         import torch.distributed as dist
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
-    from solidcloth_b200 import api
-    sc = _scene(args.config, args.self_mode)
-    w, p = api.load_scene(sc)
+    from solidcloth_b200 import api, scenes
+    if args.config == "cfg3":
+        # instances shard over ranks (no collective on the data path): strong scaling
+        sc = _Batch(scenes.cfg3_instances(), rank, ws)
+        p = api.load_batch(sc.mine)
+    else:
+        sc = _scene(args.config, args.self_mode)
+        w, p = api.load_scene(sc)
     stream = torch.cuda.ExternalStream(p.cuda_stream(), device=torch.device("cuda", local))
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     # CUDA events inside the frame graph bracket the solve and the broad phases of
@@ -245,7 +324,12 @@ def run_ours(args):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         tot_ms = float(t.item())
     vsub = sc.num_vertices * sc.params.substeps
-    value = ws * vsub * args.steps / (tot_ms * 1e-3)
+    if isinstance(sc, _Batch):
+        # every rank steps its own instances: all ranks' vertex-substeps over the slowest rank's time
+        all_vsub = sum(s.num_vertices for s in sc.all) * sc.params.substeps
+        value = all_vsub * args.steps / (tot_ms * 1e-3)
+    else:
+        value = ws * vsub * args.steps / (tot_ms * 1e-3)
     status = st | p.status()
 
     # end to end through the C ABI with host buffers
@@ -271,7 +355,8 @@ def run_ours(args):
             t = torch.tensor([e2e_s], device="cuda")
             torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
             e2e_s = float(t.item())
-        e2e = {"value": ws * vsub * args.steps / e2e_s, "unit": UNIT,
+        e2e_units = (sum(s.num_vertices for s in sc.all) * sc.params.substeps) if isinstance(sc, _Batch) else ws * vsub
+        e2e = {"value": e2e_units * args.steps / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": 3 * 16 * sc.num_vertices,
                "d2h_bytes_per_step": 3 * 16 * sc.num_vertices,
                "path": "scSetParticleState -> scStepCloth -> scGetParticlePositions/Prev/Velocities"}
@@ -316,15 +401,25 @@ def run_ours(args):
                     "ccd_broad_vt_ms_per_launch": (sections["ccd_broad_vt"][0] / sections["ccd_broad_vt"][1]
                                                    if sections.get("ccd_broad_vt", (0, 0))[1] else None)}
 
+    # plain versus learned warm start at the residual target (trained weights from
+    # solidcloth_b200/data/warmstart.npz, held-out 64x64 drapes)
+    learned_ab = None
+    if rank == 0 and not args.no_learned:
+        try:
+            learned_ab = _learned_ab()
+        except Exception as e:  # reported, not fatal
+            learned_ab = {"error": str(e)}
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
             from oracle.bridge import available
             if available("ref"):
-                nsub = 2 if sc.num_vertices > 4096 else 32
-                v, secs, cores = cpu_reference_rate(sc, nsub)
+                ref_sc = sc.mine[len(sc.mine) // 2] if isinstance(sc, _Batch) else sc
+                nsub = 2 if ref_sc.num_vertices > 4096 else 32
+                v, secs, cores = cpu_reference_rate(ref_sc, nsub)
                 cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
-                       "sample": f"{nsub} substeps of {sc.name} after one untimed substep ({secs:.1f} s), "
+                       "sample": f"{nsub} substeps of {ref_sc.name} after one untimed substep ({secs:.1f} s), "
                                  f"the reference's own C++ (oracle/_ref, OpenMP {cores} threads)"}
         except Exception as e:  # reported, not fatal
             cpu = {"value": None, "unit": UNIT, "cores": None, "kind": "reference", "sample": f"failed: {e}"}
@@ -332,8 +427,9 @@ def run_ours(args):
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": tot_ms / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
-                "config": _workload(sc), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "scaling": "strong" if isinstance(sc, _Batch) else "weak", "vs_baseline": None, "dtype": "fp32",
+                "data": "synthetic", "config": _workload(sc), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "learned": learned_ab,
                 "gpu_launches": kernels_per_frame * args.steps, "kernels_per_frame": kernels_per_frame,
                 "clocks": clk.summary(), "device_status": status}
         print(json.dumps(line))
