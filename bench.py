@@ -58,6 +58,7 @@ def _args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the plain-vs-learned warm-start comparison")
+    ap.add_argument("--instances", type=int, default=512, help="cfg3: number of instances (the first K of the 512)")
     return ap.parse_args()
 
 
@@ -282,7 +283,7 @@ def run_ours(args):
     from solidcloth_b200 import api, scenes
     if args.config == "cfg3":
         # instances shard over ranks (no collective on the data path): strong scaling
-        sc = _Batch(scenes.cfg3_instances(), rank, ws)
+        sc = _Batch(scenes.cfg3_instances()[:args.instances], rank, ws)
         p = api.load_batch(sc.mine)
     else:
         sc = _scene(args.config, args.self_mode)
@@ -371,9 +372,17 @@ def run_ours(args):
         "gs_solve": it * 144 * T + ((it + 1) // 2) * 144 * B + 48 * N,
         # per query: 2 endpoints x (pos, prev) 64 B + edge 16 B + count 4 B; 4 B per pair; tree read once
         "ccd_broad_ee": E * 84 + 4 * ee_pairs + 32 * (2 * E - 1),
+        # per particle: pos + prev 32 B read, one 64 B contact slot written per collider hit (upper bound: one per particle)
+        "colliders": 96 * N,
     }
-    kernel_names = {"gs_solve": "k_gs_cluster (one substep's Gauss-Seidel loop + velocity, one cluster launch)",
-                    "ccd_broad_ee": "k_ccd_broad_ee (edge-edge swept-box LBVH query, both passes)"}
+    ch, _ = p.model.solver_choice()
+    solver = {1: "k_gs_cluster (one substep's Gauss-Seidel loop + velocity, one cluster launch)",
+              2: f"k_gs_grid variant {ch[1]} ({ch[3]} threads, {ch[2]} CTAs/SM; one substep's Gauss-Seidel loop + velocity, one cooperative launch)",
+              3: "k_fem / k_bends per colour (one substep's Gauss-Seidel loop)"}.get(ch[0], "solver")
+    kernel_names = {"gs_solve": solver,
+                    "ccd_broad_ee": "k_ccd_broad_ee (edge-edge swept-box LBVH query, both passes)",
+                    "colliders": "k_vertex_colliders + k_tri_colliders + k_edge_colliders (collider detection)"}
+    walk, walk_ms = p.model.broad_phase_mode()
     per = {}
     for k in algo:
         tot, cnt = sections.get(k, (0.0, 0))
@@ -383,12 +392,12 @@ def run_ours(args):
                       "achieved_gbs": algo[k] / (avg * 1e-3) / 1e9, "share_of_frame": tot / tot_ms}
     dom = max(per, key=lambda k: per[k]["ms_per_launch"] * per[k]["launches"]) if per else None
     traffic = None
-    tj = ROOT / "profiles" / "traffic.json"
-    if dom and tj.exists():
-        try:
-            traffic = json.loads(tj.read_text()).get(f"{args.config}_{dom}_bytes_per_launch")
-        except Exception:
-            traffic = None
+    tt = ROOT / "profiles" / "traffic.txt"     # DRAM bytes per launch from the ncu captures
+    if dom and tt.exists():
+        for line in tt.read_text().splitlines():
+            f = line.split()
+            if len(f) == 3 and not line.startswith("#") and f[0] == args.config and f[1] == dom:
+                traffic = int(f[2])
     roofline = None
     if dom:
         d = per[dom]
@@ -399,7 +408,9 @@ def run_ours(args):
                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, burst copy)",
                     "sections": per,
                     "ccd_broad_vt_ms_per_launch": (sections["ccd_broad_vt"][0] / sections["ccd_broad_vt"][1]
-                                                   if sections.get("ccd_broad_vt", (0, 0))[1] else None)}
+                                                   if sections.get("ccd_broad_vt", (0, 0))[1] else None),
+                    "broad_phase_walk": {"chosen": ["per-query stack walk", "warp packet"][walk],
+                                         "tuned_ms": walk_ms.tolist()}}
 
     # plain versus learned warm start at the residual target (trained weights from
     # solidcloth_b200/data/warmstart.npz, held-out 64x64 drapes)

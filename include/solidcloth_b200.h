@@ -245,6 +245,13 @@ SCEXP void scSetGridSolver(scModel model, int variant, int blocksPerSm);
    tuneMs (4 floats per candidate: kind, variant, CTAs per SM, ms per substep)
    gets up to cap candidates of the last tuning; returns the candidate count */
 SCEXP int scGetSolverChoice(scModel model, int* out4, float* tuneMs, int cap);
+/* Continuous-collision broad phase walk (additions): 0 = one tree walk per query
+   (lane), 1 = warp packets (32 neighbouring queries walk together, broadcast
+   node loads), -1 (default) = timed at the first step and the faster kept. Same
+   candidate sets. scGetBroadPhaseMode returns the walk in use and, in ms2, the
+   tuned times of both (ms per substep's detection). */
+SCEXP void scSetBroadPhaseMode(scModel model, int mode);
+SCEXP int scGetBroadPhaseMode(scModel model, float* ms2);
 /* info3 = {threads per CTA, FEM constraints per thread, bends per thread} per variant */
 SCEXP int scGetGridVariants(int* info3, int cap);
 /* true (default): the cluster solver copies each CTA's FEM and bend records to
@@ -301,11 +308,12 @@ SCEXP int scGetGraphKernelCount(scClothPatch patch);
 SCEXP float scProfileSweep(scClothPatch patch, int kind, int reps);
 /* Section timing inside the frame graph (additions, no reference counterpart):
    frames > 0 brackets, in every substep, the Gauss-Seidel solve (section 0), the
-   edge-edge (1) and vertex-triangle (2) continuous-collision broad phases with
+   edge-edge (1) and vertex-triangle (2) continuous-collision broad phases and the
+   collider detection (3: walls, spheres, SDFs, meshes) with
    CUDA events, fresh ones for each of the next `frames` frames, so no host
    synchronisation enters a timed run; 0 turns it off. Re-captures the graph. */
 SCEXP bool scSetKernelTiming(scClothPatch patch, int frames);
-/* Synchronises; ms[3] = summed event time per section, counts[3] = timed
+/* Synchronises; ms[4] = summed event time per section, counts[4] = timed
    instances, over the frames since the last read; returns those frames. */
 SCEXP int scGetKernelTiming(scClothPatch patch, float* ms, int* counts);
 

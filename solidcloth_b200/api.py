@@ -133,6 +133,8 @@ SIGNATURES = {
     "scSetGridSolver": ([scModel, C.c_int, C.c_int], None),
     "scGetSolverChoice": ([scModel, _i, _f, C.c_int], C.c_int),
     "scGetGridVariants": ([_i, C.c_int], C.c_int),
+    "scSetBroadPhaseMode": ([scModel, C.c_int], None),
+    "scGetBroadPhaseMode": ([scModel, _f], C.c_int),
     "scGetSolverIterations": ([scModel], C.c_int),
     "scGetResidual": ([scModel], C.c_float),
     "scSetResidualTarget": ([scModel, C.c_float, C.c_int], None),
@@ -328,6 +330,17 @@ class ClothModel:
         n = lib().scGetSolverChoice(self.h, out.ctypes.data_as(_i), log.ctypes.data_as(_f), 64)
         return tuple(int(x) for x in out), log[:min(n, 64)].copy()
 
+    def set_broad_phase_mode(self, mode: int):
+        """0 per-query walks, 1 warp packets, -1 tuned"""
+        lib().scSetBroadPhaseMode(self.h, int(mode))
+        _check("scSetBroadPhaseMode")
+
+    def broad_phase_mode(self):
+        """(walk in use, tuned ms of [per-query, packet])"""
+        ms = np.zeros(2, np.float32)
+        mode = lib().scGetBroadPhaseMode(self.h, ms.ctypes.data_as(_f))
+        return int(mode), ms.copy()
+
     def set_cluster_staging(self, on: bool):
         lib().scSetClusterStaging(self.h, bool(on))
 
@@ -479,10 +492,10 @@ class ClothPatch:
 
     def kernel_timing(self):
         """{section: (total ms, instances)} since the last read, and the frames covered"""
-        ms = np.zeros(3, np.float32)
-        cnt = np.zeros(3, np.int32)
+        ms = np.zeros(4, np.float32)
+        cnt = np.zeros(4, np.int32)
         frames = lib().scGetKernelTiming(self.h, ms.ctypes.data_as(_f), cnt.ctypes.data_as(_i))
-        names = ("gs_solve", "ccd_broad_ee", "ccd_broad_vt")
+        names = ("gs_solve", "ccd_broad_ee", "ccd_broad_vt", "colliders")
         return {n: (float(ms[k]), int(cnt[k])) for k, n in enumerate(names)}, int(frames)
 
     def mesh_buffers(self):

@@ -472,6 +472,22 @@ int scGetSolverChoice(scModel m, int* out4, float* tuneMs, int cap)
         }
     return (int)log.size();
 }
+void scSetBroadPhaseMode(scModel m, int mode)
+{
+    if (!M(m) || mode < -1 || mode > 1) { set_error(SC_ERR_ARG, "broad-phase mode must be -1, 0 or 1"); return; }
+    M(m)->broadMode = mode;
+    if (mode >= 0) { M(m)->broadPacket = mode; M(m)->buf.broadPacket = mode; }
+    M(m)->tuned = false;
+    M(m)->touch();
+}
+
+int scGetBroadPhaseMode(scModel m, float* ms2)
+{
+    if (!M(m)) return -1;
+    if (ms2) { ms2[0] = M(m)->broadMs[0]; ms2[1] = M(m)->broadMs[1]; }
+    return M(m)->broadPacket;
+}
+
 int scGetGridVariants(int* info3, int cap)
 {
     const int n = gs_grid_variants();

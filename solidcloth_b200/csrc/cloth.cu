@@ -936,6 +936,7 @@ bool ClothModel::ensure_buffers(const CollisionWorld& world, cudaStream_t s)
     buf.scanOff = (int*)dalloc(sizeof(int) * (maxScan + 1), true);
     buf.scanBlock = (int*)dalloc(sizeof(int) * (maxScan / 1024 + 8), true);
     buf.scanBlock2 = (int*)dalloc(sizeof(int) * (maxScan / 1024 + 8), true);
+    buf.broadPacket = broadPacket;
     bufWorldVersion = world.version;
     bufFlags = prm.flags;
     bufCcd = ccd;
@@ -1191,8 +1192,10 @@ void ClothPatch::record_substep(float h)
     cudaStream_t s = stream;
     launch_predict(s, c, P);
     // ClothModel::DetectCollisions (Physics/ClothCollision.cpp:17-48)
+    timing_mark(SEC_COLLIDERS, false, s);
     launch_vertex_colliders(s, c, P, b, m.vcollHost.data());
     launch_tri_edge_colliders(s, c, P, b, m.vcollHost.data(), (int)m.vcollHost.size(), m.prm.flags);
+    timing_mark(SEC_COLLIDERS, true, s);
     const bool self = (m.prm.flags & CF_SELF) != 0, ccd = m.prm.ccd;
     if (self)
     {
@@ -1320,13 +1323,21 @@ bool ClothPatch::autotune(float h)
     ClothModel& m = model;
     const SolverParams P = m.solver_params(h);
     std::vector<int> key = {m.N, m.dc.T, m.dc.B, m.prm.iterations, m.prm.dihedral, m.prm.fem, m.prm.fixedIterations,
-                            (int)m.buf.numVColl, m.prm.bendFreq, (int)m.prm.stageRecords, m.solverMode};
+                            (int)m.buf.numVColl, m.prm.bendFreq, (int)m.prm.stageRecords, m.solverMode,
+                            (int)m.prm.ccd, m.broadMode};
     key.insert(key.end(), m.triColourStart.begin(), m.triColourStart.end());
     key.insert(key.end(), m.bendColourStart.begin(), m.bendColourStart.end());
     {
         std::lock_guard<std::mutex> lk(g_tuneMutex);
         for (auto& kv : g_tuneCache)
-            if (kv.first == key) { m.choice = kv.second; m.tuned = true; return true; }
+            if (kv.first == key)
+            {
+                m.choice = kv.second;
+                m.broadPacket = m.broadMode >= 0 ? m.broadMode : kv.second.broad;
+                m.buf.broadPacket = m.broadPacket;
+                m.tuned = true;
+                return true;
+            }
     }
     std::vector<SolverChoice> cand;
     int shift = 0; size_t smem = 0;
@@ -1387,10 +1398,45 @@ bool ClothPatch::autotune(float h)
         cudaMemcpyAsync(m.dc.vel, backup + m.N, bytes, cudaMemcpyDeviceToDevice, stream);
     }
     cudaStreamSynchronize(stream);
-    cudaEventDestroy(e0); cudaEventDestroy(e1);
     cudaFree(backup);
     m.tuneLog = cand;
     m.choice = best;
+    // continuous broad phase: per-lane walks or warp packets (same pair sets), timed
+    // on this cloth's current state (the detection changes no particle)
+    if (m.prm.ccd && m.buf.ccdVtCnt)
+    {
+        for (int mode = 0; mode < 2; mode++)
+        {
+            m.buf.broadPacket = mode;
+            m.broadMs[mode] = 1e30f;
+            cudaGraph_t g = nullptr;
+            cudaGraphExec_t ge = nullptr;
+            if (cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) continue;
+            launch_ccd(stream, side, evFork, evJoin, m.dc, P, m.buf, m.sweptTriBvh, m.sweptEdgeBvh);
+            if (cudaStreamEndCapture(stream, &g) != cudaSuccess || cudaGraphInstantiate(&ge, g, 0) != cudaSuccess)
+            {
+                if (g) cudaGraphDestroy(g);
+                cudaGetLastError();
+                continue;
+            }
+            cudaGraphDestroy(g);
+            cudaGraphLaunch(ge, stream);
+            cudaEventRecord(e0, stream);
+            for (int r = 0; r < 3; r++) cudaGraphLaunch(ge, stream);
+            cudaEventRecord(e1, stream);
+            float ms = 0.f;
+            if (cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
+                m.broadMs[mode] = ms / 3;
+            cudaGetLastError();
+            cudaGraphExecDestroy(ge);
+        }
+        m.broadPacket = m.broadMs[1] < m.broadMs[0] ? 1 : 0;
+    }
+    if (m.broadMode >= 0) m.broadPacket = m.broadMode;
+    m.buf.broadPacket = m.broadPacket;
+    best.broad = m.broadPacket;
+    m.choice = best;
+    cudaEventDestroy(e0); cudaEventDestroy(e1);
     m.tuned = true;
     std::lock_guard<std::mutex> lk(g_tuneMutex);
     g_tuneCache.push_back({key, best});

@@ -105,7 +105,7 @@ struct BatchColl { std::shared_ptr<Collidable> coll; int vBegin, vCount, inst; }
 
 // solver selection (autotuned unless forced)
 enum SolverKind { SOLVE_AUTO = 0, SOLVE_CLUSTER = 1, SOLVE_GRID = 2, SOLVE_KERNELS = 3 };
-struct SolverChoice { int kind, variant, blocksPerSm; float ms; };
+struct SolverChoice { int kind, variant, blocksPerSm; float ms; int broad; };
 
 struct FemHost { uint32_t i1, i2, i3; float du1, du2, dv1, dv2, det, invDet, lu0, lv0, su, sv, lu2, lv2, area; };
 
@@ -177,6 +177,9 @@ public:
     bool tuned = false;
     uint64_t tunedVersion = 0;
     std::vector<SolverChoice> tuneLog;          // candidates and their times of the last tuning
+    int broadPacket = 0;                        // tuned: continuous broad phase per warp packet
+    int broadMode = -1;                         // forced walk (0 per lane, 1 packets) or -1: tuned
+    float broadMs[2] = {0.f, 0.f};              // tuned times of the two broad-phase walks
     void colour_constraints();
     void touch() { paramVersion++; }
 };
@@ -209,7 +212,7 @@ public:
     // and the two broad phases of every substep; before each replay they are
     // pointed at fresh events (cudaGraphExecEventRecordNodeSetEvent affects only
     // later launches), so a run of frames is timed with no host synchronisation.
-    enum { SEC_GS = 0, SEC_BROAD_EE = 1, SEC_BROAD_VT = 2, NSEC = 3 };
+    enum { SEC_GS = 0, SEC_BROAD_EE = 1, SEC_BROAD_VT = 2, SEC_COLLIDERS = 3, NSEC = 4 };
     int timingFrames = 0;                       // frames the pool can hold (0: off)
     int timingUsed = 0;                         // frames recorded since the last read
     std::vector<cudaEvent_t> timingCapture;     // events named at capture: [substep][section][start/end]

@@ -46,6 +46,7 @@ struct Buffers
     int numVColl;
     const VColl* vcoll;       // device copy
     const int2* instColl;     // batch: (first collider, count) per instance; null: all colliders act on all
+    int broadPacket;          // 1: continuous broad phase walks the tree per warp packet (tuned)
     // triangle / edge contacts: per-collider slot arrays, flags, dense lists
     TC* tcSlot; int* tcFlag; TC* tcList; int* tcCount; int tcCap;
     EC* ecSlot; int* ecFlag; EC* ecList; int* ecCount; int ecCap;

@@ -1422,6 +1422,61 @@ __device__ __forceinline__ void bvh_query2(const DevBVH& t, const Box& q, bool a
     }
 }
 
+// Warp-packet form of bvh_query2: the 32 lanes (spatially adjacent queries in
+// the same tree) walk it together, testing both children of an entered node per
+// step; a child is entered when any lane's box overlaps it (ballot), so every
+// node load is one broadcast request instead of up to 32 scattered ones, at the
+// price of visiting the union of the lanes' nodes. Each lane reports exactly its
+// own leaves. All 32 lanes must call it; a warp whose lanes start in different
+// trees (a batch instance boundary) takes the per-lane walk.
+template <typename F>
+__device__ __forceinline__ void bvh_query2_warp(const DevBVH& t, const Box& q, bool active, F&& f, int above, int root)
+{
+    const unsigned full = 0xffffffffu;
+    const unsigned act = __ballot_sync(full, active);
+    if (!act) return;
+    const int r0 = __shfl_sync(full, root, __ffs(act) - 1);
+    if (!__all_sync(full, !active || root == r0)) { bvh_query2(t, q, active, f, above, root); return; }
+    auto over = [&](const float4& lo, const float4& hi) {
+        return !(hi.x < q.lo.x || hi.y < q.lo.y || hi.z < q.lo.z || q.hi.x < lo.x || q.hi.y < lo.y || q.hi.z < lo.z);
+    };
+    const float4 rlo = __ldg(&t.lo[r0]), rhi = __ldg(&t.hi[r0]);
+    bool rootHit = active && over(rlo, rhi) && (above < 0 || __ldg(&t.maxPrim[r0]) > above);
+    if (__float_as_int(rlo.w) < 0) { if (rootHit) f(~__float_as_int(rlo.w)); return; }
+    if (!__any_sync(full, rootHit)) return;
+    int stack[32];
+    int sp = 0;
+    int node = r0, ch = __float_as_int(rlo.w);
+    while (true)
+    {
+        const int L = node + 1, R = ch;
+        const float4 loL = __ldg(&t.lo[L]), hiL = __ldg(&t.hi[L]), loR = __ldg(&t.lo[R]), hiR = __ldg(&t.hi[R]);
+        bool oL = active && over(loL, hiL), oR = active && over(loR, hiR);
+        if (above >= 0)
+        {
+            const int mL = __ldg(&t.maxPrim[L]), mR = __ldg(&t.maxPrim[R]);
+            oL = oL && mL > above;
+            oR = oR && mR > above;
+        }
+        const int cL = __float_as_int(loL.w), cR = __float_as_int(loR.w);
+        if (cL < 0) { if (oL) f(~cL); oL = false; }
+        if (cR < 0) { if (oR) f(~cR); oR = false; }
+        const bool anyL = __any_sync(full, oL), anyR = __any_sync(full, oR);
+        if (anyL)
+        {
+            if (anyR && sp < 32) stack[sp++] = R;
+            node = L; ch = cL;
+        }
+        else if (anyR) { node = R; ch = cR; }
+        else
+        {
+            if (sp == 0) break;
+            node = stack[--sp];
+            ch = __float_as_int(__ldg(&t.lo[node]).w);
+        }
+    }
+}
+
 // tree root for a query on particle v: its instance's tree in a batch
 __device__ __forceinline__ int tree_root(const DevCloth& c, const DevBVH& t, int v)
 {
@@ -1704,7 +1759,7 @@ __global__ void __launch_bounds__(128) k_ccd_broad_vt(DevCloth c, SolverParams P
     const int r0 = c.vTriStart[i], nInc = c.vTriStart[i + 1] - r0;
 #pragma unroll
     for (int k = 0; k < KADJ; k++) inc[k] = k < nInc ? c.vTri[r0 + k].x : -1;
-    bvh_query2(tb, vb, active, [&](int t) {
+    auto emitT = [&](int t) {
         if (nInc <= KADJ)
         {
             bool adj = false;
@@ -1715,7 +1770,9 @@ __global__ void __launch_bounds__(128) k_ccd_broad_vt(DevCloth c, SolverParams P
         else if ((int)c.tri[3 * t] == i || (int)c.tri[3 * t + 1] == i || (int)c.tri[3 * t + 2] == i) return;
         if (pool || n < KCCD) out[n] = t;
         n++;
-    }, -1, tree_root(c, tb, i));
+    };
+    if (b.broadPacket) bvh_query2_warp(tb, vb, active, emitT, -1, tree_root(c, tb, i));
+    else bvh_query2(tb, vb, active, emitT, -1, tree_root(c, tb, i));
     if (!active) return;
     b.ccdVtCnt[i] = n;
 }
@@ -1746,7 +1803,7 @@ __global__ void __launch_bounds__(128) k_ccd_broad_ee(DevCloth c, SolverParams P
 #pragma unroll
     for (int k = 0; k < KADJ; k++)
         adjE[k] = !inRegs ? -1 : k < na ? c.eRing[a0 + k] : k < na + nb ? c.eRing[b0 + k - na] : -1;
-    bvh_query2(eb, qb, active, [&](int e) {
+    auto emitE = [&](int e) {
         if (e <= i) return;
         if (inRegs)
         {
@@ -1762,7 +1819,9 @@ __global__ void __launch_bounds__(128) k_ccd_broad_ee(DevCloth c, SolverParams P
         }
         if (pool || n < KCCD) out[n] = e;
         n++;
-    }, i, tree_root(c, eb, e1.x));
+    };
+    if (b.broadPacket) bvh_query2_warp(eb, qb, active, emitE, i, tree_root(c, eb, e1.x));
+    else bvh_query2(eb, qb, active, emitE, i, tree_root(c, eb, e1.x));
     if (!active) return;
     b.ccdEeCnt[i] = n;
 }

@@ -56,13 +56,15 @@ def test_batch_matches_standalone(solver):
     b.free()
 
 
-def test_batch_queries_stay_inside_instances():
+@pytest.mark.parametrize("walk", [0, 1])
+def test_batch_queries_stay_inside_instances(walk):
     """Two copies of a folded demo-scale cloth at the same place: the batch's
     continuous-collision candidate pairs are the union of each copy's own pairs
     (offset), with no pair between the copies, and its self contacts likewise."""
     from solidcloth_b200 import api
     sc, state = scenes.ccd_scene(16)
     b = api.load_batch([sc, sc])
+    b.model.set_broad_phase_mode(walk)
     n = sc.num_vertices
     pos, prev, vel = state
     b.model.set_state(np.concatenate([pos, pos]), np.concatenate([prev, prev]), np.concatenate([vel, vel]))

@@ -163,15 +163,18 @@ def test_self_check_mode_trajectory():
         assert _same(p.model.positions(), o.positions()), (f, float(np.abs(p.model.positions() - o.positions()).max()))
 
 
+@pytest.mark.parametrize("walk", [0, 1])
 @pytest.mark.parametrize("thickness", [0.5, 1.5])
-def test_ccd_broadphase_and_hits_bitexact(thickness):
-    """Candidate pair sets and hit lists of the continuous detector are bit-exact.
+def test_ccd_broadphase_and_hits_bitexact(thickness, walk):
+    """Candidate pair sets and hit lists of the continuous detector are bit-exact,
+    with either tree walk (per query, or per warp packet).
     At thickness 1.5 (boxes two grid cells wide around each edge, two layers)
     edge queries have more candidates than their own 64 slots hold and take the
     overflow-pool pass."""
     sc, state = scenes.ccd_scene(16)
     sc.params.thickness = thickness
     w, p, o = _pair(sc, ccd=True, state=state)
+    p.model.set_broad_phase_mode(walk)            # per-query walks or warp packets
     p.step(sc.dt)
     # broad phase: all-pairs overlap set of the oracle from the same predicted state
     o2 = __import__("oracle.bridge", fromlist=["PortCloth"]).PortCloth.from_scene(sc)
