@@ -260,7 +260,7 @@ SCEXP int scGetGridVariants(int* info3, int cap);
 SCEXP void scSetClusterStaging(scModel model, bool val);
 
 /* ---- additions: inspection for parity checks ---- */
-/* kind 0: FEM triangles, 1: bends. Writes the solve order (a permutation) and
+/* kind 0: FEM triangles, 1: bends, 2: links. Writes the solve order (a permutation) and
    returns the number of colours; colourStart gets numColours+1 offsets if not NULL. */
 SCEXP int scGetConstraintOrder(scModel model, int kind, int* order, int* colourStart);
 SCEXP int scGetNumBends(scModel model);

@@ -91,7 +91,10 @@ def _load(path: Path, prefix: str):
                     "portable_acos": ([C.c_float], C.c_float),
                     "self_contact_colours": ([C.c_void_p, C.c_int, _i], None),
                     "ccd_broadphase": ([C.c_void_p, C.c_float, C.c_int, _i, C.c_int], C.c_int),
-                    "residual": ([C.c_void_p], C.c_float)})
+                    "residual": ([C.c_void_p], C.c_float),
+                    "set_link_order": ([C.c_void_p, _i, C.c_int], None),
+                    "num_links": ([C.c_void_p], C.c_int),
+                    "get_links": ([C.c_void_p, _u, _f], None)})
     for name, (args, res) in sig.items():
         fn = getattr(lib, P + name)
         fn.argtypes = args
@@ -298,6 +301,18 @@ class PortCloth(CpuCloth):
         c = np.zeros(n, np.int32)
         self._fn("self_contact_colours")(self.h, kind, _ip(c))
         return c
+
+    def set_link_order(self, order):
+        o = np.ascontiguousarray(order, np.int32)
+        self._fn("set_link_order")(self.h, _ip(o), o.size)
+
+    def links(self):
+        """(n, 2) indices and (n, 2) rest length / stiffness, in creation order"""
+        n = self._fn("num_links")(self.h)
+        idx = np.zeros((n, 2), np.uint32)
+        ls = np.zeros((n, 2), np.float32)
+        self._fn("get_links")(self.h, _up(idx), _fp(ls))
+        return idx, ls
 
     def residual(self) -> float:
         """max |C| over the warp, weft and shear constraints at the current positions"""

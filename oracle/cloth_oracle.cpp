@@ -716,7 +716,7 @@ struct Cloth
 {
     /* parameters, defaults as Physics/ClothModel.cpp:10-36 */
     float unit = 10, thickness = 0.3f, tolerance = 0.2f, shear = 5e8f, bendStiff = 5.f, stretch = 2e10f;
-    float poisson = 0.5f, friction = 0.4f, drag = 1.f, selfShrink = 0.9f, selfThreshold = 0.003f;
+    float poisson = 0.5f, friction = 0.4f, drag = 1.f, selfShrink = 0.9f, selfThreshold = 0.003f, area = 10.f;
     int iterations = 50, substeps = 1, flags = 0, bendFreq = 2;
     bool fem = false, dihedral = true;
     bool ccd = false;
@@ -727,9 +727,11 @@ struct Cloth
     std::vector<V3> uv;
     std::vector<Tri> tris;
     std::vector<Bend> bends;
+    struct Link { u32 i1, i2; float len, stiffness; };   /* Physics/ClothTypes.h:94-99 */
+    std::vector<Link> links;
     Topo mesh, prevMesh;
 
-    std::vector<int> triOrder, bendOrder;
+    std::vector<int> triOrder, bendOrder, linkOrder;
     int contactOrder = 0;
 
     std::vector<Collider> colliders;
@@ -765,15 +767,28 @@ struct Cloth
         tris.push_back(t);
     }
 
+    /* ClothModel::AddLink (Physics/ClothModel.inl:12-31): skipped when both ends
+       are pinned or the stiffness is zero; rest length from the current positions */
+    void add_link(u32 a, u32 b, float stiff)
+    {
+        if (invMass[a] == 0 && invMass[b] == 0) return;
+        if (stiff == 0) return;
+        Link l;
+        l.i1 = a; l.i2 = b; l.stiffness = stiff;
+        l.len = len(pos[a] - pos[b]);
+        links.push_back(l);
+    }
+
     /* ClothPatch::Init(grid) (Physics/ClothPatch.cpp:135-246): positions, uv,
-       alternating-diagonal triangles, pins, edges and bends. Links are not
-       built: the FEM path never reads them. */
+       links (stretch, shear and, without dihedral bending, bend links) in the
+       reference's creation order, alternating-diagonal triangles, pins, edges
+       and bends. */
     void init_grid(int divX, int divY, float inc, V3 offset, bool horizontal, bool attached)
     {
         N = divX * divY;
         pos.assign(N, v3(0, 0, 0)); prev.assign(N, v3(0, 0, 0)); vel.assign(N, v3(0, 0, 0));
         invMass.assign(N, 1.f); uv.assign(N, v3(0, 0, 0));
-        tris.clear(); bends.clear();
+        tris.clear(); bends.clear(); links.clear();
         mesh = Topo();
         float x = -0.5f * divX * inc;
         const float startY = x;
@@ -784,6 +799,12 @@ struct Cloth
             if (!horizontal) pos[base] = v3(x, startY, 0) + offset;
             prev[base] = pos[base];
             uv[base] = v3(x, 0, 0);
+            if (base >= divY)
+            {
+                add_link(base - divY, base, stretch);
+                add_link(base - divY + 1, base, shear);
+                if (base >= 2 * divY && !dihedral) add_link(base - 2 * divY, base, bendStiff);
+            }
             for (int i = 1; i < divY; i++)
             {
                 int idx = base + i;
@@ -791,6 +812,15 @@ struct Cloth
                 else pos[idx] = v3(x, startY + inc * i, 0) + offset; /* incline unsupported */
                 prev[idx] = pos[idx];
                 uv[idx] = v3(x, inc * i, 0);
+                add_link(idx - 1, idx, stretch);
+                if (idx > base + 1 && !dihedral) add_link(idx - 2, idx, bendStiff);
+                if (idx >= divY)
+                {
+                    add_link(idx - divY, idx, stretch);
+                    if (i < divY - 1) add_link(idx - divY + 1, idx, shear);
+                    if (j > 1 && !dihedral) add_link(idx - 2 * divY, idx, bendStiff);
+                }
+                if (idx > divY) add_link(idx - divY - 1, idx, shear);
                 if (idx > base && idx > divY)
                 {
                     u32 a = idx - divY - 1, b = idx - divY, c = idx, d = idx - 1;
@@ -1159,6 +1189,27 @@ struct Cloth
     }
 
     /* ---- solver ---- */
+    /* SolveLinks (Physics/ClothPBD.cpp:9-50) for one link; returns |s err| or -1 */
+    float solve_link(const Link& link, float k, float omega)
+    {
+        const float w1 = invMass[link.i1], w2 = invMass[link.i2];
+        if (w1 + w2 == 0) return -1;
+        const float mu = 1.f / (w1 + w2);
+        V3 delta = pos[link.i1] - pos[link.i2];
+        const float len0 = link.len;
+        const float l = len(delta);
+        if (l == 0 || std::isnan(l) || std::isinf(l)) return -1;
+        const float err = l - len0;
+        delta = (1 / l) * delta;
+        const float epsilon = len0 / (k * link.stiffness);
+        const float s = 1.f / (1.f + mu * epsilon);
+        const float lambda = err * mu * s;
+        const V3 fc = omega * lambda * delta;
+        pos[link.i1] = pos[link.i1] - w1 * fc;
+        pos[link.i2] = pos[link.i2] + w2 * fc;
+        return std::fabs(s * err);
+    }
+
     /* SolveTriangles (Physics/ClothPBD.cpp:52-108) for one triangle */
     void solve_triangle(const Tri& tri, float h2, float epsUV)
     {
@@ -1523,6 +1574,8 @@ struct Cloth
         const float invH = 1.f / h;
         std::vector<int> tOrd = triOrder.size() == tris.size() ? triOrder : seq(tris.size());
         std::vector<int> bOrd = bendOrder.size() == bends.size() ? bendOrder : seq(bends.size());
+        std::vector<int> lOrd = linkOrder.size() == links.size() ? linkOrder : seq(links.size());
+        const float kLink = h2 * area * unit;
         auto v3of = [](const SContact& c, u32* v) { v[0] = c.i1; v[1] = c.i2; v[2] = c.i3; v[3] = c.i4; return 4; };
         auto v3t = [](const TContact& c, u32* v) { v[0] = c.i1; v[1] = c.i2; v[2] = c.i3; return 3; };
         auto v2e = [](const EContact& c, u32* v) { v[0] = c.i1; v[1] = c.i2; return 2; };
@@ -1536,6 +1589,11 @@ struct Cloth
         {
             if (fem)
                 for (int t : tOrd) solve_triangle(tris[t], h2, epsUV);
+            else
+            {
+                cl = 0;
+                for (int li : lOrd) { float e = solve_link(links[li], kLink, 1.f); if (e > cl) cl = e; }
+            }
             if (dihedral && k % bendFreq == 0)
             {
                 cb = 0;
@@ -1985,6 +2043,24 @@ void orc_set_bend_order(void* h, const int* o, int n)
 }
 
 void orc_set_contact_order(void* h, int mode) { ((Cloth*)h)->contactOrder = mode; }
+
+void orc_set_link_order(void* h, const int* o, int n)
+{
+    Cloth* c = (Cloth*)h;
+    if (!o) c->linkOrder.clear(); else c->linkOrder.assign(o, o + n);
+}
+
+int orc_num_links(void* h) { return (int)((Cloth*)h)->links.size(); }
+
+void orc_get_links(void* h, unsigned* idx2, float* lenStiff)
+{
+    Cloth* c = (Cloth*)h;
+    for (size_t k = 0; k < c->links.size(); k++)
+    {
+        if (idx2) { idx2[2 * k] = c->links[k].i1; idx2[2 * k + 1] = c->links[k].i2; }
+        if (lenStiff) { lenStiff[2 * k] = c->links[k].len; lenStiff[2 * k + 1] = c->links[k].stiffness; }
+    }
+}
 
 /* 0: libm acosf as the reference; 1: the library's portable arc cosine (check mode).
    Process-wide, since the initial normals are computed when a grid is built. */

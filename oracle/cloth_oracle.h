@@ -42,6 +42,9 @@ void orc_set_bend_order(void* h, const int* order, int n);
 /* Check mode for multi-vertex contacts: 0 = list order (reference), 1 = the
    GPU's deterministic independent-set colouring order (colour, then list index). */
 void orc_set_contact_order(void* h, int mode);
+void orc_set_link_order(void* h, const int* order, int n);
+int orc_num_links(void* h);
+void orc_get_links(void* h, unsigned* idx2, float* lenStiff);
 void orc_set_portable_math(int on);
 float orc_portable_acos(float x);
 void orc_step(void* h, float dt);

@@ -345,7 +345,7 @@ class ClothModel:
         lib().scSetClusterStaging(self.h, bool(on))
 
     def constraint_order(self, kind):
-        n = lib().scGetNumTris(self.h) if kind == 0 else lib().scGetNumBends(self.h)
+        n = (lib().scGetNumTris(self.h), lib().scGetNumBends(self.h), lib().scGetNumLinks(self.h))[kind]
         order = np.zeros(n, np.int32)
         start = np.zeros(70, np.int32)
         nc = lib().scGetConstraintOrder(self.h, kind, order.ctypes.data_as(_i), start.ctypes.data_as(_i))

@@ -603,8 +603,9 @@ int scGetSolverIterations(scModel m)
 int scGetConstraintOrder(scModel m, int kind, int* order, int* colourStart)
 {
     if (!M(m)) return 0;
-    const std::vector<int>& o = kind == 0 ? M(m)->triOrder : M(m)->bendOrder;
-    const std::vector<int>& s = kind == 0 ? M(m)->triColourStart : M(m)->bendColourStart;
+    const std::vector<int>& o = kind == 0 ? M(m)->triOrder : kind == 1 ? M(m)->bendOrder : M(m)->linkOrder;
+    const std::vector<int>& s = kind == 0 ? M(m)->triColourStart : kind == 1 ? M(m)->bendColourStart : M(m)->linkColourStart;
+    if (s.empty()) return 0;
     if (order) memcpy(order, o.data(), sizeof(int) * o.size());
     if (colourStart) memcpy(colourStart, s.data(), sizeof(int) * s.size());
     return (int)s.size() - 1;

@@ -462,6 +462,7 @@ SolverParams ClothModel::solver_params(float h) const
     P.iterations = prm.iterations; P.flags = prm.flags; P.fem = prm.fem; P.dihedral = prm.dihedral;
     P.fixedIterations = prm.fixedIterations; P.bendFreq = prm.bendFreq;
     P.resTol = prm.resTol;
+    P.area = prm.area;
     P.resScale = resScale;
     P.selfThreshold = prm.selfThreshold;
     return P;
@@ -503,6 +504,8 @@ void ClothModel::colour_constraints()
                      triOrder, triColourStart);
     greedy_colour<4>((int)bends.size(), N, [&](int i, uint32_t* v) { v[0] = bends[i].x; v[1] = bends[i].y; v[2] = bends[i].z; v[3] = bends[i].w; },
                      bendOrder, bendColourStart);
+    greedy_colour<2>((int)links.size(), N, [&](int i, uint32_t* v) { v[0] = links[i].x; v[1] = links[i].y; },
+                     linkOrder, linkColourStart);
 }
 
 bool ClothModel::upload_topology(const HMesh& mesh)
@@ -528,6 +531,18 @@ bool ClothModel::upload_topology(const HMesh& mesh)
     float4* dfem = (float4*)dalloc(sizeof(float4) * 3 * (size_t)T);
     SC_CUDA(cudaMemcpy(dfem, fem.data(), sizeof(float4) * 3 * (size_t)T, cudaMemcpyHostToDevice));
     dc.fem = dfem;
+    // link records in colour order (mass-spring path)
+    const int L = (int)links.size();
+    std::vector<float4> lk(std::max(1, L));
+    for (int k = 0; k < L; k++)
+    {
+        const int li = linkOrder[k];
+        lk[k] = make_float4(bits_f(links[li].x), bits_f(links[li].y), linkRest[li].x, linkRest[li].y);
+    }
+    float4* dlink = (float4*)dalloc(sizeof(float4) * lk.size());
+    SC_CUDA(cudaMemcpy(dlink, lk.data(), sizeof(float4) * lk.size(), cudaMemcpyHostToDevice));
+    dc.link = dlink;
+    dc.L = L;
     std::vector<uint4> bd(B);
     for (int k = 0; k < B; k++) bd[k] = bends[bendOrder[k]];
     uint4* dbend = (uint4*)dalloc(sizeof(uint4) * B);
@@ -1000,14 +1015,18 @@ bool ClothPatch::init_grid(int divX, int divY, float inc, V3 offset, bool horizo
     m.N = N;
     m.hpos.assign(N, mk(0, 0, 0)); m.hprev.assign(N, mk(0, 0, 0)); m.hvel.assign(N, mk(0, 0, 0));
     m.invMass.assign(N, 1.f); m.uvx.assign(N, 0.f); m.uvy.assign(N, 0.f);
-    m.tris.clear(); m.bends.clear(); m.links.clear(); m.quads.clear();
+    m.tris.clear(); m.bends.clear(); m.links.clear(); m.linkRest.clear(); m.quads.clear();
     mesh = HMesh();
     isQuadMesh = true;
     const bool dihedral = m.prm.dihedral;
-    auto addLink = [&](uint32_t a, uint32_t b) {
-        // ClothModel::AddLink (Physics/ClothModel.inl:12-31): skipped when both pinned
+    const float stretch = m.prm.stretch, shear = m.prm.shear, bend = m.prm.bend;
+    auto addLink = [&](uint32_t a, uint32_t b, float stiff) {
+        // ClothModel::AddLink (Physics/ClothModel.inl:12-31): skipped when both
+        // ends are pinned or the stiffness is zero; rest length from the positions
         if (m.invMass[a] == 0 && m.invMass[b] == 0) return;
+        if (stiff == 0) return;
         m.links.push_back(make_uint2(a, b));
+        m.linkRest.push_back(make_float2(len(m.hpos[a] - m.hpos[b]), stiff));
     };
     float x = -0.5f * divX * inc;
     const float startY = x;
@@ -1018,9 +1037,9 @@ bool ClothPatch::init_grid(int divX, int divY, float inc, V3 offset, bool horizo
         m.uvx[base] = x; m.uvy[base] = 0;
         if (base >= divY)
         {
-            addLink(base - divY, base);
-            addLink(base - divY + 1, base);
-            if (base >= 2 * divY && !dihedral) addLink(base - 2 * divY, base);
+            addLink(base - divY, base, stretch);
+            addLink(base - divY + 1, base, shear);
+            if (base >= 2 * divY && !dihedral) addLink(base - 2 * divY, base, bend);
         }
         for (int i = 1; i < divY; i++)
         {
@@ -1028,17 +1047,17 @@ bool ClothPatch::init_grid(int divX, int divY, float inc, V3 offset, bool horizo
             m.hpos[idx] = horizontal ? mk(x, 0, startY + inc * i) + offset : mk(x, startY + inc * i, 0) + offset;
             m.hprev[idx] = m.hpos[idx];
             m.uvx[idx] = x; m.uvy[idx] = inc * i;
-            addLink(idx - 1, idx);
-            if (idx > base + 1 && !dihedral) addLink(idx - 2, idx);
+            addLink(idx - 1, idx, stretch);
+            if (idx > base + 1 && !dihedral) addLink(idx - 2, idx, bend);
             if (idx >= divY)
             {
-                addLink(idx - divY, idx);
-                if (i < divY - 1) addLink(idx - divY + 1, idx);
-                if (j > 1 && !dihedral) addLink(idx - 2 * divY, idx);
+                addLink(idx - divY, idx, stretch);
+                if (i < divY - 1) addLink(idx - divY + 1, idx, shear);
+                if (j > 1 && !dihedral) addLink(idx - 2 * divY, idx, bend);
             }
             if (idx > divY)
             {
-                addLink(idx - divY - 1, idx);
+                addLink(idx - divY - 1, idx, shear);
                 const uint32_t a = idx - divY - 1, b = idx - divY, c = idx, d = idx - 1;
                 m.quads.push_back(make_uint4(a, b, c, d));
                 uint32_t t[6];
@@ -1113,7 +1132,7 @@ bool ClothPatch::init_batch(const std::vector<ClothPatch*>& parts)
     numSteps = parts[0]->numSteps;
     m.N = 0;
     m.hpos.clear(); m.hprev.clear(); m.hvel.clear(); m.invMass.clear(); m.uvx.clear(); m.uvy.clear();
-    m.tris.clear(); m.bends.clear(); m.links.clear(); m.quads.clear();
+    m.tris.clear(); m.bends.clear(); m.links.clear(); m.linkRest.clear(); m.quads.clear();
     m.instV = {0}; m.instT = {0}; m.instE = {0}; m.instB = {0};
     m.batchColl.clear();
     mesh = HMesh();
@@ -1131,6 +1150,7 @@ bool ClothPatch::init_batch(const std::vector<ClothPatch*>& parts)
         for (FemHost t : q.tris) { t.i1 += vo; t.i2 += vo; t.i3 += vo; m.tris.push_back(t); }
         for (uint4 b : q.bends) m.bends.push_back(make_uint4(b.x + vo, b.y + vo, b.z + vo, b.w + vo));
         for (uint2 l : q.links) m.links.push_back(make_uint2(l.x + vo, l.y + vo));
+        m.linkRest.insert(m.linkRest.end(), q.linkRest.begin(), q.linkRest.end());
         for (uint4 d : q.quads) m.quads.push_back(make_uint4(d.x + vo, d.y + vo, d.z + vo, d.w + vo));
         mesh.verts.insert(mesh.verts.end(), qm.verts.begin(), qm.verts.end());
         mesh.normals.insert(mesh.normals.end(), qm.normals.begin(), qm.normals.end());
@@ -1247,7 +1267,7 @@ bool ClothPatch::record_solve(cudaStream_t s, const SolverParams& P, const Solve
     // the reference's loop tests its exit conditions after the body, so it always
     // runs at least one iteration (Physics/ClothPBD.cpp:335-362)
     const int iterations = m.prm.iterations > 1 ? m.prm.iterations : 1;
-    const bool planFits = m.triColourStart.size() <= 65 && m.bendColourStart.size() <= 65;
+    const bool planFits = m.triColourStart.size() <= 65 && m.bendColourStart.size() <= 65 && m.linkColourStart.size() <= 65;
     GsPlan plan = {};
     plan.iterations = iterations;
     plan.nFemCol = (int)m.triColourStart.size() - 1;
@@ -1256,6 +1276,8 @@ bool ClothPatch::record_solve(cudaStream_t s, const SolverParams& P, const Solve
     {
         for (size_t k = 0; k < m.triColourStart.size(); k++) plan.femStart[k] = m.triColourStart[k];
         for (size_t k = 0; k < m.bendColourStart.size(); k++) plan.bendStart[k] = m.bendColourStart[k];
+        plan.nLinkCol = (int)m.linkColourStart.size() - 1;
+        for (size_t k = 0; k < m.linkColourStart.size(); k++) plan.linkStart[k] = m.linkColourStart[k];
     }
     int shift = 0;
     size_t smem = 0;
@@ -1297,6 +1319,12 @@ bool ClothPatch::record_solve(cudaStream_t s, const SolverParams& P, const Solve
         if (m.prm.fem)
             for (size_t col = 0; col + 1 < m.triColourStart.size(); col++)
                 launch_fem(s, c, P, m.triColourStart[col], m.triColourStart[col + 1] - m.triColourStart[col]);
+        else
+        {
+            launch_reset_link_error(s, c);
+            for (size_t col = 0; col + 1 < m.linkColourStart.size(); col++)
+                launch_links(s, c, P, m.linkColourStart[col], m.linkColourStart[col + 1] - m.linkColourStart[col]);
+        }
         if (m.prm.dihedral && k % m.prm.bendFreq == 0)
             for (size_t col = 0; col + 1 < m.bendColourStart.size(); col++)
                 launch_bends(s, c, P, m.bendColourStart[col], m.bendColourStart[col + 1] - m.bendColourStart[col], col == 0);
@@ -1341,7 +1369,7 @@ bool ClothPatch::autotune(float h)
     }
     std::vector<SolverChoice> cand;
     int shift = 0; size_t smem = 0;
-    const bool fits = m.triColourStart.size() <= 65 && m.bendColourStart.size() <= 65;
+    const bool fits = m.triColourStart.size() <= 65 && m.bendColourStart.size() <= 65 && m.linkColourStart.size() <= 65;
     if (fits && m.solverMode != SOLVE_GRID && gs_cluster_size(m.N, shift, smem) > 0) cand.push_back({SOLVE_CLUSTER, 0, 0, 0.f});
     if (fits && m.solverMode != SOLVE_CLUSTER)
         for (int v = 0; v < gs_grid_variants(); v++)
@@ -1499,11 +1527,6 @@ bool ClothPatch::step(float dt)
 {
     ClothModel& m = model;
     if (m.N == 0) { set_error(SC_ERR_STATE, "cloth not initialised"); return false; }
-    if (!m.prm.fem && m.prm.iterations > 0)
-    {
-        set_error(SC_ERR_UNSUPPORTED, "mass-spring (links) solver is not implemented on the GPU; enable FEM");
-        return false;
-    }
     if (!m.ensure_buffers(world, stream)) return false;
     const int n = numSteps;
     const float h = dt / n;

@@ -136,6 +136,8 @@ public:
     std::vector<FemHost> tris;
     std::vector<uint4> bends;
     std::vector<uint2> links;
+    std::vector<float2> linkRest;              // rest length, stiffness (ClothModel::AddLink)
+    std::vector<int> linkOrder, linkColourStart;
     std::vector<uint4> quads;
     std::vector<int> triOrder, bendOrder;      // colour order
     std::vector<int> triColourStart, bendColourStart;

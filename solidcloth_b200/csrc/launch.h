@@ -74,6 +74,8 @@ struct Buffers
 void launch_predict(cudaStream_t s, const DevCloth& c, const SolverParams& P);
 void launch_velocity(cudaStream_t s, const DevCloth& c, const SolverParams& P);
 void launch_fem(cudaStream_t s, const DevCloth& c, const SolverParams& P, int first, int count);
+void launch_links(cudaStream_t s, const DevCloth& c, const SolverParams& P, int first, int count);
+void launch_reset_link_error(cudaStream_t s, const DevCloth& c);
 void launch_bends(cudaStream_t s, const DevCloth& c, const SolverParams& P, int first, int count, int resetErr);
 void launch_normals(cudaStream_t s, const DevCloth& c, bool prevMesh, const float4* verts);
 void launch_vertex_colliders(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b, const VColl* hostColl);
@@ -111,6 +113,8 @@ struct GsPlan
     int femStage, bendStage; // records per CTA when staged (max over the cluster's CTAs)
     int femStart[65];
     int bendStart[65];
+    int nLinkCol;            // mass-spring path (FEM off): link colours
+    int linkStart[65];
 };
 // cluster size usable for N particles (0: too large or unsupported); sets the
 // log2 particles-per-CTA and the dynamic shared memory per CTA

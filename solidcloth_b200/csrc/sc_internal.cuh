@@ -35,6 +35,7 @@ struct SolverParams
     float h, h2, invH, epsUV;
     int iterations, flags, fem, dihedral, fixedIterations, bendFreq;
     float selfThreshold;
+    float area;              // ClothModel::mArea (link compliance: k = h^2 area unit)
     float resTol;            // > 0: iterate until the update residual <= resTol
     float resScale;          // 1 / mean rest edge length (the update residual's unit)
 };
@@ -47,6 +48,8 @@ struct DevCloth
     float4* prev;
     float4* vel;
     const float4* fem;          // 3*T, colour order
+    const float4* link;         // L, colour order: i1, i2 (bits), rest length, stiffness
+    int L;
     const uint4* bend;          // B, colour order
     const uint32_t* tri;        // 3*T original (mesh) order
     const uint32_t* triE;       // 3*T triangle -> edge ids (Mesh::Triangle::e)

@@ -132,6 +132,42 @@ __device__ __forceinline__ void fem_project(const PA& pa, float4 r0, float4 r1, 
     pa.st(i3, make_float4(x3.x, x3.y, x3.z, w3));
 }
 
+// SolveLinks (Physics/ClothPBD.cpp:9-50), omega = 1, for one link record
+// {i1, i2 (bits), rest length, stiffness}; returns |s err| or -1 when skipped
+template <class PA>
+__device__ __forceinline__ float link_project(const PA& pa, float4 rec, const SolverParams& P)
+{
+    const uint32_t i1 = __float_as_uint(rec.x), i2 = __float_as_uint(rec.y);
+    float4 a = pa.ld(i1), b = pa.ld(i2);
+    const float w1 = a.w, w2 = b.w;
+    if (w1 + w2 == 0) return -1.f;
+    const float mu = 1.f / (w1 + w2);
+    V3 delta = mk(a.x, a.y, a.z) - mk(b.x, b.y, b.z);
+    const float len0 = rec.z;
+    const float l = len(delta);
+    if (l == 0 || isnan(l) || isinf(l)) return -1.f;
+    const float err = l - len0;
+    delta = (1 / l) * delta;
+    const float k = P.h2 * P.area * P.unit;
+    const float epsilon = len0 / (k * rec.w);
+    const float s = 1.f / (1.f + mu * epsilon);
+    const float lambda = err * mu * s;
+    const float omega = 1.f;
+    const V3 fc = omega * lambda * delta;
+    const V3 x1 = mk(a.x, a.y, a.z) - w1 * fc, x2 = mk(b.x, b.y, b.z) + w2 * fc;
+    pa.st(i1, make_float4(x1.x, x1.y, x1.z, w1));
+    pa.st(i2, make_float4(x2.x, x2.y, x2.z, w2));
+    return fabsf(s * err);
+}
+
+__global__ void __launch_bounds__(256) k_links(DevCloth c, SolverParams P, int first, int count)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count || gs_done(c)) return;
+    const float e = link_project(GlobalPos{c.pos}, c.link[first + k], P);
+    if (!P.fixedIterations && e > 0.f) atomic_max_pos(&c.scal[1], e);
+}
+
 __global__ void __launch_bounds__(256) k_fem(DevCloth c, SolverParams P, int first, int count)
 {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1171,7 +1207,8 @@ __global__ void k_gs_exit(DevCloth c, SolverParams P, int iter)
     if (P.fixedIterations) return;
     const float eps = 0.01f;
     float cb = c.scal[2], cv = c.scal[3], ce = c.scal[4], ct = c.scal[5], sct = c.scal[6], see = c.scal[7];
-    if (0.f < 0.05f && cb < 0.005f && see < P.selfThreshold && sct < P.selfThreshold && cv < eps && ce < eps && ct < eps)
+    const float cl = P.fem ? 0.f : c.scal[1];
+    if (cl < 0.05f && cb < 0.005f && see < P.selfThreshold && sct < P.selfThreshold && cv < eps && ce < eps && ct < eps)
         c.scal[8] = 1.f;
 }
 
@@ -1196,6 +1233,12 @@ __global__ void k_reset_iter_errors(DevCloth c)
     // cv is a per-iteration maximum written with atomics; cb persists between
     // bend iterations (it is only recomputed when bends run)
     if (threadIdx.x == 0) c.scal[3] = 0.f;
+}
+
+// cl (the links' error) is a per-iteration maximum: cleared before the link sweep
+__global__ void k_reset_link_error(DevCloth c)
+{
+    if (threadIdx.x == 0 && !gs_done(c)) c.scal[1] = 0.f;
 }
 
 __global__ void k_reset_bend_error(DevCloth c)
@@ -2212,6 +2255,18 @@ __global__ void __launch_bounds__(GS_THREADS) k_gs_cluster(DevCloth c, SolverPar
                 }
                 cl.sync();
             }
+        else
+            for (int col = 0; col < plan.nLinkCol; col++)
+            {
+                int a, e;
+                range(plan.linkStart[col], plan.linkStart[col + 1], a, e);
+                for (int j = a + threadIdx.x; j < e; j += blockDim.x)
+                {
+                    const float err = link_project(pa, c.link[j], P);
+                    if (track && err > 0.f) atomicMax((int*)&sErr[1], __float_as_int(err));
+                }
+                cl.sync();
+            }
         if (P.dihedral && k % P.bendFreq == 0)
             for (int col = 0; col < plan.nBendCol; col++)
             {
@@ -2296,15 +2351,17 @@ __global__ void __launch_bounds__(GS_THREADS) k_gs_cluster(DevCloth c, SolverPar
         if (track)
         {
             // SolveGS exit test (Physics/ClothPBD.cpp:354-361) on cluster-wide maxima
-            if (threadIdx.x < 8 && threadIdx.x >= 2 && sErr[threadIdx.x] > 0.f)
+            if (threadIdx.x < 8 && threadIdx.x >= 1 && sErr[threadIdx.x] > 0.f)
                 atomic_max_pos(&c.scal[threadIdx.x], sErr[threadIdx.x]);
             cl.sync();
             if (rank == 0 && threadIdx.x == 0)
             {
                 const float eps = 0.01f;
                 float cb = c.scal[2], cv = c.scal[3], ce = c.scal[4], ct = c.scal[5], sct = c.scal[6], see = c.scal[7];
-                if (cb < 0.005f && see < P.selfThreshold && sct < P.selfThreshold && cv < eps && ce < eps && ct < eps)
+                const float clk = P.fem ? 0.f : c.scal[1];
+                if (clk < 0.05f && cb < 0.005f && see < P.selfThreshold && sct < P.selfThreshold && cv < eps && ce < eps && ct < eps)
                     c.scal[8] = 1.f;
+                c.scal[1] = 0.f;
                 for (int s = 3; s < 8; s++) c.scal[s] = 0.f;          // per-iteration maxima
                 if ((k + 1) % P.bendFreq == 0) c.scal[2] = 0.f;       // recomputed by the next bend sweep
             }
@@ -2450,6 +2507,16 @@ __global__ void __launch_bounds__(NT) k_gs_grid(DevCloth c, SolverParams P, Buff
                 fem_tiles<FT>(c, P, plan.femStart[col], plan.femStart[col + 1], tid, nth);
                 grid.sync();
             }
+        else
+            for (int col = 0; col < plan.nLinkCol; col++)
+            {
+                for (int j = plan.linkStart[col] + tid; j < plan.linkStart[col + 1]; j += nth)
+                {
+                    const float err = link_project(pa, c.link[j], P);
+                    if (track && err > 0.f) atomicMax((int*)&sErr[1], __float_as_int(err));
+                }
+                grid.sync();
+            }
         if (P.dihedral && k % P.bendFreq == 0)
             for (int col = 0; col < plan.nBendCol; col++)
             {
@@ -2521,15 +2588,17 @@ __global__ void __launch_bounds__(NT) k_gs_grid(DevCloth c, SolverParams P, Buff
         {
             // SolveGS exit test (Physics/ClothPBD.cpp:354-361) on grid-wide maxima
             __syncthreads();
-            if (threadIdx.x < 8 && threadIdx.x >= 2 && sErr[threadIdx.x] > 0.f)
+            if (threadIdx.x < 8 && threadIdx.x >= 1 && sErr[threadIdx.x] > 0.f)
                 atomic_max_pos(&c.scal[threadIdx.x], sErr[threadIdx.x]);
             grid.sync();
             if (tid == 0)
             {
                 const float eps = 0.01f;
                 float cb = c.scal[2], cv = c.scal[3], ce = c.scal[4], ct = c.scal[5], sct = c.scal[6], see = c.scal[7];
-                if (cb < 0.005f && see < P.selfThreshold && sct < P.selfThreshold && cv < eps && ce < eps && ct < eps)
+                const float clk = P.fem ? 0.f : c.scal[1];
+                if (clk < 0.05f && cb < 0.005f && see < P.selfThreshold && sct < P.selfThreshold && cv < eps && ce < eps && ct < eps)
                     c.scal[8] = 1.f;
+                c.scal[1] = 0.f;
                 for (int s2 = 3; s2 < 8; s2++) c.scal[s2] = 0.f;
                 if ((k + 1) % P.bendFreq == 0) c.scal[2] = 0.f;
             }
@@ -2660,6 +2729,16 @@ void launch_predict(cudaStream_t s, const DevCloth& c, const SolverParams& P)
 void launch_velocity(cudaStream_t s, const DevCloth& c, const SolverParams& P)
 {
     k_velocity<<<blocks_for(c.N), 256, 0, s>>>(c, P);
+}
+
+void launch_reset_link_error(cudaStream_t s, const DevCloth& c)
+{
+    k_reset_link_error<<<1, 32, 0, s>>>(c);
+}
+
+void launch_links(cudaStream_t s, const DevCloth& c, const SolverParams& P, int first, int count)
+{
+    if (count > 0) k_links<<<blocks_for(count), 256, 0, s>>>(c, P, first, count);
 }
 
 void launch_fem(cudaStream_t s, const DevCloth& c, const SolverParams& P, int first, int count)

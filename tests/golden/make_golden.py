@@ -109,12 +109,39 @@ def case_mesh():
     return out
 
 
-CASES = {"cfg0": case_cfg0, "sdf": case_sdf, "self": case_self, "ccd": case_ccd, "mesh": case_mesh}
+def links_scene(dihedral):
+    """the mass-spring path (FEM off): stretch, shear and, without dihedral
+    bending, bend links (ClothPatch::Init, Physics/ClothPatch.cpp:170-207)"""
+    sc = scenes.cfg0()
+    sc.params.fem = False
+    sc.params.dihedral = dihedral
+    sc.params.stretch, sc.params.shear, sc.params.bend = 1e3, 5e2, 2.0
+    return sc
+
+
+def case_links():
+    out = {}
+    for dih in (False, True):
+        sc = links_scene(dih)
+        r = RefCloth.from_scene(sc)
+        for f in range(8):
+            r.step(sc.dt)
+        pos, prev, vel, _ = r.state()
+        out[f"pos_dihedral{int(dih)}"] = pos
+        out[f"vel_dihedral{int(dih)}"] = vel
+    return out
+
+
+CASES = {"cfg0": case_cfg0, "sdf": case_sdf, "self": case_self, "ccd": case_ccd, "mesh": case_mesh,
+         "links": case_links}
 
 
 if __name__ == "__main__":
     RefCloth.set_threads(1)
+    only = set(sys.argv[1:])
     for name, fn in CASES.items():
+        if only and name not in only:
+            continue
         d = fn()
         np.savez_compressed(HERE / f"{name}.npz", **d)
         print(name, {k: v.shape for k, v in d.items()})

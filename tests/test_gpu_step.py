@@ -29,6 +29,8 @@ def _pair(sc, ccd=False, state=None):
         o.set_state(*state)
     o.set_tri_order(p.model.constraint_order(0)[0])
     o.set_bend_order(p.model.constraint_order(1)[0])
+    if not sc.params.fem:
+        o.set_link_order(p.model.constraint_order(2)[0])
     o.set_contact_order(1)
     return w, p, o
 
@@ -210,7 +212,33 @@ def test_ccd_broadphase_and_hits_bitexact(thickness, walk):
     assert p.status() & ~16 == 0
 
 
-@pytest.mark.parametrize("scene", ["cfg0", "sdf", "fold", "ccd"])
+def _links_scene(dihedral=False):
+    sc = scenes.cfg0()
+    sc.params.fem = False
+    sc.params.dihedral = dihedral
+    sc.params.stretch, sc.params.shear, sc.params.bend = 1e3, 5e2, 2.0
+    return sc
+
+
+@pytest.mark.parametrize("dihedral", [False, True])
+@pytest.mark.parametrize("fixed", [True, False])
+def test_mass_spring_check_mode(dihedral, fixed):
+    """The mass-spring path (FEM off: SolveLinks, Physics/ClothPBD.cpp:9-50, with
+    the reference's stretch / shear / bend links) equals the oracle run in the
+    GPU's link colour order, bit for bit, with fixed iterations and with the
+    reference's exit test."""
+    sc = _links_scene(dihedral)
+    sc.params.fixed_iterations = fixed
+    w, p, o = _pair(sc)
+    assert p.model.constraint_order(2)[0].size == o.links()[0].shape[0]
+    for f in range(10):
+        p.step(sc.dt)
+        o.step(sc.dt)
+        assert _same(p.model.positions(), o.positions()), (f, float(np.abs(p.model.positions() - o.positions()).max()))
+    assert p.status() == 0
+
+
+@pytest.mark.parametrize("scene", ["cfg0", "sdf", "fold", "ccd", "links"])
 def test_solvers_are_bit_identical(scene):
     """The cluster-resident solver (one launch per substep, particles in
     distributed shared memory, records staged in shared memory or read from
@@ -224,6 +252,8 @@ def test_solvers_are_bit_identical(scene):
     elif scene == "sdf":
         sc = _sdf_scene()
         sc.params.substeps = 4
+    elif scene == "links":
+        sc = _links_scene(False)
     elif scene == "fold":
         sc = scenes.cfg1(n=16, self_mode="proximity")
         sc.sdfs.clear()

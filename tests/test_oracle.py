@@ -269,3 +269,39 @@ def test_sphere_sdf_samples():
     g = scenes.sphere_sdf((0, 0, 0), 0.3, 63, 0.1)
     assert g.values.size == 64 ** 3
     assert abs(g.values.min() + 0.3) < 0.02
+
+
+# ------------------------------------------------------- mass-spring path
+def test_golden_links():
+    """The mass-spring path (FEM off; SolveLinks, Physics/ClothPBD.cpp:9-50) of the
+    oracle against fixtures from the reference build, with and without dihedral
+    bending (without it, ClothPatch::Init adds bend links)."""
+    P = port()
+    P.set_portable_math(False)
+    g = np.load(GOLD / "links.npz")
+    mg = golden_module()
+    for dih in (False, True):
+        sc = mg.links_scene(dih)
+        o = P.from_scene(sc)
+        for _ in range(8):
+            o.step(sc.dt)
+        pos, prev, vel, _ = o.state()
+        assert np.array_equal(bits(pos), bits(g[f"pos_dihedral{int(dih)}"])), dih
+        assert np.array_equal(bits(vel), bits(g[f"vel_dihedral{int(dih)}"])), dih
+
+
+@pytest.mark.parametrize("fixed", [True, False])
+def test_port_matches_reference_links(fixed, ref_threads):
+    """Live: links path bit-exact, in fixed-iteration mode and with the
+    reference's exit test (links error below 0.05, Physics/ClothPBD.cpp:357)."""
+    R, P = ref(), port()
+    P.set_portable_math(False)
+    mg = golden_module()
+    for dih in (False, True):
+        sc = mg.links_scene(dih)
+        sc.params.fixed_iterations = fixed
+        r, o = R.from_scene(sc), P.from_scene(sc)
+        for _ in range(6):
+            r.step(sc.dt)
+            o.step(sc.dt)
+        assert np.array_equal(bits(r.positions()), bits(o.positions())), dih
