@@ -369,11 +369,17 @@ constexpr int MESH_STACK = 48;
 
 struct PointHit { float dist; int tri; V3 cp, bary, normal; int region; };
 
-__device__ PointHit mesh_point_query(const DevMesh& m, V3 p, int* status)
+// The three nearest-feature searches take `bound`, the contact threshold of
+// their caller: a result at or beyond it is discarded there, and starting the
+// search's best distance at the bound prunes exactly the subtrees that could
+// only produce such results — every node nearer than the bound is visited in the
+// same order as by the unbounded search, so results below the bound (and ties
+// among them) are unchanged.
+__device__ PointHit mesh_point_query(const DevMesh& m, V3 p, int* status, float bound)
 {
     PointHit r; r.dist = FLT_MAX; r.tri = -1; r.region = -1;
     r.cp = r.bary = r.normal = mk(0.f, 0.f, 0.f);
-    float minDist = FLT_MAX;
+    float minDist = bound;
     int stNode[MESH_STACK]; float stDist[MESH_STACK];
     int sp = 0;
     int node = 0;
@@ -427,11 +433,11 @@ __device__ PointHit mesh_point_query(const DevMesh& m, V3 p, int* status)
 
 struct VtxHit { float dist; int vertex; V3 cpMesh, cpTri, bary, normal; int region; };
 
-__device__ VtxHit mesh_triangle_query(const DevMesh& m, V3 a, V3 b, V3 cc, int* status)
+__device__ VtxHit mesh_triangle_query(const DevMesh& m, V3 a, V3 b, V3 cc, int* status, float bound)
 {
     VtxHit r; r.dist = -FLT_MAX; r.vertex = -1; r.region = 0;
     r.cpMesh = r.cpTri = r.bary = r.normal = mk(0.f, 0.f, 0.f);
-    float minDist = FLT_MAX;
+    float minDist = bound;
     Box tb = Box::empty(); tb.add(a); tb.add(b); tb.add(cc);
     int stNode[MESH_STACK]; float stDist[MESH_STACK];
     int sp = 0, node = 0;
@@ -490,12 +496,12 @@ __device__ __forceinline__ V3 mesh_edge_normal(const DevMesh& m, int e, float pa
     return n;
 }
 
-__device__ SegHit mesh_segment_query(const DevMesh& m, V3 p, V3 q, int* status)
+__device__ SegHit mesh_segment_query(const DevMesh& m, V3 p, V3 q, int* status, float bound)
 {
     SegHit r; r.dist = -FLT_MAX; r.edge = -1; r.region = -1;
     r.cpMesh = r.cpSegm = r.normal = mk(0.f, 0.f, 0.f);
     r.cs0 = r.cs1 = r.cm0 = r.cm1 = 0.f;
-    float minDist = FLT_MAX;
+    float minDist = bound;
     Box eb = Box::empty(); eb.add(p); eb.add(q);
     int stNode[MESH_STACK]; float stDist[MESH_STACK];
     int sp = 0, node = 0;
@@ -597,7 +603,7 @@ __global__ void k_vertex_colliders(DevCloth c, SolverParams P, Buffers b)
         {
             if (P.flags & CF_VERTICES)
             {
-                PointHit h = mesh_point_query(b.meshes[g.mesh], prev, c.status);
+                PointHit h = mesh_point_query(b.meshes[g.mesh], prev, c.status, radTolMesh);
                 if (h.dist < radTolMesh && h.dist >= 0) add(h.cp, h.normal, h.tri, g.mesh);
             }
         }
@@ -663,8 +669,8 @@ __global__ void k_tri_colliders(DevCloth c, SolverParams P, Buffers b, VColl g, 
     if (g.type == 4)
     {
         // MeshCollisions: per-triangle threshold with 1.2 x travel (ClothCollision.cpp:137-160)
-        VtxHit h = mesh_triangle_query(b.meshes[g.mesh], a, bb, cc, c.status);
         float rt = P.thickness + mx(P.tolerance, tvm * 1.2f);
+        VtxHit h = mesh_triangle_query(b.meshes[g.mesh], a, bb, cc, c.status, rt);
         if (h.dist < rt && h.dist >= 0)
         {
             rec.point = f4(h.cpMesh, 0.f); rec.normal = f4(h.normal, 0.f);
@@ -714,7 +720,7 @@ __global__ void k_edge_colliders(DevCloth c, SolverParams P, Buffers b, VColl g,
     if (g.type == 4)
     {
         const float radTol = P.thickness + mx(P.tolerance, c.scal[0] * 1.5f);
-        SegHit h = mesh_segment_query(b.meshes[g.mesh], p, q, c.status);
+        SegHit h = mesh_segment_query(b.meshes[g.mesh], p, q, c.status, radTol);
         if (h.dist < radTol && h.dist >= 0)
         {
             rec.point = f4(h.cpMesh, 0.f); rec.normal = f4(h.normal, 0.f);
