@@ -83,6 +83,23 @@ SCEXP scHandle scCreateCapsule(scVector3 c, float rad, float halfHeight, scQuate
    float grid over `box`, x fastest, as Geometry::SDF::Create(nx, ny, nz, box) +
    values + ComputeGradient() (Geometry/SDF.cpp:10-56,210-256). Values are copied. */
 SCEXP scHandle scCreateSDFGrid(int nx, int ny, int nz, scAabb3 box, const float* values);
+/* SDF::Create(nx, ny, nz, box) + SDF::CreateFromMesh (Geometry/SDF.cpp:10-18,58-76),
+   computed on the GPU: every grid node's distance to the nearest triangle found
+   through the mesh tree ComputeMeshTree(mesh, ATF_TRIANGLES, 10, 0.1) builds. As
+   in the reference, with its default delta normal the field is unsigned.
+   Returns an SDF collidable (gradient computed). Addition. */
+SCEXP scHandle scCreateSDFFromMesh(const float* vertices, int nv, const unsigned* indices, int ni,
+                                   int nx, int ny, int nz, scAabb3 box);
+/* SDF::WriteToFile / SDF::LoadFromFile (Geometry/SDF.cpp:78-151): the reference's
+   binary format (3 ints, box and values as doubles). Additions. */
+SCEXP bool scSaveSDF(scHandle sdf, const char* path);
+SCEXP scHandle scLoadSDF(const char* path);
+/* addition: an SDF collidable's grid (cells per side, box min / max, up to cap
+   values); returns the value count */
+SCEXP int scGetSDFGrid(scHandle sdf, int* cells3, float* box6, float* values, int cap);
+/* addition: delete a collidable that was never added to a world (a world owns
+   the collidables added to it) */
+SCEXP void scFreeCollidable(scHandle collidable);
 /* Replaces scCreateMesh(Geometry::Mesh*) (Demo/ClothAPI.h:81): a triangle mesh
    prepared as Demo/ClothDemo.cpp:100-103 does (normals, edges, edge one-rings).
    Arrays are copied. */

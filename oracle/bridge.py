@@ -82,7 +82,10 @@ def _load(path: Path, prefix: str):
                     "ccd_midphase": ([C.c_void_p], None),
                     "ccd_num_candidates": ([C.c_void_p, C.c_int], C.c_int),
                     "ccd_get_candidates": ([C.c_void_p, C.c_int, _i], None),
-                    "solver_iterations": ([C.c_void_p], C.c_int)})
+                    "solver_iterations": ([C.c_void_p], C.c_int),
+                    "sdf_from_mesh": ([C.c_int, _f, C.c_int, _u, C.c_int, C.c_int, C.c_int, _f, _f], None),
+                    "sdf_write": ([C.c_int, C.c_int, C.c_int, _f, _f, C.c_char_p], None),
+                    "sdf_read": ([C.c_char_p, _i, _f, _f, C.c_int], C.c_int)})
     else:
         sig.update({"set_tri_order": ([C.c_void_p, _i, C.c_int], None),
                     "set_bend_order": ([C.c_void_p, _i, C.c_int], None),
@@ -326,3 +329,32 @@ class PortCloth(CpuCloth):
 
 def available(kind: str = "ref") -> bool:
     return (REF_LIB if kind == "ref" else PORT_LIB).exists()
+
+
+def ref_sdf_from_mesh(vertices, indices, cells, box6):
+    """the reference's SDF::CreateFromMesh on a (cells+1)^3 grid over box6"""
+    lib = _load(REF_LIB, "ref_")
+    v = np.ascontiguousarray(vertices, np.float32)
+    idx = np.ascontiguousarray(indices, np.uint32)
+    b = np.ascontiguousarray(box6, np.float32)
+    out = np.zeros((cells[0] + 1) * (cells[1] + 1) * (cells[2] + 1), np.float32)
+    lib.ref_sdf_from_mesh(v.shape[0], _fp(v), idx.size // 3, _up(idx), int(cells[0]), int(cells[1]), int(cells[2]),
+                          _fp(b), _fp(out))
+    return out
+
+
+def ref_sdf_write(cells, box6, values, path):
+    lib = _load(REF_LIB, "ref_")
+    b = np.ascontiguousarray(box6, np.float32)
+    vals = np.ascontiguousarray(values, np.float32)
+    lib.ref_sdf_write(int(cells[0]), int(cells[1]), int(cells[2]), _fp(b), _fp(vals), str(path).encode())
+
+
+def ref_sdf_read(path, cap=1 << 24):
+    lib = _load(REF_LIB, "ref_")
+    cells = np.zeros(3, np.int32)
+    box = np.zeros(6, np.float32)
+    vals = np.zeros(cap, np.float32)
+    n = lib.ref_sdf_read(str(path).encode(), _ip(cells), _fp(box), _fp(vals), cap)
+    return cells, box, vals[:n].copy()
+

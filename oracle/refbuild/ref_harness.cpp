@@ -113,6 +113,44 @@ void ref_add_mesh(void* h, int nv, const float* verts, int nt, const unsigned* i
     s->world.AddCollidable(c);
 }
 
+/* SDF::Create + SDF::CreateFromMesh (Geometry/SDF.cpp:10-18,58-76) over a triangle
+   mesh; out gets (nx+1)(ny+1)(nz+1) values, x fastest. */
+void ref_sdf_from_mesh(int nv, const float* verts, int nt, const unsigned* idx, int nx, int ny, int nz,
+                       const float* box6, float* out)
+{
+    Mesh m;
+    m.vertices.resize(nv);
+    for (int i = 0; i < nv; i++) m.vertices[i] = Vector3(verts[3 * i], verts[3 * i + 1], verts[3 * i + 2]);
+    m.indices.assign(idx, idx + 3 * nt);
+    SDF sdf;
+    sdf.Create(nx, ny, nz, Aabb3(Vector3(box6[0], box6[1], box6[2]), Vector3(box6[3], box6[4], box6[5])));
+    sdf.CreateFromMesh(m);
+    const std::vector<float>& d = sdf.GetData();
+    for (size_t i = 0; i < d.size(); i++) out[i] = d[i];
+}
+
+/* SDF::WriteToFile / SDF::LoadFromFile (Geometry/SDF.cpp:78-151) */
+void ref_sdf_write(int nx, int ny, int nz, const float* box6, const float* values, const char* path)
+{
+    SDF sdf;
+    sdf.Create(nx, ny, nz, Aabb3(Vector3(box6[0], box6[1], box6[2]), Vector3(box6[3], box6[4], box6[5])));
+    std::vector<float>& d = sdf.GetData();
+    for (size_t i = 0; i < d.size(); i++) d[i] = values[i];
+    sdf.WriteToFile(path);
+}
+
+int ref_sdf_read(const char* path, int* cells3, float* box6, float* values, int cap)
+{
+    SDF sdf;
+    sdf.LoadFromFile(path);
+    const std::vector<float>& d = sdf.GetData();
+    Aabb3 b = sdf.GetBox();
+    if (box6) { box6[0] = b.min.x; box6[1] = b.min.y; box6[2] = b.min.z; box6[3] = b.max.x; box6[4] = b.max.y; box6[5] = b.max.z; }
+    if (cells3) sdf.GetNumCellsPerSide(cells3);
+    for (size_t i = 0; values && i < d.size() && (int)i < cap; i++) values[i] = d[i];
+    return (int)d.size();
+}
+
 /* ---- cloth ---- */
 void ref_init_grid(void* h, int divX, int divY, float inc, float ox, float oy, float oz, int horizontal, int attached)
 {

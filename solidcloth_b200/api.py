@@ -55,6 +55,11 @@ SIGNATURES = {
     "scCreateSphere": ([scVector3, C.c_float], C.c_void_p),
     "scCreateCapsule": ([scVector3, C.c_float, C.c_float, scQuaternion], C.c_void_p),
     "scCreateSDFGrid": ([C.c_int, C.c_int, C.c_int, scAabb3, _f], C.c_void_p),
+    "scCreateSDFFromMesh": ([_f, C.c_int, _u, C.c_int, C.c_int, C.c_int, C.c_int, scAabb3], C.c_void_p),
+    "scSaveSDF": ([C.c_void_p, C.c_char_p], C.c_bool),
+    "scLoadSDF": ([C.c_char_p], C.c_void_p),
+    "scGetSDFGrid": ([C.c_void_p, _i, _f, _f, C.c_int], C.c_int),
+    "scFreeCollidable": ([C.c_void_p], None),
     "scCreateMeshCollider": ([_f, C.c_int, _u, C.c_int], C.c_void_p),
     "scGetCollidableType": ([C.c_void_p], C.c_int),
     "scGetMeshTree": ([C.c_void_p], C.c_void_p),
@@ -546,6 +551,50 @@ def load_batch(scenes_, ccd: bool | None = None):
         p.free()
         w.free()
     return b
+
+
+class SDFHandle:
+    """An SDF collidable made outside a world (from a mesh or a file)."""
+
+    def __init__(self, h):
+        if not h:
+            raise RuntimeError("SDF creation failed")
+        self.h = h
+
+    @classmethod
+    def from_mesh(cls, vertices, indices, cells, box6):
+        v = np.ascontiguousarray(vertices, np.float32)
+        idx = np.ascontiguousarray(indices, np.uint32)
+        b = scAabb3(v3(box6[:3]), v3(box6[3:]))
+        h = lib().scCreateSDFFromMesh(_fp(v), v.shape[0], idx.ctypes.data_as(_u), idx.size,
+                                      int(cells[0]), int(cells[1]), int(cells[2]), b)
+        _check("scCreateSDFFromMesh")
+        return cls(h)
+
+    @classmethod
+    def load(cls, path):
+        h = lib().scLoadSDF(str(path).encode())
+        _check("scLoadSDF")
+        return cls(h)
+
+    def save(self, path):
+        ok = lib().scSaveSDF(self.h, str(path).encode())
+        _check("scSaveSDF")
+        return bool(ok)
+
+    def grid(self):
+        """(cells (3,), box (6,), values ((nx+1)(ny+1)(nz+1),) x fastest)"""
+        cells = np.zeros(3, np.int32)
+        box = np.zeros(6, np.float32)
+        n = lib().scGetSDFGrid(self.h, cells.ctypes.data_as(_i), _fp(box), None, 0)
+        vals = np.zeros(n, np.float32)
+        lib().scGetSDFGrid(self.h, None, None, _fp(vals), n)
+        return cells, box, vals
+
+    def free(self):
+        if self.h:
+            lib().scFreeCollidable(self.h)
+            self.h = None
 
 
 def grid_variants():

@@ -3,6 +3,8 @@
 #include "cloth.h"
 #include "../../include/solidcloth_b200.h"
 #include <cstring>
+#include <cstdio>
+#include <string>
 #include <algorithm>
 #include <cmath>
 
@@ -101,6 +103,129 @@ scHandle scCreateSDFGrid(int nx, int ny, int nz, scAabb3 box, const float* value
     s->steps = mk(ext.x * inv.x, ext.y * inv.y, ext.z * inv.z);
     size_t n = (size_t)(nx + 1) * (ny + 1) * (nz + 1);
     s->values.assign(values, values + n);
+    s->compute_gradient();
+    return s;
+}
+
+static SDFC* new_sdf(int nx, int ny, int nz, scAabb3 box)
+{
+    SDFC* s = new SDFC();
+    s->type = CT_SDF;
+    s->nc[0] = nx; s->nc[1] = ny; s->nc[2] = nz;
+    s->box.lo = v3(box.min); s->box.hi = v3(box.max);
+    V3 ext = s->box.hi - s->box.lo;
+    V3 inv = mk(1.f / nx, 1.f / ny, 1.f / nz);
+    s->steps = mk(ext.x * inv.x, ext.y * inv.y, ext.z * inv.z);
+    return s;
+}
+
+scHandle scCreateSDFFromMesh(const float* vertices, int nv, const unsigned* indices, int ni, int nx, int ny, int nz,
+                             scAabb3 box)
+{
+    if (!vertices || !indices || nv <= 0 || ni <= 0 || ni % 3 || nx < 1 || ny < 1 || nz < 1)
+    {
+        set_error(SC_ERR_ARG, "bad mesh or SDF grid");
+        return nullptr;
+    }
+    // the mesh and its triangle tree as SDF::CreateFromMesh builds them
+    // (ComputeMeshTree(mesh, ATF_TRIANGLES, 10, 0.1f), Geometry/SDF.cpp:60-61)
+    MeshC m;
+    m.mesh.verts.resize(nv);
+    for (int i = 0; i < nv; i++) m.mesh.verts[i] = mk(vertices[3 * i], vertices[3 * i + 1], vertices[3 * i + 2]);
+    m.mesh.idx.assign(indices, indices + ni);
+    m.mesh.compute_normals();
+    m.mesh.construct_edges();
+    m.build_tree(0.1f, 10, 1);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!m.upload(dev)) return nullptr;
+    SDFC* s = new_sdf(nx, ny, nz, box);
+    const size_t n = (size_t)(nx + 1) * (ny + 1) * (nz + 1);
+    float* d = nullptr;
+    int* st = nullptr;
+    if (cudaMalloc(&d, sizeof(float) * n) != cudaSuccess || cudaMalloc(&st, sizeof(int)) != cudaSuccess)
+    {
+        if (d) cudaFree(d);
+        delete s;
+        set_error(SC_ERR_CUDA, "cudaMalloc failed");
+        return nullptr;
+    }
+    cudaMemset(st, 0, sizeof(int));
+    bool ok = launch_sdf_from_mesh(m.dev, nx, ny, nz, f4(s->box.lo, 0.f), f4(s->steps, 0.f), d, st);
+    s->values.resize(n);
+    int status = 0;
+    ok = ok && cudaMemcpy(s->values.data(), d, sizeof(float) * n, cudaMemcpyDeviceToHost) == cudaSuccess;
+    cudaMemcpy(&status, st, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    cudaFree(st);
+    if (!ok) { delete s; set_error(SC_ERR_CUDA, "SDF from mesh failed"); return nullptr; }
+    if (status) set_error(SC_ERR_DEVICE_STATUS, "mesh tree search stack overflow");
+    s->compute_gradient();
+    return s;
+}
+
+int scGetSDFGrid(scHandle sdf, int* cells3, float* box6, float* values, int cap)
+{
+    SDFC* s = (SDFC*)sdf;
+    if (!s || s->type != CT_SDF) { set_error(SC_ERR_ARG, "not an SDF"); return 0; }
+    if (cells3) { cells3[0] = s->nc[0]; cells3[1] = s->nc[1]; cells3[2] = s->nc[2]; }
+    if (box6)
+    {
+        box6[0] = s->box.lo.x; box6[1] = s->box.lo.y; box6[2] = s->box.lo.z;
+        box6[3] = s->box.hi.x; box6[4] = s->box.hi.y; box6[5] = s->box.hi.z;
+    }
+    for (size_t i = 0; values && i < s->values.size() && (int)i < cap; i++) values[i] = s->values[i];
+    return (int)s->values.size();
+}
+
+void scFreeCollidable(scHandle c) { delete (Collidable*)c; }
+
+// SDF::WriteToFile (Geometry/SDF.cpp:78-114): 3 ints (cells per side), the box as
+// doubles (min.x, max.x, min.y, max.y, min.z, max.z), the values as doubles, x fastest
+bool scSaveSDF(scHandle sdf, const char* path)
+{
+    SDFC* s = (SDFC*)sdf;
+    if (!s || s->type != CT_SDF || !path) { set_error(SC_ERR_ARG, "not an SDF"); return false; }
+    FILE* f = fopen(path, "wb");
+    if (!f) { set_error(SC_ERR_ARG, std::string("cannot write ") + path); return false; }
+    bool ok = fwrite(s->nc, sizeof(int), 3, f) == 3;
+    const double b[6] = {s->box.lo.x, s->box.hi.x, s->box.lo.y, s->box.hi.y, s->box.lo.z, s->box.hi.z};
+    ok = ok && fwrite(b, sizeof(double), 6, f) == 6;
+    for (size_t i = 0; ok && i < s->values.size(); i++)
+    {
+        const double v = s->values[i];
+        ok = fwrite(&v, sizeof(double), 1, f) == 1;
+    }
+    fclose(f);
+    if (!ok) set_error(SC_ERR_ARG, std::string("short write to ") + path);
+    return ok;
+}
+
+// SDF::LoadFromFile (Geometry/SDF.cpp:116-151) into a new SDF collidable (gradient computed)
+scHandle scLoadSDF(const char* path)
+{
+    if (!path) { set_error(SC_ERR_ARG, "null path"); return nullptr; }
+    FILE* f = fopen(path, "rb");
+    if (!f) { set_error(SC_ERR_ARG, std::string("cannot read ") + path); return nullptr; }
+    int nc[3] = {0, 0, 0};
+    double b[6];
+    bool ok = fread(nc, sizeof(int), 3, f) == 3 && fread(b, sizeof(double), 6, f) == 6 &&
+              nc[0] > 0 && nc[1] > 0 && nc[2] > 0 && nc[0] < 65536 && nc[1] < 65536 && nc[2] < 65536;
+    if (!ok) { fclose(f); set_error(SC_ERR_ARG, std::string("not an SDF file: ") + path); return nullptr; }
+    scAabb3 box;
+    box.min.x = (float)b[0]; box.max.x = (float)b[1]; box.min.y = (float)b[2];
+    box.max.y = (float)b[3]; box.min.z = (float)b[4]; box.max.z = (float)b[5];
+    SDFC* s = new_sdf(nc[0], nc[1], nc[2], box);
+    const size_t n = (size_t)(nc[0] + 1) * (nc[1] + 1) * (nc[2] + 1);
+    s->values.resize(n);
+    for (size_t i = 0; ok && i < n; i++)
+    {
+        double v;
+        ok = fread(&v, sizeof(double), 1, f) == 1;
+        s->values[i] = (float)v;
+    }
+    fclose(f);
+    if (!ok) { delete s; set_error(SC_ERR_ARG, std::string("truncated SDF file: ") + path); return nullptr; }
     s->compute_gradient();
     return s;
 }

@@ -207,20 +207,21 @@ MeshC::~MeshC() { if (dmem) cudaFree(dmem); }
 
 // Geometry::ComputeMeshTree + SplitNode, exclusive child assignment,
 // maxPrims 40 (Geometry/AabbTree.cpp:9-178)
-void MeshC::build_tree(float tol)
+void MeshC::build_tree(float tol, int maxLevel, int flags)
 {
     tree.clear();
     MeshTreeNode root;
     root.box = Box::empty();
     for (V3 v : mesh.verts) { root.box.lo = vmin(root.box.lo, v); root.box.hi = vmax(root.box.hi, v); }
-    for (uint32_t i = 0; i < (uint32_t)mesh.ntris(); i++) root.tris.push_back(i);
-    for (uint32_t i = 0; i < (uint32_t)mesh.verts.size(); i++) root.verts.push_back(i);
-    for (uint32_t i = 0; i < (uint32_t)mesh.edges.size(); i++) root.edges.push_back(i);
+    if (flags & 1) for (uint32_t i = 0; i < (uint32_t)mesh.ntris(); i++) root.tris.push_back(i);
+    if (flags & 2) for (uint32_t i = 0; i < (uint32_t)mesh.verts.size(); i++) root.verts.push_back(i);
+    if (flags & 4) for (uint32_t i = 0; i < (uint32_t)mesh.edges.size(); i++) root.edges.push_back(i);
     tree.push_back(root);
+    built = true;
+    if (maxLevel <= 0) return;
     struct Item { int node, level; };
     // recursion order of SplitNode: node, then left subtree, then right subtree
     std::vector<Item> stack{{0, 1}};
-    const int maxLevel = 20;
     while (!stack.empty())
     {
         Item it = stack.back();

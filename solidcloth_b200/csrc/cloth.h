@@ -77,7 +77,9 @@ struct MeshC : Collidable
     void* dmem = nullptr;
     DevMesh dev{};
     ~MeshC();
-    void build_tree(float tol);
+    // Geometry::ComputeMeshTree(mesh, flags, maxLevel, tol): flags 1 triangles,
+    // 2 vertices, 4 edges (ATF_*); the collider uses all three, maxLevel 20
+    void build_tree(float tol, int maxLevel = 20, int flags = 7);
     bool upload(int dev);
 };
 

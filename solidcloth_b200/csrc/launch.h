@@ -140,6 +140,9 @@ bool launch_mlp_grad(cudaStream_t s, const float* X, const float* T, int S, cons
                      float* grad, float* loss);
 void launch_adam(cudaStream_t s, float* prm, const float* grad, float* m, float* v, int step, float lr);
 
+// SDF::CreateFromMesh on the device: (nx+1)(ny+1)(nz+1) values, x fastest
+bool launch_sdf_from_mesh(const DevMesh& m, int nx, int ny, int nz, float4 lo, float4 steps, float* out, int* status);
+
 // exclusive scan of n ints (out may alias nothing); total written to *total if not null
 void scan_ints(cudaStream_t s, const int* in, int* out, int n, int* total, int* tmp);
 

@@ -2960,6 +2960,37 @@ void launch_gs_exit_test(cudaStream_t s, const DevCloth& c, const SolverParams& 
 
 } // namespace sc
 
+namespace sc {
+
+// ------------------------------------------------------- SDF from a mesh
+// SDF::CreateFromMesh (Geometry/SDF.cpp:58-76): at every grid node the distance
+// to the nearest mesh triangle (ClosestPointOnMeshToPointAcc with its default
+// delta normal), negated when the offset points against that normal — which,
+// with the delta normal, never happens: the reference's field is unsigned.
+__global__ void k_sdf_from_mesh(DevMesh m, int4 vals, float4 lo, float4 steps, float* out, int* status)
+{
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    const int count = vals.x * vals.y * vals.z;
+    if (idx >= count) return;
+    const int x = idx % vals.x, w = idx / vals.x, y = w % vals.y, z = w / vals.y;
+    V3 org = mk((float)x * steps.x, (float)y * steps.y, (float)z * steps.z);
+    org = org + mk(lo.x, lo.y, lo.z);
+    PointHit h = mesh_point_query(m, org, status, FLT_MAX);
+    float val = h.dist;
+    const V3 delta = org - h.cp;
+    if (dot(delta, h.normal) < 0) val = -val;
+    out[idx] = val;
+}
+
+bool launch_sdf_from_mesh(const DevMesh& m, int nx, int ny, int nz, float4 lo, float4 steps, float* out, int* status)
+{
+    const int count = (nx + 1) * (ny + 1) * (nz + 1);
+    k_sdf_from_mesh<<<blocks_for(count, 128), 128>>>(m, make_int4(nx + 1, ny + 1, nz + 1, 0), lo, steps, out, status);
+    return cudaGetLastError() == cudaSuccess;
+}
+
+} // namespace sc
+
 // ----------------------------------------------------- learned warm start
 #include "mlp_kernels.cuh"
 

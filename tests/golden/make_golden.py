@@ -132,8 +132,18 @@ def case_links():
     return out
 
 
+def case_sdf_mesh():
+    """SDF::CreateFromMesh of a level-2 icosphere (radius 0.25) on a 16^3-cell grid"""
+    from oracle.bridge import ref_sdf_from_mesh
+    m = scenes.icosphere(2, 0.25, (0.0, 0.0, 0.0))
+    box = np.array([-0.4, -0.4, -0.4, 0.4, 0.4, 0.4], np.float32)
+    vals = ref_sdf_from_mesh(m.vertices, m.indices, (16, 16, 16), box)
+    return dict(vertices=np.asarray(m.vertices, np.float32), indices=np.asarray(m.indices, np.uint32),
+                box=box, values=vals)
+
+
 CASES = {"cfg0": case_cfg0, "sdf": case_sdf, "self": case_self, "ccd": case_ccd, "mesh": case_mesh,
-         "links": case_links}
+         "links": case_links, "sdf_mesh": case_sdf_mesh}
 
 
 if __name__ == "__main__":
