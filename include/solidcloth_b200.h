@@ -128,6 +128,20 @@ SCEXP void scGetBatchInstance(scClothPatch batch, int k, int* firstParticle, int
 SCEXP scModel scGetClothModel(scClothPatch patch);
 SCEXP scMesh scGetClothMesh(scClothPatch patch);
 SCEXP void scInitCloth(scClothPatch patch, int divX, int divY, float inc, scVector3 offset, bool horizontal, bool attached);
+/* ClothPatch::Init(mesh, offset, attached) (Physics/ClothPatch.cpp:42-133), which
+   the reference's C API does not expose: a cloth from a triangle mesh (nv
+   vertices, ni indices); uvs (nv x 2) give the rest shape, colors (nv x 3) pin
+   vertices whose red channel is non-zero when `attached`; both may be NULL.
+   Coincident vertices merge into one particle (the reference's merge). The
+   patch's mesh buffers then hold the particles and their triangles;
+   scGetMeshParticleMap gives the input vertex -> particle map. Additions. */
+SCEXP void scInitClothMesh(scClothPatch patch, const float* vertices, int nv, const unsigned* indices, int ni,
+                           const float* uvs, const float* colors, scVector3 offset, bool attached);
+SCEXP int scGetMeshParticleMap(scClothPatch patch, int* map, int cap);
+/* addition: scInitClothMesh from a Wavefront OBJ file (v, vt, f; polygons fanned
+   into triangles; one vertex per face corner with its uv, as the demo's mesh
+   importer delivers meshes, Geometry/Assets.cpp:103); false if unreadable */
+SCEXP bool scInitClothObj(scClothPatch patch, const char* path, scVector3 offset, bool attached);
 /* The hot entry point: ClothPatch::Step (Demo/ClothAPI.cpp:146-150). */
 SCEXP void scStepCloth(scClothPatch patch, float dt);
 SCEXP void scUpdateClothMesh(scClothPatch patch);
@@ -281,6 +295,10 @@ SCEXP void scSetClusterStaging(scModel model, bool val);
    returns the number of colours; colourStart gets numColours+1 offsets if not NULL. */
 SCEXP int scGetConstraintOrder(scModel model, int kind, int* order, int* colourStart);
 SCEXP int scGetNumBends(scModel model);
+/* FEM rest data of every triangle: du1 du2 dv1 dv2 invDet lu0 lv0 lu2 lv2 area
+   (Physics/ClothTypes.h:37-62); links' rest length and stiffness */
+SCEXP void scGetTriangleRest(scModel model, float* rest10);
+SCEXP void scGetLinkRest(scModel model, float* rest2);
 SCEXP void scGetBends(scModel model, unsigned* idx4);
 SCEXP int scGetNumEdges(scModel model);
 SCEXP void scGetEdges(scModel model, int* e4);

@@ -64,6 +64,8 @@ def _load(path: Path, prefix: str):
         "get_tris": ([C.c_void_p, _u, _f], None),
         "get_bends": ([C.c_void_p, _u], None),
         "get_edges": ([C.c_void_p, _i], None),
+        "num_links": ([C.c_void_p], C.c_int),
+        "get_links": ([C.c_void_p, _u, _f], None),
         "step": ([C.c_void_p, C.c_float], None),
         "update_mesh": ([C.c_void_p], None),
         "predict_detect": ([C.c_void_p, C.c_float, C.c_int], None),
@@ -83,6 +85,7 @@ def _load(path: Path, prefix: str):
                     "ccd_num_candidates": ([C.c_void_p, C.c_int], C.c_int),
                     "ccd_get_candidates": ([C.c_void_p, C.c_int, _i], None),
                     "solver_iterations": ([C.c_void_p], C.c_int),
+                    "init_mesh": ([C.c_void_p, C.c_int, _f, C.c_int, _u, _f, _f, C.c_float, C.c_float, C.c_float, C.c_int], None),
                     "sdf_from_mesh": ([C.c_int, _f, C.c_int, _u, C.c_int, C.c_int, C.c_int, _f, _f], None),
                     "sdf_write": ([C.c_int, C.c_int, C.c_int, _f, _f, C.c_char_p], None),
                     "sdf_read": ([C.c_char_p, _i, _f, _f, C.c_int], C.c_int)})
@@ -96,8 +99,8 @@ def _load(path: Path, prefix: str):
                     "ccd_broadphase": ([C.c_void_p, C.c_float, C.c_int, _i, C.c_int], C.c_int),
                     "residual": ([C.c_void_p], C.c_float),
                     "set_link_order": ([C.c_void_p, _i, C.c_int], None),
-                    "num_links": ([C.c_void_p], C.c_int),
-                    "get_links": ([C.c_void_p, _u, _f], None)})
+                    "load_topology": ([C.c_void_p, C.c_int, _f, _f, C.c_int, _u, _f, C.c_int, _u, C.c_int, _u, _f], None),
+                    })
     for name, (args, res) in sig.items():
         fn = getattr(lib, P + name)
         fn.argtypes = args
@@ -199,6 +202,14 @@ class CpuCloth:
         self._fn("get_edges")(self.h, _ip(out))
         return out
 
+    def links(self):
+        """(n, 2) indices and (n, 2) rest length / stiffness, in creation order"""
+        n = self._fn("num_links")(self.h)
+        idx = np.zeros((n, 2), np.uint32)
+        ls = np.zeros((n, 2), np.float32)
+        self._fn("get_links")(self.h, _up(idx), _fp(ls))
+        return idx, ls
+
     def step(self, dt):
         self._fn("step")(self.h, float(dt))
 
@@ -247,6 +258,16 @@ class RefCloth(CpuCloth):
 
     def __init__(self):
         super().__init__(REF_LIB, "ref_")
+
+    def init_mesh(self, vertices, indices, uvs=None, colors=None, offset=(0, 0, 0), attached=False):
+        """ClothPatch::Init(mesh, offset, attached) in the reference build"""
+        v = np.ascontiguousarray(vertices, np.float32)
+        idx = np.ascontiguousarray(indices, np.uint32)
+        u = None if uvs is None else np.ascontiguousarray(uvs, np.float32)
+        c = None if colors is None else np.ascontiguousarray(colors, np.float32)
+        self._fn("init_mesh")(self.h, v.shape[0], _fp(v), idx.size, _up(idx), None if u is None else _fp(u),
+                              None if c is None else _fp(c), float(offset[0]), float(offset[1]), float(offset[2]),
+                              int(attached))
 
     @staticmethod
     def set_threads(n: int):
@@ -305,17 +326,17 @@ class PortCloth(CpuCloth):
         self._fn("self_contact_colours")(self.h, kind, _ip(c))
         return c
 
+    def load_topology(self, pos, inv_mass, tris, rest10, bends, links, link_rest):
+        """replace the model by an explicit topology (see orc_load_topology)"""
+        a = [np.ascontiguousarray(x, t) for x, t in ((pos, np.float32), (inv_mass, np.float32), (tris, np.uint32),
+                                                       (rest10, np.float32), (bends, np.uint32), (links, np.uint32),
+                                                       (link_rest, np.float32))]
+        self._fn("load_topology")(self.h, a[0].shape[0], _fp(a[0]), _fp(a[1]), a[2].shape[0], _up(a[2]), _fp(a[3]),
+                                  a[4].shape[0], _up(a[4]), a[5].shape[0], _up(a[5]), _fp(a[6]))
+
     def set_link_order(self, order):
         o = np.ascontiguousarray(order, np.int32)
         self._fn("set_link_order")(self.h, _ip(o), o.size)
-
-    def links(self):
-        """(n, 2) indices and (n, 2) rest length / stiffness, in creation order"""
-        n = self._fn("num_links")(self.h)
-        idx = np.zeros((n, 2), np.uint32)
-        ls = np.zeros((n, 2), np.float32)
-        self._fn("get_links")(self.h, _up(idx), _fp(ls))
-        return idx, ls
 
     def residual(self) -> float:
         """max |C| over the warp, weft and shear constraints at the current positions"""

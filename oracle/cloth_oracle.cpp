@@ -2044,6 +2044,52 @@ void orc_set_bend_order(void* h, const int* o, int n)
 
 void orc_set_contact_order(void* h, int mode) { ((Cloth*)h)->contactOrder = mode; }
 
+/* Replace the cloth's model by an explicit topology (particles, FEM triangles
+   with their rest data du1 du2 dv1 dv2 invDet lu0 lv0 lu2 lv2 area, bends, links
+   with rest length and stiffness), e.g. the one ClothPatch::Init(mesh) built in
+   the reference; the collision mesh is rebuilt from the triangles. */
+void orc_load_topology(void* h, int n, const float* pos, const float* invMass, int nt, const unsigned* tri,
+                       const float* rest10, int nb, const unsigned* bend4, int nl, const unsigned* link2,
+                       const float* linkRest2)
+{
+    Cloth* c = (Cloth*)h;
+    c->N = n;
+    c->pos.assign(n, v3(0, 0, 0)); c->prev.assign(n, v3(0, 0, 0)); c->vel.assign(n, v3(0, 0, 0));
+    c->invMass.assign(invMass, invMass + n); c->uv.assign(n, v3(0, 0, 0));
+    for (int i = 0; i < n; i++) { c->pos[i] = v3(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]); c->prev[i] = c->pos[i]; }
+    c->tris.clear(); c->bends.clear(); c->links.clear();
+    c->triOrder.clear(); c->bendOrder.clear(); c->linkOrder.clear();
+    std::vector<u32> idxs;
+    for (int t = 0; t < nt; t++)
+    {
+        Tri r;
+        r.i1 = tri[3 * t]; r.i2 = tri[3 * t + 1]; r.i3 = tri[3 * t + 2];
+        const float* q = rest10 + 10 * t;
+        r.du1 = q[0]; r.du2 = q[1]; r.dv1 = q[2]; r.dv2 = q[3]; r.invDet = q[4];
+        r.lu0 = q[5]; r.lv0 = q[6]; r.lu2 = q[7]; r.lv2 = q[8]; r.area = q[9];
+        r.det = r.du1 * r.dv2 - r.du2 * r.dv1;
+        c->tris.push_back(r);
+        idxs.push_back(r.i1); idxs.push_back(r.i2); idxs.push_back(r.i3);
+    }
+    for (int b = 0; b < nb; b++)
+    {
+        Bend x; x.i1 = bend4[4 * b]; x.i2 = bend4[4 * b + 1]; x.i3 = bend4[4 * b + 2]; x.i4 = bend4[4 * b + 3];
+        c->bends.push_back(x);
+    }
+    for (int l = 0; l < nl; l++)
+    {
+        Cloth::Link x; x.i1 = link2[2 * l]; x.i2 = link2[2 * l + 1]; x.len = linkRest2[2 * l]; x.stiffness = linkRest2[2 * l + 1];
+        c->links.push_back(x);
+    }
+    c->mesh = Topo();
+    c->mesh.verts = c->pos;
+    c->mesh.idx = idxs;
+    c->mesh.compute_normals();
+    c->mesh.construct_edges();
+    c->mesh.construct_rings(true, true);
+    c->prevMesh = c->mesh;
+}
+
 void orc_set_link_order(void* h, const int* o, int n)
 {
     Cloth* c = (Cloth*)h;

@@ -43,6 +43,9 @@ void orc_set_bend_order(void* h, const int* order, int n);
    GPU's deterministic independent-set colouring order (colour, then list index). */
 void orc_set_contact_order(void* h, int mode);
 void orc_set_link_order(void* h, const int* order, int n);
+void orc_load_topology(void* h, int n, const float* pos, const float* invMass, int nt, const unsigned* tri,
+                       const float* rest10, int nb, const unsigned* bend4, int nl, const unsigned* link2,
+                       const float* linkRest2);
 int orc_num_links(void* h);
 void orc_get_links(void* h, unsigned* idx2, float* lenStiff);
 void orc_set_portable_math(int on);

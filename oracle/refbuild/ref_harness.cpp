@@ -151,6 +151,32 @@ int ref_sdf_read(const char* path, int* cells3, float* box6, float* values, int 
     return (int)d.size();
 }
 
+/* ClothPatch::Init(mesh, offset, attached) (Physics/ClothPatch.cpp:42-133): the
+   cloth from a triangle mesh; uvs (nv x 2) and colors (nv x 3) may be null. */
+void ref_init_mesh(void* h, int nv, const float* verts, int ni, const unsigned* idx, const float* uvs,
+                   const float* colors, float ox, float oy, float oz, int attached)
+{
+    RefScene* s = (RefScene*)h;
+    Mesh m;
+    m.vertices.resize(nv);
+    for (int i = 0; i < nv; i++) m.vertices[i] = Vector3(verts[3 * i], verts[3 * i + 1], verts[3 * i + 2]);
+    m.indices.assign(idx, idx + ni);
+    if (uvs) { m.uvs.resize(nv); for (int i = 0; i < nv; i++) m.uvs[i] = Vector2(uvs[2 * i], uvs[2 * i + 1]); }
+    if (colors) { m.colors.resize(nv); for (int i = 0; i < nv; i++) m.colors[i] = Vector3(colors[3 * i], colors[3 * i + 1], colors[3 * i + 2]); }
+    s->patch->Init(m, Vector3(ox, oy, oz), attached != 0);
+}
+
+void ref_get_links(void* h, unsigned* idx2, float* lenStiff)
+{
+    ClothModel& m = Model((RefScene*)h);
+    for (size_t i = 0; i < m.GetNumLinks(); i++)
+    {
+        const Physics::Link& l = m.GetLink(i);
+        if (idx2) { idx2[2 * i] = l.i1; idx2[2 * i + 1] = l.i2; }
+        if (lenStiff) { lenStiff[2 * i] = l.len; lenStiff[2 * i + 1] = l.stiffness; }
+    }
+}
+
 /* ---- cloth ---- */
 void ref_init_grid(void* h, int divX, int divY, float inc, float ox, float oy, float oz, int horizontal, int attached)
 {

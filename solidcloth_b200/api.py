@@ -58,6 +58,11 @@ SIGNATURES = {
     "scCreateSDFFromMesh": ([_f, C.c_int, _u, C.c_int, C.c_int, C.c_int, C.c_int, scAabb3], C.c_void_p),
     "scSaveSDF": ([C.c_void_p, C.c_char_p], C.c_bool),
     "scLoadSDF": ([C.c_char_p], C.c_void_p),
+    "scInitClothMesh": ([scClothPatch, _f, C.c_int, _u, C.c_int, _f, _f, scVector3, C.c_bool], None),
+    "scGetMeshParticleMap": ([scClothPatch, _i, C.c_int], C.c_int),
+    "scGetTriangleRest": ([scModel, _f], None),
+    "scInitClothObj": ([scClothPatch, C.c_char_p, scVector3, C.c_bool], C.c_bool),
+    "scGetLinkRest": ([scModel, _f], None),
     "scGetSDFGrid": ([C.c_void_p, _i, _f, _f, C.c_int], C.c_int),
     "scFreeCollidable": ([C.c_void_p], None),
     "scCreateMeshCollider": ([_f, C.c_int, _u, C.c_int], C.c_void_p),
@@ -365,6 +370,24 @@ class ClothModel:
             out[t] = (a.value, b.value, c.value)
         return out
 
+    def tri_rest(self):
+        """(T, 10): du1 du2 dv1 dv2 invDet lu0 lv0 lu2 lv2 area"""
+        out = np.zeros((lib().scGetNumTris(self.h), 10), np.float32)
+        lib().scGetTriangleRest(self.h, _fp(out))
+        return out
+
+    def links(self):
+        """(L, 2) indices and (L, 2) rest length / stiffness, in creation order"""
+        n = lib().scGetNumLinks(self.h)
+        idx = np.zeros((n, 2), np.uint32)
+        a, b = C.c_int(), C.c_int()
+        for k in range(n):
+            lib().scGetLink(self.h, k, C.byref(a), C.byref(b))
+            idx[k] = (a.value, b.value)
+        rest = np.zeros((n, 2), np.float32)
+        lib().scGetLinkRest(self.h, _fp(rest))
+        return idx, rest
+
     def bends(self):
         n = lib().scGetNumBends(self.h)
         out = np.zeros((n, 4), np.uint32)
@@ -460,6 +483,27 @@ class ClothPatch:
     def init_grid(self, div_x, div_y, inc, offset, horizontal=True, attached=False):
         lib().scInitCloth(self.h, int(div_x), int(div_y), float(inc), v3(offset), bool(horizontal), bool(attached))
         _check("scInitCloth")
+
+    def init_mesh(self, vertices, indices, uvs=None, colors=None, offset=(0, 0, 0), attached=False):
+        """ClothPatch::Init(mesh, offset, attached)"""
+        v = np.ascontiguousarray(vertices, np.float32)
+        idx = np.ascontiguousarray(indices, np.uint32)
+        u = None if uvs is None else np.ascontiguousarray(uvs, np.float32)
+        c = None if colors is None else np.ascontiguousarray(colors, np.float32)
+        lib().scInitClothMesh(self.h, _fp(v), v.shape[0], idx.ctypes.data_as(_u), idx.size,
+                              None if u is None else _fp(u), None if c is None else _fp(c), v3(offset), bool(attached))
+        _check("scInitClothMesh")
+
+    def init_obj(self, path, offset=(0, 0, 0), attached=False):
+        ok = lib().scInitClothObj(self.h, str(path).encode(), v3(offset), bool(attached))
+        _check("scInitClothObj")
+        return bool(ok)
+
+    def particle_map(self):
+        n = lib().scGetMeshParticleMap(self.h, None, 0)
+        m = np.zeros(n, np.int32)
+        lib().scGetMeshParticleMap(self.h, m.ctypes.data_as(_i), n)
+        return m
 
     def set_num_steps(self, n):
         lib().scSetNumSteps(self.h, int(n))

@@ -327,6 +327,93 @@ void scInitCloth(scClothPatch p, int divX, int divY, float inc, scVector3 offset
     P(p)->init_grid(divX, divY, inc, v3(offset), horizontal, attached);
 }
 
+void scInitClothMesh(scClothPatch p, const float* vertices, int nv, const unsigned* indices, int ni, const float* uvs,
+                     const float* colors, scVector3 offset, bool attached)
+{
+    if (!P(p) || !vertices || !indices || nv < 3 || ni < 3 || ni % 3) { set_error(SC_ERR_ARG, "bad cloth mesh"); return; }
+    std::vector<V3> v(nv);
+    for (int i = 0; i < nv; i++) v[i] = mk(vertices[3 * i], vertices[3 * i + 1], vertices[3 * i + 2]);
+    std::vector<uint32_t> idx(indices, indices + ni);
+    P(p)->init_mesh(v, idx, uvs, colors, v3(offset), attached);
+}
+
+// Wavefront OBJ (v, vt, f; polygons fanned into triangles) as a triangle soup:
+// one vertex per face corner with its uv, as a mesh importer delivers it; the
+// cloth initialisation then merges coincident corners. Returns false when the
+// file cannot be read or names an index out of range.
+static bool read_obj(const char* path, std::vector<V3>& verts, std::vector<uint32_t>& idx, std::vector<float>& uvs)
+{
+    FILE* f = fopen(path, "r");
+    if (!f) return false;
+    std::vector<V3> v;
+    std::vector<float> vt;
+    char line[4096];
+    bool ok = true;
+    while (ok && fgets(line, sizeof(line), f))
+    {
+        if (line[0] == 'v' && line[1] == ' ')
+        {
+            float x, y, z;
+            if (sscanf(line + 2, "%f %f %f", &x, &y, &z) == 3) v.push_back(mk(x, y, z));
+        }
+        else if (line[0] == 'v' && line[1] == 't' && line[2] == ' ')
+        {
+            float a = 0, b = 0;
+            if (sscanf(line + 3, "%f %f", &a, &b) >= 1) { vt.push_back(a); vt.push_back(b); }
+        }
+        else if (line[0] == 'f' && line[1] == ' ')
+        {
+            std::vector<std::pair<int, int>> corners;
+            char* q = line + 2;
+            while (*q)
+            {
+                while (*q == ' ' || *q == '\t') q++;
+                if (!*q || *q == '\n' || *q == '\r') break;
+                int vi = 0, ti = 0;
+                int nread = 0;
+                if (sscanf(q, "%d/%d%n", &vi, &ti, &nread) == 2) {}
+                else if (sscanf(q, "%d%n", &vi, &nread) == 1) ti = 0;
+                else { ok = false; break; }
+                q += nread;
+                while (*q && *q != ' ' && *q != '\t' && *q != '\n' && *q != '\r') q++;   // skip "/normal"
+                if (vi < 0) vi = (int)v.size() + 1 + vi;
+                if (ti < 0) ti = (int)(vt.size() / 2) + 1 + ti;
+                corners.push_back({vi - 1, ti - 1});
+            }
+            for (size_t k = 2; ok && k < corners.size(); k++)
+                for (size_t c : {(size_t)0, k - 1, k})
+                {
+                    const int vi = corners[c].first, ti = corners[c].second;
+                    if (vi < 0 || vi >= (int)v.size() || ti >= (int)(vt.size() / 2)) { ok = false; break; }
+                    idx.push_back((uint32_t)verts.size());
+                    verts.push_back(v[vi]);
+                    uvs.push_back(ti >= 0 ? vt[2 * ti] : 0.f);
+                    uvs.push_back(ti >= 0 ? vt[2 * ti + 1] : 0.f);
+                }
+        }
+    }
+    fclose(f);
+    return ok && !idx.empty();
+}
+
+bool scInitClothObj(scClothPatch p, const char* path, scVector3 offset, bool attached)
+{
+    if (!P(p) || !path) { set_error(SC_ERR_ARG, "null patch or path"); return false; }
+    std::vector<V3> v;
+    std::vector<uint32_t> idx;
+    std::vector<float> uv;
+    if (!read_obj(path, v, idx, uv)) { set_error(SC_ERR_ARG, std::string("cannot read OBJ mesh ") + path); return false; }
+    return P(p)->init_mesh(v, idx, uv.data(), nullptr, v3(offset), attached);
+}
+
+int scGetMeshParticleMap(scClothPatch p, int* map, int cap)
+{
+    if (!P(p)) return 0;
+    const auto& mm = P(p)->meshMap;
+    for (int i = 0; map && i < cap && i < (int)mm.size(); i++) map[i] = mm[i];
+    return (int)mm.size();
+}
+
 void scStepCloth(scClothPatch p, float dt)
 {
     if (!P(p)) { set_error(SC_ERR_ARG, "null patch"); return; }
@@ -735,6 +822,25 @@ int scGetConstraintOrder(scModel m, int kind, int* order, int* colourStart)
     if (colourStart) memcpy(colourStart, s.data(), sizeof(int) * s.size());
     return (int)s.size() - 1;
 }
+void scGetTriangleRest(scModel m, float* rest10)
+{
+    if (!M(m) || !rest10) return;
+    const auto& tr = M(m)->tris;
+    for (size_t i = 0; i < tr.size(); i++)
+    {
+        float* r = rest10 + 10 * i;
+        r[0] = tr[i].du1; r[1] = tr[i].du2; r[2] = tr[i].dv1; r[3] = tr[i].dv2; r[4] = tr[i].invDet;
+        r[5] = tr[i].lu0; r[6] = tr[i].lv0; r[7] = tr[i].lu2; r[8] = tr[i].lv2; r[9] = tr[i].area;
+    }
+}
+
+void scGetLinkRest(scModel m, float* rest2)
+{
+    if (!M(m) || !rest2) return;
+    const auto& lr = M(m)->linkRest;
+    for (size_t i = 0; i < lr.size(); i++) { rest2[2 * i] = lr[i].x; rest2[2 * i + 1] = lr[i].y; }
+}
+
 int scGetNumBends(scModel m) { return M(m) ? (int)M(m)->bends.size() : 0; }
 void scGetBends(scModel m, unsigned* idx4)
 {

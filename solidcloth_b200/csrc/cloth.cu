@@ -1193,6 +1193,146 @@ bool ClothPatch::init_batch(const std::vector<ClothPatch*>& parts)
     return true;
 }
 
+// ClothPatch::Init(mesh, offset, attached) (Physics/ClothPatch.cpp:42-133): the
+// cloth from a triangle mesh. Vertices at exactly the same place become one
+// particle (the reference's O(V^2) merge, kept); a particle is pinned when
+// `attached` and its vertex colour's red channel is non-zero; triangles take
+// their rest shape from the per-corner uvs when given (else the particles' uvs);
+// edges come from the first n-1 half-edges of the index buffer, sorted, as the
+// reference builds them (so the last triangle's closing edge is missing, as
+// there); every unique edge becomes a stretch link, an edge and a bend.
+bool ClothPatch::init_mesh(const std::vector<V3>& verts, const std::vector<uint32_t>& idx, const float* uvs,
+                           const float* colors, V3 offset, bool attached)
+{
+    if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }
+    if (verts.empty() || idx.size() < 3 || idx.size() % 3) { set_error(SC_ERR_ARG, "mesh needs vertices and triangles"); return false; }
+    for (uint32_t i : idx) if (i >= verts.size()) { set_error(SC_ERR_ARG, "mesh index out of range"); return false; }
+    ClothModel& m = model;
+    const size_t nv = verts.size();
+    std::vector<int> map(nv, -1);
+    m.N = 0;
+    m.hpos.clear(); m.hprev.clear(); m.hvel.clear(); m.invMass.clear(); m.uvx.clear(); m.uvy.clear();
+    m.tris.clear(); m.bends.clear(); m.links.clear(); m.linkRest.clear(); m.quads.clear();
+    m.instV.clear(); m.instT.clear(); m.instE.clear(); m.instB.clear(); m.batchColl.clear();
+    for (size_t i = 0; i < nv; i++)
+    {
+        if (map[i] >= 0) continue;
+        for (size_t j = i + 1; j < nv; j++)
+        {
+            const V3 d = verts[i] - verts[j];
+            if (dot(d, d) == 0) map[j] = m.N;
+        }
+        map[i] = m.N;
+        m.hpos.push_back(verts[i] + offset);
+        m.hprev.push_back(mk(0, 0, 0));
+        m.hvel.push_back(mk(0, 0, 0));
+        m.invMass.push_back((attached && colors && colors[3 * i] != 0) ? 0.f : 1.f);
+        m.uvx.push_back(uvs ? uvs[2 * i] : 0.f);
+        m.uvy.push_back(uvs ? uvs[2 * i + 1] : 0.f);
+        m.N++;
+    }
+    // ClothModel::AddTriangle with explicit uvs (Physics/ClothModel.cpp:54-92)
+    auto addTri = [&](uint32_t a, uint32_t b, uint32_t c, uint32_t ua, uint32_t ub, uint32_t uc) {
+        if (uvs)
+        {
+            // the particle uvs stand in for the corners' own: swap them in for make_triangle
+            const float sa[3] = {m.uvx[a], m.uvx[b], m.uvx[c]}, sb[3] = {m.uvy[a], m.uvy[b], m.uvy[c]};
+            m.uvx[a] = uvs[2 * ua]; m.uvy[a] = uvs[2 * ua + 1];
+            m.uvx[b] = uvs[2 * ub]; m.uvy[b] = uvs[2 * ub + 1];
+            m.uvx[c] = uvs[2 * uc]; m.uvy[c] = uvs[2 * uc + 1];
+            m.tris.push_back(make_triangle(m, a, b, c));
+            m.uvx[c] = sa[2]; m.uvy[c] = sb[2];
+            m.uvx[b] = sa[1]; m.uvy[b] = sb[1];
+            m.uvx[a] = sa[0]; m.uvy[a] = sb[0];
+        }
+        else m.tris.push_back(make_triangle(m, a, b, c));
+    };
+    const size_t n = idx.size();
+    struct HE { uint32_t i1, i2; int t1, t2; };
+    std::vector<HE> dup(n - 1);
+    for (size_t i = 0; i + 1 < n; i++)
+    {
+        uint32_t i1 = map[idx[i]], i2 = map[idx[i + 1]];
+        if ((i + 1) % 3 == 0)
+        {
+            i2 = map[idx[i - 2]];
+            addTri(i2, map[idx[i - 1]], i1, idx[i - 2], idx[i - 1], idx[i]);
+        }
+        if (i1 > i2) std::swap(i1, i2);
+        dup[i] = {i1, i2, (int)(i / 3), -1};
+    }
+    addTri(map[idx[n - 3]], map[idx[n - 2]], map[idx[n - 1]], idx[n - 3], idx[n - 2], idx[n - 1]);
+    std::sort(dup.begin(), dup.end(), [](const HE& a, const HE& b) { return a.i1 < b.i1 || (a.i1 == b.i1 && a.i2 < b.i2); });
+    const float stretch = m.prm.stretch;
+    auto addLink = [&](uint32_t a, uint32_t b) {
+        if (m.invMass[a] == 0 && m.invMass[b] == 0) return;
+        if (stretch == 0) return;
+        m.links.push_back(make_uint2(a, b));
+        m.linkRest.push_back(make_float2(len(m.hpos[a] - m.hpos[b]), stretch));
+    };
+    std::vector<HE> edges;
+    addLink(dup[0].i1, dup[0].i2);
+    HE cur = dup[0];
+    for (size_t i = 1; i < dup.size(); i++)
+    {
+        if (dup[i].i1 == dup[i - 1].i1 && dup[i].i2 == dup[i - 1].i2) { cur.t2 = dup[i].t1; continue; }
+        addLink(dup[i].i1, dup[i].i2);
+        edges.push_back(cur);
+        cur = dup[i];
+    }
+    edges.push_back(cur);
+    // the collision / render mesh over the particles, with the reference's edge list
+    mesh = HMesh();
+    mesh.verts = m.hpos;
+    for (const FemHost& t : m.tris) { mesh.idx.push_back(t.i1); mesh.idx.push_back(t.i2); mesh.idx.push_back(t.i3); }
+    mesh.compute_normals();
+    std::vector<int> slot(3 * m.tris.size(), -1);
+    for (size_t e = 0; e < edges.size(); e++)
+    {
+        HEdge h;
+        h.i1 = edges[e].i1; h.i2 = edges[e].i2; h.t1 = edges[e].t1; h.t2 = edges[e].t2;
+        h.n = h.t2 >= 0 ? normalized(mesh.triN[h.t1] + mesh.triN[h.t2]) : mesh.triN[h.t1];
+        h.origIdx = (int)e;
+        mesh.edges.push_back(h);
+        // triangle -> edge ids: the triangle side with these end points
+        for (int t : {h.t1, h.t2})
+        {
+            if (t < 0) continue;
+            for (int k = 0; k < 3; k++)
+            {
+                const uint32_t a = mesh.idx[3 * t + k], b = mesh.idx[3 * t + (k + 1) % 3];
+                if ((a == h.i1 && b == h.i2) || (a == h.i2 && b == h.i1)) slot[3 * t + k] = (int)e;
+            }
+        }
+    }
+    mesh.triE.resize(slot.size());
+    for (size_t k = 0; k < slot.size(); k++) mesh.triE[k] = slot[k] < 0 ? 0u : (uint32_t)slot[k];
+    mesh.construct_rings(true, true);
+    // ClothModel::AddBendConstraint for every edge with two triangles (Physics/ClothModel.cpp:94-126)
+    for (const HEdge& e : mesh.edges)
+    {
+        if (e.t2 < 0) continue;
+        auto opp = [&](int t) -> uint32_t {
+            const FemHost& tr = m.tris[t];
+            if (tr.i1 != e.i1 && tr.i1 != e.i2) return tr.i1;
+            if (tr.i2 != e.i1 && tr.i2 != e.i2) return tr.i2;
+            return tr.i3;
+        };
+        m.bends.push_back(make_uint4(e.i1, e.i2, opp(e.t1), opp(e.t2)));
+    }
+    meshMap = map;
+    isQuadMesh = false;
+    for (int i = 0; i < m.N; i++) m.hprev[i] = m.hpos[i];
+    prevMesh = mesh;
+    m.tuned = false;
+    m.touch();
+    if (!m.upload_topology(mesh)) return false;
+    m.bufWorldVersion = ~0ull;
+    m.upload_state(stream);
+    hostStateDirty = false;
+    return true;
+}
+
 void ClothPatch::sync()
 {
     cudaStreamSynchronize(stream);

@@ -229,6 +229,9 @@ public:
 
     bool init_grid(int divX, int divY, float inc, V3 offset, bool horizontal, bool attached);
     bool init_batch(const std::vector<ClothPatch*>& parts);
+    bool init_mesh(const std::vector<V3>& verts, const std::vector<uint32_t>& idx, const float* uvs,
+                   const float* colors, V3 offset, bool attached);
+    std::vector<int> meshMap;                  // mesh cloth: input vertex -> particle
     bool step(float dt);
     void update_mesh();
     void record_substep(float h);

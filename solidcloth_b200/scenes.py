@@ -318,3 +318,31 @@ def ccd_scene(n: int = 16, seed: int = 5):
     vel = (vel + rng.uniform(-20.0, 20.0, vel.shape)).astype(np.float32)
     sc.ccd = True
     return sc, (pos, prev, vel)
+
+
+def mesh_cloth(n: int = 10, side: float = 0.5, height: float = 0.3, seed: int = 9):
+    """A square sheet given as a triangle soup, as a mesh importer delivers it:
+    every triangle has its own three vertices (coincident corners merge into
+    particles in ClothPatch::Init(mesh)), with uvs = the rest-shape xz
+    coordinates, and red vertex colours on the two far corners (pinned when
+    attached). A little seeded noise is added to the heights. Returns
+    (vertices, indices, uvs, colors, params)."""
+    rng = np.random.default_rng(seed)
+    inc = np.float32(side / (n - 1))
+    xs = (np.arange(n, dtype=np.float32) * inc - np.float32(0.5 * side)).astype(np.float32)
+    grid = np.stack(np.meshgrid(xs, xs, indexing="ij"), -1).reshape(-1, 2)
+    ys = (np.float32(height) + _noise(rng, (n * n,), 1e-3)).astype(np.float32)
+    verts, uvs, cols, idx = [], [], [], []
+    for j in range(n - 1):
+        for i in range(n - 1):
+            a, b, c, d = j * n + i, j * n + i + 1, (j + 1) * n + i + 1, (j + 1) * n + i
+            for tri in ((a, b, c), (a, c, d)):
+                for v in tri:
+                    verts.append((grid[v, 0], ys[v], grid[v, 1]))
+                    uvs.append((grid[v, 0], grid[v, 1]))
+                    corner = v in (n - 1, n * n - 1)
+                    cols.append((1.0 if corner else 0.0, 0.0, 0.0))
+                    idx.append(len(idx))
+    p = Params(thickness=0.005, tolerance=0.005, iterations=8, substeps=4, flags=0)
+    return (np.array(verts, np.float32), np.array(idx, np.uint32), np.array(uvs, np.float32),
+            np.array(cols, np.float32), p)

@@ -305,3 +305,32 @@ def test_port_matches_reference_links(fixed, ref_threads):
             r.step(sc.dt)
             o.step(sc.dt)
         assert np.array_equal(bits(r.positions()), bits(o.positions())), dih
+
+
+# ------------------------------------------------------------- mesh cloth
+def test_port_matches_reference_mesh_cloth(ref_threads):
+    """ClothPatch::Init(mesh) (Physics/ClothPatch.cpp:42-133) in the reference
+    build, its topology loaded into the oracle: the oracle steps it bit for bit
+    (FEM + bends, and the mass-spring path)."""
+    R, P = ref(), port()
+    P.set_portable_math(False)
+    for fem in (True, False):
+        v, idx, uv, col, prm = scenes.mesh_cloth()
+        prm.fem = fem
+        r = R()
+        pa = prm.as_array()
+        r._fn("set_params")(r.h, pa.ctypes.data_as(__import__("ctypes").POINTER(__import__("ctypes").c_float)), pa.size)
+        r.init_mesh(v, idx, uv, col, (0, 0, 0), True)
+        pos, prev, vel, w = r.state()
+        assert 0 < pos.shape[0] < v.shape[0]          # coincident corners merged
+        assert np.sum(w == 0) == 2                    # the two red corners pinned
+        ti, tr = r.tris()
+        li, lr = r.links()
+        o = P()
+        o._fn("set_params")(o.h, pa.ctypes.data_as(__import__("ctypes").POINTER(__import__("ctypes").c_float)), pa.size)
+        o.load_topology(pos, w, ti, tr, r.bends(), li, lr)
+        dt = 1.0 / 60
+        for _ in range(6):
+            r.step(dt)
+            o.step(dt)
+        assert np.array_equal(bits(r.positions()), bits(o.positions())), fem
