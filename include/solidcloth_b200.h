@@ -372,6 +372,22 @@ SCEXP int scGetKernelTiming(scClothPatch patch, float* ms, int* counts);
 SCEXP int scComputeVertexNormalsNoAlloc(const float* vertices, int numVertices, const unsigned* indices,
                                         int numTriangles, float* normals, void* stream);
 
+/* ---- addition: headless picture of the cloth ----
+   Rasterises the patch's current mesh on the GPU with the demo's Phong program
+   (Shaders/shader_phong_*.glsl; drawn by Graphics3D::DrawMesh,
+   Graphics/Graphics3D.h) into `rgba` (a DEVICE buffer of width*height float4,
+   row 0 at the top). viewProj16: row-major 4x4 view-projection matrix applied to
+   column vectors (x, y, z, 1), OpenGL clip conventions. params16: light position
+   (3), eye position (3), diffuse colour kd (3), specular colour ks (3),
+   shininess, flip (+1/-1 for the normal's side), background grey, flags
+   (shader bits: 2 Oren-Nayar, 8 monochrome, 16 wireframe; others are rejected
+   with SC_ERR_UNSUPPORTED = 4). zscratch: a DEVICE buffer of width*height
+   uint64 that the call overwrites; afterwards each word holds (depth key << 32 |
+   triangle index), or all ones where no triangle covers the pixel. Blocks until
+   the picture is written. Returns 0 or an error code. */
+SCEXP int scRenderCloth(scClothPatch patch, const float* viewProj16, const float* params16, int width, int height,
+                        float* rgba, void* zscratch);
+
 #ifdef __cplusplus
 }
 #endif

@@ -178,6 +178,7 @@ SIGNATURES = {
     "scProfileSweep": ([scClothPatch, C.c_int, C.c_int], C.c_float),
     "scSetKernelTiming": ([scClothPatch, C.c_int], C.c_bool),
     "scGetKernelTiming": ([scClothPatch, _f, _i], C.c_int),
+    "scRenderCloth": ([scClothPatch, _f, _f, C.c_int, C.c_int, C.c_void_p, C.c_void_p], C.c_int),
 }
 
 _lib = None
@@ -546,6 +547,23 @@ class ClothPatch:
         frames = lib().scGetKernelTiming(self.h, ms.ctypes.data_as(_f), cnt.ctypes.data_as(_i))
         names = ("gs_solve", "ccd_broad_ee", "ccd_broad_vt", "colliders")
         return {n: (float(ms[k]), int(cnt[k])) for k, n in enumerate(names)}, int(frames)
+
+    def render(self, view_proj, width: int, height: int, light=(0.0, 2.0, 2.0), eye=(0.0, 1.0, 2.0),
+               kd=(0.8, 0.3, 0.3), ks=(0.2, 0.2, 0.2), shininess: float = 32.0, flip: float = 1.0,
+               background: float = 0.3, flags: int = 0, return_zbuf: bool = False):
+        """The current mesh drawn with the demo's Phong program into a CUDA tensor
+        (height, width, 4); with return_zbuf also the per-pixel (depth key << 32 |
+        triangle) words (int64, -1 where nothing was drawn)."""
+        import torch
+        vp = np.ascontiguousarray(view_proj, np.float32).reshape(16)
+        prm = np.array([*light, *eye, *kd, *ks, shininess, flip, background, flags], np.float32)
+        img = torch.empty((height, width, 4), dtype=torch.float32, device="cuda")
+        z = torch.empty((height, width), dtype=torch.int64, device="cuda")
+        rc = lib().scRenderCloth(self.h, _fp(vp), _fp(prm), int(width), int(height), img.data_ptr(), z.data_ptr())
+        if rc != 0:
+            _check("scRenderCloth")
+            raise RuntimeError(f"scRenderCloth: error {rc}")
+        return (img, z) if return_zbuf else img
 
     def mesh_buffers(self):
         L = lib()

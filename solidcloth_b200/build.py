@@ -18,7 +18,7 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 LIBDIR = PKG / "lib"
 LIB = LIBDIR / "libsolidcloth_b200.so"
-SOURCES = ["step_kernels.cu", "cloth.cu", "capi.cu", "noalloc.cu"]
+SOURCES = ["step_kernels.cu", "cloth.cu", "capi.cu", "noalloc.cu", "render.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "--extended-lambda",
          "-Xcompiler", "-fPIC,-ffp-contract=off,-fvisibility=hidden", "-ccbin", "g++"]
