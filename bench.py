@@ -409,7 +409,7 @@ def run_ours(args):
                     "sections": per,
                     "ccd_broad_vt_ms_per_launch": (sections["ccd_broad_vt"][0] / sections["ccd_broad_vt"][1]
                                                    if sections.get("ccd_broad_vt", (0, 0))[1] else None),
-                    "broad_phase_walk": {"chosen": ["per-query stack walk", "warp packet"][walk],
+                    "broad_phase_walk": {"chosen": p.model.BROAD_WALKS[walk],
                                          "tuned_ms": walk_ms.tolist()}}
 
     # plain versus learned warm start at the residual target (trained weights from

@@ -279,8 +279,9 @@ SCEXP int scGetSolverChoice(scModel model, int* out4, float* tuneMs, int cap);
 /* Continuous-collision broad phase walk (additions): 0 = one tree walk per query
    (lane), 1 = warp packets (32 neighbouring queries walk together, broadcast
    node loads), -1 (default) = timed at the first step and the faster kept. Same
-   candidate sets. scGetBroadPhaseMode returns the walk in use and, in ms2, the
-   tuned times of both (ms per substep's detection). */
+   candidate sets. Either walk stops a query at 128 candidates; those queries are
+   finished by a second pass, one warp per query. scGetBroadPhaseMode returns the
+   walk in use and, in ms2, the tuned times of both (ms per substep's detection). */
 SCEXP void scSetBroadPhaseMode(scModel model, int mode);
 SCEXP int scGetBroadPhaseMode(scModel model, float* ms2);
 /* info3 = {threads per CTA, FEM constraints per thread, bends per thread} per variant */

@@ -341,13 +341,15 @@ class ClothModel:
         n = lib().scGetSolverChoice(self.h, out.ctypes.data_as(_i), log.ctypes.data_as(_f), 64)
         return tuple(int(x) for x in out), log[:min(n, 64)].copy()
 
+    BROAD_WALKS = ("per-query stack walk", "warp packet")
+
     def set_broad_phase_mode(self, mode: int):
         """0 per-query walks, 1 warp packets, -1 tuned"""
         lib().scSetBroadPhaseMode(self.h, int(mode))
         _check("scSetBroadPhaseMode")
 
     def broad_phase_mode(self):
-        """(walk in use, tuned ms of [per-query, packet])"""
+        """(walk in use, tuned ms of each walk in BROAD_WALKS order)"""
         ms = np.zeros(2, np.float32)
         mode = lib().scGetBroadPhaseMode(self.h, ms.ctypes.data_as(_f))
         return int(mode), ms.copy()
@@ -542,7 +544,7 @@ class ClothPatch:
 
     def kernel_timing(self):
         """{section: (total ms, instances)} since the last read, and the frames covered"""
-        ms = np.zeros(4, np.float32)
+        ms = np.zeros(2, np.float32)
         cnt = np.zeros(4, np.int32)
         frames = lib().scGetKernelTiming(self.h, ms.ctypes.data_as(_f), cnt.ctypes.data_as(_i))
         names = ("gs_solve", "ccd_broad_ee", "ccd_broad_vt", "colliders")

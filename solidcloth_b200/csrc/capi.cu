@@ -686,9 +686,9 @@ int scGetSolverChoice(scModel m, int* out4, float* tuneMs, int cap)
 }
 void scSetBroadPhaseMode(scModel m, int mode)
 {
-    if (!M(m) || mode < -1 || mode > 1) { set_error(SC_ERR_ARG, "broad-phase mode must be -1, 0 or 1"); return; }
+    if (!M(m) || mode < -1 || mode >= BROAD_WALKS) { set_error(SC_ERR_ARG, "broad-phase mode must be -1, 0 or 1"); return; }
     M(m)->broadMode = mode;
-    if (mode >= 0) { M(m)->broadPacket = mode; M(m)->buf.broadPacket = mode; }
+    if (mode >= 0) { M(m)->broadWalk = mode; M(m)->buf.broadWalk = mode; }
     M(m)->tuned = false;
     M(m)->touch();
 }
@@ -696,8 +696,8 @@ void scSetBroadPhaseMode(scModel m, int mode)
 int scGetBroadPhaseMode(scModel m, float* ms2)
 {
     if (!M(m)) return -1;
-    if (ms2) { ms2[0] = M(m)->broadMs[0]; ms2[1] = M(m)->broadMs[1]; }
-    return M(m)->broadPacket;
+    if (ms2) for (int k = 0; k < BROAD_WALKS; k++) ms2[k] = M(m)->broadMs[k];
+    return M(m)->broadWalk;
 }
 
 int scGetGridVariants(int* info3, int cap)

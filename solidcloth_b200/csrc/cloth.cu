@@ -387,13 +387,15 @@ void LBVHHost::build(const std::vector<V3>& cen)
     for (int i = 0; i < n; i++) key[i] = {0u, order[i]};
     int next = 0;
     // iterative preorder build over (range, parent, is-right-child) jobs
-    struct Job { int lo, hi, par; bool right; };
-    std::vector<Job> jobs{{0, n, -1, false}};
+    struct Job { int lo, hi, par; bool right; int depth; };
+    std::vector<Job> jobs{{0, n, -1, false, 0}};
+    depth = 0;
     while (!jobs.empty())
     {
         Job j = jobs.back();
         jobs.pop_back();
         int node = next++;
+        depth = std::max(depth, j.depth);
         parent[node] = j.par;
         if (j.right && j.par >= 0) child[j.par] = node;
         if (j.hi - j.lo == 1)
@@ -405,8 +407,8 @@ void LBVHHost::build(const std::vector<V3>& cen)
         }
         int mid = (j.lo + j.hi) / 2;
         escape[node] = node + 2 * (j.hi - j.lo) - 1;     // subtree of k leaves has 2k-1 nodes
-        jobs.push_back({mid, j.hi, node, true});
-        jobs.push_back({j.lo, mid, node, false});
+        jobs.push_back({mid, j.hi, node, true, j.depth + 1});
+        jobs.push_back({j.lo, mid, node, false, j.depth + 1});
     }
     // children follow their parent in preorder, so a reverse sweep sees them first
     maxPrim.assign(numNodes, -1);
@@ -672,7 +674,7 @@ bool ClothModel::upload_topology(const HMesh& mesh)
     // BVH topologies from the rest shape
     // upload a built topology (h) with its node boxes' link words
     auto upload_bvh = [&](LBVHHost& h, DevBVH& out, const std::vector<int>* roots) -> bool {
-        out.numLeaves = h.numLeaves; out.numNodes = h.numNodes;
+        out.numLeaves = h.numLeaves; out.numNodes = h.numNodes; out.depth = h.depth;
         int* d = (int*)dalloc(sizeof(int) * (4 * (size_t)h.numNodes + h.numLeaves + 4));
         SC_CUDA(cudaMemcpy(d, h.child.data(), sizeof(int) * h.numNodes, cudaMemcpyHostToDevice));
         SC_CUDA(cudaMemcpy(d + h.numNodes, h.escape.data(), sizeof(int) * h.numNodes, cudaMemcpyHostToDevice));
@@ -725,6 +727,7 @@ bool ClothModel::upload_topology(const HMesh& mesh)
             for (int j = 0; j < np; j++) all.leafNode.push_back(h.leafNode[j] + o);
             all.numNodes += h.numNodes;
             all.numLeaves += h.numLeaves;
+            all.depth = std::max(all.depth, h.depth);
         }
         return upload_bvh(all, out, &roots);
     };
@@ -940,6 +943,10 @@ bool ClothModel::ensure_buffers(const CollisionWorld& world, cudaStream_t s)
     buf.ccdPoolCap = ccd ? std::max(buf.ccdEeCap, std::max(N, E) * KCCD / 2) : 1;
     buf.ccdPool = (int*)dalloc(sizeof(int) * (size_t)buf.ccdPoolCap, true);
     buf.ccdPoolUsed = counts + 6;
+    buf.ccdVtOvf = (int*)dalloc(sizeof(int) * (size_t)(ccd ? N : 1), true);
+    buf.ccdEeOvf = (int*)dalloc(sizeof(int) * (size_t)(ccd ? E : 1), true);
+    buf.ccdOvfN = (int*)dalloc(sizeof(int) * 2, true);
+    if (ccd) ccd_kernel_setup();
     // colouring
     buf.vmin = (unsigned long long*)dalloc(sizeof(unsigned long long) * N, true);
     SC_CUDA(cudaMemset(buf.vmin, 0xff, sizeof(unsigned long long) * N));
@@ -952,7 +959,7 @@ bool ClothModel::ensure_buffers(const CollisionWorld& world, cudaStream_t s)
     buf.scanOff = (int*)dalloc(sizeof(int) * (maxScan + 1), true);
     buf.scanBlock = (int*)dalloc(sizeof(int) * (maxScan / 1024 + 8), true);
     buf.scanBlock2 = (int*)dalloc(sizeof(int) * (maxScan / 1024 + 8), true);
-    buf.broadPacket = broadPacket;
+    buf.broadWalk = broadWalk;
     bufWorldVersion = world.version;
     bufFlags = prm.flags;
     bufCcd = ccd;
@@ -1502,8 +1509,8 @@ bool ClothPatch::autotune(float h)
             if (kv.first == key)
             {
                 m.choice = kv.second;
-                m.broadPacket = m.broadMode >= 0 ? m.broadMode : kv.second.broad;
-                m.buf.broadPacket = m.broadPacket;
+                m.broadWalk = m.broadMode >= 0 ? m.broadMode : kv.second.broad;
+                m.buf.broadWalk = m.broadWalk;
                 m.tuned = true;
                 return true;
             }
@@ -1570,13 +1577,13 @@ bool ClothPatch::autotune(float h)
     cudaFree(backup);
     m.tuneLog = cand;
     m.choice = best;
-    // continuous broad phase: per-lane walks or warp packets (same pair sets), timed
+    // continuous broad phase: the first-pass walks (BROAD_*; same pair sets), timed
     // on this cloth's current state (the detection changes no particle)
     if (m.prm.ccd && m.buf.ccdVtCnt)
     {
-        for (int mode = 0; mode < 2; mode++)
+        for (int mode = 0; mode < BROAD_WALKS; mode++)
         {
-            m.buf.broadPacket = mode;
+            m.buf.broadWalk = mode;
             m.broadMs[mode] = 1e30f;
             cudaGraph_t g = nullptr;
             cudaGraphExec_t ge = nullptr;
@@ -1599,11 +1606,13 @@ bool ClothPatch::autotune(float h)
             cudaGetLastError();
             cudaGraphExecDestroy(ge);
         }
-        m.broadPacket = m.broadMs[1] < m.broadMs[0] ? 1 : 0;
+        m.broadWalk = 0;
+        for (int mode = 1; mode < BROAD_WALKS; mode++)
+            if (m.broadMs[mode] < m.broadMs[m.broadWalk]) m.broadWalk = mode;
     }
-    if (m.broadMode >= 0) m.broadPacket = m.broadMode;
-    m.buf.broadPacket = m.broadPacket;
-    best.broad = m.broadPacket;
+    if (m.broadMode >= 0) m.broadWalk = m.broadMode;
+    m.buf.broadWalk = m.broadWalk;
+    best.broad = m.broadWalk;
     m.choice = best;
     cudaEventDestroy(e0); cudaEventDestroy(e1);
     m.tuned = true;

@@ -114,7 +114,7 @@ struct FemHost { uint32_t i1, i2, i3; float du1, du2, dv1, dv2, det, invDet, lu0
 struct LBVHHost
 {
     std::vector<int> child, escape, parent, leafNode, maxPrim;
-    int numLeaves = 0, numNodes = 0;
+    int numLeaves = 0, numNodes = 0, depth = 0;
     void build(const std::vector<V3>& centroids);
 };
 
@@ -181,9 +181,9 @@ public:
     bool tuned = false;
     uint64_t tunedVersion = 0;
     std::vector<SolverChoice> tuneLog;          // candidates and their times of the last tuning
-    int broadPacket = 0;                        // tuned: continuous broad phase per warp packet
-    int broadMode = -1;                         // forced walk (0 per lane, 1 packets) or -1: tuned
-    float broadMs[2] = {0.f, 0.f};              // tuned times of the two broad-phase walks
+    int broadWalk = 0;                          // tuned: continuous broad phase first-pass walk (BROAD_*)
+    int broadMode = -1;                         // forced walk (BROAD_*) or -1: tuned
+    float broadMs[BROAD_WALKS] = {};            // tuned times of the broad-phase walks
     void colour_constraints();
     void touch() { paramVersion++; }
 };

@@ -9,6 +9,10 @@ constexpr int KCAND = 256;     // BVH candidates kept per proximity query
 constexpr int KRES = 96;       // distinct features tracked per vertex for the dedup
 constexpr int KADJ = 16;       // adjacent primitives held in registers by a broad-phase query
 constexpr int KCCD = 128;      // continuous-collision candidates kept in a query's own slots
+// second broad-phase pass: warps per block, blocks, stack entries per depth level
+constexpr int CCD_COOP_THREADS = 128, CCD_COOP_BLOCKS = 4 * 148, CCD_COOP_GROUP = 64;
+// first-pass walks: one query per lane, or warp packets
+enum { BROAD_LANE = 0, BROAD_PACKET = 1, BROAD_WALKS = 2 };
 constexpr int CCD_VT_PAIRS = 128, CCD_EE_PAIRS = 96; // pair store per vertex / edge
 constexpr int CCD_VT_HITS = 32, CCD_EE_HITS = 16;   // continuous contacts per vertex / edge
 constexpr int MAX_COLOURS = 128; // independent-set colouring rounds per contact class
@@ -46,7 +50,7 @@ struct Buffers
     int numVColl;
     const VColl* vcoll;       // device copy
     const int2* instColl;     // batch: (first collider, count) per instance; null: all colliders act on all
-    int broadPacket;          // 1: continuous broad phase walks the tree per warp packet (tuned)
+    int broadWalk;            // continuous broad phase first-pass walk (BROAD_*, tuned)
     // triangle / edge contacts: per-collider slot arrays, flags, dense lists
     TC* tcSlot; int* tcFlag; TC* tcList; int* tcCount; int tcCap;
     EC* ecSlot; int* ecFlag; EC* ecList; int* ecCount; int ecCap;
@@ -61,6 +65,7 @@ struct Buffers
     int* ccdVtHitCnt; int* ccdEeHitCnt;    // hits per query
     int* ccdPool; int ccdPoolCap; int* ccdPoolUsed;  // candidate lists longer than KCCD
     int* ccdVtPoolOff; int* ccdEePoolOff;
+    int* ccdVtOvf; int* ccdEeOvf; int* ccdOvfN;      // queries with more than KCCD candidates; counts (vt, ee)
     // colouring scratch
     unsigned long long* vmin;  // N, kept at ~0
     int* colour; int* order; int* colourStart; int colourCap;
@@ -85,6 +90,8 @@ void launch_solve_vertex_contacts(cudaStream_t s, const DevCloth& c, const Solve
 void launch_solve_multi_contacts(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b, int iter);
 void launch_colour_contacts(cudaStream_t s, const DevCloth& c, const Buffers& b);
 void launch_bvh_refit(cudaStream_t s, const DevBVH& bvh, const DevCloth& c, int kind, float tol);
+size_t ccd_coop_smem(int depth);      // dynamic shared memory of the second broad-phase pass
+void ccd_kernel_setup();              // kernel attributes (once per device, outside capture)
 void launch_self_proximity(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b,
                            const DevBVH& triBvh, const DevBVH& edgeBvh);
 // swept-tree refits + continuous-collision broad and narrow phases; the

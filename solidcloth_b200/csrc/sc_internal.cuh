@@ -83,6 +83,7 @@ struct DevCloth
 struct DevBVH
 {
     int numLeaves, numNodes;
+    int depth;              // largest number of edges from a root to a leaf
     const int* child;       // numNodes: internal -> right child index; leaf -> ~primitive
     const int* escape;      // numNodes: preorder index after the subtree
     const int* parent;      // numNodes (root -1)

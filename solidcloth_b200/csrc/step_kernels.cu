@@ -1428,9 +1428,11 @@ __device__ __forceinline__ void bvh_query(const DevBVH& t, const Box& q, F&& f, 
 // stack: the dependent-load chain is the number of entered internal nodes, about
 // a third of the stackless walk's. Reports the same leaf set as bvh_query, in a
 // different order. A median-split tree over n < 2^31 leaves is at most 31 deep,
-// so the 32-entry stack cannot overflow.
+// so the 32-entry stack cannot overflow. A walk ends early once *stop is set
+// (by f).
 template <typename F>
-__device__ __forceinline__ void bvh_query2(const DevBVH& t, const Box& q, bool active, F&& f, int above = -1, int root = 0)
+__device__ __forceinline__ void bvh_query2(const DevBVH& t, const Box& q, bool active, F&& f, int above = -1, int root = 0,
+                                           const bool* stop = nullptr)
 {
     if (!active || t.numNodes == 0) return;
     auto over = [&](const float4& lo, const float4& hi) {
@@ -1442,7 +1444,7 @@ __device__ __forceinline__ void bvh_query2(const DevBVH& t, const Box& q, bool a
     int stack[32];
     int sp = 0;
     int node = root, ch = __float_as_int(rlo.w);
-    while (true)
+    while (!(stop && *stop))
     {
         const int L = node + 1, R = ch;
         const float4 loL = __ldg(&t.lo[L]), hiL = __ldg(&t.hi[L]), loR = __ldg(&t.lo[R]), hiR = __ldg(&t.hi[R]);
@@ -1477,15 +1479,17 @@ __device__ __forceinline__ void bvh_query2(const DevBVH& t, const Box& q, bool a
 // node load is one broadcast request instead of up to 32 scattered ones, at the
 // price of visiting the union of the lanes' nodes. Each lane reports exactly its
 // own leaves. All 32 lanes must call it; a warp whose lanes start in different
-// trees (a batch instance boundary) takes the per-lane walk.
+// trees (a batch instance boundary) takes the per-lane walk. A lane whose *stop
+// is set (by f) stops reporting and no longer steers the walk.
 template <typename F>
-__device__ __forceinline__ void bvh_query2_warp(const DevBVH& t, const Box& q, bool active, F&& f, int above, int root)
+__device__ __forceinline__ void bvh_query2_warp(const DevBVH& t, const Box& q, bool active, F&& f, int above, int root,
+                                                const bool* stop = nullptr)
 {
     const unsigned full = 0xffffffffu;
     const unsigned act = __ballot_sync(full, active);
     if (!act) return;
     const int r0 = __shfl_sync(full, root, __ffs(act) - 1);
-    if (!__all_sync(full, !active || root == r0)) { bvh_query2(t, q, active, f, above, root); return; }
+    if (!__all_sync(full, !active || root == r0)) { bvh_query2(t, q, active, f, above, root, stop); return; }
     auto over = [&](const float4& lo, const float4& hi) {
         return !(hi.x < q.lo.x || hi.y < q.lo.y || hi.z < q.lo.z || q.hi.x < lo.x || q.hi.y < lo.y || q.hi.z < lo.z);
     };
@@ -1500,7 +1504,8 @@ __device__ __forceinline__ void bvh_query2_warp(const DevBVH& t, const Box& q, b
     {
         const int L = node + 1, R = ch;
         const float4 loL = __ldg(&t.lo[L]), hiL = __ldg(&t.hi[L]), loR = __ldg(&t.lo[R]), hiR = __ldg(&t.hi[R]);
-        bool oL = active && over(loL, hiL), oR = active && over(loR, hiR);
+        const bool live = active && !(stop && *stop);
+        bool oL = live && over(loL, hiL), oR = live && over(loR, hiR);
         if (above >= 0)
         {
             const int mL = __ldg(&t.maxPrim[L]), mR = __ldg(&t.maxPrim[R]);
@@ -1524,6 +1529,81 @@ __device__ __forceinline__ void bvh_query2_warp(const DevBVH& t, const Box& q, b
             ch = __float_as_int(__ldg(&t.lo[node]).w);
         }
     }
+}
+
+// Cooperative walk of ONE query box by a group of W lanes (W a power of two up
+// to 32; every lane of the group holds the same box), for queries with long candidate
+// lists: each step the group takes up to W entered nodes from its stack, each
+// lane tests both children of its node (one round trip), and the entered
+// internal children are pushed as a new group. Only the top group is ever
+// popped, so group g holds nodes of depth g exactly: at most depth groups of at
+// most 2W entries, the bound the caller sizes the stack by (int2: node, its
+// right child). f(a, b) is called by all lanes of the group once per step with
+// the lane's overlapping leaves (-1 for none) and returns false to end the walk
+// (uniformly across the group). The leaf set is bvh_query2's.
+template <int W, typename F>
+__device__ __forceinline__ void bvh_query_coop(const DevBVH& t, const Box& q, int above, int root, int2* stack, int cap,
+                                               int* groups, int gcap, int* status, F&& f)
+{
+    const int lane = threadIdx.x & 31, sl = lane & (W - 1);
+    const unsigned mask = W == 32 ? 0xffffffffu : (((1u << W) - 1u) << (lane & ~(W - 1)));
+    const unsigned lt = (1u << lane) - 1u;
+    auto over = [&](const float4& lo, const float4& hi) {
+        return !(hi.x < q.lo.x || hi.y < q.lo.y || hi.z < q.lo.z || q.hi.x < lo.x || q.hi.y < lo.y || q.hi.z < lo.z);
+    };
+    const float4 rlo = __ldg(&t.lo[root]), rhi = __ldg(&t.hi[root]);
+    if (!over(rlo, rhi) || (above >= 0 && __ldg(&t.maxPrim[root]) <= above)) return;
+    const int rch = __float_as_int(rlo.w);
+    if (rch < 0) { f(sl == 0 ? ~rch : -1, -1); return; }
+    if (sl == 0) { stack[0] = make_int2(root, rch); groups[0] = 1; }
+    int sp = 1, m = 1;
+    __syncwarp(mask);
+    while (m > 0)
+    {
+        const int g = groups[m - 1];
+        const int take = min(g, W);
+        const int2 nd = sl < take ? stack[sp - 1 - sl] : make_int2(-1, 0);
+        __syncwarp(mask);
+        sp -= take;
+        int leafA = -1, leafB = -1, cL = 0, cR = 0;
+        bool pushL = false, pushR = false;
+        const int L = nd.x + 1, R = nd.y;
+        if (nd.x >= 0)
+        {
+            const float4 loL = __ldg(&t.lo[L]), hiL = __ldg(&t.hi[L]), loR = __ldg(&t.lo[R]), hiR = __ldg(&t.hi[R]);
+            bool oL = over(loL, hiL), oR = over(loR, hiR);
+            if (above >= 0)
+            {
+                oL = oL && __ldg(&t.maxPrim[L]) > above;
+                oR = oR && __ldg(&t.maxPrim[R]) > above;
+            }
+            cL = __float_as_int(loL.w);
+            cR = __float_as_int(loR.w);
+            if (oL) { if (cL < 0) leafA = ~cL; else pushL = true; }
+            if (oR) { if (cR < 0) leafB = ~cR; else pushR = true; }
+        }
+        if (!f(leafA, leafB)) break;
+        const unsigned bl = __ballot_sync(mask, pushL), br = __ballot_sync(mask, pushR);
+        const int nl = __popc(bl), cnt = nl + __popc(br);
+        if (g == take) m--;
+        else if (sl == 0) groups[m - 1] = g - take;
+        if (cnt > 0)
+        {
+            if (sp + cnt > cap || m >= gcap)
+            {
+                // unreachable for a tree of the stated depth; recorded, never written out of bounds
+                if (sl == 0) atomicOr(status, ST_CCD_OVERFLOW);
+                break;
+            }
+            if (pushL) stack[sp + __popc(bl & lt)] = make_int2(L, cL);
+            if (pushR) stack[sp + nl + __popc(br & lt)] = make_int2(R, cR);
+            if (sl == 0) groups[m] = cnt;
+            sp += cnt;
+            m++;
+        }
+        __syncwarp(mask);
+    }
+    __syncwarp(mask);
 }
 
 // tree root for a query on particle v: its instance's tree in a batch
@@ -1764,115 +1844,214 @@ __global__ void __launch_bounds__(128) k_self_ee(DevCloth c, SolverParams P, Buf
 // Broad phase: every (triangle, vertex) and (edge, edge) pair whose swept boxes
 // overlap, with the Midphase's filters (vertex not on the triangle and not
 // pinned; edges sharing no vertex), Physics/SelfCollisionDetector.cpp:60-135,
-// but over all pairs rather than same-leaf pairs only. Per-query candidate
-// lists are sorted so the pair list order is canonical: (vertex, triangle)
-// and (edge, higher edge).
-// Two passes, both through these kernels: the first keeps up to KCCD candidates
-// in the query's own slots and counts all of them; the second (pool = true) runs
-// only the queries that had more, storing their full lists in a shared pool.
-// Lists stay in traversal order: only the (rare) hits are put in candidate order.
-__device__ __forceinline__ int* ccd_pool_alloc(const Buffers& b, int m, int* poolOff, int* status)
+// but over all pairs rather than same-leaf pairs only. Pairs are listed per
+// query: (vertex, triangle) and (edge, higher edge).
+// Two passes: the first walks one query per thread and keeps up to KCCD
+// candidates in the query's own slots; the queries that find more go to a list
+// that the second pass walks one query per warp, storing the full lists in a
+// shared pool. Lists stay in traversal order: only the (rare) hits are put in
+// candidate order.
+// A vertex query: its swept box and the triangles incident to it (held in
+// registers, so a reported leaf costs no load).
+struct VtQuery
 {
-    const int base = atomicAdd(b.ccdPoolUsed, m);
-    if (base + m > b.ccdPoolCap)
-    {
-        atomicOr(status, ST_CCD_OVERFLOW);
-        *poolOff = -1;
-        return nullptr;
-    }
-    *poolOff = base;
-    return b.ccdPool + base;
-}
-
-__global__ void __launch_bounds__(128) k_ccd_broad_vt(DevCloth c, SolverParams P, Buffers b, DevBVH tb, float tol, bool pool)
-{
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g - (int)(threadIdx.x & 31) >= c.N) return;          // whole warp past the end
-    const int i = g < c.N ? c.vQuery[g] : 0;
-    bool active = g < c.N;
-    if (active && !pool) b.ccdVtCnt[i] = 0;
-    if (active && pool && b.ccdVtCnt[i] <= KCCD) active = false;
-    float4 p4 = c.pos[i];
-    if (p4.w == 0.f) active = false;
-    Box vb = Box::empty(); vb.add(ld3(c.prev, i)); vb.add(mk(p4.x, p4.y, p4.z)); vb.extrude(tol);
-    int* out = b.ccdVtCand + (size_t)i * KCCD;
-    int n = 0;
-    if (active && pool)
-    {
-        // second pass for a query with more than KCCD candidates: all of them into the pool
-        out = ccd_pool_alloc(b, b.ccdVtCnt[i], b.ccdVtPoolOff + i, c.status);
-        if (!out) { b.ccdVtCnt[i] = 0; active = false; }
-    }
-    // triangles incident to i, held in registers (no load per reported leaf)
+    int i, nInc;
+    bool pinned;
+    Box box;
     int inc[KADJ];
-    const int r0 = c.vTriStart[i], nInc = c.vTriStart[i + 1] - r0;
+    __device__ __forceinline__ void init(const DevCloth& c, int v, float tol)
+    {
+        i = v;
+        const float4 p4 = c.pos[v];
+        pinned = p4.w == 0.f;
+        box = Box::empty(); box.add(ld3(c.prev, v)); box.add(mk(p4.x, p4.y, p4.z)); box.extrude(tol);
+        const int r0 = c.vTriStart[v];
+        nInc = c.vTriStart[v + 1] - r0;
 #pragma unroll
-    for (int k = 0; k < KADJ; k++) inc[k] = k < nInc ? c.vTri[r0 + k].x : -1;
-    auto emitT = [&](int t) {
+        for (int k = 0; k < KADJ; k++) inc[k] = k < nInc ? c.vTri[r0 + k].x : -1;
+    }
+    __device__ __forceinline__ bool accept(const DevCloth& c, int t) const
+    {
         if (nInc <= KADJ)
         {
             bool adj = false;
 #pragma unroll
             for (int k = 0; k < KADJ; k++) adj |= inc[k] == t;
-            if (adj) return;
+            return !adj;
         }
-        else if ((int)c.tri[3 * t] == i || (int)c.tri[3 * t + 1] == i || (int)c.tri[3 * t + 2] == i) return;
-        if (pool || n < KCCD) out[n] = t;
-        n++;
-    };
-    if (b.broadPacket) bvh_query2_warp(tb, vb, active, emitT, -1, tree_root(c, tb, i));
-    else bvh_query2(tb, vb, active, emitT, -1, tree_root(c, tb, i));
-    if (!active) return;
-    b.ccdVtCnt[i] = n;
-}
-
-__global__ void __launch_bounds__(128) k_ccd_broad_ee(DevCloth c, SolverParams P, Buffers b, DevBVH eb, float tol, bool pool)
-{
-    const int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g - (int)(threadIdx.x & 31) >= c.E) return;
-    const int i = g < c.E ? c.eQuery[g] : 0;
-    bool active = g < c.E;
-    if (active && pool && b.ccdEeCnt[i] <= KCCD) active = false;
-    int* out = b.ccdEeCand + (size_t)i * KCCD;
-    if (active && pool)
-    {
-        out = ccd_pool_alloc(b, b.ccdEeCnt[i], b.ccdEePoolOff + i, c.status);
-        if (!out) { b.ccdEeCnt[i] = 0; active = false; }
+        return !((int)c.tri[3 * t] == i || (int)c.tri[3 * t + 1] == i || (int)c.tri[3 * t + 2] == i);
     }
-    const int4 e1 = c.edge[i];
-    Box qb = Box::empty();
-    qb.add(ld3(c.pos, e1.x)); qb.add(ld3(c.pos, e1.y)); qb.add(ld3(c.prev, e1.x)); qb.add(ld3(c.prev, e1.y));
-    qb.extrude(tol);
-    int n = 0;
-    // edges sharing a vertex with e1 (both vertices' edge rings), in registers
+};
+
+// An edge query: its swept box and the edges sharing one of its vertices (both
+// vertices' edge rings, in registers when they fit).
+struct EeQuery
+{
+    int i;
+    int4 e1;
+    bool inRegs;
+    Box box;
     int adjE[KADJ];
-    const int a0 = c.eRingStart[e1.x], na = c.eRingStart[e1.x + 1] - a0;
-    const int b0 = c.eRingStart[e1.y], nb = c.eRingStart[e1.y + 1] - b0;
-    const bool inRegs = na + nb <= KADJ;
+    __device__ __forceinline__ void init(const DevCloth& c, int e, float tol)
+    {
+        i = e;
+        e1 = c.edge[e];
+        box = Box::empty();
+        box.add(ld3(c.pos, e1.x)); box.add(ld3(c.pos, e1.y)); box.add(ld3(c.prev, e1.x)); box.add(ld3(c.prev, e1.y));
+        box.extrude(tol);
+        const int a0 = c.eRingStart[e1.x], na = c.eRingStart[e1.x + 1] - a0;
+        const int b0 = c.eRingStart[e1.y], nb = c.eRingStart[e1.y + 1] - b0;
+        inRegs = na + nb <= KADJ;
 #pragma unroll
-    for (int k = 0; k < KADJ; k++)
-        adjE[k] = !inRegs ? -1 : k < na ? c.eRing[a0 + k] : k < na + nb ? c.eRing[b0 + k - na] : -1;
-    auto emitE = [&](int e) {
-        if (e <= i) return;
+        for (int k = 0; k < KADJ; k++)
+            adjE[k] = !inRegs ? -1 : k < na ? c.eRing[a0 + k] : k < na + nb ? c.eRing[b0 + k - na] : -1;
+    }
+    __device__ __forceinline__ bool accept(const DevCloth& c, int e) const
+    {
+        if (e <= i) return false;
         if (inRegs)
         {
             bool adj = false;
 #pragma unroll
             for (int k = 0; k < KADJ; k++) adj |= adjE[k] == e;
-            if (adj) return;
+            return !adj;
         }
-        else
-        {
-            int4 e2 = c.edge[e];
-            if (e1.x == e2.x || e1.y == e2.y || e1.x == e2.y || e1.y == e2.x) return;
-        }
-        if (pool || n < KCCD) out[n] = e;
-        n++;
+        const int4 e2 = c.edge[e];
+        return !(e1.x == e2.x || e1.y == e2.y || e1.x == e2.y || e1.y == e2.x);
+    }
+};
+
+// First pass: one query per thread (or per lane of a warp packet), at most KCCD
+// candidates into the query's own slots. A query that finds more stops walking,
+// keeps a count above KCCD and joins the overflow list for the second pass.
+__global__ void __launch_bounds__(128) k_ccd_broad_vt(DevCloth c, SolverParams P, Buffers b, DevBVH tb, float tol)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g - (int)(threadIdx.x & 31) >= c.N) return;          // whole warp past the end
+    const int i = g < c.N ? c.vQuery[g] : 0;
+    bool active = g < c.N;
+    if (active) b.ccdVtCnt[i] = 0;
+    VtQuery Q;
+    Q.init(c, i, tol);
+    if (Q.pinned) active = false;
+    int* out = b.ccdVtCand + (size_t)i * KCCD;
+    int n = 0;
+    bool stop = false;
+    auto emitT = [&](int t) {
+        if (!Q.accept(c, t)) return;
+        if (n < KCCD) out[n] = t;
+        if (++n > KCCD) stop = true;
     };
-    if (b.broadPacket) bvh_query2_warp(eb, qb, active, emitE, i, tree_root(c, eb, e1.x));
-    else bvh_query2(eb, qb, active, emitE, i, tree_root(c, eb, e1.x));
+    if (b.broadWalk == BROAD_PACKET) bvh_query2_warp(tb, Q.box, active, emitT, -1, tree_root(c, tb, i), &stop);
+    else bvh_query2(tb, Q.box, active, emitT, -1, tree_root(c, tb, i), &stop);
+    if (!active) return;
+    b.ccdVtCnt[i] = n;
+    if (n > KCCD) b.ccdVtOvf[atomicAdd(b.ccdOvfN, 1)] = i;
+}
+
+__global__ void __launch_bounds__(128) k_ccd_broad_ee(DevCloth c, SolverParams P, Buffers b, DevBVH eb, float tol)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g - (int)(threadIdx.x & 31) >= c.E) return;
+    const int i = g < c.E ? c.eQuery[g] : 0;
+    const bool active = g < c.E;
+    EeQuery Q;
+    Q.init(c, i, tol);
+    int* out = b.ccdEeCand + (size_t)i * KCCD;
+    int n = 0;
+    bool stop = false;
+    auto emitE = [&](int e) {
+        if (!Q.accept(c, e)) return;
+        if (n < KCCD) out[n] = e;
+        if (++n > KCCD) stop = true;
+    };
+    if (b.broadWalk == BROAD_PACKET) bvh_query2_warp(eb, Q.box, active, emitE, i, tree_root(c, eb, Q.e1.x), &stop);
+    else bvh_query2(eb, Q.box, active, emitE, i, tree_root(c, eb, Q.e1.x), &stop);
     if (!active) return;
     b.ccdEeCnt[i] = n;
+    if (n > KCCD) b.ccdEeOvf[atomicAdd(b.ccdOvfN + 1, 1)] = i;
+}
+
+// Second pass over the overflow list: one warp per query walks the tree
+// cooperatively (bvh_query_coop) twice, counting its candidates, then writing
+// them into a pool block of exactly that size. The lane order of a step and the
+// step order are fixed, so each list (and the pair list) is deterministic.
+template <bool VT>
+__global__ void __launch_bounds__(CCD_COOP_THREADS) k_ccd_broad_coop(DevCloth c, SolverParams P, Buffers b, DevBVH t, float tol)
+{
+    extern __shared__ int2 sCoop[];
+    const unsigned full = 0xffffffffu;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const int cap = CCD_COOP_GROUP * (t.depth + 1), gcap = t.depth + 2;
+    int2* stack = sCoop + warp * (cap + (gcap + 1) / 2);
+    int* groups = reinterpret_cast<int*>(stack + cap);
+    const int nOvf = b.ccdOvfN[VT ? 0 : 1];
+    const int* ovf = VT ? b.ccdVtOvf : b.ccdEeOvf;
+    int* cnt = VT ? b.ccdVtCnt : b.ccdEeCnt;
+    int* poolOff = VT ? b.ccdVtPoolOff : b.ccdEePoolOff;
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    for (int w = blockIdx.x * (blockDim.x >> 5) + warp; w < nOvf; w += warps)
+    {
+        const int i = ovf[w];
+        VtQuery qv;
+        EeQuery qe;
+        int root, above;
+        Box box;
+        if (VT) { qv.init(c, i, tol); box = qv.box; root = tree_root(c, t, i); above = -1; }
+        else { qe.init(c, i, tol); box = qe.box; root = tree_root(c, t, qe.e1.x); above = i; }
+        auto ok = [&](int leaf) { return leaf >= 0 && (VT ? qv.accept(c, leaf) : qe.accept(c, leaf)); };
+        int total = 0;
+        bvh_query_coop<32>(t, box, above, root, stack, cap, groups, gcap, c.status, [&](int la, int lb) {
+            total += __popc(__ballot_sync(full, ok(la))) + __popc(__ballot_sync(full, ok(lb)));
+            return true;
+        });
+        int base = 0;
+        if (lane == 0)
+        {
+            base = atomicAdd(b.ccdPoolUsed, total);
+            if (base + total > b.ccdPoolCap) { atomicOr(c.status, ST_CCD_OVERFLOW); base = -1; }
+        }
+        base = __shfl_sync(full, base, 0);
+        if (base < 0)
+        {
+            if (lane == 0) cnt[i] = 0;
+            continue;
+        }
+        int* out = b.ccdPool + base;
+        int pos = 0;
+        bvh_query_coop<32>(t, box, above, root, stack, cap, groups, gcap, c.status, [&](int la, int lb) {
+            const bool ka = ok(la), kb = ok(lb);
+            const unsigned ba = __ballot_sync(full, ka), bb = __ballot_sync(full, kb);
+            if (ka) out[pos + __popc(ba & lt)] = la;
+            if (kb) out[pos + __popc(ba) + __popc(bb & lt)] = lb;
+            pos += __popc(ba) + __popc(bb);
+            return true;
+        });
+        if (lane == 0) { cnt[i] = total; poolOff[i] = base; }
+        __syncwarp();
+    }
+}
+
+size_t ccd_coop_smem(int depth)
+{
+    const int cap = CCD_COOP_GROUP * (depth + 1), gcap = depth + 2;
+    return sizeof(int2) * (size_t)(cap + (gcap + 1) / 2) * (CCD_COOP_THREADS / 32);
+}
+
+void ccd_kernel_setup()
+{
+    cudaFuncSetAttribute(k_ccd_broad_coop<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ccd_coop_smem(40));
+    cudaFuncSetAttribute(k_ccd_broad_coop<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ccd_coop_smem(40));
+}
+
+// first pass in the walk the model uses (BROAD_* in launch.h)
+static void launch_broad_pass1(cudaStream_t s, bool vt, const DevCloth& c, const SolverParams& P, const Buffers& b,
+                               const DevBVH& t, float tol)
+{
+    const int n = vt ? c.N : c.E;
+    if (vt) k_ccd_broad_vt<<<blocks_for(n, 128), 128, 0, s>>>(c, P, b, t, tol);
+    else k_ccd_broad_ee<<<blocks_for(n, 128), 128, 0, s>>>(c, P, b, t, tol);
 }
 
 // expand per-query candidate lists (own slots, or the pool for long lists)
@@ -2881,12 +3060,13 @@ void launch_ccd(cudaStream_t s, cudaStream_t side, cudaEvent_t fork, cudaEvent_t
     // only part of the GPU. They share nothing but the pool counter (atomic).
     const float tol = P.thickness + P.tolerance * 0.5f;
     cudaMemsetAsync(b.ccdPoolUsed, 0, sizeof(int), s);
+    cudaMemsetAsync(b.ccdOvfN, 0, 2 * sizeof(int), s);
     cudaEventRecord(fork, s);
     cudaStreamWaitEvent(side, fork, 0);
     launch_bvh_refit(side, triBvh, c, 2, tol);
     mark(2, side);
-    for (bool pool : {false, true})
-        k_ccd_broad_vt<<<blocks_for(c.N, 128), 128, 0, side>>>(c, P, b, triBvh, tol, pool);
+    launch_broad_pass1(side, true, c, P, b, triBvh, tol);
+    k_ccd_broad_coop<true><<<CCD_COOP_BLOCKS, CCD_COOP_THREADS, ccd_coop_smem(triBvh.depth), side>>>(c, P, b, triBvh, tol);
     mark(3, side);
     scan_ints(side, b.ccdVtCnt, b.ccdVtOff, c.N, b.ccdVtPairCount, b.scanBlock2);
     k_ccd_pairs<<<blocks_for(32 * c.N), 256, 0, side>>>(b.ccdVtCnt, b.ccdVtOff, b.ccdVtCand, b.ccdPool, b.ccdVtPoolOff, c.N,
@@ -2896,8 +3076,8 @@ void launch_ccd(cudaStream_t s, cudaStream_t side, cudaEvent_t fork, cudaEvent_t
 
     launch_bvh_refit(s, edgeBvh, c, 3, tol);
     mark(0, s);
-    for (bool pool : {false, true})
-        k_ccd_broad_ee<<<blocks_for(c.E, 128), 128, 0, s>>>(c, P, b, edgeBvh, tol, pool);
+    launch_broad_pass1(s, false, c, P, b, edgeBvh, tol);
+    k_ccd_broad_coop<false><<<CCD_COOP_BLOCKS, CCD_COOP_THREADS, ccd_coop_smem(edgeBvh.depth), s>>>(c, P, b, edgeBvh, tol);
     mark(1, s);
     scan_ints(s, b.ccdEeCnt, b.ccdEeOff, c.E, b.ccdEePairCount, b.scanBlock);
     k_ccd_pairs<<<blocks_for(32 * c.E), 256, 0, s>>>(b.ccdEeCnt, b.ccdEeOff, b.ccdEeCand, b.ccdPool, b.ccdEePoolOff, c.E,

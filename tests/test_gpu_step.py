@@ -166,17 +166,17 @@ def test_self_check_mode_trajectory():
 
 
 @pytest.mark.parametrize("walk", [0, 1])
-@pytest.mark.parametrize("thickness", [0.5, 1.5])
+@pytest.mark.parametrize("thickness", [0.5, 1.5, 3.0])
 def test_ccd_broadphase_and_hits_bitexact(thickness, walk):
     """Candidate pair sets and hit lists of the continuous detector are bit-exact,
-    with either tree walk (per query, or per warp packet).
-    At thickness 1.5 (boxes two grid cells wide around each edge, two layers)
-    edge queries have more candidates than their own 64 slots hold and take the
-    overflow-pool pass."""
+    with either first-pass walk (per query, or per warp packet). At thickness 3
+    (boxes several grid cells wide around each edge, two layers) queries have
+    more candidates than their own 128 slots hold and are finished by the
+    second, one-warp-per-query pass."""
     sc, state = scenes.ccd_scene(16)
     sc.params.thickness = thickness
     w, p, o = _pair(sc, ccd=True, state=state)
-    p.model.set_broad_phase_mode(walk)            # per-query walks or warp packets
+    p.model.set_broad_phase_mode(walk)
     p.step(sc.dt)
     # broad phase: all-pairs overlap set of the oracle from the same predicted state
     o2 = __import__("oracle.bridge", fromlist=["PortCloth"]).PortCloth.from_scene(sc)
@@ -195,6 +195,8 @@ def test_ccd_broadphase_and_hits_bitexact(thickness, walk):
     most = max(np.bincount(gvt[:, 0]).max(), np.bincount(gee[:, 0]).max())
     if thickness > 1.0:
         assert most > 64
+    if thickness > 2.0:
+        assert most > 128
     assert p.status() & 4 == 0
     if p.status() & ~16:
         return   # proximity slots overflowed at this thickness; the pair sets were the point
