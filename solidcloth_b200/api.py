@@ -544,7 +544,7 @@ class ClothPatch:
 
     def kernel_timing(self):
         """{section: (total ms, instances)} since the last read, and the frames covered"""
-        ms = np.zeros(2, np.float32)
+        ms = np.zeros(4, np.float32)
         cnt = np.zeros(4, np.int32)
         frames = lib().scGetKernelTiming(self.h, ms.ctypes.data_as(_f), cnt.ctypes.data_as(_i))
         names = ("gs_solve", "ccd_broad_ee", "ccd_broad_vt", "colliders")

@@ -14,6 +14,7 @@
 // by a few ulp (bend angles, angle-weighted normals).
 #include "launch.h"
 #include <cooperative_groups.h>
+#include <cuda/atomic>
 #include <cstdio>
 #include <climits>
 
@@ -1373,7 +1374,11 @@ __device__ __forceinline__ Box leaf_box(const DevCloth& c, int kind, int prim, f
 }
 
 // Bottom-up refit with one atomic per internal node: the second child to
-// arrive builds the parent's box and continues upwards (no waiting).
+// arrive builds the parent's box and continues upwards (no waiting). The
+// atomic is acquire-release (it publishes this thread's box and makes the
+// sibling's visible), the arriving thread keeps its own box in registers and
+// loads only the sibling's, and it puts the counter back to zero for the next
+// refit (counters start at zero when the tree is allocated).
 __global__ void k_bvh_refit(DevBVH t, DevCloth c, int kind, float tol)
 {
     int prim = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1382,18 +1387,25 @@ __global__ void k_bvh_refit(DevBVH t, DevCloth c, int kind, float tol)
     Box b = leaf_box(c, kind, prim, tol);
     t.lo[node] = f4(b.lo, __int_as_float(~prim));
     t.hi[node] = f4(b.hi, __int_as_float(node + 1));
-    __threadfence();
     int p = t.parent[node];
     while (p >= 0)
     {
-        if (atomicAdd(&t.visit[p], 1) == 0) return;
-        __threadfence();
-        int l = p + 1, r = t.child[p];
-        float4 al = __ldcg(&t.lo[l]), ar = __ldcg(&t.lo[r]), bl = __ldcg(&t.hi[l]), br = __ldcg(&t.hi[r]);
-        V3 lo = vmin(mk(al.x, al.y, al.z), mk(ar.x, ar.y, ar.z)), hi = vmax(mk(bl.x, bl.y, bl.z), mk(br.x, br.y, br.z));
-        t.lo[p] = f4(lo, __int_as_float(r));
-        t.hi[p] = f4(hi, __int_as_float(t.escape[p]));
-        __threadfence();
+        cuda::atomic_ref<int, cuda::thread_scope_device> visit(t.visit[p]);
+        if (visit.fetch_add(1, cuda::memory_order_acq_rel) == 0) return;
+        visit.store(0, cuda::memory_order_relaxed);
+        const int l = p + 1, r = t.child[p];
+        const int sib = node == l ? r : l;
+        const float4 sl = __ldcg(&t.lo[sib]), sh = __ldcg(&t.hi[sib]);
+        const Box o = {mk(sl.x, sl.y, sl.z), mk(sh.x, sh.y, sh.z)};
+        const Box& L = node == l ? b : o;
+        const Box& R = node == l ? o : b;
+        Box m;
+        m.lo = vmin(L.lo, R.lo);
+        m.hi = vmax(L.hi, R.hi);
+        b = m;
+        t.lo[p] = f4(b.lo, __int_as_float(r));
+        t.hi[p] = f4(b.hi, __int_as_float(t.escape[p]));
+        node = p;
         p = t.parent[p];
     }
 }
@@ -3012,7 +3024,6 @@ void launch_solve_multi_contacts(cudaStream_t s, const DevCloth& c, const Solver
 
 void launch_bvh_refit(cudaStream_t s, const DevBVH& t, const DevCloth& c, int kind, float tol)
 {
-    cudaMemsetAsync(t.visit, 0, sizeof(int) * t.numNodes, s);
     k_bvh_refit<<<blocks_for(t.numLeaves), 256, 0, s>>>(t, c, kind, tol);
 }
 
