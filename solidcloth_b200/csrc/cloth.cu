@@ -701,6 +701,22 @@ bool ClothModel::upload_topology(const HMesh& mesh)
         SC_CUDA(cudaMemcpy(out.lo, lo.data(), sizeof(float4) * h.numNodes, cudaMemcpyHostToDevice));
         SC_CUDA(cudaMemcpy(out.hi, hi.data(), sizeof(float4) * h.numNodes, cudaMemcpyHostToDevice));
         out.visit = (int*)dalloc(sizeof(int) * h.numNodes);
+        // child records: static link and maximum words (the refit fills the boxes)
+        std::vector<float4> rec(4 * (size_t)h.numNodes, make_float4(0.f, 0.f, 0.f, 0.f));
+        for (int k = 0; k < h.numNodes; k++)
+        {
+            if (h.child[k] < 0) continue;
+            const int side[2] = {k + 1, h.child[k]};
+            for (int j = 0; j < 2; j++)
+            {
+                const int ch = side[j];
+                const int link = h.child[ch] < 0 ? h.child[ch] : ch;
+                rec[4 * (size_t)k + 2 * j + 1].z = bits_f((uint32_t)link);
+                rec[4 * (size_t)k + 2 * j + 1].w = bits_f((uint32_t)h.maxPrim[ch]);
+            }
+        }
+        out.rec = (float4*)dalloc(sizeof(float4) * rec.size());
+        SC_CUDA(cudaMemcpy(out.rec, rec.data(), sizeof(float4) * rec.size(), cudaMemcpyHostToDevice));
         return true;
     };
     // batch: one tree per instance over its own primitives [start[k], start[k+1]),
@@ -748,6 +764,8 @@ bool ClothModel::upload_topology(const HMesh& mesh)
         SC_CUDA(cudaMemcpy(out.lo, lo.data(), sizeof(float4) * out.numNodes, cudaMemcpyHostToDevice));
         SC_CUDA(cudaMemcpy(out.hi, hi.data(), sizeof(float4) * out.numNodes, cudaMemcpyHostToDevice));
         out.visit = (int*)dalloc(sizeof(int) * out.numNodes);
+        out.rec = (float4*)dalloc(sizeof(float4) * 4 * (size_t)out.numNodes);
+        SC_CUDA(cudaMemcpy(out.rec, shareTopo->rec, sizeof(float4) * 4 * (size_t)out.numNodes, cudaMemcpyDeviceToDevice));
         return true;
     };
     std::vector<V3> tc(T), ec(E);

@@ -92,6 +92,7 @@ struct DevBVH
     const int* instRoot;    // batch: root node of each instance's tree (a forest); null: one tree at 0
     float4* lo;             // numNodes: box min; w = child[] as int bits
     float4* hi;             // numNodes: box max; w = escape[] as int bits
+    float4* rec;            // numNodes x 4: an internal node's two child records (box, link, max primitive)
     int* visit;             // numNodes refit counters
 };
 

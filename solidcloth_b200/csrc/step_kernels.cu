@@ -1379,6 +1379,15 @@ __device__ __forceinline__ Box leaf_box(const DevCloth& c, int kind, int prim, f
 // sibling's visible), the arriving thread keeps its own box in registers and
 // loads only the sibling's, and it puts the counter back to zero for the next
 // refit (counters start at zero when the tree is allocated).
+// a child's box into its half of the parent's record (the link and maximum
+// words after it are static)
+__device__ __forceinline__ void store_child_box(float4* rec, int parent, int node, const Box& b)
+{
+    float4* h = rec + 4 * (size_t)parent + (node == parent + 1 ? 0 : 2);
+    h[0] = make_float4(b.lo.x, b.lo.y, b.lo.z, b.hi.x);
+    *reinterpret_cast<float2*>(h + 1) = make_float2(b.hi.y, b.hi.z);
+}
+
 __global__ void k_bvh_refit(DevBVH t, DevCloth c, int kind, float tol)
 {
     int prim = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1388,6 +1397,7 @@ __global__ void k_bvh_refit(DevBVH t, DevCloth c, int kind, float tol)
     t.lo[node] = f4(b.lo, __int_as_float(~prim));
     t.hi[node] = f4(b.hi, __int_as_float(node + 1));
     int p = t.parent[node];
+    if (p >= 0) store_child_box(t.rec, p, node, b);
     while (p >= 0)
     {
         cuda::atomic_ref<int, cuda::thread_scope_device> visit(t.visit[p]);
@@ -1405,8 +1415,10 @@ __global__ void k_bvh_refit(DevBVH t, DevCloth c, int kind, float tol)
         b = m;
         t.lo[p] = f4(b.lo, __int_as_float(r));
         t.hi[p] = f4(b.hi, __int_as_float(t.escape[p]));
+        const int gp = t.parent[p];
+        if (gp >= 0) store_child_box(t.rec, gp, p, b);
         node = p;
-        p = t.parent[p];
+        p = gp;
     }
 }
 
@@ -1435,10 +1447,35 @@ __device__ __forceinline__ void bvh_query(const DevBVH& t, const Box& q, F&& f, 
     }
 }
 
+// Child records: every internal node keeps, for each of its two children, one
+// 32-byte half with the child's box, its link (node index, or ~primitive for a
+// leaf) and the largest primitive index below it, so one step of a walk is two
+// 256-bit loads from one 64-byte record (the refit writes the boxes, the links
+// and maxima are static).
+struct ChildRec { float lx, ly, lz, hx, hy, hz; int link, maxPrim; };
+
+__device__ __forceinline__ ChildRec ld_child(const float4* rec, int node, int side)
+{
+    const float* a = reinterpret_cast<const float*>(rec + 4 * (size_t)node + 2 * side);
+    float v[8];
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7])
+        : "l"(a));
+    ChildRec r;
+    r.lx = v[0]; r.ly = v[1]; r.lz = v[2]; r.hx = v[3]; r.hy = v[4]; r.hz = v[5];
+    r.link = __float_as_int(v[6]); r.maxPrim = __float_as_int(v[7]);
+    return r;
+}
+
+__device__ __forceinline__ bool overlaps(const ChildRec& c, const Box& q)
+{
+    return !(c.hx < q.lo.x || c.hy < q.lo.y || c.hz < q.lo.z || q.hi.x < c.lx || q.hi.y < c.ly || q.hi.z < c.lz);
+}
+
 // Per-thread traversal that tests both children of an entered node in one round
-// trip (four independent 16-byte loads) and keeps the second one on a short
-// stack: the dependent-load chain is the number of entered internal nodes, about
-// a third of the stackless walk's. Reports the same leaf set as bvh_query, in a
+// trip (the node's two child records) and keeps the second one on a short stack:
+// the dependent-load chain is the number of entered internal nodes, about a
+// third of the stackless walk's. Reports the same leaf set as bvh_query, in a
 // different order. A median-split tree over n < 2^31 leaves is at most 31 deep,
 // so the 32-entry stack cannot overflow. A walk ends early once *stop is set
 // (by f).
@@ -1447,40 +1484,31 @@ __device__ __forceinline__ void bvh_query2(const DevBVH& t, const Box& q, bool a
                                            const bool* stop = nullptr)
 {
     if (!active || t.numNodes == 0) return;
-    auto over = [&](const float4& lo, const float4& hi) {
-        return !(hi.x < q.lo.x || hi.y < q.lo.y || hi.z < q.lo.z || q.hi.x < lo.x || q.hi.y < lo.y || q.hi.z < lo.z);
-    };
     const float4 rlo = __ldg(&t.lo[root]), rhi = __ldg(&t.hi[root]);
-    if (!over(rlo, rhi) || (above >= 0 && __ldg(&t.maxPrim[root]) <= above)) return;
+    const bool rootHit = !(rhi.x < q.lo.x || rhi.y < q.lo.y || rhi.z < q.lo.z || q.hi.x < rlo.x || q.hi.y < rlo.y ||
+                           q.hi.z < rlo.z);
+    if (!rootHit || (above >= 0 && __ldg(&t.maxPrim[root]) <= above)) return;
     if (__float_as_int(rlo.w) < 0) { f(~__float_as_int(rlo.w)); return; }
     int stack[32];
     int sp = 0;
-    int node = root, ch = __float_as_int(rlo.w);
+    int node = root;
     while (!(stop && *stop))
     {
-        const int L = node + 1, R = ch;
-        const float4 loL = __ldg(&t.lo[L]), hiL = __ldg(&t.hi[L]), loR = __ldg(&t.lo[R]), hiR = __ldg(&t.hi[R]);
-        bool oL = over(loL, hiL), oR = over(loR, hiR);
-        if (above >= 0)
-        {
-            const int mL = __ldg(&t.maxPrim[L]), mR = __ldg(&t.maxPrim[R]);
-            oL = oL && mL > above;
-            oR = oR && mR > above;
-        }
-        const int cL = __float_as_int(loL.w), cR = __float_as_int(loR.w);
-        if (oL && cL < 0) { f(~cL); oL = false; }
-        if (oR && cR < 0) { f(~cR); oR = false; }
+        const ChildRec cl = ld_child(t.rec, node, 0), cr = ld_child(t.rec, node, 1);
+        bool oL = overlaps(cl, q) && (above < 0 || cl.maxPrim > above);
+        bool oR = overlaps(cr, q) && (above < 0 || cr.maxPrim > above);
+        if (oL && cl.link < 0) { f(~cl.link); oL = false; }
+        if (oR && cr.link < 0) { f(~cr.link); oR = false; }
         if (oL)
         {
-            if (oR && sp < 32) stack[sp++] = R;
-            node = L; ch = cL;
+            if (oR && sp < 32) stack[sp++] = cr.link;
+            node = cl.link;
         }
-        else if (oR) { node = R; ch = cR; }
+        else if (oR) node = cr.link;
         else
         {
             if (sp == 0) break;
             node = stack[--sp];
-            ch = __float_as_int(__ldg(&t.lo[node]).w);
         }
     }
 }
@@ -1488,11 +1516,11 @@ __device__ __forceinline__ void bvh_query2(const DevBVH& t, const Box& q, bool a
 // Warp-packet form of bvh_query2: the 32 lanes (spatially adjacent queries in
 // the same tree) walk it together, testing both children of an entered node per
 // step; a child is entered when any lane's box overlaps it (ballot), so every
-// node load is one broadcast request instead of up to 32 scattered ones, at the
-// price of visiting the union of the lanes' nodes. Each lane reports exactly its
-// own leaves. All 32 lanes must call it; a warp whose lanes start in different
-// trees (a batch instance boundary) takes the per-lane walk. A lane whose *stop
-// is set (by f) stops reporting and no longer steers the walk.
+// record load is one broadcast request instead of up to 32 scattered ones, at
+// the price of visiting the union of the lanes' nodes. Each lane reports exactly
+// its own leaves. All 32 lanes must call it; a warp whose lanes start in
+// different trees (a batch instance boundary) takes the per-lane walk. A lane
+// whose *stop is set (by f) stops reporting and no longer steers the walk.
 template <typename F>
 __device__ __forceinline__ void bvh_query2_warp(const DevBVH& t, const Box& q, bool active, F&& f, int above, int root,
                                                 const bool* stop = nullptr)
@@ -1502,97 +1530,83 @@ __device__ __forceinline__ void bvh_query2_warp(const DevBVH& t, const Box& q, b
     if (!act) return;
     const int r0 = __shfl_sync(full, root, __ffs(act) - 1);
     if (!__all_sync(full, !active || root == r0)) { bvh_query2(t, q, active, f, above, root, stop); return; }
-    auto over = [&](const float4& lo, const float4& hi) {
-        return !(hi.x < q.lo.x || hi.y < q.lo.y || hi.z < q.lo.z || q.hi.x < lo.x || q.hi.y < lo.y || q.hi.z < lo.z);
-    };
     const float4 rlo = __ldg(&t.lo[r0]), rhi = __ldg(&t.hi[r0]);
-    bool rootHit = active && over(rlo, rhi) && (above < 0 || __ldg(&t.maxPrim[r0]) > above);
+    const bool rootHit = active &&
+                         !(rhi.x < q.lo.x || rhi.y < q.lo.y || rhi.z < q.lo.z || q.hi.x < rlo.x || q.hi.y < rlo.y ||
+                           q.hi.z < rlo.z) &&
+                         (above < 0 || __ldg(&t.maxPrim[r0]) > above);
     if (__float_as_int(rlo.w) < 0) { if (rootHit) f(~__float_as_int(rlo.w)); return; }
     if (!__any_sync(full, rootHit)) return;
     int stack[32];
     int sp = 0;
-    int node = r0, ch = __float_as_int(rlo.w);
+    int node = r0;
     while (true)
     {
-        const int L = node + 1, R = ch;
-        const float4 loL = __ldg(&t.lo[L]), hiL = __ldg(&t.hi[L]), loR = __ldg(&t.lo[R]), hiR = __ldg(&t.hi[R]);
+        const ChildRec cl = ld_child(t.rec, node, 0), cr = ld_child(t.rec, node, 1);
         const bool live = active && !(stop && *stop);
-        bool oL = live && over(loL, hiL), oR = live && over(loR, hiR);
-        if (above >= 0)
-        {
-            const int mL = __ldg(&t.maxPrim[L]), mR = __ldg(&t.maxPrim[R]);
-            oL = oL && mL > above;
-            oR = oR && mR > above;
-        }
-        const int cL = __float_as_int(loL.w), cR = __float_as_int(loR.w);
-        if (cL < 0) { if (oL) f(~cL); oL = false; }
-        if (cR < 0) { if (oR) f(~cR); oR = false; }
+        bool oL = live && overlaps(cl, q) && (above < 0 || cl.maxPrim > above);
+        bool oR = live && overlaps(cr, q) && (above < 0 || cr.maxPrim > above);
+        if (cl.link < 0) { if (oL) f(~cl.link); oL = false; }
+        if (cr.link < 0) { if (oR) f(~cr.link); oR = false; }
         const bool anyL = __any_sync(full, oL), anyR = __any_sync(full, oR);
         if (anyL)
         {
-            if (anyR && sp < 32) stack[sp++] = R;
-            node = L; ch = cL;
+            if (anyR && sp < 32) stack[sp++] = cr.link;
+            node = cl.link;
         }
-        else if (anyR) { node = R; ch = cR; }
+        else if (anyR) node = cr.link;
         else
         {
             if (sp == 0) break;
             node = stack[--sp];
-            ch = __float_as_int(__ldg(&t.lo[node]).w);
         }
     }
 }
 
 // Cooperative walk of ONE query box by a group of W lanes (W a power of two up
-// to 32; every lane of the group holds the same box), for queries with long candidate
-// lists: each step the group takes up to W entered nodes from its stack, each
-// lane tests both children of its node (one round trip), and the entered
-// internal children are pushed as a new group. Only the top group is ever
-// popped, so group g holds nodes of depth g exactly: at most depth groups of at
-// most 2W entries, the bound the caller sizes the stack by (int2: node, its
-// right child). f(a, b) is called by all lanes of the group once per step with
-// the lane's overlapping leaves (-1 for none) and returns false to end the walk
-// (uniformly across the group). The leaf set is bvh_query2's.
+// to 32; every lane of the group holds the same box), for queries with long
+// candidate lists: each step the group takes up to W entered nodes from its
+// stack, each lane tests both children of its node (one round trip), and the
+// entered internal children are pushed as a new group. Only the top group is
+// ever popped, so group g holds nodes of depth g exactly: at most depth groups
+// of at most 2W entries, the bound the caller sizes the stack (node indices)
+// by. f(a, b) is called by all lanes of the group once per step with the lane's
+// overlapping leaves (-1 for none) and returns false to end the walk (uniformly
+// across the group). The leaf set is bvh_query2's.
 template <int W, typename F>
-__device__ __forceinline__ void bvh_query_coop(const DevBVH& t, const Box& q, int above, int root, int2* stack, int cap,
+__device__ __forceinline__ void bvh_query_coop(const DevBVH& t, const Box& q, int above, int root, int* stack, int cap,
                                                int* groups, int gcap, int* status, F&& f)
 {
     const int lane = threadIdx.x & 31, sl = lane & (W - 1);
     const unsigned mask = W == 32 ? 0xffffffffu : (((1u << W) - 1u) << (lane & ~(W - 1)));
     const unsigned lt = (1u << lane) - 1u;
-    auto over = [&](const float4& lo, const float4& hi) {
-        return !(hi.x < q.lo.x || hi.y < q.lo.y || hi.z < q.lo.z || q.hi.x < lo.x || q.hi.y < lo.y || q.hi.z < lo.z);
-    };
     const float4 rlo = __ldg(&t.lo[root]), rhi = __ldg(&t.hi[root]);
-    if (!over(rlo, rhi) || (above >= 0 && __ldg(&t.maxPrim[root]) <= above)) return;
+    const bool rootHit = !(rhi.x < q.lo.x || rhi.y < q.lo.y || rhi.z < q.lo.z || q.hi.x < rlo.x || q.hi.y < rlo.y ||
+                           q.hi.z < rlo.z);
+    if (!rootHit || (above >= 0 && __ldg(&t.maxPrim[root]) <= above)) return;
     const int rch = __float_as_int(rlo.w);
     if (rch < 0) { f(sl == 0 ? ~rch : -1, -1); return; }
-    if (sl == 0) { stack[0] = make_int2(root, rch); groups[0] = 1; }
+    if (sl == 0) { stack[0] = root; groups[0] = 1; }
     int sp = 1, m = 1;
     __syncwarp(mask);
     while (m > 0)
     {
         const int g = groups[m - 1];
         const int take = min(g, W);
-        const int2 nd = sl < take ? stack[sp - 1 - sl] : make_int2(-1, 0);
+        const int node = sl < take ? stack[sp - 1 - sl] : -1;
         __syncwarp(mask);
         sp -= take;
-        int leafA = -1, leafB = -1, cL = 0, cR = 0;
+        int leafA = -1, leafB = -1, linkL = 0, linkR = 0;
         bool pushL = false, pushR = false;
-        const int L = nd.x + 1, R = nd.y;
-        if (nd.x >= 0)
+        if (node >= 0)
         {
-            const float4 loL = __ldg(&t.lo[L]), hiL = __ldg(&t.hi[L]), loR = __ldg(&t.lo[R]), hiR = __ldg(&t.hi[R]);
-            bool oL = over(loL, hiL), oR = over(loR, hiR);
-            if (above >= 0)
-            {
-                oL = oL && __ldg(&t.maxPrim[L]) > above;
-                oR = oR && __ldg(&t.maxPrim[R]) > above;
-            }
-            cL = __float_as_int(loL.w);
-            cR = __float_as_int(loR.w);
-            if (oL) { if (cL < 0) leafA = ~cL; else pushL = true; }
-            if (oR) { if (cR < 0) leafB = ~cR; else pushR = true; }
+            const ChildRec cl = ld_child(t.rec, node, 0), cr = ld_child(t.rec, node, 1);
+            const bool oL = overlaps(cl, q) && (above < 0 || cl.maxPrim > above);
+            const bool oR = overlaps(cr, q) && (above < 0 || cr.maxPrim > above);
+            linkL = cl.link;
+            linkR = cr.link;
+            if (oL) { if (linkL < 0) leafA = ~linkL; else pushL = true; }
+            if (oR) { if (linkR < 0) leafB = ~linkR; else pushR = true; }
         }
         if (!f(leafA, leafB)) break;
         const unsigned bl = __ballot_sync(mask, pushL), br = __ballot_sync(mask, pushR);
@@ -1607,8 +1621,8 @@ __device__ __forceinline__ void bvh_query_coop(const DevBVH& t, const Box& q, in
                 if (sl == 0) atomicOr(status, ST_CCD_OVERFLOW);
                 break;
             }
-            if (pushL) stack[sp + __popc(bl & lt)] = make_int2(L, cL);
-            if (pushR) stack[sp + nl + __popc(br & lt)] = make_int2(R, cR);
+            if (pushL) stack[sp + __popc(bl & lt)] = linkL;
+            if (pushR) stack[sp + nl + __popc(br & lt)] = linkR;
             if (sl == 0) groups[m] = cnt;
             sp += cnt;
             m++;
@@ -1991,13 +2005,13 @@ __global__ void __launch_bounds__(128) k_ccd_broad_ee(DevCloth c, SolverParams P
 template <bool VT>
 __global__ void __launch_bounds__(CCD_COOP_THREADS) k_ccd_broad_coop(DevCloth c, SolverParams P, Buffers b, DevBVH t, float tol)
 {
-    extern __shared__ int2 sCoop[];
+    extern __shared__ int sCoop[];
     const unsigned full = 0xffffffffu;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
     const int cap = CCD_COOP_GROUP * (t.depth + 1), gcap = t.depth + 2;
-    int2* stack = sCoop + warp * (cap + (gcap + 1) / 2);
-    int* groups = reinterpret_cast<int*>(stack + cap);
+    int* stack = sCoop + warp * (cap + gcap);
+    int* groups = stack + cap;
     const int nOvf = b.ccdOvfN[VT ? 0 : 1];
     const int* ovf = VT ? b.ccdVtOvf : b.ccdEeOvf;
     int* cnt = VT ? b.ccdVtCnt : b.ccdEeCnt;
@@ -2048,7 +2062,7 @@ __global__ void __launch_bounds__(CCD_COOP_THREADS) k_ccd_broad_coop(DevCloth c,
 size_t ccd_coop_smem(int depth)
 {
     const int cap = CCD_COOP_GROUP * (depth + 1), gcap = depth + 2;
-    return sizeof(int2) * (size_t)(cap + (gcap + 1) / 2) * (CCD_COOP_THREADS / 32);
+    return sizeof(int) * (size_t)(cap + gcap) * (CCD_COOP_THREADS / 32);
 }
 
 void ccd_kernel_setup()
