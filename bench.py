@@ -380,7 +380,8 @@ def run_ours(args):
               2: f"k_gs_grid variant {ch[1]} ({ch[3]} threads, {ch[2]} CTAs/SM; one substep's Gauss-Seidel loop + velocity, one cooperative launch)",
               3: "k_fem / k_bends per colour (one substep's Gauss-Seidel loop)"}.get(ch[0], "solver")
     kernel_names = {"gs_solve": solver,
-                    "ccd_broad_ee": "k_ccd_broad_ee (edge-edge swept-box LBVH query, both passes)",
+                    "ccd_broad_ee": "k_bvh_refit + k_ccd_broad_ee + k_ccd_broad_coop (edge-edge swept-box LBVH "
+                                    "refit and query: one walk per lane, long lists one warp per query)",
                     "colliders": "k_vertex_colliders + k_tri_colliders + k_edge_colliders (collider detection)"}
     walk, walk_ms = p.model.broad_phase_mode()
     per = {}
