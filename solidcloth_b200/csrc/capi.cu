@@ -628,13 +628,7 @@ void scSetParticleState(scModel m, const float* pos, const float* prev, const fl
 {
     if (!check_model(M(m)) || !pos || !prev || !vel) return;
     host_sync(M(m));
-    for (int i = 0; i < M(m)->N; i++)
-    {
-        M(m)->hpos[i] = mk(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
-        M(m)->hprev[i] = mk(prev[3 * i], prev[3 * i + 1], prev[3 * i + 2]);
-        M(m)->hvel[i] = mk(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]);
-    }
-    M(m)->upload_state(M(m)->owner->stream);
+    M(m)->set_state(pos, prev, vel, M(m)->owner->stream);
 }
 static void get3(scModel m, float* xyz, int which)
 {

@@ -451,6 +451,23 @@ void ClothModel::release_device()
     for (void* p : allocs) cudaFree(p);
     allocs.clear();
     dc = DevCloth{};
+    if (stageHost) cudaFreeHost(stageHost);
+    stageHost = nullptr;
+    stageDev = nullptr;          // one of allocs
+}
+
+bool ClothModel::ensure_stage()
+{
+    if (stageHost && stageDev) return true;
+    if (N == 0) return false;
+    if (cudaHostAlloc((void**)&stageHost, sizeof(float) * 10 * (size_t)N, cudaHostAllocDefault) != cudaSuccess)
+    {
+        cudaGetLastError();
+        stageHost = nullptr;
+        return false;
+    }
+    stageDev = (float*)dalloc(sizeof(float) * 10 * (size_t)N);
+    return stageDev != nullptr;
 }
 
 SolverParams ClothModel::solver_params(float h) const
@@ -805,6 +822,19 @@ void ClothModel::upload_state(cudaStream_t s)
 
 void ClothModel::download_state(cudaStream_t s)
 {
+    static_assert(sizeof(V3) == 3 * sizeof(float), "packed xyz");
+    if (ensure_stage())
+    {
+        const size_t n = N;
+        launch_pack_state(s, dc, stageDev);
+        cudaMemcpyAsync(stageHost, stageDev, sizeof(float) * 10 * n, cudaMemcpyDeviceToHost, s);
+        cudaStreamSynchronize(s);
+        memcpy(hpos.data(), stageHost, sizeof(float) * 3 * n);
+        memcpy(hvel.data(), stageHost + 3 * n, sizeof(float) * 3 * n);
+        memcpy(hprev.data(), stageHost + 6 * n, sizeof(float) * 3 * n);
+        memcpy(invMass.data(), stageHost + 9 * n, sizeof(float) * n);
+        return;
+    }
     std::vector<float4> p(N), q(N), v(N);
     cudaMemcpyAsync(p.data(), dc.pos, sizeof(float4) * N, cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(q.data(), dc.prev, sizeof(float4) * N, cudaMemcpyDeviceToHost, s);
@@ -816,6 +846,22 @@ void ClothModel::download_state(cudaStream_t s)
         hprev[i] = mk(q[i]);
         hvel[i] = mk(v[i]);
     }
+}
+
+void ClothModel::set_state(const float* pos, const float* prev, const float* vel, cudaStream_t s)
+{
+    const size_t n = N;
+    memcpy(hpos.data(), pos, sizeof(float) * 3 * n);
+    memcpy(hprev.data(), prev, sizeof(float) * 3 * n);
+    memcpy(hvel.data(), vel, sizeof(float) * 3 * n);
+    if (!ensure_stage()) { upload_state(s); return; }
+    memcpy(stageHost, pos, sizeof(float) * 3 * n);
+    memcpy(stageHost + 3 * n, vel, sizeof(float) * 3 * n);
+    memcpy(stageHost + 6 * n, prev, sizeof(float) * 3 * n);
+    memcpy(stageHost + 9 * n, invMass.data(), sizeof(float) * n);
+    cudaMemcpyAsync(stageDev, stageHost, sizeof(float) * 10 * n, cudaMemcpyHostToDevice, s);
+    launch_unpack_state(s, dc, stageDev);
+    cudaStreamSynchronize(s);            // the staging buffer is reused by the next transfer
 }
 
 // Contact buffers depend on the world's colliders, the collision flags and the

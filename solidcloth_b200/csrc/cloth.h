@@ -164,6 +164,12 @@ public:
     bool ensure_buffers(const CollisionWorld& world, cudaStream_t s);
     void download_state(cudaStream_t s);
     void upload_state(cudaStream_t s);
+    // scSetParticleState: caller arrays (xyz triples) to the host copies and the device
+    void set_state(const float* pos, const float* prev, const float* vel, cudaStream_t s);
+    // pinned host / device staging of the packed state (10 N floats), made on first use
+    float* stageHost = nullptr;
+    float* stageDev = nullptr;
+    bool ensure_stage();
     SolverParams solver_params(float h) const;
     // batch of independent clothes (empty: one cloth): first particle / triangle /
     // edge / bend of each instance (+ end), and each instance's colliders

@@ -77,6 +77,9 @@ struct Buffers
 };
 
 void launch_predict(cudaStream_t s, const DevCloth& c, const SolverParams& P);
+// state <-> 10 N floats: positions, velocities, previous positions (xyz), inverse masses
+void launch_pack_state(cudaStream_t s, const DevCloth& c, float* out);
+void launch_unpack_state(cudaStream_t s, const DevCloth& c, const float* in);
 void launch_velocity(cudaStream_t s, const DevCloth& c, const SolverParams& P);
 void launch_fem(cudaStream_t s, const DevCloth& c, const SolverParams& P, int first, int count);
 void launch_links(cudaStream_t s, const DevCloth& c, const SolverParams& P, int first, int count);

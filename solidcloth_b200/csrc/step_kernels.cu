@@ -2931,6 +2931,43 @@ void launch_gs_cluster(cudaStream_t s, const DevCloth& c, const SolverParams& P,
 }
 
 // ------------------------------------------------------------- launchers
+// particle state <-> the packed host layout of the state transfers: positions,
+// velocities and previous positions as xyz triples, then inverse masses (one
+// copy each way instead of three of float4 arrays)
+__global__ void k_pack_state(DevCloth c, float* out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.N) return;
+    const size_t n = c.N;
+    const float4 p = c.pos[i], v = c.vel[i], q = c.prev[i];
+    float* a = out + 3 * (size_t)i;
+    a[0] = p.x; a[1] = p.y; a[2] = p.z;
+    a[3 * n] = v.x; a[3 * n + 1] = v.y; a[3 * n + 2] = v.z;
+    a[6 * n] = q.x; a[6 * n + 1] = q.y; a[6 * n + 2] = q.z;
+    out[9 * n + i] = p.w;
+}
+
+__global__ void k_unpack_state(DevCloth c, const float* in)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.N) return;
+    const size_t n = c.N;
+    const float* a = in + 3 * (size_t)i;
+    c.pos[i] = make_float4(a[0], a[1], a[2], in[9 * n + i]);
+    c.vel[i] = make_float4(a[3 * n], a[3 * n + 1], a[3 * n + 2], 0.f);
+    c.prev[i] = make_float4(a[6 * n], a[6 * n + 1], a[6 * n + 2], 0.f);
+}
+
+void launch_pack_state(cudaStream_t s, const DevCloth& c, float* out)
+{
+    k_pack_state<<<blocks_for(c.N), 256, 0, s>>>(c, out);
+}
+
+void launch_unpack_state(cudaStream_t s, const DevCloth& c, const float* in)
+{
+    k_unpack_state<<<blocks_for(c.N), 256, 0, s>>>(c, in);
+}
+
 void launch_predict(cudaStream_t s, const DevCloth& c, const SolverParams& P)
 {
     cudaMemsetAsync(c.scal, 0, sizeof(float), s);
