@@ -7,6 +7,9 @@
 #include <cstring>
 #include <cstdio>
 #include <numeric>
+#include <array>
+#include <functional>
+#include <map>
 #include <mutex>
 
 namespace sc {
@@ -518,12 +521,127 @@ static void greedy_colour(int n, int N, Get verts, std::vector<int>& order, std:
     for (int c = 0; c < maxc; c++) start[c + 1] += start[c];
 }
 
+// Bends of grid clothes, coloured with a pattern of period 4 in both grid
+// directions: the 48 bends of the 4 x 4 torus triangulated like the grid
+// (alternating diagonals by cell parity) are coloured once by an exact search
+// with 16 colours — the most bends that share one particle, so the fewest
+// possible — and every bend takes the colour of its edge's image on the torus.
+// Two bends sharing a particle have images sharing a vertex, and distinct bends
+// within reach of each other have distinct images, so the colouring is proper;
+// it is checked anyway, and false means "use the greedy colouring".
+static bool periodic_bend_colours(const std::vector<uint4>& bends, const std::vector<int2>& ij, int N, std::vector<int>& col)
+{
+    const int P = 4, K = 16;
+    auto T = [&](int j, int i) { return ((j % P + P) % P) * P + ((i % P + P) % P); };
+    // torus triangles, the cell rule of ClothPatch::Init(grid)
+    std::vector<std::array<int, 3>> tri;
+    for (int j = 0; j < P; j++)
+        for (int i = 0; i < P; i++)
+        {
+            const int a = T(j - 1, i - 1), b = T(j - 1, i), c = T(j, i), d = T(j, i - 1);
+            if ((i & 1) == (j & 1)) { tri.push_back({a, c, b}); tri.push_back({a, d, c}); }
+            else { tri.push_back({b, d, c}); tri.push_back({d, b, a}); }
+        }
+    std::map<std::pair<int, int>, std::vector<int>> opp;
+    for (auto& t : tri)
+        for (int k = 0; k < 3; k++)
+        {
+            const int x = t[k], y = t[(k + 1) % 3], z = t[(k + 2) % 3];
+            opp[{std::min(x, y), std::max(x, y)}].push_back(z);
+        }
+    std::vector<std::pair<int, int>> key;
+    std::vector<std::array<int, 4>> tv;
+    for (auto& e : opp)
+    {
+        if (e.second.size() != 2) return false;
+        key.push_back(e.first);
+        tv.push_back({e.first.first, e.first.second, e.second[0], e.second[1]});
+    }
+    const int m = (int)key.size();
+    std::vector<std::vector<int>> nb(m);
+    for (int a = 0; a < m; a++)
+        for (int b = 0; b < m; b++)
+        {
+            if (a == b) continue;
+            bool share = false;
+            for (int x : tv[a]) for (int y : tv[b]) share |= x == y;
+            if (share) nb[a].push_back(b);
+        }
+    // DSatur order with backtracking (bounded)
+    std::vector<int> tc(m, -1);
+    long budget = 5000000;
+    std::function<bool()> search = [&]() -> bool {
+        int best = -1, bs = -1, bd = -1;
+        for (int a = 0; a < m; a++)
+        {
+            if (tc[a] >= 0) continue;
+            uint32_t used = 0;
+            for (int b : nb[a]) if (tc[b] >= 0) used |= 1u << tc[b];
+            const int s = __builtin_popcount(used), d = (int)nb[a].size();
+            if (s > bs || (s == bs && d > bd)) { best = a; bs = s; bd = d; }
+        }
+        if (best < 0) return true;
+        if (--budget < 0) return false;
+        uint32_t used = 0;
+        int top = -1;
+        for (int a = 0; a < m; a++) top = std::max(top, tc[a]);
+        for (int b : nb[best]) if (tc[b] >= 0) used |= 1u << tc[b];
+        for (int k = 0; k < K && k <= top + 1; k++)
+        {
+            if (used >> k & 1u) continue;
+            tc[best] = k;
+            if (search()) return true;
+            tc[best] = -1;
+        }
+        return false;
+    };
+    if (!search()) return false;
+    std::map<std::pair<int, int>, int> colourOf;
+    for (int a = 0; a < m; a++) colourOf[key[a]] = tc[a];
+    col.assign(bends.size(), 0);
+    for (size_t k = 0; k < bends.size(); k++)
+    {
+        const int2 p = ij[bends[k].x], q = ij[bends[k].y];
+        const int u = T(p.x, p.y), v = T(q.x, q.y);
+        auto it = colourOf.find({std::min(u, v), std::max(u, v)});
+        if (it == colourOf.end()) return false;
+        col[k] = it->second;
+    }
+    // proper: no particle in two bends of one colour
+    std::vector<uint32_t> seen(N, 0);
+    for (size_t k = 0; k < bends.size(); k++)
+    {
+        const uint32_t v[4] = {bends[k].x, bends[k].y, bends[k].z, bends[k].w};
+        for (uint32_t x : v)
+        {
+            if (seen[x] >> col[k] & 1u) return false;
+            seen[x] |= 1u << col[k];
+        }
+    }
+    return true;
+}
+
 void ClothModel::colour_constraints()
 {
     greedy_colour<3>((int)tris.size(), N, [&](int i, uint32_t* v) { v[0] = tris[i].i1; v[1] = tris[i].i2; v[2] = tris[i].i3; },
                      triOrder, triColourStart);
     greedy_colour<4>((int)bends.size(), N, [&](int i, uint32_t* v) { v[0] = bends[i].x; v[1] = bends[i].y; v[2] = bends[i].z; v[3] = bends[i].w; },
                      bendOrder, bendColourStart);
+    std::vector<int> col;
+    if ((int)gridIJ.size() == N && !bends.empty() && periodic_bend_colours(bends, gridIJ, N, col))
+    {
+        const int K = *std::max_element(col.begin(), col.end()) + 1;
+        if (K < (int)bendColourStart.size() - 1)
+        {
+            // solve order = (colour, index), as the greedy colouring's
+            bendOrder.resize(bends.size());
+            std::iota(bendOrder.begin(), bendOrder.end(), 0);
+            std::stable_sort(bendOrder.begin(), bendOrder.end(), [&](int a, int b) { return col[a] < col[b]; });
+            bendColourStart.assign(K + 1, 0);
+            for (int c : col) bendColourStart[c + 1]++;
+            for (int c = 0; c < K; c++) bendColourStart[c + 1] += bendColourStart[c];
+        }
+    }
     greedy_colour<2>((int)links.size(), N, [&](int i, uint32_t* v) { v[0] = links[i].x; v[1] = links[i].y; },
                      linkOrder, linkColourStart);
 }
@@ -1087,6 +1205,9 @@ bool ClothPatch::init_grid(int divX, int divY, float inc, V3 offset, bool horizo
     m.N = N;
     m.hpos.assign(N, mk(0, 0, 0)); m.hprev.assign(N, mk(0, 0, 0)); m.hvel.assign(N, mk(0, 0, 0));
     m.invMass.assign(N, 1.f); m.uvx.assign(N, 0.f); m.uvy.assign(N, 0.f);
+    m.gridIJ.resize(N);
+    for (int j = 0; j < divX; j++)
+        for (int i = 0; i < divY; i++) m.gridIJ[j * divY + i] = make_int2(j, i);
     m.tris.clear(); m.bends.clear(); m.links.clear(); m.linkRest.clear(); m.quads.clear();
     mesh = HMesh();
     isQuadMesh = true;
@@ -1206,6 +1327,9 @@ bool ClothPatch::init_batch(const std::vector<ClothPatch*>& parts)
     m.hpos.clear(); m.hprev.clear(); m.hvel.clear(); m.invMass.clear(); m.uvx.clear(); m.uvy.clear();
     m.tris.clear(); m.bends.clear(); m.links.clear(); m.linkRest.clear(); m.quads.clear();
     m.instV = {0}; m.instT = {0}; m.instE = {0}; m.instB = {0};
+    m.gridIJ.clear();
+    bool allGrids = true;
+    for (ClothPatch* q : parts) allGrids = allGrids && (int)q->model.gridIJ.size() == q->model.N;
     m.batchColl.clear();
     mesh = HMesh();
     for (size_t k = 0; k < parts.size(); k++)
@@ -1219,6 +1343,7 @@ bool ClothPatch::init_batch(const std::vector<ClothPatch*>& parts)
         m.invMass.insert(m.invMass.end(), q.invMass.begin(), q.invMass.end());
         m.uvx.insert(m.uvx.end(), q.uvx.begin(), q.uvx.end());
         m.uvy.insert(m.uvy.end(), q.uvy.begin(), q.uvy.end());
+        if (allGrids) m.gridIJ.insert(m.gridIJ.end(), q.gridIJ.begin(), q.gridIJ.end());
         for (FemHost t : q.tris) { t.i1 += vo; t.i2 += vo; t.i3 += vo; m.tris.push_back(t); }
         for (uint4 b : q.bends) m.bends.push_back(make_uint4(b.x + vo, b.y + vo, b.z + vo, b.w + vo));
         for (uint2 l : q.links) m.links.push_back(make_uint2(l.x + vo, l.y + vo));
@@ -1285,6 +1410,7 @@ bool ClothPatch::init_mesh(const std::vector<V3>& verts, const std::vector<uint3
     m.hpos.clear(); m.hprev.clear(); m.hvel.clear(); m.invMass.clear(); m.uvx.clear(); m.uvy.clear();
     m.tris.clear(); m.bends.clear(); m.links.clear(); m.linkRest.clear(); m.quads.clear();
     m.instV.clear(); m.instT.clear(); m.instE.clear(); m.instB.clear(); m.batchColl.clear();
+    m.gridIJ.clear();
     for (size_t i = 0; i < nv; i++)
     {
         if (map[i] >= 0) continue;

@@ -135,6 +135,9 @@ public:
     std::vector<V3> hpos, hprev, hvel;
     std::vector<float> invMass;
     std::vector<float> uvx, uvy;
+    // grid clothes (ClothPatch::Init(grid)): each particle's (column, row); empty
+    // for a cloth from a mesh (and for a batch with such a part)
+    std::vector<int2> gridIJ;
     std::vector<FemHost> tris;
     std::vector<uint4> bends;
     std::vector<uint2> links;

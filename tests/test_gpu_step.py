@@ -81,6 +81,10 @@ def test_colouring_is_valid():
     for c in range(len(start) - 1):
         ids = bends[order[start[c]:start[c + 1]]].reshape(-1)
         assert len(np.unique(ids)) == ids.size
+    # grid bends take the period-4 colouring: 16 colours, the most bends sharing
+    # one particle (index-order greedy needs 18-19 on these grids)
+    per = np.bincount(bends.reshape(-1), minlength=sc.num_vertices).max()
+    assert len(start) - 1 == per == 16
 
 
 def test_topology_matches_oracle():
