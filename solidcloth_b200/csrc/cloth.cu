@@ -1141,6 +1141,7 @@ bool ClothModel::ensure_buffers(const CollisionWorld& world, cudaStream_t s)
     buf.scanOff = (int*)dalloc(sizeof(int) * (maxScan + 1), true);
     buf.scanBlock = (int*)dalloc(sizeof(int) * (maxScan / 1024 + 8), true);
     buf.scanBlock2 = (int*)dalloc(sizeof(int) * (maxScan / 1024 + 8), true);
+    buf.scanOff2 = (int*)dalloc(sizeof(int) * (maxScan + 1), true);
     buf.broadWalk = broadWalk;
     bufWorldVersion = world.version;
     bufFlags = prm.flags;
@@ -1575,7 +1576,7 @@ void ClothPatch::record_substep(float h)
         }
         launch_ccd(s, side, evFork, evJoin, c, P, b, m.sweptTriBvh, m.sweptEdgeBvh, marks);
     }
-    if (self || ccd) launch_compact_self(s, c, P, b, ccd);
+    if (self || ccd) launch_compact_self(s, side, evFork, evJoin, c, P, b, self, ccd);
     else cudaMemsetAsync(b.stCount, 0, 2 * sizeof(int), s);
     launch_colour_contacts(s, c, b);
     // learned warm start (no reference counterpart): record the features and the

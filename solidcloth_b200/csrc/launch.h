@@ -72,6 +72,7 @@ struct Buffers
     // scan scratch: block sums, per-item offsets, totals
     int* scanBlock; int* scanOff; int* scanTot;
     int* scanBlock2;           // second block-sum scratch for scans on the side stream
+    int* scanOff2;             // second per-item offsets (side stream)
     const DevMesh* meshes;     // device array
     int numMeshes;
 };
@@ -104,7 +105,10 @@ void launch_self_proximity(cudaStream_t s, const DevCloth& c, const SolverParams
 void launch_ccd(cudaStream_t s, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join, const DevCloth& c,
                 const SolverParams& P, const Buffers& b, const DevBVH& triBvh, const DevBVH& edgeBvh,
                 const cudaEvent_t* marks = nullptr);
-void launch_compact_self(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b, bool ccd);
+// self-contact lists: proximity contacts (self) compacted, then the continuous
+// hits appended (ccd; vertex-triangle on `side` between fork and join)
+void launch_compact_self(cudaStream_t s, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join, const DevCloth& c,
+                         const SolverParams& P, const Buffers& b, bool self, bool ccd);
 void launch_reset_gs(cudaStream_t s, const DevCloth& c);
 // max |C| over warp / weft / shear constraints, as float bits into *out
 void launch_residual(cudaStream_t s, const DevCloth& c, unsigned* out);

@@ -3085,29 +3085,42 @@ void launch_self_proximity(cudaStream_t s, const DevCloth& c, const SolverParams
     k_self_ee<<<blocks_for(c.E, 128), 128, 0, s>>>(c, P, b, edgeBvh);
 }
 
-void launch_compact_self(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b, bool ccd)
+void launch_compact_self(cudaStream_t s, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join, const DevCloth& c,
+                         const SolverParams& P, const Buffers& b, bool self, bool ccd)
 {
-    int* off = b.scanOff;
-    scan_ints(s, b.stCnt, off, c.N, b.stCount, b.scanBlock);
-    k_compact<SCt><<<blocks_for(c.N), 256, 0, s>>>(b.stCnt, off, b.stSlot, KVT, b.stList, c.N, nullptr, b.stCap, c.status, ST_SELF_VT_OVERFLOW);
-    scan_ints(s, b.seFlag, off, c.E, b.seCount, b.scanBlock);
-    k_compact<SCt><<<blocks_for(c.E), 256, 0, s>>>(b.seFlag, off, b.seSlot, 1, b.seList, c.E, nullptr, b.seCap, c.status, ST_SELF_EE_OVERFLOW);
+    if (self)
+    {
+        int* off = b.scanOff;
+        scan_ints(s, b.stCnt, off, c.N, b.stCount, b.scanBlock);
+        k_compact<SCt><<<blocks_for(c.N), 256, 0, s>>>(b.stCnt, off, b.stSlot, KVT, b.stList, c.N, nullptr, b.stCap, c.status, ST_SELF_VT_OVERFLOW);
+        scan_ints(s, b.seFlag, off, c.E, b.seCount, b.scanBlock);
+        k_compact<SCt><<<blocks_for(c.E), 256, 0, s>>>(b.seFlag, off, b.seSlot, 1, b.seList, c.E, nullptr, b.seCap, c.status, ST_SELF_EE_OVERFLOW);
+    }
+    else cudaMemsetAsync(b.stCount, 0, 2 * sizeof(int), s);     // no proximity contacts (stCount, seCount)
     if (ccd)
     {
         // continuous hits go after the proximity contacts, as the detector's
-        // AddSelfTriangle / AddSelfEdge would append them (in pair order)
-        int* tot = b.scanTot;
-        k_ccd_hit_count<<<blocks_for(32 * c.N), 256, 0, s>>>(b.ccdVtCnt, b.ccdVtOff, b.ccdVtHit, c.N, b.ccdVtCap, b.ccdVtHitCnt);
-        scan_ints(s, b.ccdVtHitCnt, off, c.N, tot, b.scanBlock);
-        k_ccd_gather<true><<<blocks_for(32 * c.N), 256, 0, s>>>(c, P, b, off, b.stList, b.stCount, b.stCap);
-        k_add_counts<<<1, 32, 0, s>>>(b.stCount, b.stCount, tot, b.stCap);
+        // AddSelfTriangle / AddSelfEdge would append them (in pair order); the
+        // vertex-triangle list is assembled on the side stream beside the
+        // edge-edge one (own offsets, block sums and total)
+        cudaEventRecord(fork, s);
+        cudaStreamWaitEvent(side, fork, 0);
+        k_ccd_hit_count<<<blocks_for(32 * c.N), 256, 0, side>>>(b.ccdVtCnt, b.ccdVtOff, b.ccdVtHit, c.N, b.ccdVtCap, b.ccdVtHitCnt);
+        scan_ints(side, b.ccdVtHitCnt, b.scanOff2, c.N, b.scanTot + 1, b.scanBlock2);
+        k_ccd_gather<true><<<blocks_for(32 * c.N), 256, 0, side>>>(c, P, b, b.scanOff2, b.stList, b.stCount, b.stCap);
+        k_add_counts<<<1, 32, 0, side>>>(b.stCount, b.stCount, b.scanTot + 1, b.stCap);
+        cudaEventRecord(join, side);
         k_ccd_hit_count<<<blocks_for(32 * c.E), 256, 0, s>>>(b.ccdEeCnt, b.ccdEeOff, b.ccdEeHit, c.E, b.ccdEeCap, b.ccdEeHitCnt);
-        scan_ints(s, b.ccdEeHitCnt, off, c.E, tot, b.scanBlock);
-        k_ccd_gather<false><<<blocks_for(32 * c.E), 256, 0, s>>>(c, P, b, off, b.seList, b.seCount, b.seCap);
-        k_add_counts<<<1, 32, 0, s>>>(b.seCount, b.seCount, tot, b.seCap);
+        scan_ints(s, b.ccdEeHitCnt, b.scanOff, c.E, b.scanTot, b.scanBlock);
+        k_ccd_gather<false><<<blocks_for(32 * c.E), 256, 0, s>>>(c, P, b, b.scanOff, b.seList, b.seCount, b.seCap);
+        k_add_counts<<<1, 32, 0, s>>>(b.seCount, b.seCount, b.scanTot, b.seCap);
+        cudaStreamWaitEvent(s, join, 0);
     }
-    k_add_counts<<<1, 32, 0, s>>>(b.stCount, b.stCount, nullptr, b.stCap);
-    k_add_counts<<<1, 32, 0, s>>>(b.seCount, b.seCount, nullptr, b.seCap);
+    if (self)
+    {
+        k_add_counts<<<1, 32, 0, s>>>(b.stCount, b.stCount, nullptr, b.stCap);
+        k_add_counts<<<1, 32, 0, s>>>(b.seCount, b.seCount, nullptr, b.seCap);
+    }
 }
 
 void launch_ccd(cudaStream_t s, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join, const DevCloth& c,
