@@ -18,9 +18,10 @@ iterations a substep to the residual target and vertex-substeps/s.
 
 Timing: W untimed frames, then K frames each bracketed by CUDA events on the
 patch's stream; L2 is flushed (a 256 MiB write) before every timed frame,
-outside the events. `e2e` runs K more frames through the C ABI with host
-buffers: the state is uploaded from pinned host memory before each frame and
-read back after it, wall-clock timed.
+outside the events. `e2e` replays the same K frames (from the state the timed
+frames started from) through the C ABI with host buffers: the state is uploaded
+from pinned host memory before each frame and read back after it, wall-clock
+timed, so e2e against `value` is the cost of the transfers and the host calls.
 
 --impl reference times the SolidCloth reference's own CPU step (compiled from
 its sources into oracle/_ref) on the host cores, one substep per step.
@@ -298,6 +299,8 @@ def run_ours(args):
     p.synchronize()
     p.kernel_timing()                      # drop the warm-up frames' records
     st = p.status()
+    # the state the timed frames start from: the end-to-end run replays the same frames
+    start_state = (p.model.positions(), p.model.prev_positions(), p.model.velocities()) if not args.no_e2e else None
     kernels_per_frame = p.graph_kernel_count()
 
     def barrier():
@@ -339,9 +342,7 @@ def run_ours(args):
         pos = torch.empty((sc.num_vertices, 3), dtype=torch.float32).pin_memory().numpy()
         prev = torch.empty_like(torch.from_numpy(pos)).pin_memory().numpy()
         vel = torch.empty_like(torch.from_numpy(pos)).pin_memory().numpy()
-        pos[:] = p.model.positions()
-        prev[:] = p.model.prev_positions()
-        vel[:] = p.model.velocities()
+        pos[:], prev[:], vel[:] = start_state
         barrier()
         t0 = time.perf_counter()
         for _ in range(args.steps):

@@ -2083,10 +2083,11 @@ static void launch_broad_pass1(cudaStream_t s, bool vt, const DevCloth& c, const
 // expand per-query candidate lists (own slots, or the pool for long lists)
 // into the dense pair list; one warp per query, coalesced copies
 __global__ void k_ccd_pairs(const int* cnt, const int* off, const int* cand, const int* pool, const int* poolOff,
-                            int n, int2* pairs, int cap, int* status)
+                            int n, int2* pairs, int cap, int* status, int* hitCnt)
 {
     const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (i >= n) return;
+    if (lane == 0) hitCnt[i] = 0;                 // counted by the narrow phase
     const int m = cnt[i], o = off[i];
     const int* src = m > KCCD ? pool + poolOff[i] : cand + (size_t)i * KCCD;
     for (int k = lane; k < m; k += 32)
@@ -2247,6 +2248,8 @@ __device__ int ccd_ee_test(const DevCloth& c, const SolverParams& P, const Buffe
 
 // narrow phase over the device-counted pair lists (grid-stride; every pair
 // gets its hit flag, so no clearing is needed)
+// per pair: hit flag, and the query's hit count (zeroed by k_ccd_pairs; hits
+// are rare, so the atomics are too)
 __global__ void k_ccd_narrow_vt(DevCloth c, SolverParams P, Buffers b)
 {
     int n = *b.ccdVtPairCount;
@@ -2254,7 +2257,9 @@ __global__ void k_ccd_narrow_vt(DevCloth c, SolverParams P, Buffers b)
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
     {
         SCt rec;
-        b.ccdVtHit[k] = (uint8_t)ccd_vt_test(c, P, b, k, rec);
+        const bool hit = ccd_vt_test(c, P, b, k, rec);
+        b.ccdVtHit[k] = (uint8_t)hit;
+        if (hit) atomicAdd(&b.ccdVtHitCnt[b.ccdVtPairs[k].x], 1);
     }
 }
 
@@ -2265,20 +2270,10 @@ __global__ void k_ccd_narrow_ee(DevCloth c, SolverParams P, Buffers b)
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
     {
         SCt rec;
-        b.ccdEeHit[k] = (uint8_t)ccd_ee_test(c, P, b, k, rec);
+        const bool hit = ccd_ee_test(c, P, b, k, rec);
+        b.ccdEeHit[k] = (uint8_t)hit;
+        if (hit) atomicAdd(&b.ccdEeHitCnt[b.ccdEePairs[k].x], 1);
     }
-}
-
-// hits per query (its pairs are contiguous from off[i]); one warp per query
-__global__ void k_ccd_hit_count(const int* cnt, const int* off, const uint8_t* hit, int n, int cap, int* hcnt)
-{
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (i >= n) return;
-    const int o = off[i], e = min(cap, o + cnt[i]);
-    int h = 0;
-    for (int k = o + lane; k < e; k += 32) h += hit[k];
-    h = __reduce_add_sync(0xffffffffu, h);
-    if (lane == 0) hcnt[i] = h;
 }
 
 // append the hit records after the list's current count, per query in ascending
@@ -3105,12 +3100,10 @@ void launch_compact_self(cudaStream_t s, cudaStream_t side, cudaEvent_t fork, cu
         // edge-edge one (own offsets, block sums and total)
         cudaEventRecord(fork, s);
         cudaStreamWaitEvent(side, fork, 0);
-        k_ccd_hit_count<<<blocks_for(32 * c.N), 256, 0, side>>>(b.ccdVtCnt, b.ccdVtOff, b.ccdVtHit, c.N, b.ccdVtCap, b.ccdVtHitCnt);
         scan_ints(side, b.ccdVtHitCnt, b.scanOff2, c.N, b.scanTot + 1, b.scanBlock2);
         k_ccd_gather<true><<<blocks_for(32 * c.N), 256, 0, side>>>(c, P, b, b.scanOff2, b.stList, b.stCount, b.stCap);
         k_add_counts<<<1, 32, 0, side>>>(b.stCount, b.stCount, b.scanTot + 1, b.stCap);
         cudaEventRecord(join, side);
-        k_ccd_hit_count<<<blocks_for(32 * c.E), 256, 0, s>>>(b.ccdEeCnt, b.ccdEeOff, b.ccdEeHit, c.E, b.ccdEeCap, b.ccdEeHitCnt);
         scan_ints(s, b.ccdEeHitCnt, b.scanOff, c.E, b.scanTot, b.scanBlock);
         k_ccd_gather<false><<<blocks_for(32 * c.E), 256, 0, s>>>(c, P, b, b.scanOff, b.seList, b.seCount, b.seCap);
         k_add_counts<<<1, 32, 0, s>>>(b.seCount, b.seCount, b.scanTot, b.seCap);
@@ -3145,7 +3138,7 @@ void launch_ccd(cudaStream_t s, cudaStream_t side, cudaEvent_t fork, cudaEvent_t
     mark(3, side);
     scan_ints(side, b.ccdVtCnt, b.ccdVtOff, c.N, b.ccdVtPairCount, b.scanBlock2);
     k_ccd_pairs<<<blocks_for(32 * c.N), 256, 0, side>>>(b.ccdVtCnt, b.ccdVtOff, b.ccdVtCand, b.ccdPool, b.ccdVtPoolOff, c.N,
-                                                   b.ccdVtPairs, b.ccdVtCap, c.status);
+                                                   b.ccdVtPairs, b.ccdVtCap, c.status, b.ccdVtHitCnt);
     k_ccd_narrow_vt<<<4 * 148, 128, 0, side>>>(c, P, b);
     cudaEventRecord(join, side);
 
@@ -3156,7 +3149,7 @@ void launch_ccd(cudaStream_t s, cudaStream_t side, cudaEvent_t fork, cudaEvent_t
     mark(1, s);
     scan_ints(s, b.ccdEeCnt, b.ccdEeOff, c.E, b.ccdEePairCount, b.scanBlock);
     k_ccd_pairs<<<blocks_for(32 * c.E), 256, 0, s>>>(b.ccdEeCnt, b.ccdEeOff, b.ccdEeCand, b.ccdPool, b.ccdEePoolOff, c.E,
-                                                b.ccdEePairs, b.ccdEeCap, c.status);
+                                                b.ccdEePairs, b.ccdEeCap, c.status, b.ccdEeHitCnt);
     // narrow phase: a fixed grid strides over the device-side pair counts
     k_ccd_narrow_ee<<<8 * 148, 128, 0, s>>>(c, P, b);
     cudaStreamWaitEvent(s, join, 0);
