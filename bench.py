@@ -104,11 +104,12 @@ def _workload(sc):
 
 
 def _peaks():
+    """HBM copy bandwidth (GB/s) of this pool's B200s and where it comes from"""
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
         d = json.loads(p.read_text())
-        return float(d["hbm_gbs"]), "measured"
-    return 6650.0, "fallback"
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs, burst copy)"
+    return 6650.0, "fallback (MEASURED_PEAKS.json absent: an earlier copy measurement on this pool)"
 
 
 class Clocks:
@@ -407,7 +408,7 @@ def run_ours(args):
                     "frac": d["achieved_gbs"] / peak, "traffic": traffic, "kernel": kernel_names[dom],
                     "algorithmic_bytes_per_launch": d["algorithmic_bytes_per_launch"],
                     "ms_per_launch": d["ms_per_launch"], "launches_timed": d["launches"],
-                    "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs, burst copy)",
+                    "peak_source": peak_kind,
                     "sections": per,
                     "ccd_broad_vt_ms_per_launch": (sections["ccd_broad_vt"][0] / sections["ccd_broad_vt"][1]
                                                    if sections.get("ccd_broad_vt", (0, 0))[1] else None),
