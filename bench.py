@@ -384,7 +384,8 @@ def run_ours(args):
     kernel_names = {"gs_solve": solver,
                     "ccd_broad_ee": "k_bvh_refit + k_ccd_broad_ee + k_ccd_broad_coop (edge-edge swept-box LBVH "
                                     "refit and query: one walk per lane, long lists one warp per query)",
-                    "colliders": "k_vertex_colliders + k_tri_colliders + k_edge_colliders (collider detection)"}
+                    "colliders": "k_vertex_colliders (+ k_tri_colliders, k_edge_colliders when continuous collision is "
+                                 "off: with it on they run on another branch, untimed)"}
     walk, walk_ms = p.model.broad_phase_mode()
     per = {}
     for k in algo:

@@ -1550,12 +1550,27 @@ void ClothPatch::record_substep(float h)
     Buffers& b = m.buf;
     cudaStream_t s = stream;
     launch_predict(s, c, P);
-    // ClothModel::DetectCollisions (Physics/ClothCollision.cpp:17-48)
-    timing_mark(SEC_COLLIDERS, false, s);
-    launch_vertex_colliders(s, c, P, b, m.vcollHost.data());
-    launch_tri_edge_colliders(s, c, P, b, m.vcollHost.data(), (int)m.vcollHost.size(), m.prm.flags);
-    timing_mark(SEC_COLLIDERS, true, s);
     const bool self = (m.prm.flags & CF_SELF) != 0, ccd = m.prm.ccd;
+    // ClothModel::DetectCollisions (Physics/ClothCollision.cpp:17-48)
+    if (ccd)
+    {
+        // the vertex contacts only read the predicted positions: they run on the
+        // side stream ahead of its continuous-collision branch, which the main
+        // stream joins before anything reads them
+        cudaEventRecord(evFork, s);
+        cudaStreamWaitEvent(side, evFork, 0);
+        timing_mark(SEC_COLLIDERS, false, side);
+        launch_vertex_colliders(side, c, P, b, m.vcollHost.data());
+        timing_mark(SEC_COLLIDERS, true, side);
+        launch_tri_edge_colliders(s, c, P, b, m.vcollHost.data(), (int)m.vcollHost.size(), m.prm.flags);
+    }
+    else
+    {
+        timing_mark(SEC_COLLIDERS, false, s);
+        launch_vertex_colliders(s, c, P, b, m.vcollHost.data());
+        launch_tri_edge_colliders(s, c, P, b, m.vcollHost.data(), (int)m.vcollHost.size(), m.prm.flags);
+        timing_mark(SEC_COLLIDERS, true, s);
+    }
     if (self)
     {
         launch_bvh_refit(s, m.triBvh, c, 0, 0.f);
