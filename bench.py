@@ -29,6 +29,7 @@ its sources into oracle/_ref) on the host cores, one substep per step.
 from __future__ import annotations
 
 import argparse
+import contextlib
 import json
 import os
 import statistics
@@ -173,6 +174,22 @@ def _dist():
     return ws, rank, local
 
 
+@contextlib.contextmanager
+def _reference_output_to_stderr():
+    """The reference's C++ prints diagnostics (printf) while it sets a cloth up;
+    send file descriptor 1 to stderr meanwhile, so stdout carries only the JSON line."""
+    import ctypes as C
+    sys.stdout.flush()
+    saved = os.dup(1)
+    os.dup2(2, 1)
+    try:
+        yield
+    finally:
+        C.CDLL(None).fflush(None)          # the C library's buffered stdout goes to stderr too
+        os.dup2(saved, 1)
+        os.close(saved)
+
+
 def cpu_reference_rate(sc, substeps: int, threads: int | None = None):
     """Time the reference's own CPU step (oracle/_ref) on a bounded sample:
     `substeps` substeps of the scene after one untimed substep."""
@@ -220,21 +237,22 @@ def run_reference(args):
         work = sample[0]
         label = sample[0].name
     clothes = []
-    for sc in sample:
-        r = RefCloth.from_scene(sc)
-        pa = sc.params.as_array().copy()
-        pa[9] = 1
-        r._fn("set_params")(r.h, pa.ctypes.data_as(C.POINTER(C.c_float)), pa.size)
-        clothes.append((r, sc.dt / sc.params.substeps))
-    for _ in range(args.warmup):
-        for r, h in clothes:
-            r.step(h)
     times = []
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        for r, h in clothes:
-            r.step(h)
-        times.append(time.perf_counter() - t0)
+    with _reference_output_to_stderr():
+        for sc in sample:
+            r = RefCloth.from_scene(sc)
+            pa = sc.params.as_array().copy()
+            pa[9] = 1
+            r._fn("set_params")(r.h, pa.ctypes.data_as(C.POINTER(C.c_float)), pa.size)
+            clothes.append((r, sc.dt / sc.params.substeps))
+        for _ in range(args.warmup):
+            for r, h in clothes:
+                r.step(h)
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            for r, h in clothes:
+                r.step(h)
+            times.append(time.perf_counter() - t0)
     tot = sum(times)
     value = sum(sc.num_vertices for sc in sample) * args.steps / tot
     line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
@@ -432,7 +450,8 @@ def run_ours(args):
             if available("ref"):
                 ref_sc = sc.mine[len(sc.mine) // 2] if isinstance(sc, _Batch) else sc
                 nsub = 2 if ref_sc.num_vertices > 4096 else 32
-                v, secs, cores = cpu_reference_rate(ref_sc, nsub)
+                with _reference_output_to_stderr():
+                    v, secs, cores = cpu_reference_rate(ref_sc, nsub)
                 cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
                        "sample": f"{nsub} substeps of {ref_sc.name} after one untimed substep ({secs:.1f} s), "
                                  f"the reference's own C++ (oracle/_ref, OpenMP {cores} threads)"}
