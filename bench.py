@@ -433,6 +433,19 @@ def run_ours(args):
                                                    if sections.get("ccd_broad_vt", (0, 0))[1] else None),
                     "broad_phase_walk": {"chosen": p.model.BROAD_WALKS[walk],
                                          "tuned_ms": walk_ms.tolist()}}
+        if dom == "gs_solve" and ch[0] == 1:
+            # the cluster solve is a chain of colour phases: its latency floor is the
+            # phase count times the cost of one phase with no projection arithmetic
+            n_fem = len(p.model.constraint_order(0)[1]) - 1
+            n_bend = len(p.model.constraint_order(1)[1]) - 1
+            phases = it * n_fem + ((it + 1) // 2) * n_bend + (it if sc.sdfs or sc.spheres or sc.walls is not None else 0)
+            us0 = float(api.lib().scProbeClusterPhase(0, 20000))
+            us1 = float(api.lib().scProbeClusterPhase(1, 20000))
+            if us1 > 0:
+                floor_ms = phases * us1 * 1e-3
+                roofline["latency"] = {"phases_per_launch": phases, "us_per_phase_barrier": us0,
+                                       "us_per_phase_barrier_dsmem": us1, "floor_ms": floor_ms,
+                                       "frac": floor_ms / d["ms_per_launch"]}
 
     # plain versus learned warm start at the residual target (trained weights from
     # solidcloth_b200/data/warmstart.npz, held-out 64x64 drapes)

@@ -342,6 +342,13 @@ SCEXP int scGetGraphKernelCount(scClothPatch patch);
    the patch stream; returns milliseconds per sweep, or a negative value on error.
    Particle positions are modified. */
 SCEXP float scProfileSweep(scClothPatch patch, int kind, int reps);
+/* Latency floor of the cluster solver's colour phases (addition, no reference
+   counterpart): runs `phases` phases on one thread-block cluster of the solver's
+   size and block shape, separated by cluster barriers, with nothing else in a
+   phase (kind 0) or one distributed-shared-memory read and write per thread
+   (kind 1), and returns microseconds per phase (negative on error). Uses the
+   current device and the legacy default stream; allocates nothing. */
+SCEXP float scProbeClusterPhase(int kind, int phases);
 /* Section timing inside the frame graph (additions, no reference counterpart):
    frames > 0 brackets, in every substep, the Gauss-Seidel solve (section 0), the
    edge-edge (1) and vertex-triangle (2) continuous-collision broad phases and the

@@ -176,6 +176,7 @@ SIGNATURES = {
     "scGetCudaStream": ([scClothPatch], C.c_void_p),
     "scGetGraphKernelCount": ([scClothPatch], C.c_int),
     "scProfileSweep": ([scClothPatch, C.c_int, C.c_int], C.c_float),
+    "scProbeClusterPhase": ([C.c_int, C.c_int], C.c_float),
     "scSetKernelTiming": ([scClothPatch, C.c_int], C.c_bool),
     "scGetKernelTiming": ([scClothPatch, _f, _i], C.c_int),
     "scRenderCloth": ([scClothPatch, _f, _f, C.c_int, C.c_int, C.c_void_p, C.c_void_p], C.c_int),

@@ -1023,6 +1023,18 @@ int scGetKernelTiming(scClothPatch p, float* ms, int* counts)
     return cp->read_timing(ms, counts);
 }
 
+float scProbeClusterPhase(int kind, int phases)
+{
+    if ((kind != 0 && kind != 1) || phases < 1 || phases > 10000000)
+    {
+        set_error(SC_ERR_ARG, "probe kind must be 0 or 1, phases 1 .. 1e7");
+        return -1.f;
+    }
+    const float us = probe_cluster_phase(kind, phases);
+    if (us < 0.f) set_error(SC_ERR_UNSUPPORTED, "no thread-block cluster of the solver's size fits on this device");
+    return us;
+}
+
 float scProfileSweep(scClothPatch p, int kind, int reps)
 {
     ClothPatch* cp = P(p);

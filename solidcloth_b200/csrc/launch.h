@@ -95,6 +95,10 @@ void launch_solve_multi_contacts(cudaStream_t s, const DevCloth& c, const Solver
 void launch_colour_contacts(cudaStream_t s, const DevCloth& c, const Buffers& b);
 void launch_bvh_refit(cudaStream_t s, const DevBVH& bvh, const DevCloth& c, int kind, float tol);
 size_t ccd_coop_smem(int depth);      // dynamic shared memory of the second broad-phase pass
+// microseconds a phase of the cluster solver's barrier structure costs (kind 0:
+// barrier only; 1: plus one distributed-shared-memory read and write), -1 if no
+// cluster of the solver's size fits
+float probe_cluster_phase(int kind, int phases);
 void ccd_kernel_setup();              // kernel attributes (once per device, outside capture)
 void launch_self_proximity(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b,
                            const DevBVH& triBvh, const DevBVH& edgeBvh);

@@ -2910,6 +2910,65 @@ int gs_cluster_size(int N, int& shift, size_t& smem)
     return cs;
 }
 
+// Latency probe of the cluster solver's phase structure: `phases` phases of one
+// cluster of the solver's size and block shape, separated by cluster barriers,
+// with nothing in a phase (kind 0) or one distributed-shared-memory read and
+// write per thread (kind 1: every CTA updates its neighbour's block, a
+// permutation, so no two CTAs write one word in a phase). Its time per phase is
+// what a colour phase costs before any projection arithmetic.
+__device__ int g_phaseProbeSink;
+
+__global__ void __launch_bounds__(GS_THREADS) k_phase_probe(int phases, int kind)
+{
+    __shared__ int cell[GS_THREADS];
+    cg::cluster_group cl = cg::this_cluster();
+    const unsigned rank = cl.block_rank(), n = cl.num_blocks();
+    cell[threadIdx.x] = (int)threadIdx.x;
+    cl.sync();
+    int acc = 0;
+    for (int k = 0; k < phases; k++)
+    {
+        if (kind == 1)
+        {
+            int* peer = cl.map_shared_rank(cell, (rank + 1 + (unsigned)k) % n);
+            const int v = peer[threadIdx.x];
+            peer[threadIdx.x] = v + 1;
+            acc += v;
+        }
+        cl.sync();                                   // also keeps every block alive until the last access
+    }
+    if (acc == 0x7fffffff) g_phaseProbeSink = acc;   // keeps the loads; never true
+}
+
+float probe_cluster_phase(int kind, int phases)
+{
+    int shift = 0;
+    size_t smem = 0;
+    const int cs = gs_cluster_size(1, shift, smem);
+    if (cs == 0 || phases < 1) return -1.f;
+    cudaFuncSetAttribute(k_phase_probe, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cs);
+    cfg.blockDim = dim3(GS_THREADS);
+    cudaLaunchAttribute at;
+    at.id = cudaLaunchAttributeClusterDimension;
+    at.val.clusterDim.x = cs; at.val.clusterDim.y = 1; at.val.clusterDim.z = 1;
+    cfg.attrs = &at; cfg.numAttrs = 1;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0); cudaEventCreate(&e1);
+    float ms = -1.f;
+    if (cudaLaunchKernelEx(&cfg, k_phase_probe, 1000, kind) == cudaSuccess)       // warm-up
+    {
+        cudaEventRecord(e0, 0);
+        cudaLaunchKernelEx(&cfg, k_phase_probe, phases, kind);
+        cudaEventRecord(e1, 0);
+        if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) ms = -1.f;
+    }
+    cudaEventDestroy(e0); cudaEventDestroy(e1);
+    cudaGetLastError();
+    return ms < 0.f ? -1.f : 1000.f * ms / (float)phases;
+}
+
 void launch_gs_cluster(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b, GsPlan plan,
                        int clusterSize, size_t smem)
 {
