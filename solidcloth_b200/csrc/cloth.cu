@@ -521,6 +521,70 @@ static void greedy_colour(int n, int N, Get verts, std::vector<int>& order, std:
     for (int c = 0; c < maxc; c++) start[c + 1] += start[c];
 }
 
+// Exact colouring of a small conflict graph (items sharing a vertex conflict)
+// with at most K colours: DSatur order with backtracking, bounded. Empty if none
+// is found within the budget.
+static std::vector<int> exact_colouring(const std::vector<std::vector<int>>& verts, int K)
+{
+    const int m = (int)verts.size();
+    std::vector<std::vector<int>> nb(m);
+    for (int a = 0; a < m; a++)
+        for (int b = 0; b < m; b++)
+        {
+            if (a == b) continue;
+            bool share = false;
+            for (int x : verts[a]) for (int y : verts[b]) share |= x == y;
+            if (share) nb[a].push_back(b);
+        }
+    std::vector<int> tc(m, -1);
+    long budget = 5000000;
+    std::function<bool()> search = [&]() -> bool {
+        int best = -1, bs = -1, bd = -1;
+        for (int a = 0; a < m; a++)
+        {
+            if (tc[a] >= 0) continue;
+            uint32_t used = 0;
+            for (int b : nb[a]) if (tc[b] >= 0) used |= 1u << tc[b];
+            const int s = __builtin_popcount(used), d = (int)nb[a].size();
+            if (s > bs || (s == bs && d > bd)) { best = a; bs = s; bd = d; }
+        }
+        if (best < 0) return true;
+        if (--budget < 0) return false;
+        uint32_t used = 0;
+        int top = -1;
+        for (int a = 0; a < m; a++) top = std::max(top, tc[a]);
+        for (int b : nb[best]) if (tc[b] >= 0) used |= 1u << tc[b];
+        for (int k = 0; k < K && k <= top + 1; k++)
+        {
+            if (used >> k & 1u) continue;
+            tc[best] = k;
+            if (search()) return true;
+            tc[best] = -1;
+        }
+        return false;
+    };
+    if (K > 32 || !search()) return {};
+    return tc;
+}
+
+// true if no particle is in two constraints of one colour
+template <int V, typename Get>
+static bool proper_colouring(int n, int N, Get verts, const std::vector<int>& col)
+{
+    std::vector<uint64_t> seen(N, 0);
+    for (int k = 0; k < n; k++)
+    {
+        uint32_t v[V];
+        verts(k, v);
+        for (uint32_t x : v)
+        {
+            if (col[k] < 0 || col[k] >= 64 || (seen[x] >> col[k] & 1ull)) return false;
+            seen[x] |= 1ull << col[k];
+        }
+    }
+    return true;
+}
+
 // Bends of grid clothes, coloured with a pattern of period 4 in both grid
 // directions: the 48 bends of the 4 x 4 torus triangulated like the grid
 // (alternating diagonals by cell parity) are coloured once by an exact search
@@ -550,54 +614,17 @@ static bool periodic_bend_colours(const std::vector<uint4>& bends, const std::ve
             opp[{std::min(x, y), std::max(x, y)}].push_back(z);
         }
     std::vector<std::pair<int, int>> key;
-    std::vector<std::array<int, 4>> tv;
+    std::vector<std::vector<int>> tv;
     for (auto& e : opp)
     {
         if (e.second.size() != 2) return false;
         key.push_back(e.first);
         tv.push_back({e.first.first, e.first.second, e.second[0], e.second[1]});
     }
-    const int m = (int)key.size();
-    std::vector<std::vector<int>> nb(m);
-    for (int a = 0; a < m; a++)
-        for (int b = 0; b < m; b++)
-        {
-            if (a == b) continue;
-            bool share = false;
-            for (int x : tv[a]) for (int y : tv[b]) share |= x == y;
-            if (share) nb[a].push_back(b);
-        }
-    // DSatur order with backtracking (bounded)
-    std::vector<int> tc(m, -1);
-    long budget = 5000000;
-    std::function<bool()> search = [&]() -> bool {
-        int best = -1, bs = -1, bd = -1;
-        for (int a = 0; a < m; a++)
-        {
-            if (tc[a] >= 0) continue;
-            uint32_t used = 0;
-            for (int b : nb[a]) if (tc[b] >= 0) used |= 1u << tc[b];
-            const int s = __builtin_popcount(used), d = (int)nb[a].size();
-            if (s > bs || (s == bs && d > bd)) { best = a; bs = s; bd = d; }
-        }
-        if (best < 0) return true;
-        if (--budget < 0) return false;
-        uint32_t used = 0;
-        int top = -1;
-        for (int a = 0; a < m; a++) top = std::max(top, tc[a]);
-        for (int b : nb[best]) if (tc[b] >= 0) used |= 1u << tc[b];
-        for (int k = 0; k < K && k <= top + 1; k++)
-        {
-            if (used >> k & 1u) continue;
-            tc[best] = k;
-            if (search()) return true;
-            tc[best] = -1;
-        }
-        return false;
-    };
-    if (!search()) return false;
+    const std::vector<int> tc = exact_colouring(tv, K);
+    if (tc.empty()) return false;
     std::map<std::pair<int, int>, int> colourOf;
-    for (int a = 0; a < m; a++) colourOf[key[a]] = tc[a];
+    for (size_t a = 0; a < key.size(); a++) colourOf[key[a]] = tc[a];
     col.assign(bends.size(), 0);
     for (size_t k = 0; k < bends.size(); k++)
     {
@@ -607,18 +634,61 @@ static bool periodic_bend_colours(const std::vector<uint4>& bends, const std::ve
         if (it == colourOf.end()) return false;
         col[k] = it->second;
     }
-    // proper: no particle in two bends of one colour
-    std::vector<uint32_t> seen(N, 0);
-    for (size_t k = 0; k < bends.size(); k++)
+    return proper_colouring<4>((int)bends.size(), N, [&](int k, uint32_t* v) {
+        v[0] = bends[k].x; v[1] = bends[k].y; v[2] = bends[k].z; v[3] = bends[k].w; }, col);
+}
+
+// Links of grid clothes (stretch (0,1), (1,0); shear (1,1), (1,-1); bend (0,2),
+// (2,0) in grid steps, ClothPatch::Init(grid)), coloured with a pattern of
+// period 6: the 216 links of the 6 x 6 torus are coloured once by an exact
+// search with 12 colours — the links at one particle, so the fewest possible —
+// and every link takes its image's colour. Period 6 is the smallest that keeps
+// the images of two links at one particle apart (the bend links span two steps)
+// and admits 12 colours. Checked proper; false means "use the greedy colouring".
+static bool periodic_link_colours(const std::vector<uint2>& links, const std::vector<int2>& ij, int N, std::vector<int>& col)
+{
+    const int P = 6, K = 12;
+    auto T = [&](int j, int i) { return ((j % P + P) % P) * P + ((i % P + P) % P); };
+    const int off[6][2] = {{0, 1}, {1, 0}, {1, 1}, {1, -1}, {0, 2}, {2, 0}};
+    std::map<std::pair<int, int>, int> index;
+    std::vector<std::vector<int>> tv;
+    for (int j = 0; j < P; j++)
+        for (int i = 0; i < P; i++)
+            for (auto& o : off)
+            {
+                const int u = T(j, i), v = T(j + o[0], i + o[1]);
+                const std::pair<int, int> k{std::min(u, v), std::max(u, v)};
+                if (index.count(k)) return false;            // two links with one image
+                index[k] = (int)tv.size();
+                tv.push_back({u, v});
+            }
+    const std::vector<int> tc = exact_colouring(tv, K);
+    if (tc.empty()) return false;
+    col.assign(links.size(), 0);
+    for (size_t k = 0; k < links.size(); k++)
     {
-        const uint32_t v[4] = {bends[k].x, bends[k].y, bends[k].z, bends[k].w};
-        for (uint32_t x : v)
-        {
-            if (seen[x] >> col[k] & 1u) return false;
-            seen[x] |= 1u << col[k];
-        }
+        const int2 p = ij[links[k].x], q = ij[links[k].y];
+        const int u = T(p.x, p.y), v = T(q.x, q.y);
+        auto it = index.find({std::min(u, v), std::max(u, v)});
+        if (it == index.end()) return false;
+        col[k] = tc[it->second];
     }
-    return true;
+    return proper_colouring<2>((int)links.size(), N, [&](int k, uint32_t* v) { v[0] = links[k].x; v[1] = links[k].y; },
+                               col);
+}
+
+// replace a greedy (colour, index) order by the one of `col` when it needs fewer colours
+static void adopt_colours(const std::vector<int>& col, std::vector<int>& order, std::vector<int>& start)
+{
+    if (col.empty()) return;
+    const int K = *std::max_element(col.begin(), col.end()) + 1;
+    if (K >= (int)start.size() - 1) return;
+    order.resize(col.size());
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return col[a] < col[b]; });
+    start.assign(K + 1, 0);
+    for (int c : col) start[c + 1]++;
+    for (int c = 0; c < K; c++) start[c + 1] += start[c];
 }
 
 void ClothModel::colour_constraints()
@@ -627,23 +697,16 @@ void ClothModel::colour_constraints()
                      triOrder, triColourStart);
     greedy_colour<4>((int)bends.size(), N, [&](int i, uint32_t* v) { v[0] = bends[i].x; v[1] = bends[i].y; v[2] = bends[i].z; v[3] = bends[i].w; },
                      bendOrder, bendColourStart);
-    std::vector<int> col;
-    if ((int)gridIJ.size() == N && !bends.empty() && periodic_bend_colours(bends, gridIJ, N, col))
-    {
-        const int K = *std::max_element(col.begin(), col.end()) + 1;
-        if (K < (int)bendColourStart.size() - 1)
-        {
-            // solve order = (colour, index), as the greedy colouring's
-            bendOrder.resize(bends.size());
-            std::iota(bendOrder.begin(), bendOrder.end(), 0);
-            std::stable_sort(bendOrder.begin(), bendOrder.end(), [&](int a, int b) { return col[a] < col[b]; });
-            bendColourStart.assign(K + 1, 0);
-            for (int c : col) bendColourStart[c + 1]++;
-            for (int c = 0; c < K; c++) bendColourStart[c + 1] += bendColourStart[c];
-        }
-    }
     greedy_colour<2>((int)links.size(), N, [&](int i, uint32_t* v) { v[0] = links[i].x; v[1] = links[i].y; },
                      linkOrder, linkColourStart);
+    // grid clothes: the periodic colourings, where they need fewer colours
+    if ((int)gridIJ.size() == N)
+    {
+        std::vector<int> col;
+        if (!bends.empty() && periodic_bend_colours(bends, gridIJ, N, col)) adopt_colours(col, bendOrder, bendColourStart);
+        col.clear();
+        if (!links.empty() && periodic_link_colours(links, gridIJ, N, col)) adopt_colours(col, linkOrder, linkColourStart);
+    }
 }
 
 bool ClothModel::upload_topology(const HMesh& mesh)

@@ -227,6 +227,25 @@ def _links_scene(dihedral=False):
 
 
 @pytest.mark.parametrize("dihedral", [False, True])
+def test_link_colouring(dihedral):
+    """Grid links (stretch, shear and, without dihedral bending, bend links) are
+    coloured properly; with all three kinds the period-6 pattern needs 12
+    colours, the most links at one particle."""
+    from solidcloth_b200 import api
+    sc = _links_scene(dihedral)
+    w, p = api.load_scene(sc)
+    idx, _ = p.model.links()
+    order, start = p.model.constraint_order(2)
+    assert sorted(order.tolist()) == list(range(len(idx)))
+    for c in range(len(start) - 1):
+        ids = idx[order[start[c]:start[c + 1]]].reshape(-1)
+        assert len(np.unique(ids)) == ids.size, "two links of one colour share a particle"
+    per = np.bincount(idx.reshape(-1).astype(np.int64), minlength=sc.num_vertices).max()
+    if not dihedral:
+        assert len(start) - 1 == per == 12
+
+
+@pytest.mark.parametrize("dihedral", [False, True])
 @pytest.mark.parametrize("fixed", [True, False])
 def test_mass_spring_check_mode(dihedral, fixed):
     """The mass-spring path (FEM off: SolveLinks, Physics/ClothPBD.cpp:9-50, with
