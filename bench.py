@@ -1,16 +1,19 @@
 """Cloth-step benchmark: vertex-substeps/s on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config cfg1]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config cfg2]
 
-Workload (default): the 128x128 drape onto a 64^3 sphere SDF with self-collision,
-8 substeps x 15 iterations per frame (scenes.cfg1). One "step" is one frame,
-i.e. one scStepCloth(1/60) call = 8 substeps. Multi-GPU (torchrun, one process
-per GPU) runs independent replicas (a single cloth does not shard): scaling is
-weak and `value` is the sum over ranks of the device-timed throughput, using the
-max time over ranks. --config cfg3 steps the 512 uneven instances as one batch
-patch; under torchrun the instances are partitioned over the ranks (no
-collective on the data path, strong scaling) and `value` is all instances'
-vertex-substeps over the slowest rank's time.
+Workload (default): the 256x256 self-colliding drape (65,536 vertices, 1.5 m)
+dropped 0.5 m onto a level-5 icosphere mesh collider (10,242 vertices, 20,480
+triangles, radius 0.25 m) standing on a ground plane; mesh contacts through the
+collider's AABB tree, continuous self-collision, 8 substeps x 20 iterations per
+frame (scenes.cfg2). One "step" is one frame, i.e. one scStepCloth(1/60) call =
+8 substeps, in both arms. Multi-GPU (torchrun, one process per GPU) runs
+independent replicas (a single cloth does not shard): scaling is weak and
+`value` is the sum over ranks of the device-timed throughput, using the max time
+over ranks. --config cfg3 steps the 512 uneven instances as one batch patch;
+under torchrun the instances are partitioned over the ranks (no collective on
+the data path, strong scaling) and `value` is all instances' vertex-substeps
+over the slowest rank's time.
 
 The line's `learned` object compares the plain solver with the learned warm
 start (solidcloth_b200/data/warmstart.npz) on held-out drapes: Gauss-Seidel
@@ -22,9 +25,13 @@ outside the events. `e2e` replays the same K frames (from the state the timed
 frames started from) through the C ABI with host buffers: the state is uploaded
 from pinned host memory before each frame and read back after it, wall-clock
 timed, so e2e against `value` is the cost of the transfers and the host calls.
+SM clocks and throttle reasons are sampled through NVML every 10 ms during the
+timed frames.
 
 --impl reference times the SolidCloth reference's own CPU step (compiled from
-its sources into oracle/_ref) on the host cores, one substep per step.
+its sources into oracle/_ref, OpenMP on all host threads) on the same frames:
+W untimed frames from the same initial state, then K timed frames, one frame
+(8 substeps) per step, with the same `config`.
 """
 from __future__ import annotations
 
@@ -51,12 +58,12 @@ UNIT = "vertex-substeps/s"
 def _args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--self", dest="self_mode", default="ccd", choices=["ccd", "proximity", "both"],
                     help="self-collision: the continuous detector (default), the live proximity path, or both")
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="cfg1", choices=["cfg0", "cfg1", "cfg2", "cfg3"])
+    ap.add_argument("--config", default="cfg2", choices=["cfg0", "cfg1", "cfg2", "cfg3"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the plain-vs-learned warm-start comparison")
@@ -95,13 +102,13 @@ def _workload(sc):
                             f"one batch patch (one graph per frame, one solver launch per substep)",
                 "flags": sc.params.flags, "iterations": "fixed",
                 "l2": "flushed (256 MiB write) before every timed frame; the batch state (~30 MB/1M vertices) exceeds L2 anyway",
-                "step": "one frame = one scStepCloth call on the batch"}
+                "step": f"one frame = one scStepCloth(1/60) call on the batch ({sc.params.substeps} substeps)"}
     return {"workload": f"{sc.name}: {sc.n}x{sc.n} grid ({sc.num_vertices} vertices), "
                         f"{sc.params.substeps} substeps x {sc.params.iterations} iterations per frame, dt 1/60",
             "flags": sc.params.flags, "colliders": {"sdf": len(sc.sdfs), "mesh": len(sc.meshes),
                                                       "walls": sc.walls is not None},
             "iterations": "fixed", "l2": "flushed (256 MiB write) before every timed frame",
-            "step": "one frame = one scStepCloth call"}
+            "step": f"one frame = one scStepCloth(1/60) call ({sc.params.substeps} substeps)"}
 
 
 def _peaks():
@@ -114,14 +121,52 @@ def _peaks():
 
 
 class Clocks:
-    """nvidia-smi sampler running during the timed region."""
+    """SM clock and throttle-reason sampler running during the timed region:
+    NVML read every 10 ms from a thread (nvidia-smi -lms 50 as the fallback)."""
+
+    # NVML clocks-event reason bits
+    _REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+                "sw_power_cap": 0x4}
 
     def __init__(self, index: int):
         self.index = index
+        self.rows = []          # (sm MHz, max sm MHz, reason bits)
         self.proc = None
         self.path = None
+        self._stop = None
+        self._thread = None
+
+    def _nvml_loop(self, nv, h):
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self._stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.rows.append((float(sm), float(mx), int(bits)))
+            except Exception:
+                pass
+            self._stop.wait(0.01)
 
     def __enter__(self):
+        import threading
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            h = None
+            try:
+                # the CUDA device's own GPU (NVML numbers GPUs without CUDA_VISIBLE_DEVICES)
+                import torch
+                pr = torch.cuda.get_device_properties(self.index)
+                h = nv.nvmlDeviceGetHandleByPciBusId(
+                    f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0".encode())
+            except Exception:
+                h = nv.nvmlDeviceGetHandleByIndex(self.index)
+            self._stop = threading.Event()
+            self._thread = threading.Thread(target=self._nvml_loop, args=(nv, h), daemon=True)
+            self._thread.start()
+            return self
+        except Exception:
+            self._thread = None
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
         try:
@@ -137,6 +182,9 @@ class Clocks:
         return self
 
     def __exit__(self, *a):
+        if self._thread is not None:
+            self._stop.set()
+            self._thread.join(timeout=5)
         if self.proc:
             self.proc.terminate()
             try:
@@ -145,6 +193,13 @@ class Clocks:
                 self.proc.kill()
 
     def summary(self):
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        if self._thread is not None:
+            if not self.rows:
+                return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+            reasons = sorted({n for _, _, b in self.rows for n in names if b & self._REASONS[n]})
+            return {"sm_mhz": statistics.median(r[0] for r in self.rows), "sm_max_mhz": max(r[1] for r in self.rows),
+                    "reasons": reasons, "samples": len(self.rows), "source": "NVML every 10 ms"}
         rows = []
         try:
             for line in Path(self.path).read_text().splitlines():
@@ -158,13 +213,12 @@ class Clocks:
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
         reasons = set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for r in rows:
             for k, n in enumerate(names):
                 if r[5 + k].lower() == "active":
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(rows)}
+                "reasons": sorted(reasons), "samples": len(rows), "source": "nvidia-smi -lms 50"}
 
 
 def _dist():
@@ -190,27 +244,41 @@ def _reference_output_to_stderr():
         os.close(saved)
 
 
-def cpu_reference_rate(sc, substeps: int, threads: int | None = None):
-    """Time the reference's own CPU step (oracle/_ref) on a bounded sample:
-    `substeps` substeps of the scene after one untimed substep."""
+def cpu_reference_rate(sc, frames: int = 1, serial: bool = False, substeps: int | None = None):
+    """Time the reference's own CPU step (oracle/_ref) on a bounded sample of the
+    workload: `frames` whole frames (scStepCloth(1/60), all substeps) from the
+    scene's initial state, or, with `substeps`, that many single substeps from
+    it. serial=True: the build without OpenMP (one thread, as the reference's
+    C-ABI library); else the OpenMP build on all host threads.
+    Returns (vertex-substeps/s, seconds, threads)."""
     import ctypes as C
-    from oracle.bridge import RefCloth, _load, REF_LIB
-    if threads:
-        RefCloth.set_threads(threads)
-    cores = _load(REF_LIB, "ref_").ref_max_threads()
-    r = RefCloth.from_scene(sc)
-    h = sc.dt / sc.params.substeps
-    # one substep per call: a patch with numSteps = 1 and dt = h
-    pa = sc.params.as_array().copy()
-    pa[9] = 1
-    r._fn("set_params")(r.h, pa.ctypes.data_as(C.POINTER(C.c_float)), pa.size)
-    r.step(h)
+    from oracle.bridge import RefCloth, _load, REF_LIB, REF_SERIAL_LIB
+    cores = 1 if serial else _load(REF_LIB, "ref_").ref_max_threads()
+    r = RefCloth.from_scene(sc, serial=serial)
+    if substeps:
+        # one substep per call: a patch with numSteps = 1 and dt = h
+        pa = sc.params.as_array().copy()
+        pa[9] = 1
+        r._fn("set_params")(r.h, pa.ctypes.data_as(C.POINTER(C.c_float)), pa.size)
+        h, calls, per_call = sc.dt / sc.params.substeps, substeps, 1
+    else:
+        h, calls, per_call = sc.dt, frames, sc.params.substeps
     t0 = time.perf_counter()
-    for _ in range(substeps):
+    for _ in range(calls):
         r.step(h)
     dt = time.perf_counter() - t0
     r.close()
-    return sc.num_vertices * substeps / dt, dt, int(cores)
+    return sc.num_vertices * calls * per_call / dt, dt, int(cores)
+
+
+def _cpu_model():
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
 
 
 def run_reference(args):
@@ -222,14 +290,13 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libscref.so not built (reference sources absent at build time)"}))
         return
     from oracle.bridge import RefCloth, _load, REF_LIB
-    import ctypes as C
     lib = _load(REF_LIB, "ref_")
     cores = lib.ref_max_threads()
     if args.config == "cfg3":
-        # a bounded sample of the batch: 8 instances spread over the list, one substep each per step
+        # a bounded sample of the batch: 8 instances spread over the list, one frame each per step
         from solidcloth_b200 import scenes
-        insts = scenes.cfg3_instances()
-        sample = insts[::len(insts) // 8][:8]
+        insts = scenes.cfg3_instances()[:args.instances]
+        sample = insts[::max(1, len(insts) // 8)][:8]
         work = _Batch(insts, 0, 1)
         label = f"{len(sample)} of the {len(insts)} cfg3 instances ({sum(x.num_vertices for x in sample)} vertices)"
     else:
@@ -240,28 +307,28 @@ def run_reference(args):
     times = []
     with _reference_output_to_stderr():
         for sc in sample:
-            r = RefCloth.from_scene(sc)
-            pa = sc.params.as_array().copy()
-            pa[9] = 1
-            r._fn("set_params")(r.h, pa.ctypes.data_as(C.POINTER(C.c_float)), pa.size)
-            clothes.append((r, sc.dt / sc.params.substeps))
+            clothes.append(RefCloth.from_scene(sc))
+        # the same frames as the GPU arm: W untimed frames from the initial state, then K timed ones
         for _ in range(args.warmup):
-            for r, h in clothes:
-                r.step(h)
+            for r, sc in zip(clothes, sample):
+                r.step(sc.dt)
         for _ in range(args.steps):
             t0 = time.perf_counter()
-            for r, h in clothes:
-                r.step(h)
+            for r, sc in zip(clothes, sample):
+                r.step(sc.dt)
             times.append(time.perf_counter() - t0)
     tot = sum(times)
-    value = sum(sc.num_vertices for sc in sample) * args.steps / tot
+    subs = sample[0].params.substeps
+    value = sum(sc.num_vertices for sc in sample) * subs * args.steps / tot
     line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
             "higher_is_better": True, "scaling": "strong" if args.config == "cfg3" else "weak", "vs_baseline": None,
-            "dtype": "fp32", "data": "synthetic", "config": dict(_workload(work), step="one substep (reference CPU)"),
+            "dtype": "fp32", "data": "synthetic", "config": _workload(work),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
-                             "sample": f"{args.steps} substeps of {label} after {args.warmup} warm-up substeps, "
-                                       f"OpenMP threads = {cores}"},
+                             "cpu": _cpu_model(),
+                             "sample": f"frames {args.warmup + 1}-{args.warmup + args.steps} of {label} (one frame = "
+                                       f"{subs} substeps per step) after {args.warmup} untimed frames from the initial "
+                                       f"state, the reference's own C++ (oracle/_ref), OpenMP threads = {cores}"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -462,12 +529,21 @@ def run_ours(args):
             from oracle.bridge import available
             if available("ref"):
                 ref_sc = sc.mine[len(sc.mine) // 2] if isinstance(sc, _Batch) else sc
-                nsub = 2 if ref_sc.num_vertices > 4096 else 32
                 with _reference_output_to_stderr():
-                    v, secs, cores = cpu_reference_rate(ref_sc, nsub)
-                cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
-                       "sample": f"{nsub} substeps of {ref_sc.name} after one untimed substep ({secs:.1f} s), "
-                                 f"the reference's own C++ (oracle/_ref, OpenMP {cores} threads)"}
+                    v, secs, cores = cpu_reference_rate(ref_sc, frames=1)
+                cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "reference", "cpu": _cpu_model(),
+                       "sample": f"the first frame ({ref_sc.params.substeps} substeps) of {ref_sc.name} from its "
+                                 f"initial state ({secs:.1f} s), the reference's own C++ (oracle/_ref, OpenMP "
+                                 f"{cores} threads)"}
+                if available("ref_serial"):
+                    nsub = 2 if ref_sc.num_vertices > 16384 else ref_sc.params.substeps
+                    with _reference_output_to_stderr():
+                        v1, secs1, _ = cpu_reference_rate(ref_sc, serial=True, substeps=nsub)
+                    cpu["single_thread"] = {
+                        "value": v1, "unit": UNIT, "cores": 1,
+                        "sample": f"the first {nsub} substeps of {ref_sc.name} from its initial state ({secs1:.1f} s), "
+                                  f"the reference built without OpenMP (oracle/_ref/libscref_serial.so), as its "
+                                  f"C-ABI library ships"}
         except Exception as e:  # reported, not fatal
             cpu = {"value": None, "unit": UNIT, "cores": None, "kind": "reference", "sample": f"failed: {e}"}
 

@@ -369,14 +369,20 @@ SCEXP int scGetKernelTiming(scClothPatch patch, float* ms, int* counts);
    vertices and normals are numVertices packed xyz floats, indices 3*numTriangles.
    Its only scratch is a fixed file-scope device array of SC_NOALLOC_MAX_VERTICES
    float4 accumulators (1 MiB, resident on every GPU that loads the library until
-   the process exits); meshes with more vertices are rejected (SC_ERR_ARG = 2).
+   the process exits); meshes with more vertices, or more than
+   SC_NOALLOC_MAX_TRIANGLES triangles, are rejected (SC_ERR_ARG = 2).
+   Every triangle index is checked on the device: a triangle with an index
+   >= numVertices is skipped (nothing is written for it) and the call returns
+   SC_ERR_ARG; to report that, the call waits for its work on `stream` to finish.
    Every call shares that scratch and leaves its contents behind; a call clears
    what it uses first, but calls that overlap on the GPU race and must be
    serialised by the caller. The first call on a device looks the scratch's
    device address up, so make it before any stream capture that includes later
-   calls. Work is enqueued on `stream` (a cudaStream_t, NULL = legacy default).
+   calls; later calls on a stream that is not capturing look it up again.
+   Work is enqueued on `stream` (a cudaStream_t, NULL = legacy default).
    Returns 0 or an error code (details from scGetLastErrorString). */
 #define SC_NOALLOC_MAX_VERTICES 65536
+#define SC_NOALLOC_MAX_TRIANGLES 16777216
 SCEXP int scComputeVertexNormalsNoAlloc(const float* vertices, int numVertices, const unsigned* indices,
                                         int numTriangles, float* normals, void* stream);
 

@@ -16,6 +16,9 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REF_LIB = HERE / "_ref" / "libscref.so"
+# the same reference sources built without -fopenmp: single-threaded, as the
+# reference's C-ABI library (ClothLib, CMakeLists.txt:42) is
+REF_SERIAL_LIB = HERE / "_ref" / "libscref_serial.so"
 PORT_LIB = HERE / "_build" / "liboracle.so"
 
 _f = C.POINTER(C.c_float)
@@ -254,10 +257,11 @@ class CpuCloth:
 
 
 class RefCloth(CpuCloth):
-    """The SolidCloth reference compiled from its own sources (oracle/_ref)."""
+    """The SolidCloth reference compiled from its own sources (oracle/_ref);
+    serial=True loads the build without OpenMP."""
 
-    def __init__(self):
-        super().__init__(REF_LIB, "ref_")
+    def __init__(self, serial: bool = False):
+        super().__init__(REF_SERIAL_LIB if serial else REF_LIB, "ref_")
 
     def init_mesh(self, vertices, indices, uvs=None, colors=None, offset=(0, 0, 0), attached=False):
         """ClothPatch::Init(mesh, offset, attached) in the reference build"""
@@ -349,7 +353,7 @@ class PortCloth(CpuCloth):
 
 
 def available(kind: str = "ref") -> bool:
-    return (REF_LIB if kind == "ref" else PORT_LIB).exists()
+    return {"ref": REF_LIB, "ref_serial": REF_SERIAL_LIB}.get(kind, PORT_LIB).exists()
 
 
 def ref_sdf_from_mesh(vertices, indices, cells, box6):

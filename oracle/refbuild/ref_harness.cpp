@@ -28,7 +28,9 @@
 #undef private
 #undef protected
 
+#ifdef _OPENMP
 #include <omp.h>
+#endif
 
 using namespace Physics;
 using namespace Geometry;
@@ -65,8 +67,14 @@ void* ref_create()
 
 void ref_destroy(void* h) { delete (RefScene*)h; }
 
+#ifdef _OPENMP
 void ref_set_threads(int n) { omp_set_num_threads(n); }
 int ref_max_threads() { return omp_get_max_threads(); }
+#else
+// the single-threaded build (no -fopenmp), like the reference's C-ABI library
+void ref_set_threads(int) {}
+int ref_max_threads() { return 1; }
+#endif
 
 /* ---- colliders (Physics/Common.h:32-149) ---- */
 void ref_add_walls(void* h, const float* box6)

@@ -11,6 +11,10 @@
 // Properties a caller must know:
 //   * capacity: at most SC_NOALLOC_MAX_VERTICES vertices (65,536: a 256 x 256
 //     grid); larger meshes are rejected with SC_ERR_ARG;
+//   * every triangle index is checked against numVertices on the device: a
+//     triangle with an index out of range is skipped (nothing is written for it)
+//     and the call returns SC_ERR_ARG. To report that, the call waits for its
+//     work on the stream to finish before it returns;
 //   * the scratch array (1 MiB) is resident on every GPU that loads this library
 //     until the process exits;
 //   * every call shares that array and it keeps the last call's contents; a call
@@ -18,7 +22,9 @@
 //     streams, or another thread) race on it and must be serialised by the caller;
 //   * the first call on a device looks the array's device address up
 //     (cudaGetSymbolAddress) with that device current; make that first call
-//     before any stream capture that would include later calls;
+//     before any stream capture that would include later calls. Later calls
+//     look it up again (it is cheap) unless the stream is capturing, so a
+//     context reset between calls does not leave a stale address behind;
 //   * the per-vertex sums use atomic adds, so the order of additions (and the
 //     last bits of the result) can differ from scUpdateClothMesh's ordered sum.
 #include "cloth.h"
@@ -28,20 +34,30 @@
 namespace sc {
 
 static __device__ __align__(256) float4 g_noalloc_normal_acc[SC_NOALLOC_MAX_VERTICES];
+// number of triangles of the last call that had an index >= numVertices
+static __device__ int g_noalloc_bad_triangles;
 
 __global__ void k_noalloc_clear(float4* acc, int n)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) g_noalloc_bad_triangles = 0;
     if (i < n) acc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
 // per triangle: unit normal and corner angles as k_tri_normals computes them,
-// accumulated into the three corner vertices
-__global__ void k_noalloc_tri(const float* v, const unsigned* idx, int T, float4* acc)
+// accumulated into the three corner vertices; a triangle with an index outside
+// [0, n) is counted and skipped, so no write leaves acc[0, n)
+__global__ void k_noalloc_tri(const float* v, const unsigned* idx, int T, int n, float4* acc)
 {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= T) return;
-    const unsigned i1 = idx[3 * t], i2 = idx[3 * t + 1], i3 = idx[3 * t + 2];
+    const size_t o = 3 * (size_t)t;
+    const unsigned i1 = idx[o], i2 = idx[o + 1], i3 = idx[o + 2];
+    if (i1 >= (unsigned)n || i2 >= (unsigned)n || i3 >= (unsigned)n)
+    {
+        atomicAdd(&g_noalloc_bad_triangles, 1);
+        return;
+    }
     V3 a = mk(v[3 * i1], v[3 * i1 + 1], v[3 * i1 + 2]);
     V3 b = mk(v[3 * i2], v[3 * i2 + 1], v[3 * i2 + 2]);
     V3 c = mk(v[3 * i3], v[3 * i3 + 1], v[3 * i3 + 2]);
@@ -77,11 +93,11 @@ __global__ void k_noalloc_normalise(const float4* acc, int n, float* out)
 static std::mutex g_noalloc_mutex;
 static float4* g_noalloc_ptr[64] = {nullptr};
 
-static float4* noalloc_scratch(int dev)
+static float4* noalloc_scratch(int dev, bool capturing)
 {
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
     if (dev < 0 || dev >= 64) return nullptr;
-    if (!g_noalloc_ptr[dev])
+    if (!g_noalloc_ptr[dev] || !capturing)
     {
         float4* p = nullptr;
         // host code must not take the array's address directly: that is a host
@@ -109,24 +125,42 @@ extern "C" int scComputeVertexNormalsNoAlloc(const float* vertices, int numVerti
         set_error(SC_ERR_ARG, "scComputeVertexNormalsNoAlloc: null buffer");
         return SC_ERR_ARG;
     }
-    if (numVertices <= 0 || numVertices > SC_NOALLOC_MAX_VERTICES || numTriangles < 0)
+    if (numVertices <= 0 || numVertices > SC_NOALLOC_MAX_VERTICES || numTriangles < 0 ||
+        numTriangles > SC_NOALLOC_MAX_TRIANGLES)
     {
         set_error(SC_ERR_ARG, "scComputeVertexNormalsNoAlloc: numVertices must be in [1, " +
-                                  std::to_string(SC_NOALLOC_MAX_VERTICES) + "] and numTriangles >= 0, got " +
+                                  std::to_string(SC_NOALLOC_MAX_VERTICES) + "] and numTriangles in [0, " +
+                                  std::to_string(SC_NOALLOC_MAX_TRIANGLES) + "], got " +
                                   std::to_string(numVertices) + " / " + std::to_string(numTriangles));
         return SC_ERR_ARG;
     }
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) { set_error(SC_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e)); return SC_ERR_CUDA; }
-    float4* acc = noalloc_scratch(dev);
-    if (!acc) return SC_ERR_CUDA;
     cudaStream_t s = (cudaStream_t)stream;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    e = cudaStreamIsCapturing(s, &cap);
+    if (e != cudaSuccess) { set_error(SC_ERR_CUDA, std::string("cudaStreamIsCapturing: ") + cudaGetErrorString(e)); return SC_ERR_CUDA; }
+    float4* acc = noalloc_scratch(dev, cap != cudaStreamCaptureStatusNone);
+    if (!acc) return SC_ERR_CUDA;
     const int nb = (numVertices + 255) / 256;
     k_noalloc_clear<<<nb, 256, 0, s>>>(acc, numVertices);
-    if (numTriangles > 0) k_noalloc_tri<<<(numTriangles + 255) / 256, 256, 0, s>>>(vertices, indices, numTriangles, acc);
+    if (numTriangles > 0)
+        k_noalloc_tri<<<(numTriangles + 255) / 256, 256, 0, s>>>(vertices, indices, numTriangles, numVertices, acc);
     k_noalloc_normalise<<<nb, 256, 0, s>>>(acc, numVertices, normals);
     e = cudaGetLastError();
     if (e != cudaSuccess) { set_error(SC_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e)); return SC_ERR_CUDA; }
+    // the index check's verdict: read the device counter once the work is done
+    int bad = 0;
+    e = cudaMemcpyFromSymbolAsync(&bad, g_noalloc_bad_triangles, sizeof(int), 0, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) { set_error(SC_ERR_CUDA, std::string("status read: ") + cudaGetErrorString(e)); return SC_ERR_CUDA; }
+    if (bad > 0)
+    {
+        set_error(SC_ERR_ARG, "scComputeVertexNormalsNoAlloc: " + std::to_string(bad) +
+                                  " triangle(s) have an index >= numVertices (" + std::to_string(numVertices) +
+                                  "); they were skipped");
+        return SC_ERR_ARG;
+    }
     return SC_OK;
 }

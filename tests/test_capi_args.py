@@ -30,6 +30,7 @@ def test_noalloc_normals_rejects_sizes_and_null_buffers(lib):
     assert lib.scComputeVertexNormalsNoAlloc(buf, 0, idx, 1, buf, None) == SC_ERR_ARG
     assert lib.scComputeVertexNormalsNoAlloc(buf, 65537, idx, 1, buf, None) == SC_ERR_ARG   # above the scratch
     assert lib.scComputeVertexNormalsNoAlloc(buf, 3, idx, -1, buf, None) == SC_ERR_ARG
+    assert lib.scComputeVertexNormalsNoAlloc(buf, 3, idx, 16777217, buf, None) == SC_ERR_ARG  # above the triangle cap
     assert _last(lib) == SC_ERR_ARG
     assert _last(lib) == 0                                                                # read and cleared
 
