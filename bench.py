@@ -68,6 +68,8 @@ def _args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the plain-vs-learned warm-start comparison")
     ap.add_argument("--instances", type=int, default=512, help="cfg3: number of instances (the first K of the 512)")
+    ap.add_argument("--precision", default="default", choices=["default", "ieee", "fast"],
+                    help="solver numerics (scSetSolverPrecision): the library default, IEEE or the fast build")
     return ap.parse_args()
 
 
@@ -375,6 +377,8 @@ def run_ours(args):
     else:
         sc = _scene(args.config, args.self_mode)
         w, p = api.load_scene(sc)
+    if args.precision != "default":
+        p.model.set_fast_math(args.precision == "fast")
     stream = torch.cuda.ExternalStream(p.cuda_stream(), device=torch.device("cuda", local))
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     # CUDA events inside the frame graph bracket the solve and the broad phases of
@@ -554,7 +558,8 @@ def run_ours(args):
                 "data": "synthetic", "config": _workload(sc), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "learned": learned_ab,
                 "gpu_launches": kernels_per_frame * args.steps, "kernels_per_frame": kernels_per_frame,
-                "clocks": clk.summary(), "device_status": status}
+                "clocks": clk.summary(), "device_status": status,
+                "solver_precision": "fast" if p.model.fast_math() else "ieee"}
         print(json.dumps(line))
     p.free()
     if ws > 1:

@@ -267,11 +267,16 @@ SCEXP void scSetClusterSolver(scModel model, bool val);
    give the same results): 0 = autotuned at the first step (default: the fastest
    of the cluster kernel, the grid-resident cooperative kernel's variants and the
    per-colour kernels, timed on this cloth), 1 = cluster kernel (clothes up to
-   131,072 particles), 2 = grid kernel (tuned variant), 3 = per-colour kernels.
+   131,072 particles), 2 = grid kernel (tuned variant), 3 = per-colour kernels,
+   4 = tiled grid kernel (tuned variant: each CTA owns a patch of the cloth and
+   waits only for the patches it shares particles with between colours).
    scSetClusterSolver(true/false) is mode 1 / 3. */
 SCEXP void scSetSolverMode(scModel model, int mode);
 /* force grid variant `variant` (0 .. scGetGridVariants()-1) with blocksPerSm CTAs per SM */
 SCEXP void scSetGridSolver(scModel model, int variant, int blocksPerSm);
+/* force the tiled grid kernel: variant as for scSetGridSolver, one tile per CTA,
+   blocksPerSm (1 or 2) CTAs per SM */
+SCEXP void scSetTiledSolver(scModel model, int variant, int blocksPerSm);
 /* out4 = {kind, grid variant, CTAs per SM, threads per CTA} of the solver in use;
    tuneMs (4 floats per candidate: kind, variant, CTAs per SM, ms per substep)
    gets up to cap candidates of the last tuning; returns the candidate count */
@@ -290,6 +295,14 @@ SCEXP int scGetGridVariants(int* info3, int cap);
    shared memory once per substep when they fit; false: read them from global
    memory in every sweep. Same results. */
 SCEXP void scSetClusterStaging(scModel model, bool val);
+/* Numerics of the Gauss-Seidel projections and contact solves. 0 (default):
+   IEEE division and square root without FMA contraction, the reference's
+   operation order bit for bit. 1: the fast build of the same solver (FMA
+   contraction, approximate division and square root): every projection within
+   1e-5 relative of the IEEE one. Detection (boxes, candidate pairs, contacts)
+   is exact in both. Other values are rejected (SC_ERR_ARG). */
+SCEXP void scSetSolverPrecision(scModel model, int mode);
+SCEXP int scGetSolverPrecision(scModel model);
 
 /* ---- additions: inspection for parity checks ---- */
 /* kind 0: FEM triangles, 1: bends, 2: links. Writes the solve order (a permutation) and

@@ -100,6 +100,7 @@ def _load(path: Path, prefix: str):
                     "portable_acos": ([C.c_float], C.c_float),
                     "self_contact_colours": ([C.c_void_p, C.c_int, _i], None),
                     "ccd_broadphase": ([C.c_void_p, C.c_float, C.c_int, _i, C.c_int], C.c_int),
+                    "set_bruteforce_broadphase": ([C.c_void_p, C.c_int], None),
                     "residual": ([C.c_void_p], C.c_float),
                     "set_link_order": ([C.c_void_p, _i, C.c_int], None),
                     "load_topology": ([C.c_void_p, C.c_int, _f, _f, C.c_int, _u, _f, C.c_int, _u, C.c_int, _u, _f], None),
@@ -345,6 +346,10 @@ class PortCloth(CpuCloth):
     def residual(self) -> float:
         """max |C| over the warp, weft and shear constraints at the current positions"""
         return float(self._fn("residual")(self.h))
+
+    def set_bruteforce_broadphase(self, on: bool):
+        """True: the plain all-pairs loop instead of the (exact) sweep over sorted boxes"""
+        self._fn("set_bruteforce_broadphase")(self.h, int(on))
 
     def ccd_broadphase(self, tol, kind, cap=1 << 24):
         out = np.zeros((cap, 2), np.int32)

@@ -22,6 +22,15 @@
 #include <cstdint>
 #include <cstring>
 #include <memory>
+#include <algorithm>
+#ifdef _OPENMP
+#include <omp.h>
+static int omp_threads() { return omp_get_max_threads(); }
+static int omp_thread() { return omp_get_thread_num(); }
+#else
+static int omp_threads() { return 1; }
+static int omp_thread() { return 0; }
+#endif
 
 using namespace orc;
 typedef uint32_t u32;
@@ -1052,28 +1061,41 @@ struct Cloth
        Geometry/ClosestPointsBetweenMeshes.cpp:595-695) */
     void mesh_collisions(int meshId, float radTol, const std::vector<float>& tvs)
     {
+        /* The queries are independent (const tree walks); they run in parallel
+           and their results are appended in query order, as the serial loops do. */
         MeshCollider& mc = *meshes[meshId];
         if (!mc.built) mc.build(thickness);
         const Topo& cm = prevMesh;
         if (flags & CF_VERTICES)
         {
+            std::vector<TriInfo> res(N);
+#pragma omp parallel for schedule(dynamic, 64)
             for (int i = 0; i < N; i++)
             {
-                TriInfo info;
                 float minDist = FLT_MAX;
-                mc.point_rec(cm.verts[i], 0, minDist, info);
+                mc.point_rec(cm.verts[i], 0, minDist, res[i]);
+            }
+            for (int i = 0; i < N; i++)
+            {
+                const TriInfo& info = res[i];
                 float dist = info.distance;
                 if (dist < radTol && dist >= 0) add_contact(i, info.cp, info.normal, info.tri, meshId);
             }
         }
         if (flags & CF_TRIANGLES)
         {
-            for (size_t j = 0; j < tris.size(); j++)
+            const int nt = (int)tris.size();
+            std::vector<VtxInfo> res(nt);
+#pragma omp parallel for schedule(dynamic, 64)
+            for (int j = 0; j < nt; j++)
             {
                 u32 a = cm.idx[j * 3], b = cm.idx[j * 3 + 1], c = cm.idx[j * 3 + 2];
-                VtxInfo info;
                 float minDist = FLT_MAX;
-                mc.tri_rec(cm.verts[a], cm.verts[b], cm.verts[c], 0, minDist, info);
+                mc.tri_rec(cm.verts[a], cm.verts[b], cm.verts[c], 0, minDist, res[j]);
+            }
+            for (int j = 0; j < nt; j++)
+            {
+                const VtxInfo& info = res[j];
                 u32 i1 = tris[j].i1, i2 = tris[j].i2, i3 = tris[j].i3;
                 float tv = std::max(tvs[i1], std::max(tvs[i2], tvs[i3]));
                 float rt = thickness + std::max(tolerance, tv * 1.2f);
@@ -1090,12 +1112,18 @@ struct Cloth
         }
         if (flags & CF_EDGES)
         {
-            for (size_t e = 0; e < cm.edges.size(); e++)
+            const int ne = (int)cm.edges.size();
+            std::vector<EdgeInfo> res(ne);
+#pragma omp parallel for schedule(dynamic, 64)
+            for (int e = 0; e < ne; e++)
             {
-                EdgeInfo info;
-                info.edge1 = (int)e;
+                res[e].edge1 = e;
                 float minDist = FLT_MAX;
-                mc.seg_rec(cm.verts[cm.edges[e].i1], cm.verts[cm.edges[e].i2], 0, minDist, info);
+                mc.seg_rec(cm.verts[cm.edges[e].i1], cm.verts[cm.edges[e].i2], 0, minDist, res[e]);
+            }
+            for (int e = 0; e < ne; e++)
+            {
+                const EdgeInfo& info = res[e];
                 float dist = info.distance;
                 if (dist < radTol && dist >= 0)
                 {
@@ -1678,9 +1706,16 @@ struct Cloth
 
     /* All-pairs version of the Midphase filters (Physics/SelfCollisionDetector.cpp:60-135):
        VT (triangle, vertex) with the vertex not on the triangle and not pinned,
-       EE (e1 < e2) sharing no vertex, in both cases with overlapping swept boxes. */
+       EE (e1 < e2) sharing no vertex, in both cases with overlapping swept boxes.
+       Pairs come out in ascending (triangle, vertex) / (edge, higher edge) order.
+       The default is an exact sweep over the boxes sorted by min x (the same
+       pair sets as the all-pairs loop, bruteforce = true, at the sizes of the
+       benchmark configurations). */
+    bool bruteforce = false;
+
     void broadphase(float tol, std::vector<std::pair<int, int>>& vt, std::vector<std::pair<int, int>>& ee) const
     {
+        if (!bruteforce) { broadphase_sweep(tol, vt, ee); return; }
         std::vector<Box> tb, vb, eb;
         swept_boxes(tol, tb, vb, eb);
         vt.clear(); ee.clear();
@@ -1698,6 +1733,89 @@ struct Cloth
                 if (i1 == i3 || i2 == i4 || i1 == i4 || i2 == i3) continue;
                 if (overlap(eb[a], eb[b])) ee.push_back({(int)a, (int)b});
             }
+    }
+
+    /* Sweep along x: for boxes a, b with a.mn.x <= b.mn.x (and mx >= mn, which
+       box construction guarantees for finite coordinates) the x part of
+       overlap() reduces to b.mn.x <= a.mx.x, so scanning the sorted list
+       forward from each box while that holds meets every overlapping pair once;
+       overlap() itself then decides, as in the all-pairs loop. A box with a NaN
+       coordinate (for which overlap() can answer true against anything) is
+       tested against every box, as the all-pairs loop does. */
+    static bool has_nan(const Box& b)
+    {
+        return b.mn.x != b.mn.x || b.mn.y != b.mn.y || b.mn.z != b.mn.z ||
+               b.mx.x != b.mx.x || b.mx.y != b.mx.y || b.mx.z != b.mx.z;
+    }
+
+    template <typename F>
+    static void sweep_pairs(const std::vector<Box>& A, const std::vector<Box>& B, bool same, F&& emit)
+    {
+        /* entries: (min x, kind, index); kind 0 = A, 1 = B (same: all from A) */
+        struct Ent { float x; int kind; int idx; };
+        std::vector<Ent> ent;
+        std::vector<int> nanA, nanB;
+        for (size_t i = 0; i < A.size(); i++)
+            if (has_nan(A[i])) nanA.push_back((int)i); else ent.push_back({A[i].mn.x, 0, (int)i});
+        if (!same)
+            for (size_t i = 0; i < B.size(); i++)
+                if (has_nan(B[i])) nanB.push_back((int)i); else ent.push_back({B[i].mn.x, 1, (int)i});
+        std::sort(ent.begin(), ent.end(), [](const Ent& a, const Ent& b) { return a.x < b.x; });
+        const int n = (int)ent.size();
+        std::vector<std::vector<std::pair<int, int>>> part;
+#pragma omp parallel
+        {
+#pragma omp single
+            part.resize(omp_threads());
+            std::vector<std::pair<int, int>>& mine = part[omp_thread()];
+#pragma omp for schedule(dynamic, 256)
+            for (int k = 0; k < n; k++)
+            {
+                const Ent& e = ent[k];
+                const Box& a = e.kind == 0 ? A[e.idx] : B[e.idx];
+                for (int m = k + 1; m < n && ent[m].x <= a.mx.x; m++)
+                {
+                    const Ent& f = ent[m];
+                    if (!same && f.kind == e.kind) continue;
+                    const Box& b = f.kind == 0 ? A[f.idx] : B[f.idx];
+                    if (!overlap(a, b)) continue;
+                    if (same) mine.push_back({std::min(e.idx, f.idx), std::max(e.idx, f.idx)});
+                    else if (e.kind == 0) mine.push_back({e.idx, f.idx});
+                    else mine.push_back({f.idx, e.idx});
+                }
+            }
+        }
+        std::vector<std::pair<int, int>> all;
+        for (auto& v : part) all.insert(all.end(), v.begin(), v.end());
+        /* NaN boxes against everything (A side and B side) */
+        for (int i : nanA)
+        {
+            if (same) { for (size_t j = 0; j < A.size(); j++) if ((int)j != i && overlap(A[i], A[j])) all.push_back({std::min(i, (int)j), std::max(i, (int)j)}); }
+            else for (size_t j = 0; j < B.size(); j++) if (overlap(A[i], B[j])) all.push_back({i, (int)j});
+        }
+        for (int j : nanB)
+            for (size_t i = 0; i < A.size(); i++)
+                if (!has_nan(A[i]) && overlap(A[i], B[j])) all.push_back({(int)i, j});
+        std::sort(all.begin(), all.end());
+        all.erase(std::unique(all.begin(), all.end()), all.end());
+        for (auto& pr : all) emit(pr.first, pr.second);
+    }
+
+    void broadphase_sweep(float tol, std::vector<std::pair<int, int>>& vt, std::vector<std::pair<int, int>>& ee) const
+    {
+        std::vector<Box> tb, vb, eb;
+        swept_boxes(tol, tb, vb, eb);
+        vt.clear(); ee.clear();
+        sweep_pairs(tb, vb, false, [&](int t, int i) {
+            if ((u32)i == tris[t].i1 || (u32)i == tris[t].i2 || (u32)i == tris[t].i3 || invMass[i] == 0) return;
+            vt.push_back({t, i});
+        });
+        const std::vector<Edge>& E = mesh.edges;
+        sweep_pairs(eb, eb, true, [&](int a, int b) {
+            u32 i1 = E[a].i1, i2 = E[a].i2, i3 = E[b].i1, i4 = E[b].i2;
+            if (i1 == i3 || i2 == i4 || i1 == i4 || i2 == i3) return;
+            ee.push_back({a, b});
+        });
     }
 
     float coplanarity(float t, V3 x1, V3 x2, V3 x3, V3 x4, V3 v1, V3 v2, V3 v3_, V3 v4) const
@@ -2218,6 +2336,8 @@ void orc_self_contact_colours(void* h, int kind, int* colours)
     c->colour_order(kind == 3 ? c->selfTris : c->selfEdges, vf, &col);
     for (size_t i = 0; i < col.size(); i++) colours[i] = col[i];
 }
+
+void orc_set_bruteforce_broadphase(void* h, int on) { ((Cloth*)h)->bruteforce = on != 0; }
 
 int orc_ccd_broadphase(void* h, float tol, int kind, int* pairs, int cap)
 {

@@ -62,7 +62,10 @@ void orc_get_mesh_normals(void* h, int prev, float* n);
 void orc_get_mesh_tri_normals(void* h, int prev, float* n);
 /* colour of each self contact under the independent-set colouring (kind 3/4) */
 void orc_self_contact_colours(void* h, int kind, int* colours);
-/* Continuous self-collision: all-pairs swept-box broad phase and narrow phase. */
+/* Continuous self-collision: all-pairs swept-box broad phase and narrow phase.
+   The broad phase sweeps boxes sorted by min x (exact: the all-pairs set);
+   orc_set_bruteforce_broadphase(h, 1) selects the plain all-pairs loop. */
+void orc_set_bruteforce_broadphase(void* h, int on);
 int orc_ccd_broadphase(void* h, float tol, int kind, int* pairs, int cap);
 void orc_ccd_narrow_on(void* h, int nvt, const int* vt, int nee, const int* ee);
 void orc_swept_boxes(void* h, int kind, float tol, float* out);

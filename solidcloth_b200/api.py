@@ -136,6 +136,9 @@ SIGNATURES = {
     "scSetSelfCCD": ([scModel, C.c_bool], None),
     "scSetClusterSolver": ([scModel, C.c_bool], None),
     "scSetClusterStaging": ([scModel, C.c_bool], None),
+    "scSetSolverPrecision": ([scModel, C.c_int], None),
+    "scSetTiledSolver": ([scModel, C.c_int, C.c_int], None),
+    "scGetSolverPrecision": ([scModel], C.c_int),
     "scCreateClothBatch": ([scCollisionWorld, C.POINTER(scClothPatch), C.c_int], scClothPatch),
     "scGetBatchSize": ([scClothPatch], C.c_int),
     "scGetBatchInstance": ([scClothPatch, C.c_int, _i, _i], None),
@@ -327,7 +330,7 @@ class ClothModel:
         lib().scSetClusterSolver(self.h, bool(on))
 
     def set_solver_mode(self, mode: int):
-        """0 autotuned, 1 cluster kernel, 2 grid kernel, 3 per-colour kernels"""
+        """0 autotuned, 1 cluster kernel, 2 grid kernel, 3 per-colour kernels, 4 tiled grid kernel"""
         lib().scSetSolverMode(self.h, int(mode))
         _check("scSetSolverMode")
 
@@ -357,6 +360,19 @@ class ClothModel:
 
     def set_cluster_staging(self, on: bool):
         lib().scSetClusterStaging(self.h, bool(on))
+
+    def set_tiled_solver(self, variant: int, blocks_per_sm: int):
+        lib().scSetTiledSolver(self.h, int(variant), int(blocks_per_sm))
+        _check("scSetTiledSolver")
+
+    def set_fast_math(self, on: bool):
+        """solver numerics: True = the fast build (FMA, approximate div/sqrt),
+        False = IEEE, bit-exact with the reference's operation order"""
+        lib().scSetSolverPrecision(self.h, int(bool(on)))
+        _check("scSetSolverPrecision")
+
+    def fast_math(self) -> bool:
+        return bool(lib().scGetSolverPrecision(self.h))
 
     def constraint_order(self, kind):
         n = (lib().scGetNumTris(self.h), lib().scGetNumBends(self.h), lib().scGetNumLinks(self.h))[kind]

@@ -5,7 +5,8 @@
 The kernels are compiled with -fmad=false and IEEE division/square root
 (nvcc's defaults without --use_fast_math) so their arithmetic follows the
 reference's operation order; host code with -ffp-contract=off for the same
-reason.
+reason. solver_fast.cu, the fast build of the solver (csrc/solver.cuh), is the
+one exception: FMA contraction and approximate division / square root.
 """
 from __future__ import annotations
 
@@ -18,7 +19,9 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 LIBDIR = PKG / "lib"
 LIB = LIBDIR / "libsolidcloth_b200.so"
-SOURCES = ["step_kernels.cu", "cloth.cu", "capi.cu", "noalloc.cu", "render.cu"]
+SOURCES = ["step_kernels.cu", "solver_fast.cu", "cloth.cu", "capi.cu", "noalloc.cu", "render.cu"]
+# per-source replacements of the default numerics flags
+FAST = {"solver_fast.cu": ["-fmad=true", "-prec-div=false", "-prec-sqrt=false", "-ftz=false"]}
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "--extended-lambda",
          "-Xcompiler", "-fPIC,-ffp-contract=off,-fvisibility=hidden", "-ccbin", "g++"]
@@ -38,7 +41,8 @@ def build(verbose: bool = False, ptxas_v: bool = False) -> Path:
         s = CSRC / src
         o = LIBDIR / (s.stem + ".o")
         if not o.exists() or o.stat().st_mtime < max(s.stat().st_mtime, hdr_time):
-            cmd = [nvcc(), *ARCH, *FLAGS, "-c", str(s), "-o", str(o)]
+            flags = [f for f in FLAGS if not (src in FAST and f == "-fmad=false")] + FAST.get(src, [])
+            cmd = [nvcc(), *ARCH, *flags, "-c", str(s), "-o", str(o)]
             if ptxas_v:
                 cmd += ["-Xptxas", "-v"]
             if verbose:

@@ -645,7 +645,7 @@ void scSetSelfCCD(scModel m, bool v) { if (M(m)) { M(m)->prm.ccd = v; M(m)->touc
 void scSetClusterSolver(scModel m, bool v) { scSetSolverMode(m, v ? SOLVE_CLUSTER : SOLVE_KERNELS); }
 void scSetSolverMode(scModel m, int mode)
 {
-    if (!M(m) || mode < SOLVE_AUTO || mode > SOLVE_KERNELS) { set_error(SC_ERR_ARG, "solver mode must be 0..3"); return; }
+    if (!M(m) || mode < SOLVE_AUTO || mode > SOLVE_TILED) { set_error(SC_ERR_ARG, "solver mode must be 0..4"); return; }
     M(m)->solverMode = mode;
     M(m)->tuned = false;
     M(m)->touch();
@@ -659,6 +659,19 @@ void scSetGridSolver(scModel m, int variant, int blocksPerSm)
     M(m)->touch();
     M(m)->tunedVersion = M(m)->paramVersion;
 }
+void scSetTiledSolver(scModel m, int variant, int blocksPerSm)
+{
+    if (!M(m) || variant < 0 || variant >= gs_grid_variants() || blocksPerSm < 1 || blocksPerSm > 2)
+    {
+        set_error(SC_ERR_ARG, "bad tiled solver variant");
+        return;
+    }
+    M(m)->solverMode = SOLVE_TILED;
+    M(m)->choice = {SOLVE_TILED, variant, blocksPerSm, 0.f};
+    M(m)->tuned = true;
+    M(m)->touch();
+    M(m)->tunedVersion = M(m)->paramVersion;
+}
 int scGetSolverChoice(scModel m, int* out4, float* tuneMs, int cap)
 {
     if (!M(m)) return 0;
@@ -666,7 +679,7 @@ int scGetSolverChoice(scModel m, int* out4, float* tuneMs, int cap)
     if (out4)
     {
         int th = 0, ft = 0, bt = 0;
-        if (ch.kind == SOLVE_GRID) gs_grid_variant_info(ch.variant, th, ft, bt);
+        if (ch.kind == SOLVE_GRID || ch.kind == SOLVE_TILED) gs_grid_variant_info(ch.variant, th, ft, bt);
         out4[0] = ch.kind; out4[1] = ch.variant; out4[2] = ch.blocksPerSm; out4[3] = th;
     }
     const auto& log = M(m)->tuneLog;
@@ -701,6 +714,13 @@ int scGetGridVariants(int* info3, int cap)
     return n;
 }
 void scSetClusterStaging(scModel m, bool v) { if (M(m)) { M(m)->prm.stageRecords = v; M(m)->touch(); } }
+void scSetSolverPrecision(scModel m, int mode)
+{
+    ClothModel* c = M(m);
+    if (!c || (mode != 0 && mode != 1)) { set_error(SC_ERR_ARG, "scSetSolverPrecision: mode must be 0 (IEEE) or 1 (fast)"); return; }
+    if (c->prm.fastMath != (mode == 1)) { c->prm.fastMath = mode == 1; c->touch(); }
+}
+int scGetSolverPrecision(scModel m) { return M(m) ? (int)M(m)->prm.fastMath : -1; }
 void scSetResidualTarget(scModel m, float tol, int maxIterations)
 {
     ClothModel* c = M(m);

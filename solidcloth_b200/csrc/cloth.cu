@@ -453,6 +453,8 @@ void ClothModel::release_device()
     release_buffers();
     for (void* p : allocs) cudaFree(p);
     allocs.clear();
+    tilePlans.clear();
+    tilePlanFailed.clear();
     dc = DevCloth{};
     if (stageHost) cudaFreeHost(stageHost);
     stageHost = nullptr;
@@ -1672,6 +1674,195 @@ void ClothPatch::record_substep(float h)
     recordingSubstep++;
 }
 
+
+// ---------------------------------------------------- tiled solver plans
+// Particles are ordered by (instance, Morton code) — of the grid (column, row)
+// for grid clothes, else of the position quantised over the instance's box —
+// and cut into `tiles` chunks of equal count: compact patches of the cloth. A
+// constraint belongs to the tile of its first particle; inside each colour the
+// records are regrouped by tile (a permutation within the colour: the colour's
+// constraints share no particle, so the sweep's result is unchanged). Two tiles
+// are neighbours when a particle is touched by both: by their constraints, or
+// as a particle a tile owns (vertex contacts, velocity).
+static int sm_count()
+{
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms > 0 ? sms : 1;
+}
+
+// tiles of the tiled solver at blocksPerSm CTAs per SM: one per CTA, at least
+// 32 particles each
+static int tiled_tile_count(int N, int blocksPerSm)
+{
+    return std::max(1, std::min(blocksPerSm * sm_count(), N / 32));
+}
+
+static inline uint32_t spread_bits16(uint32_t v)
+{
+    v &= 0xffffu;
+    v = (v | (v << 8)) & 0x00ff00ffu;
+    v = (v | (v << 4)) & 0x0f0f0f0fu;
+    v = (v | (v << 2)) & 0x33333333u;
+    v = (v | (v << 1)) & 0x55555555u;
+    return v;
+}
+static inline uint32_t spread_bits10(uint32_t v)
+{
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000ffu;
+    v = (v | (v << 8)) & 0x0300f00fu;
+    v = (v | (v << 4)) & 0x030c30c3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
+const TilePlan* ClothModel::tile_plan(int tiles)
+{
+    auto it = tilePlans.find(tiles);
+    if (it != tilePlans.end()) return &it->second;
+    if (tilePlanFailed.count(tiles) || tiles < 1 || N < 1 || !dc.pos) return nullptr;
+    const int T = (int)tris.size(), B = (int)bends.size(), L = (int)links.size();
+    // particle order and chunks
+    std::vector<int> inst(N, 0);
+    for (size_t k = 0; k + 1 < instV.size(); k++)
+        for (int v = instV[k]; v < instV[k + 1]; v++) inst[v] = (int)k;
+    const int numInst = instV.size() > 1 ? (int)instV.size() - 1 : 1;
+    std::vector<V3> lo(numInst, mk(1e30f, 1e30f, 1e30f)), hi(numInst, mk(-1e30f, -1e30f, -1e30f));
+    const bool grid = (int)gridIJ.size() == N;
+    if (!grid)
+        for (int v = 0; v < N; v++) { lo[inst[v]] = vmin(lo[inst[v]], hpos[v]); hi[inst[v]] = vmax(hi[inst[v]], hpos[v]); }
+    std::vector<uint64_t> key(N);
+    for (int v = 0; v < N; v++)
+    {
+        uint32_t code;
+        if (grid) code = spread_bits16((uint32_t)gridIJ[v].x) | (spread_bits16((uint32_t)gridIJ[v].y) << 1);
+        else
+        {
+            const V3 a = lo[inst[v]], d = hi[inst[v]] - a;
+            auto q = [](float x, float lo_, float ext) {
+                const float t = ext > 0.f ? (x - lo_) / ext : 0.f;
+                return (uint32_t)std::min(1023.f, std::max(0.f, t * 1023.f));
+            };
+            code = spread_bits10(q(hpos[v].x, a.x, d.x)) | (spread_bits10(q(hpos[v].y, a.y, d.y)) << 1) |
+                   (spread_bits10(q(hpos[v].z, a.z, d.z)) << 2);
+        }
+        key[v] = ((uint64_t)inst[v] << 32) | code;
+    }
+    std::vector<int> ptcl(N);
+    for (int v = 0; v < N; v++) ptcl[v] = v;
+    std::stable_sort(ptcl.begin(), ptcl.end(), [&](int a, int b) { return key[a] < key[b]; });
+    std::vector<int> tileStart(tiles + 1), tileOf(N);
+    for (int t = 0; t <= tiles; t++) tileStart[t] = (int)((int64_t)t * N / tiles);
+    for (int t = 0; t < tiles; t++)
+        for (int k = tileStart[t]; k < tileStart[t + 1]; k++) tileOf[ptcl[k]] = t;
+    // touching tiles per particle (owner first), at most KT
+    constexpr int KT = 16;
+    std::vector<int> touchN(N, 1), touch((size_t)N * KT);
+    for (int v = 0; v < N; v++) touch[(size_t)v * KT] = tileOf[v];
+    bool ok = true;
+    auto add_touch = [&](uint32_t v, int t) {
+        int* a = &touch[(size_t)v * KT];
+        for (int k = 0; k < touchN[v]; k++) if (a[k] == t) return;
+        if (touchN[v] == KT) { ok = false; return; }
+        a[touchN[v]++] = t;
+    };
+    // (colour, tile) regrouping of one constraint kind: order[k] = colour-order
+    // position of the k-th record of the tiled layout
+    auto regroup = [&](const std::vector<int>& colourStart, int count, auto firstOf, auto particlesOf,
+                       std::vector<int>& order, std::vector<int>& start) {
+        const int ncol = colourStart.empty() ? 0 : (int)colourStart.size() - 1;
+        order.assign(count, 0);
+        start.assign((size_t)ncol * tiles + 1, 0);
+        std::vector<int> cnt(tiles);
+        for (int c = 0; c < ncol; c++)
+        {
+            std::fill(cnt.begin(), cnt.end(), 0);
+            for (int k = colourStart[c]; k < colourStart[c + 1]; k++) cnt[tileOf[firstOf(k)]]++;
+            int acc = colourStart[c];
+            for (int t = 0; t < tiles; t++) { start[(size_t)c * tiles + t] = acc; acc += cnt[t]; cnt[t] = start[(size_t)c * tiles + t]; }
+            for (int k = colourStart[c]; k < colourStart[c + 1]; k++)
+            {
+                const int t = tileOf[firstOf(k)];
+                order[cnt[t]++] = k;
+                particlesOf(k, t);
+            }
+        }
+        start[(size_t)ncol * tiles] = count;
+    };
+    std::vector<int> femOrd, femSt, bendOrd, bendSt, linkOrd, linkSt;
+    regroup(triColourStart, T, [&](int k) { return (int)tris[triOrder[k]].i1; },
+            [&](int k, int t) { const FemHost& f = tris[triOrder[k]]; add_touch(f.i1, t); add_touch(f.i2, t); add_touch(f.i3, t); },
+            femOrd, femSt);
+    regroup(bendColourStart, B, [&](int k) { return (int)bends[bendOrder[k]].x; },
+            [&](int k, int t) { const uint4 q = bends[bendOrder[k]]; add_touch(q.x, t); add_touch(q.y, t); add_touch(q.z, t); add_touch(q.w, t); },
+            bendOrd, bendSt);
+    regroup(linkColourStart, L, [&](int k) { return (int)links[linkOrder[k]].x; },
+            [&](int k, int t) { const uint2 q = links[linkOrder[k]]; add_touch(q.x, t); add_touch(q.y, t); },
+            linkOrd, linkSt);
+    if (!ok) { tilePlanFailed[tiles] = true; return nullptr; }
+    std::vector<std::vector<int>> nb(tiles);
+    for (int v = 0; v < N; v++)
+    {
+        const int* a = &touch[(size_t)v * KT];
+        for (int x = 0; x < touchN[v]; x++)
+            for (int y = 0; y < touchN[v]; y++)
+                if (x != y) nb[a[x]].push_back(a[y]);
+    }
+    std::vector<int> nbrStart(tiles + 1, 0), nbr;
+    for (int t = 0; t < tiles; t++)
+    {
+        std::sort(nb[t].begin(), nb[t].end());
+        nb[t].erase(std::unique(nb[t].begin(), nb[t].end()), nb[t].end());
+        if ((int)nb[t].size() > TILED_MAX_NEIGHBOURS) { tilePlanFailed[tiles] = true; return nullptr; }
+        nbr.insert(nbr.end(), nb[t].begin(), nb[t].end());
+        nbrStart[t + 1] = (int)nbr.size();
+    }
+    // records in the tiled layout (the formats of upload_topology)
+    std::vector<float4> fem(3 * (size_t)std::max(1, T));
+    for (int k = 0; k < T; k++)
+    {
+        const FemHost& t = tris[triOrder[femOrd[k]]];
+        fem[3 * (size_t)k] = make_float4(bits_f(t.i1), bits_f(t.i2), bits_f(t.i3), t.du1);
+        fem[3 * (size_t)k + 1] = make_float4(t.du2, t.dv1, t.dv2, t.invDet);
+        fem[3 * (size_t)k + 2] = make_float4(t.lu2, t.lv2, t.lu0 * t.lv0, t.area);
+    }
+    std::vector<uint4> bd(std::max(1, B));
+    for (int k = 0; k < B; k++) bd[k] = bends[bendOrder[bendOrd[k]]];
+    std::vector<float4> lk(std::max(1, L));
+    for (int k = 0; k < L; k++)
+    {
+        const int li = linkOrder[linkOrd[k]];
+        lk[k] = make_float4(bits_f(links[li].x), bits_f(links[li].y), linkRest[li].x, linkRest[li].y);
+    }
+    auto up = [&](const void* src, size_t bytes) -> void* {
+        void* d = dalloc(std::max<size_t>(bytes, 16));
+        if (d && bytes && cudaMemcpy(d, src, bytes, cudaMemcpyHostToDevice) != cudaSuccess) return nullptr;
+        return d;
+    };
+    TilePlan tp{};
+    tp.tiles = tiles;
+    tp.fem = (const float4*)up(fem.data(), sizeof(float4) * 3 * (size_t)T);
+    tp.femStart = (const int*)up(femSt.data(), sizeof(int) * femSt.size());
+    tp.bend = (const uint4*)up(bd.data(), sizeof(uint4) * (size_t)B);
+    tp.bendStart = (const int*)up(bendSt.data(), sizeof(int) * bendSt.size());
+    tp.link = (const float4*)up(lk.data(), sizeof(float4) * (size_t)L);
+    tp.linkStart = (const int*)up(linkSt.data(), sizeof(int) * linkSt.size());
+    tp.tileStart = (const int*)up(tileStart.data(), sizeof(int) * tileStart.size());
+    tp.ptcl = (const int*)up(ptcl.data(), sizeof(int) * (size_t)N);
+    tp.nbrStart = (const int*)up(nbrStart.data(), sizeof(int) * nbrStart.size());
+    tp.nbr = (const int*)up(nbr.data(), sizeof(int) * nbr.size());
+    tp.flags = (unsigned*)dalloc(sizeof(unsigned) * (size_t)tiles);
+    if (!tp.fem || !tp.femStart || !tp.bend || !tp.bendStart || !tp.link || !tp.linkStart || !tp.tileStart || !tp.ptcl ||
+        !tp.nbrStart || !tp.nbr || !tp.flags)
+    {
+        tilePlanFailed[tiles] = true;
+        return nullptr;
+    }
+    return &(tilePlans[tiles] = tp);
+}
+
 // One substep's Gauss-Seidel loop and velocity update, by the chosen solver:
 // the cluster-resident kernel, the grid-resident cooperative kernel (a tuned
 // variant), or one kernel per colour. The three are the same algorithm in the
@@ -1681,6 +1872,7 @@ bool ClothPatch::record_solve(cudaStream_t s, const SolverParams& P, const Solve
     ClothModel& m = model;
     const DevCloth& c = m.dc;
     Buffers& b = m.buf;
+    const SolverOps& ops = solver_ops(m.prm.fastMath);
     // the reference's loop tests its exit conditions after the body, so it always
     // runs at least one iteration (Physics/ClothPBD.cpp:335-362)
     const int iterations = m.prm.iterations > 1 ? m.prm.iterations : 1;
@@ -1698,7 +1890,7 @@ bool ClothPatch::record_solve(cudaStream_t s, const SolverParams& P, const Solve
     }
     int shift = 0;
     size_t smem = 0;
-    const int cluster = (ch.kind == SOLVE_CLUSTER && planFits) ? gs_cluster_size(m.N, shift, smem) : 0;
+    const int cluster = (ch.kind == SOLVE_CLUSTER && planFits) ? ops.cluster_size(m.N, shift, smem) : 0;
     if (cluster > 0)
     {
         plan.shift = shift;
@@ -1725,28 +1917,34 @@ bool ClothPatch::record_solve(cudaStream_t s, const SolverParams& P, const Solve
             plan.stage = 1;
             smem = staged;
         }
-        launch_gs_cluster(s, c, P, b, plan, cluster, smem);   // includes the velocity update
+        ops.cluster(s, c, P, b, plan, cluster, smem);   // includes the velocity update
         return true;
     }
-    if (ch.kind == SOLVE_GRID && planFits && launch_gs_grid(s, c, P, b, plan, ch.variant, ch.blocksPerSm))
+    if (ch.kind == SOLVE_GRID && planFits && ops.grid(s, c, P, b, plan, ch.variant, ch.blocksPerSm))
         return true;
+    if (ch.kind == SOLVE_TILED && planFits)
+    {
+        // the plan was built before capture (ClothPatch::step, autotune)
+        auto it = m.tilePlans.find(tiled_tile_count(m.N, ch.blocksPerSm));
+        if (it != m.tilePlans.end() && ops.tiled(s, c, P, b, plan, it->second, ch.variant)) return true;
+    }
     if (P.resTol > 0.f) launch_residual_exit(s, c, P, -1);
     for (int k = 0; k < iterations; k++)
     {
         if (m.prm.fem)
             for (size_t col = 0; col + 1 < m.triColourStart.size(); col++)
-                launch_fem(s, c, P, m.triColourStart[col], m.triColourStart[col + 1] - m.triColourStart[col]);
+                ops.fem(s, c, P, m.triColourStart[col], m.triColourStart[col + 1] - m.triColourStart[col]);
         else
         {
-            launch_reset_link_error(s, c);
+            ops.reset_link_error(s, c);
             for (size_t col = 0; col + 1 < m.linkColourStart.size(); col++)
-                launch_links(s, c, P, m.linkColourStart[col], m.linkColourStart[col + 1] - m.linkColourStart[col]);
+                ops.links(s, c, P, m.linkColourStart[col], m.linkColourStart[col + 1] - m.linkColourStart[col]);
         }
         if (m.prm.dihedral && k % m.prm.bendFreq == 0)
             for (size_t col = 0; col + 1 < m.bendColourStart.size(); col++)
-                launch_bends(s, c, P, m.bendColourStart[col], m.bendColourStart[col + 1] - m.bendColourStart[col], col == 0);
-        launch_solve_vertex_contacts(s, c, P, b);
-        launch_solve_multi_contacts(s, c, P, b, k);
+                ops.bends(s, c, P, m.bendColourStart[col], m.bendColourStart[col + 1] - m.bendColourStart[col], col == 0);
+        ops.vertex_contacts(s, c, P, b);
+        ops.multi_contacts(s, c, P, b, k);
         if (P.resTol > 0.f) launch_residual_exit(s, c, P, k);
     }
     launch_iteration_total(s, c);
@@ -1769,7 +1967,7 @@ bool ClothPatch::autotune(float h)
     const SolverParams P = m.solver_params(h);
     std::vector<int> key = {m.N, m.dc.T, m.dc.B, m.prm.iterations, m.prm.dihedral, m.prm.fem, m.prm.fixedIterations,
                             (int)m.buf.numVColl, m.prm.bendFreq, (int)m.prm.stageRecords, m.solverMode,
-                            (int)m.prm.ccd, m.broadMode};
+                            (int)m.prm.ccd, m.broadMode, (int)m.prm.fastMath};
     key.insert(key.end(), m.triColourStart.begin(), m.triColourStart.end());
     key.insert(key.end(), m.bendColourStart.begin(), m.bendColourStart.end());
     {
@@ -1787,11 +1985,13 @@ bool ClothPatch::autotune(float h)
     std::vector<SolverChoice> cand;
     int shift = 0; size_t smem = 0;
     const bool fits = m.triColourStart.size() <= 65 && m.bendColourStart.size() <= 65 && m.linkColourStart.size() <= 65;
-    if (fits && m.solverMode != SOLVE_GRID && gs_cluster_size(m.N, shift, smem) > 0) cand.push_back({SOLVE_CLUSTER, 0, 0, 0.f});
-    if (fits && m.solverMode != SOLVE_CLUSTER)
+    const SolverOps& ops = solver_ops(m.prm.fastMath);
+    if (fits && (m.solverMode == SOLVE_AUTO || m.solverMode == SOLVE_CLUSTER) && ops.cluster_size(m.N, shift, smem) > 0)
+        cand.push_back({SOLVE_CLUSTER, 0, 0, 0.f});
+    if (fits && (m.solverMode == SOLVE_AUTO || m.solverMode == SOLVE_GRID))
         for (int v = 0; v < gs_grid_variants(); v++)
         {
-            const int mb = gs_grid_max_blocks_per_sm(v);
+            const int mb = ops.grid_max_blocks_per_sm(v);
             for (int bps : {1, 2, mb})
                 if (bps >= 1 && bps <= mb)
                 {
@@ -1799,6 +1999,13 @@ bool ClothPatch::autotune(float h)
                     for (auto& c : cand) dup |= c.kind == SOLVE_GRID && c.variant == v && c.blocksPerSm == bps;
                     if (!dup) cand.push_back({SOLVE_GRID, v, bps, 0.f});
                 }
+        }
+    if (fits && (m.solverMode == SOLVE_AUTO || m.solverMode == SOLVE_TILED))
+        for (int v = 0; v < gs_grid_variants(); v++)
+        {
+            const int mb = ops.tiled_max_blocks_per_sm(v);
+            for (int bps : {1, 2})
+                if (bps <= mb && m.tile_plan(tiled_tile_count(m.N, bps))) cand.push_back({SOLVE_TILED, v, bps, 0.f});
         }
     if (m.solverMode == SOLVE_AUTO) cand.push_back({SOLVE_KERNELS, 0, 0, 0.f});
     if (cand.empty()) cand.push_back({SOLVE_KERNELS, 0, 0, 0.f});
@@ -1958,6 +2165,8 @@ bool ClothPatch::step(float dt)
             if (!autotune(h)) return false;
             m.tunedVersion = m.paramVersion;
         }
+        if (m.choice.kind == SOLVE_TILED && !m.tile_plan(tiled_tile_count(m.N, m.choice.blocksPerSm)))
+            m.choice = {SOLVE_GRID, m.choice.variant, m.choice.blocksPerSm, 0.f};
         cudaGraph_t g;
         if (timingFrames && timingCapture.size() != (size_t)n * NSEC * 2) set_timing(timingFrames);
         recordingSubstep = 0;

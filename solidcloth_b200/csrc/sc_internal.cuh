@@ -26,6 +26,7 @@ enum StatusBits {
     ST_COLOUR_OVERFLOW = 16,     // contact colouring needed more rounds than supported
     ST_MESH_STACK_OVERFLOW = 32,
     ST_BVH_STACK_OVERFLOW = 64,
+    ST_SYNC_TIMEOUT = 128,       // a neighbour wait of the tiled solver gave up (bounded spin)
 };
 
 struct SolverParams

@@ -276,7 +276,8 @@ def test_mass_spring_check_mode(dihedral, fixed):
 def test_solvers_are_bit_identical(scene):
     """The cluster-resident solver (one launch per substep, particles in
     distributed shared memory, records staged in shared memory or read from
-    global memory), every variant of the grid-resident cooperative solver, the
+    global memory), every variant of the grid-resident cooperative solver and of
+    its tiled form (neighbour waits instead of grid barriers), the
     one-kernel-per-colour path and the autotuner's choice are the same algorithm
     in the same order: bit-identical trajectories."""
     from solidcloth_b200 import api
@@ -297,7 +298,8 @@ def test_solvers_are_bit_identical(scene):
         sc, state = scenes.ccd_scene(16)
     out = []
     modes = [("cluster", True), ("cluster", False), ("kernels", False)]
-    modes += [("grid", (v, 1)) for v in range(len(api.grid_variants()))] + [("grid", (0, 2)), ("auto", None)]
+    modes += [("grid", (v, 1)) for v in range(len(api.grid_variants()))] + [("grid", (0, 2))]
+    modes += [("tiled", (v, 1)) for v in range(len(api.grid_variants()))] + [("tiled", (3, 2)), ("auto", None)]
     for mode, arg in modes:
         w, p = api.load_scene(sc)
         if mode == "cluster":
@@ -307,6 +309,8 @@ def test_solvers_are_bit_identical(scene):
             p.model.set_cluster_solver(False)
         elif mode == "grid":
             p.model.set_grid_solver(*arg)
+        elif mode == "tiled":
+            p.model.set_tiled_solver(*arg)
         if state is not None:
             p.model.set_state(*state)
         for _ in range(4):
@@ -333,11 +337,12 @@ def test_early_exit_mode_matches_oracle():
     assert p.model.solver_iterations() >= 1
 
 
-def _drift_runs(sc, frames, every):
-    """GPU (coloured order, portable arc cosine) against the oracle in the
-    reference's own order with libm's acosf, i.e. the reference algorithm; plus
-    two oracle perturbations that bound what 'the same solver' means for this
-    chaotic system: one extra iteration, and last-ulp changes of the arc cosine."""
+def _drift_runs(sc, frames, every, fast=False):
+    """GPU (coloured order, portable arc cosine; the IEEE or the fast solver build)
+    against the oracle in the reference's own order with libm's acosf, i.e. the
+    reference algorithm; plus two oracle perturbations that bound what 'the same
+    solver' means for this chaotic system: one extra iteration, and last-ulp
+    changes of the arc cosine."""
     from solidcloth_b200 import api
     from oracle.bridge import PortCloth
 
@@ -357,6 +362,7 @@ def _drift_runs(sc, frames, every):
     ref, plus1, ulp = oracle(it, False), oracle(it + 1, False), oracle(it, True)
     PortCloth.set_portable_math(True)
     w, p = api.load_scene(sc)
+    p.model.set_fast_math(fast)
     gpu = []
     for f in range(frames):
         p.step(sc.dt)
