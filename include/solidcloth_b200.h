@@ -232,6 +232,9 @@ SCEXP float scGetResidual(scModel model);
    (The constraint residual above does not vanish at convergence: the shear
    constraint is compliant and contacts hold the cloth strained.) */
 SCEXP void scSetResidualTarget(scModel model, float tol, int maxIterations);
+/* addition: the update residual's unit: 0 (default) = mean rest edge lengths,
+   1 = metres (the largest displacement of the last iteration itself) */
+SCEXP void scSetResidualUnit(scModel model, int unit);
 /* addition: Gauss-Seidel iterations run by all substeps since the last call */
 SCEXP int scGetIterationTotal(scModel model);
 
@@ -267,16 +270,11 @@ SCEXP void scSetClusterSolver(scModel model, bool val);
    give the same results): 0 = autotuned at the first step (default: the fastest
    of the cluster kernel, the grid-resident cooperative kernel's variants and the
    per-colour kernels, timed on this cloth), 1 = cluster kernel (clothes up to
-   131,072 particles), 2 = grid kernel (tuned variant), 3 = per-colour kernels,
-   4 = tiled grid kernel (tuned variant: each CTA owns a patch of the cloth and
-   waits only for the patches it shares particles with between colours).
+   131,072 particles), 2 = grid kernel (tuned variant), 3 = per-colour kernels.
    scSetClusterSolver(true/false) is mode 1 / 3. */
 SCEXP void scSetSolverMode(scModel model, int mode);
 /* force grid variant `variant` (0 .. scGetGridVariants()-1) with blocksPerSm CTAs per SM */
 SCEXP void scSetGridSolver(scModel model, int variant, int blocksPerSm);
-/* force the tiled grid kernel: variant as for scSetGridSolver, one tile per CTA,
-   blocksPerSm (1 or 2) CTAs per SM */
-SCEXP void scSetTiledSolver(scModel model, int variant, int blocksPerSm);
 /* out4 = {kind, grid variant, CTAs per SM, threads per CTA} of the solver in use;
    tuneMs (4 floats per candidate: kind, variant, CTAs per SM, ms per substep)
    gets up to cap candidates of the last tuning; returns the candidate count */
@@ -309,6 +307,12 @@ SCEXP int scGetSolverPrecision(scModel model);
    returns the number of colours; colourStart gets numColours+1 offsets if not NULL. */
 SCEXP int scGetConstraintOrder(scModel model, int kind, int* order, int* colourStart);
 SCEXP int scGetNumBends(scModel model);
+/* Static colours the triangle and edge collider contacts are solved by: each
+   triangle's colour (its FEM colour; T ints) and each collision-mesh edge's
+   (E ints), counts2 = {triangle colours, edge colours}; returns E. A contact's
+   colour is its triangle's / edge's plus the colour count times its collider's
+   index among the sphere, SDF and mesh colliders (capped at 127). */
+SCEXP int scGetStaticColours(scModel model, int* triColour, int* edgeColour, int* counts2);
 /* FEM rest data of every triangle: du1 du2 dv1 dv2 invDet lu0 lv0 lu2 lv2 area
    (Physics/ClothTypes.h:37-62); links' rest length and stiffness */
 SCEXP void scGetTriangleRest(scModel model, float* rest10);

@@ -96,6 +96,7 @@ def _load(path: Path, prefix: str):
         sig.update({"set_tri_order": ([C.c_void_p, _i, C.c_int], None),
                     "set_bend_order": ([C.c_void_p, _i, C.c_int], None),
                     "set_contact_order": ([C.c_void_p, C.c_int], None),
+                    "set_static_colours": ([C.c_void_p, _i, C.c_int, C.c_int, _i, C.c_int, C.c_int], None),
                     "set_portable_math": ([C.c_int], None),
                     "portable_acos": ([C.c_float], C.c_float),
                     "self_contact_colours": ([C.c_void_p, C.c_int, _i], None),
@@ -324,6 +325,20 @@ class PortCloth(CpuCloth):
 
     def set_contact_order(self, mode: int):
         self._fn("set_contact_order")(self.h, int(mode))
+
+    def set_static_colours(self, tri_colour, n_tri, edge_colour, n_edge):
+        """the GPU's static colours of triangles and collision-mesh edges: check
+        mode orders triangle / edge collider contacts by them"""
+        t = np.ascontiguousarray(tri_colour, np.int32)
+        e = np.ascontiguousarray(edge_colour, np.int32)
+        self._fn("set_static_colours")(self.h, _ip(t), t.size, int(n_tri), _ip(e), e.size, int(n_edge))
+
+    def check_mode(self, model):
+        """run in the GPU model's order: constraint colour order, contact colourings"""
+        self.set_tri_order(model.constraint_order(0)[0])
+        self.set_bend_order(model.constraint_order(1)[0])
+        self.set_contact_order(1)
+        self.set_static_colours(*model.static_colours())
 
     def self_contact_colours(self, kind):
         n = self._fn("num_contacts")(self.h, kind)

@@ -708,8 +708,10 @@ struct Tri /* Physics/ClothTypes.h:37-62 (solver fields) */
 struct Bend { u32 i1, i2, i3, i4; };
 
 struct VContact { int idx, feature, mesh; V3 point, normal; float depth, lambda, lambdaF; };
-struct TContact { u32 i1, i2, i3; int feature, mesh; V3 point, normal; float w1, w2, w3, lambda, lambdaF; };
-struct EContact { u32 i1, i2; int feature, mesh; V3 point, normal; float w1, w2, lambda, lambdaF; };
+/* item: the cloth triangle / edge; slot: the collider's index among the sphere,
+   mesh and SDF colliders (for the static contact colouring of check mode) */
+struct TContact { u32 i1, i2, i3; int feature, mesh; V3 point, normal; float w1, w2, w3, lambda, lambdaF; int item = -1, slot = 0; };
+struct EContact { u32 i1, i2; int feature, mesh; V3 point, normal; float w1, w2, lambda, lambdaF; int item = -1, slot = 0; };
 struct SContact { u32 i1, i2, i3, i4; V3 normal; float w1, w2, w3, side, lambda, lambdaF, error; };
 
 struct Collider
@@ -915,7 +917,7 @@ struct Cloth
        handleInside = handleCurrent = handleBorder = false
        (Physics/ClothCollision.cpp:430-580; SphereSDF/GridSDF in
        Physics/ClothCollisionSDF.h:8-55,124-206) */
-    void sdf_collisions(const Collider& col)
+    void sdf_collisions(const Collider& col, int slot)
     {
         const GridSDF* g = col.type == 7 ? sdfs[col.sdf].get() : nullptr;
         auto queryPoint = [&](V3 p, V3& cp, V3& n, int& feature) -> float {
@@ -980,6 +982,7 @@ struct Cloth
                     EContact c;
                     c.i1 = i1; c.i2 = i2; c.point = cp; c.normal = n; c.w1 = c0; c.w2 = c1;
                     c.feature = -1; c.mesh = -1; c.lambda = c.lambdaF = 0;
+                    c.item = (int)i; c.slot = slot;
                     edgeContacts.push_back(c);
                 }
             }
@@ -1017,6 +1020,7 @@ struct Cloth
                     t.i1 = i1; t.i2 = i2; t.i3 = i3; t.point = cp; t.normal = n;
                     t.w1 = coords.x; t.w2 = coords.y; t.w3 = coords.z;
                     t.feature = -1; t.mesh = -1; t.lambda = t.lambdaF = 0;
+                    t.item = (int)i; t.slot = slot;
                     triContacts.push_back(t);
                 }
             }
@@ -1059,7 +1063,7 @@ struct Cloth
        (Physics/ClothCollision.cpp:89-197 with
        MeshClosestPoints::ClosestPoints(mesh1, mesh2, tree, r, false),
        Geometry/ClosestPointsBetweenMeshes.cpp:595-695) */
-    void mesh_collisions(int meshId, float radTol, const std::vector<float>& tvs)
+    void mesh_collisions(int meshId, float radTol, const std::vector<float>& tvs, int slot)
     {
         /* The queries are independent (const tree walks); they run in parallel
            and their results are appended in query order, as the serial loops do. */
@@ -1106,6 +1110,7 @@ struct Cloth
                     t.i1 = i1; t.i2 = i2; t.i3 = i3; t.point = info.cpMesh; t.normal = info.normal;
                     t.w1 = info.bary.x; t.w2 = info.bary.y; t.w3 = info.bary.z;
                     t.feature = info.vertex; t.mesh = meshId; t.lambda = t.lambdaF = 0;
+                    t.item = j; t.slot = slot;
                     triContacts.push_back(t);
                 }
             }
@@ -1131,6 +1136,7 @@ struct Cloth
                     c.i1 = mesh.edges[e].i1; c.i2 = mesh.edges[e].i2; c.point = info.cpMesh; c.normal = info.normal;
                     c.w1 = info.cs[0]; c.w2 = info.cs[1]; c.feature = info.edge; c.mesh = meshId;
                     c.lambda = c.lambdaF = 0;
+                    c.item = e; c.slot = slot;
                     edgeContacts.push_back(c);
                 }
             }
@@ -1200,12 +1206,13 @@ struct Cloth
             if (tvs[i] > maxTv) maxTv = tvs[i];
         }
         float radTol = thickness + std::max(tolerance, maxTv * 1.5f);
+        int slot = 0;
         for (size_t c = 0; c < colliders.size(); c++)
         {
             const Collider& col = colliders[c];
             if (col.type == 1 && (flags & CF_WALLS)) wall_collisions(col.walls);
-            else if (col.type == 3 || col.type == 7) sdf_collisions(col);
-            else if (col.type == 4) mesh_collisions(col.mesh, radTol, tvs);
+            else if (col.type == 3 || col.type == 7) sdf_collisions(col, slot++);
+            else if (col.type == 4) mesh_collisions(col.mesh, radTol, tvs, slot++);
         }
         if (flags & CF_SELF)
         {
@@ -1583,6 +1590,38 @@ struct Cloth
         return order;
     }
 
+    /* The GPU's order of triangle / edge collider contacts: by the static colour
+       of the contact's cloth triangle / edge, offset by the colour count per
+       collider slot (the last colour, 127, is the serial bucket), list order within
+       a colour. Without static colours (orc_set_static_colours) the independent-set
+       colouring is used. */
+    std::vector<int> triColour, edgeColour;
+    int nTriColours = 0, nEdgeColours = 0;
+    template <typename C>
+    std::vector<int> static_order(const std::vector<C>& list, const std::vector<int>& colourOf, int ncol) const
+    {
+        const int n = (int)list.size();
+        std::vector<int> colour(n);
+        for (int i = 0; i < n; i++)
+        {
+            const int it = list[i].item;
+            if (colourOf.empty() || it < 0 || it >= (int)colourOf.size()) return colour_order_any(list);
+            colour[i] = std::min(colourOf[it] + ncol * list[i].slot, 127);
+        }
+        std::vector<int> order(n);
+        for (int i = 0; i < n; i++) order[i] = i;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return colour[a] < colour[b]; });
+        return order;
+    }
+    std::vector<int> colour_order_any(const std::vector<TContact>& l) const
+    {
+        return colour_order(l, [](const TContact& c, u32* v) { v[0] = c.i1; v[1] = c.i2; v[2] = c.i3; return 3; });
+    }
+    std::vector<int> colour_order_any(const std::vector<EContact>& l) const
+    {
+        return colour_order(l, [](const EContact& c, u32* v) { v[0] = c.i1; v[1] = c.i2; return 2; });
+    }
+
     static u32 contact_hash(u32 x)
     {
         /* "lowbias32" integer finaliser (C. Wellons, public domain) */
@@ -1605,12 +1644,10 @@ struct Cloth
         std::vector<int> lOrd = linkOrder.size() == links.size() ? linkOrder : seq(links.size());
         const float kLink = h2 * area * unit;
         auto v3of = [](const SContact& c, u32* v) { v[0] = c.i1; v[1] = c.i2; v[2] = c.i3; v[3] = c.i4; return 4; };
-        auto v3t = [](const TContact& c, u32* v) { v[0] = c.i1; v[1] = c.i2; v[2] = c.i3; return 3; };
-        auto v2e = [](const EContact& c, u32* v) { v[0] = c.i1; v[1] = c.i2; return 2; };
         std::vector<int> stOrd = contactOrder ? colour_order(selfTris, v3of) : seq(selfTris.size());
         std::vector<int> seOrd = contactOrder ? colour_order(selfEdges, v3of) : seq(selfEdges.size());
-        std::vector<int> tcOrd = contactOrder ? colour_order(triContacts, v3t) : seq(triContacts.size());
-        std::vector<int> ecOrd = contactOrder ? colour_order(edgeContacts, v2e) : seq(edgeContacts.size());
+        std::vector<int> tcOrd = contactOrder ? static_order(triContacts, triColour, nTriColours) : seq(triContacts.size());
+        std::vector<int> ecOrd = contactOrder ? static_order(edgeContacts, edgeColour, nEdgeColours) : seq(edgeContacts.size());
         float cl = 0, cb = 0, cv = 0, ce = 0, ct = 0, sct = 0, see = 0;
         int k = 0;
         while (true)
@@ -2161,6 +2198,16 @@ void orc_set_bend_order(void* h, const int* o, int n)
 }
 
 void orc_set_contact_order(void* h, int mode) { ((Cloth*)h)->contactOrder = mode; }
+
+void orc_set_static_colours(void* h, const int* triColour, int nt, int nTriColours, const int* edgeColour, int ne,
+                            int nEdgeColours)
+{
+    Cloth* c = (Cloth*)h;
+    c->triColour.assign(triColour, triColour + nt);
+    c->edgeColour.assign(edgeColour, edgeColour + ne);
+    c->nTriColours = nTriColours;
+    c->nEdgeColours = nEdgeColours;
+}
 
 /* Replace the cloth's model by an explicit topology (particles, FEM triangles
    with their rest data du1 du2 dv1 dv2 invDet lu0 lv0 lu2 lv2 area, bends, links

@@ -43,6 +43,10 @@ void orc_set_bend_order(void* h, const int* order, int n);
    GPU's deterministic independent-set colouring order (colour, then list index). */
 void orc_set_contact_order(void* h, int mode);
 void orc_set_link_order(void* h, const int* order, int n);
+/* static colours of the triangles and collision-mesh edges (and their counts):
+   the GPU's order of triangle / edge collider contacts in check mode */
+void orc_set_static_colours(void* h, const int* triColour, int nt, int nTriColours, const int* edgeColour, int ne,
+                            int nEdgeColours);
 void orc_load_topology(void* h, int n, const float* pos, const float* invMass, int nt, const unsigned* tri,
                        const float* rest10, int nb, const unsigned* bend4, int nl, const unsigned* link2,
                        const float* linkRest2);

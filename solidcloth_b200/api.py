@@ -137,7 +137,8 @@ SIGNATURES = {
     "scSetClusterSolver": ([scModel, C.c_bool], None),
     "scSetClusterStaging": ([scModel, C.c_bool], None),
     "scSetSolverPrecision": ([scModel, C.c_int], None),
-    "scSetTiledSolver": ([scModel, C.c_int, C.c_int], None),
+    "scSetResidualUnit": ([scModel, C.c_int], None),
+    "scGetStaticColours": ([scModel, _i, _i, _i], C.c_int),
     "scGetSolverPrecision": ([scModel], C.c_int),
     "scCreateClothBatch": ([scCollisionWorld, C.POINTER(scClothPatch), C.c_int], scClothPatch),
     "scGetBatchSize": ([scClothPatch], C.c_int),
@@ -330,7 +331,7 @@ class ClothModel:
         lib().scSetClusterSolver(self.h, bool(on))
 
     def set_solver_mode(self, mode: int):
-        """0 autotuned, 1 cluster kernel, 2 grid kernel, 3 per-colour kernels, 4 tiled grid kernel"""
+        """0 autotuned, 1 cluster kernel, 2 grid kernel, 3 per-colour kernels"""
         lib().scSetSolverMode(self.h, int(mode))
         _check("scSetSolverMode")
 
@@ -360,10 +361,6 @@ class ClothModel:
 
     def set_cluster_staging(self, on: bool):
         lib().scSetClusterStaging(self.h, bool(on))
-
-    def set_tiled_solver(self, variant: int, blocks_per_sm: int):
-        lib().scSetTiledSolver(self.h, int(variant), int(blocks_per_sm))
-        _check("scSetTiledSolver")
 
     def set_fast_math(self, on: bool):
         """solver numerics: True = the fast build (FMA, approximate div/sqrt),
@@ -456,8 +453,11 @@ class ClothModel:
         """max |C| over the warp, weft and shear constraints at the current positions"""
         return float(lib().scGetResidual(self.h))
 
-    def set_residual_target(self, tol: float, max_iterations: int):
-        """iterate each substep until the residual <= tol (at most max_iterations)"""
+    def set_residual_target(self, tol: float, max_iterations: int, metres: bool = False):
+        """iterate each substep until the update residual <= tol (at most
+        max_iterations); the residual in metres or (default) in mean rest edges"""
+        lib().scSetResidualUnit(self.h, int(bool(metres)))
+        _check("scSetResidualUnit")
         lib().scSetResidualTarget(self.h, float(tol), int(max_iterations))
         _check("scSetResidualTarget")
 
@@ -484,6 +484,16 @@ class ClothModel:
 
     def solver_iterations(self):
         return lib().scGetSolverIterations(self.h)
+
+    def static_colours(self):
+        """(triangle colours, triangle colour count, edge colours, edge colour count):
+        the static colouring of the triangle and edge collider contacts"""
+        L = lib()
+        tri = np.zeros(max(1, self.num_tris()), np.int32)
+        edge = np.zeros(max(1, self.num_edges()), np.int32)
+        cnt = np.zeros(2, np.int32)
+        L.scGetStaticColours(self.h, tri.ctypes.data_as(_i), edge.ctypes.data_as(_i), cnt.ctypes.data_as(_i))
+        return tri[:self.num_tris()].copy(), int(cnt[0]), edge[:self.num_edges()].copy(), int(cnt[1])
 
     def contact_colours(self, cls):
         counts = np.zeros(128, np.int32)

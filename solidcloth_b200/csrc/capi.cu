@@ -645,7 +645,7 @@ void scSetSelfCCD(scModel m, bool v) { if (M(m)) { M(m)->prm.ccd = v; M(m)->touc
 void scSetClusterSolver(scModel m, bool v) { scSetSolverMode(m, v ? SOLVE_CLUSTER : SOLVE_KERNELS); }
 void scSetSolverMode(scModel m, int mode)
 {
-    if (!M(m) || mode < SOLVE_AUTO || mode > SOLVE_TILED) { set_error(SC_ERR_ARG, "solver mode must be 0..4"); return; }
+    if (!M(m) || mode < SOLVE_AUTO || mode > SOLVE_KERNELS) { set_error(SC_ERR_ARG, "solver mode must be 0..3"); return; }
     M(m)->solverMode = mode;
     M(m)->tuned = false;
     M(m)->touch();
@@ -659,19 +659,6 @@ void scSetGridSolver(scModel m, int variant, int blocksPerSm)
     M(m)->touch();
     M(m)->tunedVersion = M(m)->paramVersion;
 }
-void scSetTiledSolver(scModel m, int variant, int blocksPerSm)
-{
-    if (!M(m) || variant < 0 || variant >= gs_grid_variants() || blocksPerSm < 1 || blocksPerSm > 2)
-    {
-        set_error(SC_ERR_ARG, "bad tiled solver variant");
-        return;
-    }
-    M(m)->solverMode = SOLVE_TILED;
-    M(m)->choice = {SOLVE_TILED, variant, blocksPerSm, 0.f};
-    M(m)->tuned = true;
-    M(m)->touch();
-    M(m)->tunedVersion = M(m)->paramVersion;
-}
 int scGetSolverChoice(scModel m, int* out4, float* tuneMs, int cap)
 {
     if (!M(m)) return 0;
@@ -679,7 +666,7 @@ int scGetSolverChoice(scModel m, int* out4, float* tuneMs, int cap)
     if (out4)
     {
         int th = 0, ft = 0, bt = 0;
-        if (ch.kind == SOLVE_GRID || ch.kind == SOLVE_TILED) gs_grid_variant_info(ch.variant, th, ft, bt);
+        if (ch.kind == SOLVE_GRID) gs_grid_variant_info(ch.variant, th, ft, bt);
         out4[0] = ch.kind; out4[1] = ch.variant; out4[2] = ch.blocksPerSm; out4[3] = th;
     }
     const auto& log = M(m)->tuneLog;
@@ -733,6 +720,26 @@ void scSetResidualTarget(scModel m, float tol, int maxIterations)
     }
     c->tuned = false;
     c->touch();
+}
+
+int scGetStaticColours(scModel m, int* triColour, int* edgeColour, int* counts2)
+{
+    ClothModel* c = M(m);
+    if (!c) { set_error(SC_ERR_ARG, "scGetStaticColours: null model"); return -1; }
+    if (triColour)
+        for (int col = 0; col + 1 < (int)c->triColourStart.size(); col++)
+            for (int k = c->triColourStart[col]; k < c->triColourStart[col + 1]; k++) triColour[c->triOrder[k]] = col;
+    if (edgeColour)
+        for (size_t e = 0; e < c->edgeColourHost.size(); e++) edgeColour[e] = c->edgeColourHost[e];
+    if (counts2) { counts2[0] = c->dc.nTriColours; counts2[1] = c->dc.nEdgeColours; }
+    return (int)c->edgeColourHost.size();
+}
+
+void scSetResidualUnit(scModel m, int unit)
+{
+    ClothModel* c = M(m);
+    if (!c || (unit != 0 && unit != 1)) { set_error(SC_ERR_ARG, "scSetResidualUnit: unit must be 0 (mean rest edge) or 1 (metres)"); return; }
+    if (c->prm.resMetres != (unit == 1)) { c->prm.resMetres = unit == 1; c->touch(); }
 }
 
 int scGetIterationTotal(scModel m)

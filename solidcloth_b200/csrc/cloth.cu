@@ -453,8 +453,6 @@ void ClothModel::release_device()
     release_buffers();
     for (void* p : allocs) cudaFree(p);
     allocs.clear();
-    tilePlans.clear();
-    tilePlanFailed.clear();
     dc = DevCloth{};
     if (stageHost) cudaFreeHost(stageHost);
     stageHost = nullptr;
@@ -488,7 +486,7 @@ SolverParams ClothModel::solver_params(float h) const
     P.fixedIterations = prm.fixedIterations; P.bendFreq = prm.bendFreq;
     P.resTol = prm.resTol;
     P.area = prm.area;
-    P.resScale = resScale;
+    P.resScale = prm.resMetres ? 1.f : resScale;
     P.selfThreshold = prm.selfThreshold;
     return P;
 }
@@ -679,6 +677,37 @@ static bool periodic_link_colours(const std::vector<uint2>& links, const std::ve
                                col);
 }
 
+// Edges of a grid cloth (any particle pairs with grid coordinates), coloured with a
+// pattern of period P: the distinct images of the edges on the P x P torus are
+// coloured by an exact search with K colours and every edge takes its image's
+// colour. Checked proper; false means "keep the greedy colouring".
+static bool periodic_pair_colours(const std::vector<uint2>& pairs, const std::vector<int2>& ij, int N, int P, int K,
+                                  std::vector<int>& col)
+{
+    auto T = [&](int j, int i) { return ((j % P + P) % P) * P + ((i % P + P) % P); };
+    std::map<std::pair<int, int>, int> index;
+    std::vector<std::vector<int>> tv;
+    for (const uint2& e : pairs)
+    {
+        const int2 p = ij[e.x], q = ij[e.y];
+        const int u = T(p.x, p.y), v = T(q.x, q.y);
+        if (u == v) return false;
+        const std::pair<int, int> k{std::min(u, v), std::max(u, v)};
+        if (!index.count(k)) { index[k] = (int)tv.size(); tv.push_back({u, v}); }
+    }
+    if (tv.size() > 4096) return false;
+    const std::vector<int> tc = exact_colouring(tv, K);
+    if (tc.empty()) return false;
+    col.assign(pairs.size(), 0);
+    for (size_t k = 0; k < pairs.size(); k++)
+    {
+        const int2 p = ij[pairs[k].x], q = ij[pairs[k].y];
+        const int u = T(p.x, p.y), v = T(q.x, q.y);
+        col[k] = tc[index[{std::min(u, v), std::max(u, v)}]];
+    }
+    return proper_colouring<2>((int)pairs.size(), N, [&](int k, uint32_t* v) { v[0] = pairs[k].x; v[1] = pairs[k].y; }, col);
+}
+
 // replace a greedy (colour, index) order by the one of `col` when it needs fewer colours
 static void adopt_colours(const std::vector<int>& col, std::vector<int>& order, std::vector<int>& start)
 {
@@ -716,6 +745,12 @@ bool ClothModel::upload_topology(const HMesh& mesh)
     release_device();
     SC_CUDA(cudaGetDevice(&device));
     const int T = (int)tris.size(), E = (int)mesh.edges.size(), B = (int)bends.size();
+    if (T >= (1 << 24))
+    {
+        // triangle contacts carry the triangle index in 24 bits
+        set_error(SC_ERR_UNSUPPORTED, "cloth has more than 16,777,215 triangles");
+        return false;
+    }
     dc.N = N; dc.T = T; dc.E = E; dc.B = B;
     colour_constraints();
     // particle state
@@ -751,6 +786,40 @@ bool ClothModel::upload_topology(const HMesh& mesh)
     uint4* dbend = (uint4*)dalloc(sizeof(uint4) * B);
     if (B) SC_CUDA(cudaMemcpy(dbend, bd.data(), sizeof(uint4) * B, cudaMemcpyHostToDevice));
     dc.bend = dbend;
+    // static colours of triangles (their FEM colours) and of collision-mesh edges
+    // (greedy in index order; grids: a period-4 pattern when it needs fewer) for
+    // the triangle and edge collider contacts
+    {
+        std::vector<uint8_t> tcol(std::max(1, T), 0), ecol(std::max(1, E), 0);
+        dc.nTriColours = std::max(1, (int)triColourStart.size() - 1);
+        for (int c = 0; c + 1 < (int)triColourStart.size(); c++)
+            for (int k = triColourStart[c]; k < triColourStart[c + 1]; k++) tcol[triOrder[k]] = (uint8_t)std::min(c, 255);
+        std::vector<uint2> ep(E);
+        for (int e = 0; e < E; e++) ep[e] = make_uint2(mesh.edges[e].i1, mesh.edges[e].i2);
+        std::vector<int> eord, estart;
+        greedy_colour<2>(E, N, [&](int i, uint32_t* v) { v[0] = ep[i].x; v[1] = ep[i].y; }, eord, estart);
+        std::vector<int> col(E, 0);
+        for (int c = 0; c + 1 < (int)estart.size(); c++)
+            for (int k = estart[c]; k < estart[c + 1]; k++) col[eord[k]] = c;
+        int ncol = std::max(1, (int)estart.size() - 1);
+        if ((int)gridIJ.size() == N && E > 0)
+        {
+            std::vector<int> deg(N, 0);
+            for (const uint2& e : ep) { deg[e.x]++; deg[e.y]++; }
+            const int K = *std::max_element(deg.begin(), deg.end());
+            std::vector<int> pc;
+            if (K < ncol && periodic_pair_colours(ep, gridIJ, N, 4, K, pc)) { col = pc; ncol = K; }
+        }
+        for (int e = 0; e < E; e++) ecol[e] = (uint8_t)std::min(col[e], 255);
+        dc.nEdgeColours = ncol;
+        edgeColourHost = col;
+        uint8_t* dt = (uint8_t*)dalloc(tcol.size());
+        uint8_t* de = (uint8_t*)dalloc(ecol.size());
+        SC_CUDA(cudaMemcpy(dt, tcol.data(), tcol.size(), cudaMemcpyHostToDevice));
+        SC_CUDA(cudaMemcpy(de, ecol.data(), ecol.size(), cudaMemcpyHostToDevice));
+        dc.triColour = dt;
+        dc.edgeColour = de;
+    }
     // collision-mesh topology
     uint32_t* dtri = (uint32_t*)dalloc(sizeof(uint32_t) * 3 * (size_t)T);
     SC_CUDA(cudaMemcpy(dtri, mesh.idx.data(), sizeof(uint32_t) * 3 * (size_t)T, cudaMemcpyHostToDevice));
@@ -1675,194 +1744,6 @@ void ClothPatch::record_substep(float h)
 }
 
 
-// ---------------------------------------------------- tiled solver plans
-// Particles are ordered by (instance, Morton code) — of the grid (column, row)
-// for grid clothes, else of the position quantised over the instance's box —
-// and cut into `tiles` chunks of equal count: compact patches of the cloth. A
-// constraint belongs to the tile of its first particle; inside each colour the
-// records are regrouped by tile (a permutation within the colour: the colour's
-// constraints share no particle, so the sweep's result is unchanged). Two tiles
-// are neighbours when a particle is touched by both: by their constraints, or
-// as a particle a tile owns (vertex contacts, velocity).
-static int sm_count()
-{
-    int dev = 0, sms = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    return sms > 0 ? sms : 1;
-}
-
-// tiles of the tiled solver at blocksPerSm CTAs per SM: one per CTA, at least
-// 32 particles each
-static int tiled_tile_count(int N, int blocksPerSm)
-{
-    return std::max(1, std::min(blocksPerSm * sm_count(), N / 32));
-}
-
-static inline uint32_t spread_bits16(uint32_t v)
-{
-    v &= 0xffffu;
-    v = (v | (v << 8)) & 0x00ff00ffu;
-    v = (v | (v << 4)) & 0x0f0f0f0fu;
-    v = (v | (v << 2)) & 0x33333333u;
-    v = (v | (v << 1)) & 0x55555555u;
-    return v;
-}
-static inline uint32_t spread_bits10(uint32_t v)
-{
-    v &= 0x3ffu;
-    v = (v | (v << 16)) & 0x030000ffu;
-    v = (v | (v << 8)) & 0x0300f00fu;
-    v = (v | (v << 4)) & 0x030c30c3u;
-    v = (v | (v << 2)) & 0x09249249u;
-    return v;
-}
-
-const TilePlan* ClothModel::tile_plan(int tiles)
-{
-    auto it = tilePlans.find(tiles);
-    if (it != tilePlans.end()) return &it->second;
-    if (tilePlanFailed.count(tiles) || tiles < 1 || N < 1 || !dc.pos) return nullptr;
-    const int T = (int)tris.size(), B = (int)bends.size(), L = (int)links.size();
-    // particle order and chunks
-    std::vector<int> inst(N, 0);
-    for (size_t k = 0; k + 1 < instV.size(); k++)
-        for (int v = instV[k]; v < instV[k + 1]; v++) inst[v] = (int)k;
-    const int numInst = instV.size() > 1 ? (int)instV.size() - 1 : 1;
-    std::vector<V3> lo(numInst, mk(1e30f, 1e30f, 1e30f)), hi(numInst, mk(-1e30f, -1e30f, -1e30f));
-    const bool grid = (int)gridIJ.size() == N;
-    if (!grid)
-        for (int v = 0; v < N; v++) { lo[inst[v]] = vmin(lo[inst[v]], hpos[v]); hi[inst[v]] = vmax(hi[inst[v]], hpos[v]); }
-    std::vector<uint64_t> key(N);
-    for (int v = 0; v < N; v++)
-    {
-        uint32_t code;
-        if (grid) code = spread_bits16((uint32_t)gridIJ[v].x) | (spread_bits16((uint32_t)gridIJ[v].y) << 1);
-        else
-        {
-            const V3 a = lo[inst[v]], d = hi[inst[v]] - a;
-            auto q = [](float x, float lo_, float ext) {
-                const float t = ext > 0.f ? (x - lo_) / ext : 0.f;
-                return (uint32_t)std::min(1023.f, std::max(0.f, t * 1023.f));
-            };
-            code = spread_bits10(q(hpos[v].x, a.x, d.x)) | (spread_bits10(q(hpos[v].y, a.y, d.y)) << 1) |
-                   (spread_bits10(q(hpos[v].z, a.z, d.z)) << 2);
-        }
-        key[v] = ((uint64_t)inst[v] << 32) | code;
-    }
-    std::vector<int> ptcl(N);
-    for (int v = 0; v < N; v++) ptcl[v] = v;
-    std::stable_sort(ptcl.begin(), ptcl.end(), [&](int a, int b) { return key[a] < key[b]; });
-    std::vector<int> tileStart(tiles + 1), tileOf(N);
-    for (int t = 0; t <= tiles; t++) tileStart[t] = (int)((int64_t)t * N / tiles);
-    for (int t = 0; t < tiles; t++)
-        for (int k = tileStart[t]; k < tileStart[t + 1]; k++) tileOf[ptcl[k]] = t;
-    // touching tiles per particle (owner first), at most KT
-    constexpr int KT = 16;
-    std::vector<int> touchN(N, 1), touch((size_t)N * KT);
-    for (int v = 0; v < N; v++) touch[(size_t)v * KT] = tileOf[v];
-    bool ok = true;
-    auto add_touch = [&](uint32_t v, int t) {
-        int* a = &touch[(size_t)v * KT];
-        for (int k = 0; k < touchN[v]; k++) if (a[k] == t) return;
-        if (touchN[v] == KT) { ok = false; return; }
-        a[touchN[v]++] = t;
-    };
-    // (colour, tile) regrouping of one constraint kind: order[k] = colour-order
-    // position of the k-th record of the tiled layout
-    auto regroup = [&](const std::vector<int>& colourStart, int count, auto firstOf, auto particlesOf,
-                       std::vector<int>& order, std::vector<int>& start) {
-        const int ncol = colourStart.empty() ? 0 : (int)colourStart.size() - 1;
-        order.assign(count, 0);
-        start.assign((size_t)ncol * tiles + 1, 0);
-        std::vector<int> cnt(tiles);
-        for (int c = 0; c < ncol; c++)
-        {
-            std::fill(cnt.begin(), cnt.end(), 0);
-            for (int k = colourStart[c]; k < colourStart[c + 1]; k++) cnt[tileOf[firstOf(k)]]++;
-            int acc = colourStart[c];
-            for (int t = 0; t < tiles; t++) { start[(size_t)c * tiles + t] = acc; acc += cnt[t]; cnt[t] = start[(size_t)c * tiles + t]; }
-            for (int k = colourStart[c]; k < colourStart[c + 1]; k++)
-            {
-                const int t = tileOf[firstOf(k)];
-                order[cnt[t]++] = k;
-                particlesOf(k, t);
-            }
-        }
-        start[(size_t)ncol * tiles] = count;
-    };
-    std::vector<int> femOrd, femSt, bendOrd, bendSt, linkOrd, linkSt;
-    regroup(triColourStart, T, [&](int k) { return (int)tris[triOrder[k]].i1; },
-            [&](int k, int t) { const FemHost& f = tris[triOrder[k]]; add_touch(f.i1, t); add_touch(f.i2, t); add_touch(f.i3, t); },
-            femOrd, femSt);
-    regroup(bendColourStart, B, [&](int k) { return (int)bends[bendOrder[k]].x; },
-            [&](int k, int t) { const uint4 q = bends[bendOrder[k]]; add_touch(q.x, t); add_touch(q.y, t); add_touch(q.z, t); add_touch(q.w, t); },
-            bendOrd, bendSt);
-    regroup(linkColourStart, L, [&](int k) { return (int)links[linkOrder[k]].x; },
-            [&](int k, int t) { const uint2 q = links[linkOrder[k]]; add_touch(q.x, t); add_touch(q.y, t); },
-            linkOrd, linkSt);
-    if (!ok) { tilePlanFailed[tiles] = true; return nullptr; }
-    std::vector<std::vector<int>> nb(tiles);
-    for (int v = 0; v < N; v++)
-    {
-        const int* a = &touch[(size_t)v * KT];
-        for (int x = 0; x < touchN[v]; x++)
-            for (int y = 0; y < touchN[v]; y++)
-                if (x != y) nb[a[x]].push_back(a[y]);
-    }
-    std::vector<int> nbrStart(tiles + 1, 0), nbr;
-    for (int t = 0; t < tiles; t++)
-    {
-        std::sort(nb[t].begin(), nb[t].end());
-        nb[t].erase(std::unique(nb[t].begin(), nb[t].end()), nb[t].end());
-        if ((int)nb[t].size() > TILED_MAX_NEIGHBOURS) { tilePlanFailed[tiles] = true; return nullptr; }
-        nbr.insert(nbr.end(), nb[t].begin(), nb[t].end());
-        nbrStart[t + 1] = (int)nbr.size();
-    }
-    // records in the tiled layout (the formats of upload_topology)
-    std::vector<float4> fem(3 * (size_t)std::max(1, T));
-    for (int k = 0; k < T; k++)
-    {
-        const FemHost& t = tris[triOrder[femOrd[k]]];
-        fem[3 * (size_t)k] = make_float4(bits_f(t.i1), bits_f(t.i2), bits_f(t.i3), t.du1);
-        fem[3 * (size_t)k + 1] = make_float4(t.du2, t.dv1, t.dv2, t.invDet);
-        fem[3 * (size_t)k + 2] = make_float4(t.lu2, t.lv2, t.lu0 * t.lv0, t.area);
-    }
-    std::vector<uint4> bd(std::max(1, B));
-    for (int k = 0; k < B; k++) bd[k] = bends[bendOrder[bendOrd[k]]];
-    std::vector<float4> lk(std::max(1, L));
-    for (int k = 0; k < L; k++)
-    {
-        const int li = linkOrder[linkOrd[k]];
-        lk[k] = make_float4(bits_f(links[li].x), bits_f(links[li].y), linkRest[li].x, linkRest[li].y);
-    }
-    auto up = [&](const void* src, size_t bytes) -> void* {
-        void* d = dalloc(std::max<size_t>(bytes, 16));
-        if (d && bytes && cudaMemcpy(d, src, bytes, cudaMemcpyHostToDevice) != cudaSuccess) return nullptr;
-        return d;
-    };
-    TilePlan tp{};
-    tp.tiles = tiles;
-    tp.fem = (const float4*)up(fem.data(), sizeof(float4) * 3 * (size_t)T);
-    tp.femStart = (const int*)up(femSt.data(), sizeof(int) * femSt.size());
-    tp.bend = (const uint4*)up(bd.data(), sizeof(uint4) * (size_t)B);
-    tp.bendStart = (const int*)up(bendSt.data(), sizeof(int) * bendSt.size());
-    tp.link = (const float4*)up(lk.data(), sizeof(float4) * (size_t)L);
-    tp.linkStart = (const int*)up(linkSt.data(), sizeof(int) * linkSt.size());
-    tp.tileStart = (const int*)up(tileStart.data(), sizeof(int) * tileStart.size());
-    tp.ptcl = (const int*)up(ptcl.data(), sizeof(int) * (size_t)N);
-    tp.nbrStart = (const int*)up(nbrStart.data(), sizeof(int) * nbrStart.size());
-    tp.nbr = (const int*)up(nbr.data(), sizeof(int) * nbr.size());
-    tp.flags = (unsigned*)dalloc(sizeof(unsigned) * (size_t)tiles);
-    if (!tp.fem || !tp.femStart || !tp.bend || !tp.bendStart || !tp.link || !tp.linkStart || !tp.tileStart || !tp.ptcl ||
-        !tp.nbrStart || !tp.nbr || !tp.flags)
-    {
-        tilePlanFailed[tiles] = true;
-        return nullptr;
-    }
-    return &(tilePlans[tiles] = tp);
-}
-
 // One substep's Gauss-Seidel loop and velocity update, by the chosen solver:
 // the cluster-resident kernel, the grid-resident cooperative kernel (a tuned
 // variant), or one kernel per colour. The three are the same algorithm in the
@@ -1922,12 +1803,6 @@ bool ClothPatch::record_solve(cudaStream_t s, const SolverParams& P, const Solve
     }
     if (ch.kind == SOLVE_GRID && planFits && ops.grid(s, c, P, b, plan, ch.variant, ch.blocksPerSm))
         return true;
-    if (ch.kind == SOLVE_TILED && planFits)
-    {
-        // the plan was built before capture (ClothPatch::step, autotune)
-        auto it = m.tilePlans.find(tiled_tile_count(m.N, ch.blocksPerSm));
-        if (it != m.tilePlans.end() && ops.tiled(s, c, P, b, plan, it->second, ch.variant)) return true;
-    }
     if (P.resTol > 0.f) launch_residual_exit(s, c, P, -1);
     for (int k = 0; k < iterations; k++)
     {
@@ -1999,13 +1874,6 @@ bool ClothPatch::autotune(float h)
                     for (auto& c : cand) dup |= c.kind == SOLVE_GRID && c.variant == v && c.blocksPerSm == bps;
                     if (!dup) cand.push_back({SOLVE_GRID, v, bps, 0.f});
                 }
-        }
-    if (fits && (m.solverMode == SOLVE_AUTO || m.solverMode == SOLVE_TILED))
-        for (int v = 0; v < gs_grid_variants(); v++)
-        {
-            const int mb = ops.tiled_max_blocks_per_sm(v);
-            for (int bps : {1, 2})
-                if (bps <= mb && m.tile_plan(tiled_tile_count(m.N, bps))) cand.push_back({SOLVE_TILED, v, bps, 0.f});
         }
     if (m.solverMode == SOLVE_AUTO) cand.push_back({SOLVE_KERNELS, 0, 0, 0.f});
     if (cand.empty()) cand.push_back({SOLVE_KERNELS, 0, 0, 0.f});
@@ -2165,8 +2033,6 @@ bool ClothPatch::step(float dt)
             if (!autotune(h)) return false;
             m.tunedVersion = m.paramVersion;
         }
-        if (m.choice.kind == SOLVE_TILED && !m.tile_plan(tiled_tile_count(m.N, m.choice.blocksPerSm)))
-            m.choice = {SOLVE_GRID, m.choice.variant, m.choice.blocksPerSm, 0.f};
         cudaGraph_t g;
         if (timingFrames && timingCapture.size() != (size_t)n * NSEC * 2) set_timing(timingFrames);
         recordingSubstep = 0;

@@ -102,13 +102,14 @@ struct HostParams
     bool stageRecords = true;    // cluster solver: constraint records in shared memory
     bool fastMath = false;       // solver build: false = IEEE (bit-exact), true = FMA + approximate div/sqrt
     float resTol = 0.f;          // > 0: Gauss-Seidel runs until the residual is <= resTol (iterations = cap)
+    bool resMetres = false;      // update residual in metres (true) or in mean rest edge lengths
 };
 
 // a collider acting on the particles [vBegin, vBegin + vCount) of batch instance `inst`
 struct BatchColl { std::shared_ptr<Collidable> coll; int vBegin, vCount, inst; };
 
 // solver selection (autotuned unless forced)
-enum SolverKind { SOLVE_AUTO = 0, SOLVE_CLUSTER = 1, SOLVE_GRID = 2, SOLVE_KERNELS = 3, SOLVE_TILED = 4 };
+enum SolverKind { SOLVE_AUTO = 0, SOLVE_CLUSTER = 1, SOLVE_GRID = 2, SOLVE_KERNELS = 3 };
 struct SolverChoice { int kind, variant, blocksPerSm; float ms; int broad; };
 
 struct FemHost { uint32_t i1, i2, i3; float du1, du2, dv1, dv2, det, invDet, lu0, lv0, su, sv, lu2, lv2, area; };
@@ -148,6 +149,7 @@ public:
     std::vector<uint4> quads;
     std::vector<int> triOrder, bendOrder;      // colour order
     std::vector<int> triColourStart, bendColourStart;
+    std::vector<int> edgeColourHost;           // static colour of each collision-mesh edge (edge contacts)
     bool mouseActive = false;
 
     // device
@@ -197,12 +199,6 @@ public:
     float broadMs[BROAD_WALKS] = {};            // tuned times of the broad-phase walks
     void colour_constraints();
     void touch() { paramVersion++; }
-    // tiled solver plans, one per tile count (built on first use, outside stream
-    // capture; freed with the device topology). nullptr: no plan of that size
-    // (more neighbour tiles than TILED_MAX_NEIGHBOURS somewhere)
-    std::map<int, TilePlan> tilePlans;
-    std::map<int, bool> tilePlanFailed;
-    const TilePlan* tile_plan(int tiles);
 };
 
 class ClothPatch

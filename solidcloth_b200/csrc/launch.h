@@ -148,26 +148,6 @@ int gs_grid_max_blocks_per_sm(int variant);
 bool launch_gs_grid(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b, GsPlan plan,
                     int variant, int blocksPerSm);
 
-// Spatially tiled plan of the grid-resident solver (one tile per CTA). Tile t
-// owns the particles ptcl[tileStart[t], tileStart[t+1]) (a Morton-ordered chunk
-// of its instance) and the constraints whose first particle it owns; within a
-// colour its constraints are contiguous (records in (colour, tile) order, a
-// permutation inside each colour, so the sweep's result is unchanged). Tiles
-// whose constraints share a particle are neighbours: a colour phase waits only
-// for its neighbours' progress words (flags), not for the whole grid.
-struct TilePlan
-{
-    int tiles;
-    const float4* fem; const int* femStart;      // 3 per triangle; nFemCol * tiles + 1 offsets
-    const uint4* bend; const int* bendStart;     // nBendCol * tiles + 1
-    const float4* link; const int* linkStart;    // nLinkCol * tiles + 1
-    const int* tileStart; const int* ptcl;       // tiles + 1; N
-    const int* nbrStart; const int* nbr;         // tiles + 1; neighbour tiles
-    unsigned* flags;                             // tiles: phases completed (zeroed before each launch)
-};
-constexpr int TILED_MAX_NEIGHBOURS = 128;
-constexpr int SYNC_SPIN_LIMIT = 1 << 20;         // polls before a neighbour wait gives up (flagged)
-
 // The solver's entry points as one table per build of solver.cuh: IEEE division
 // and square root without FMA contraction (bit-exact with the reference's
 // operation order, the check-mode build) or the fast build (FMA contraction,
@@ -185,8 +165,6 @@ struct SolverOps
     void (*cluster)(cudaStream_t, const DevCloth&, const SolverParams&, const Buffers&, GsPlan, int, size_t);
     int (*grid_max_blocks_per_sm)(int);
     bool (*grid)(cudaStream_t, const DevCloth&, const SolverParams&, const Buffers&, GsPlan, int, int);
-    int (*tiled_max_blocks_per_sm)(int);
-    bool (*tiled)(cudaStream_t, const DevCloth&, const SolverParams&, const Buffers&, GsPlan, const TilePlan&, int);
 };
 const SolverOps& solver_ops(bool fast);
 

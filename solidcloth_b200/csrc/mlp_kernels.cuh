@@ -4,15 +4,20 @@
 // solution. It has no counterpart in the reference; the plain solver stays the
 // fallback and the judge (the residual decides when a substep is done).
 //
-// Forward on the tensor cores: BF16 weights and activations, FP32 accumulation,
-// mma.sync m16n8k16 (a warp owns 16-row tiles of particles; a layer's FP32
-// accumulator fragments are packed in registers into the next layer's BF16
-// operand fragments, so activations never leave the warp). Backward in FP32
-// from shared memory; weight gradients accumulate over the grid with atomics;
-// Adam updates the FP32 master weights. Included by step_kernels.cu (it uses the
-// collider queries defined there).
+// Every contraction runs on the fifth-generation tensor cores (tc05.cuh): tiles
+// of 128 particles (rows) per CTA, BF16 operands staged in shared memory, FP32
+// accumulators in tensor memory, one thread issuing tcgen05.mma and the CTA
+// waiting on an mbarrier that tcgen05.commit arrives on; the four warps read
+// their 32 rows back with tcgen05.ld for the bias / GELU epilogue, which writes
+// the next layer's BF16 operand tile. Training runs the same forward, then the
+// backward on the tensor cores too: dH = dZ W (K-major operands, transposed
+// weights in shared memory) and dW = dZ^T H (the activation tiles read
+// MN-major, summed over the CTA's tiles in tensor memory before one atomic
+// pass). Adam updates the FP32 master weights. Included by step_kernels.cu (the
+// features use the collider queries defined there).
 #pragma once
 #include <cuda_bf16.h>
+#include "tc05.cuh"
 
 namespace sc {
 
@@ -24,41 +29,69 @@ constexpr int ML_W3 = ML_B2 + ML_H, ML_B3 = ML_W3 + ML_H * ML_H;
 constexpr int ML_W4 = ML_B3 + ML_H, ML_B4 = ML_W4 + ML_OUT * ML_H;
 constexpr int ML_NPARAM = ML_B4 + ML_OUT;     // 9347
 constexpr int ML_NNORM = 2 * ML_IN + ML_OUT;  // feature mean, feature 1/std, output scale
+constexpr int ML_ROWS = 128;                  // rows (particles / samples) per tile = MMA M
 
-// BF16 weights in shared memory, [out][in] with in padded to 16 (layer 1) and out
-// padded to 8 (layer 4): the B fragment pairs (k, k+1) of one n are one 32-bit word
-struct MlpSmem
+// instruction descriptors: M = 128 rows, N = 64 hidden units or 16 (padded outputs
+// / padded inputs); forward and dH operands K-major, weight-gradient operands MN-major
+constexpr uint32_t IDESC_N64 = umma_idesc(128, 64, 0, 0);
+constexpr uint32_t IDESC_N16 = umma_idesc(128, 16, 0, 0);
+constexpr uint32_t IDESC_GRAD_N64 = umma_idesc(128, 64, 1, 1);
+constexpr uint32_t IDESC_GRAD_N16 = umma_idesc(128, 16, 1, 1);
+
+// BF16 weights in core layout: forward operands W[out][in] (layer 1 inputs padded
+// to 16, layer 4 outputs padded to 16) and, for training, the transposes
+// W^T[in][out] of layers 2-4 (layer 4's outputs padded to 16)
+struct __align__(128) MlpTcWeights
 {
-    __nv_bfloat16 w1[ML_H * 16];
-    __nv_bfloat16 w2[ML_H * ML_H];
-    __nv_bfloat16 w3[ML_H * ML_H];
-    __nv_bfloat16 w4[8 * ML_H];
-    float b1[ML_H], b2[ML_H], b3[ML_H], b4[8];
+    unsigned char w1[64 * 16 * 2];
+    unsigned char w2[64 * 64 * 2];
+    unsigned char w3[64 * 64 * 2];
+    unsigned char w4[16 * 64 * 2];
+    float b1[ML_H], b2[ML_H], b3[ML_H], b4[16];
     float mean[ML_IN], istd[ML_IN], oscale[ML_OUT];
 };
-
-__device__ __forceinline__ void mlp_load_smem(MlpSmem& s, const float* prm, const float* norm)
+struct __align__(128) MlpTcTrans
 {
-    for (int k = threadIdx.x; k < ML_H * 16; k += blockDim.x)
+    unsigned char w2t[64 * 64 * 2];
+    unsigned char w3t[64 * 64 * 2];
+    unsigned char w4t[64 * 16 * 2];
+};
+
+__device__ __forceinline__ void put_bf16(unsigned char* tile, int r, int k, int K, float v)
+{
+    *reinterpret_cast<__nv_bfloat16*>(tile + core_off(r, k, K)) = __float2bfloat16_rn(v);
+}
+
+__device__ __forceinline__ void mlp_tc_load(MlpTcWeights& s, MlpTcTrans* t, const float* prm, const float* norm)
+{
+    for (int k = threadIdx.x; k < 64 * 16; k += blockDim.x)
     {
         const int o = k / 16, i = k % 16;
-        s.w1[k] = __float2bfloat16_rn(i < ML_IN ? prm[ML_W1 + o * ML_IN + i] : 0.f);
+        put_bf16(s.w1, o, i, 16, i < ML_IN ? prm[ML_W1 + o * ML_IN + i] : 0.f);
     }
-    for (int k = threadIdx.x; k < ML_H * ML_H; k += blockDim.x)
+    for (int k = threadIdx.x; k < 64 * 64; k += blockDim.x)
     {
-        s.w2[k] = __float2bfloat16_rn(prm[ML_W2 + k]);
-        s.w3[k] = __float2bfloat16_rn(prm[ML_W3 + k]);
+        const int o = k / 64, i = k % 64;
+        put_bf16(s.w2, o, i, 64, prm[ML_W2 + k]);
+        put_bf16(s.w3, o, i, 64, prm[ML_W3 + k]);
+        if (t)
+        {
+            put_bf16(t->w2t, i, o, 64, prm[ML_W2 + k]);
+            put_bf16(t->w3t, i, o, 64, prm[ML_W3 + k]);
+        }
     }
-    for (int k = threadIdx.x; k < 8 * ML_H; k += blockDim.x)
+    for (int k = threadIdx.x; k < 16 * 64; k += blockDim.x)
     {
-        const int o = k / ML_H, i = k % ML_H;
-        s.w4[k] = __float2bfloat16_rn(o < ML_OUT ? prm[ML_W4 + o * ML_H + i] : 0.f);
+        const int o = k / 64, i = k % 64;
+        const float w = o < ML_OUT ? prm[ML_W4 + o * ML_H + i] : 0.f;
+        put_bf16(s.w4, o, i, 64, w);
+        if (t) put_bf16(t->w4t, i, o, 16, w);
     }
     for (int k = threadIdx.x; k < ML_H; k += blockDim.x)
     {
         s.b1[k] = prm[ML_B1 + k]; s.b2[k] = prm[ML_B2 + k]; s.b3[k] = prm[ML_B3 + k];
     }
-    if (threadIdx.x < 8) s.b4[threadIdx.x] = threadIdx.x < ML_OUT ? prm[ML_B4 + threadIdx.x] : 0.f;
+    if (threadIdx.x < 16) s.b4[threadIdx.x] = threadIdx.x < ML_OUT ? prm[ML_B4 + threadIdx.x] : 0.f;
     if (threadIdx.x < ML_IN) { s.mean[threadIdx.x] = norm[threadIdx.x]; s.istd[threadIdx.x] = norm[ML_IN + threadIdx.x]; }
     if (threadIdx.x < ML_OUT) s.oscale[threadIdx.x] = norm[2 * ML_IN + threadIdx.x];
 }
@@ -82,91 +115,116 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
     return *reinterpret_cast<const uint32_t*>(&v);
 }
 
-// D += A (16x16 bf16, row) * B (16x8 bf16, col), FP32 accumulate
-__device__ __forceinline__ void mma_bf16(float* d, const uint32_t* a, uint32_t b0, uint32_t b1)
+
+// this thread's row of a 16-column operand tile (K = 16) from 16 floats
+__device__ __forceinline__ void put_row16(unsigned char* tile, int r, const float* x)
 {
-    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
-                 "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
-                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+    uint4 q0, q1;
+    q0.x = pack_bf16(x[0], x[1]); q0.y = pack_bf16(x[2], x[3]); q0.z = pack_bf16(x[4], x[5]); q0.w = pack_bf16(x[6], x[7]);
+    q1.x = pack_bf16(x[8], x[9]); q1.y = pack_bf16(x[10], x[11]); q1.z = pack_bf16(x[12], x[13]); q1.w = pack_bf16(x[14], x[15]);
+    *reinterpret_cast<uint4*>(tile + core_off(r, 0, 16)) = q0;
+    *reinterpret_cast<uint4*>(tile + core_off(r, 8, 16)) = q1;
 }
 
-// One dense layer for a warp's 16-row tile: acc[NT][4] = A[KT] * W^T + bias.
-// Fragment coordinates (lane = 4 g + t): A a0 (g, 2t..2t+1) a1 (g+8, 2t..)
-// a2 (g, 2t+8..) a3 (g+8, 2t+8..); B b0 (k = 2t.., n = g) b1 (k = 2t+8.., n = g);
-// C c0,c1 (g, 2t..2t+1) c2,c3 (g+8, 2t..2t+1).
-template <int KT, int NT>
-__device__ __forceinline__ void mlp_layer(const uint32_t (&a)[KT][4], const __nv_bfloat16* w, const float* bias, float (&acc)[NT][4])
+// 32 accumulator columns of this thread's row (tensor memory at taddr) plus bias,
+// through GELU, into columns [c0, c0 + 32) of row r of a K-column operand tile
+__device__ __forceinline__ void epilogue_gelu32(uint32_t taddr, const float* bias, unsigned char* tile, int r, int c0, int K)
 {
-    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    constexpr int KP = KT * 16;
+    uint32_t v[32];
+    tc_ld32(taddr, v);
+    tc_wait_ld();
 #pragma unroll
-    for (int j = 0; j < NT; j++)
+    for (int c = 0; c < 4; c++)
     {
-        acc[j][0] = acc[j][2] = bias[8 * j + 2 * t];
-        acc[j][1] = acc[j][3] = bias[8 * j + 2 * t + 1];
-        const __nv_bfloat16* col = w + (8 * j + g) * KP + 2 * t;
+        float h[8];
 #pragma unroll
-        for (int kt = 0; kt < KT; kt++)
-        {
-            const uint32_t b0 = *reinterpret_cast<const uint32_t*>(col + 16 * kt);
-            const uint32_t b1 = *reinterpret_cast<const uint32_t*>(col + 16 * kt + 8);
-            mma_bf16(acc[j], a[kt], b0, b1);
-        }
+        for (int j = 0; j < 8; j++) h[j] = gelu(__uint_as_float(v[8 * c + j]) + bias[c0 + 8 * c + j]);
+        uint4 q;
+        q.x = pack_bf16(h[0], h[1]); q.y = pack_bf16(h[2], h[3]); q.z = pack_bf16(h[4], h[5]); q.w = pack_bf16(h[6], h[7]);
+        *reinterpret_cast<uint4*>(tile + core_off(r, c0 + 8 * c, K)) = q;
     }
 }
 
-// accumulator fragments (after GELU) -> next layer's operand fragments
-template <int NT>
-__device__ __forceinline__ void acc_to_operand(const float (&acc)[NT][4], uint32_t (&a)[NT / 2][4])
+// Shared state of a CTA driving the tensor cores: the mbarrier the commits arrive
+// on, its next parity, and the tensor-memory base.
+struct TcCtx
 {
-#pragma unroll
-    for (int j = 0; j < NT; j++)
+    uint32_t mbar, phase, tmem;
+    bool ok;
+    __device__ __forceinline__ bool wait()
     {
-        const uint32_t lo = pack_bf16(gelu(acc[j][0]), gelu(acc[j][1]));
-        const uint32_t hi = pack_bf16(gelu(acc[j][2]), gelu(acc[j][3]));
-        if (j & 1) { a[j >> 1][2] = lo; a[j >> 1][3] = hi; }
-        else { a[j >> 1][0] = lo; a[j >> 1][1] = hi; }
+        const bool done = mbar_wait(mbar, phase);
+        phase ^= 1u;
+        tc_fence_after();
+        return __syncthreads_and(done) != 0;   // every thread takes the same path
     }
+};
+
+// Forward of the CTA's 128-row tile whose normalised inputs (BF16, K = 16) are
+// already in x: hidden layers into tensor-memory columns zcol[0..2] (pre-
+// activations, no bias), their GELU outputs as operand tiles h[0..2] (each may be
+// the same buffer when they need not survive), outputs into column ycol. Returns
+// false if a wait gave up.
+__device__ __forceinline__ bool mlp_tc_forward(TcCtx& t, const MlpTcWeights& s, unsigned char* x,
+                                               unsigned char* const* h, const uint32_t* zcol, uint32_t ycol)
+{
+    const int r = threadIdx.x;
+    const uint32_t lanes = tmem_lane_base(t.tmem);
+    tc_sync_for_mma();
+    if (r == 0)
+    {
+        umma_bf16(t.tmem + zcol[0], desc_kmajor(smem_addr(x), 16), desc_kmajor(smem_addr(s.w1), 16), IDESC_N64, 0);
+        umma_commit(t.mbar);
+    }
+    if (!t.wait()) return false;
+    const float* bias[3] = {s.b1, s.b2, s.b3};
+    const unsigned char* w[3] = {s.w2, s.w3, s.w4};
+    for (int l = 0; l < 3; l++)
+    {
+        epilogue_gelu32(lanes + zcol[l], bias[l], h[l], r, 0, 64);
+        epilogue_gelu32(lanes + zcol[l] + 32, bias[l], h[l], r, 32, 64);
+        tc_sync_for_mma();
+        if (r == 0)
+        {
+            const uint32_t dst = l < 2 ? zcol[l + 1] : ycol;
+            for (int ks = 0; ks < 4; ks++)
+                umma_bf16(t.tmem + dst, desc_kmajor(smem_addr(h[l]) + 256 * ks, 64), desc_kmajor(smem_addr(w[l]) + 256 * ks, 64),
+                          l < 2 ? IDESC_N64 : IDESC_N16, ks > 0);
+            umma_commit(t.mbar);
+        }
+        if (!t.wait()) return false;
+    }
+    return true;
 }
 
-// Forward for the warp's 16 rows whose normalised inputs are x[16][16] (FP32,
-// shared memory, columns >= 12 zero). out[16][3] gets the output (before the
-// output scale). When z is given (training), the pre-activations of the three
-// hidden layers are stored to z[layer][16][64].
-__device__ __forceinline__ void mlp_forward_tile(const MlpSmem& s, const float* x, float* out, float* z)
+// the outputs (before the output scale) of this thread's row
+__device__ __forceinline__ void mlp_tc_outputs(const TcCtx& t, const MlpTcWeights& s, uint32_t ycol, float* y)
 {
-    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    uint32_t a0[1][4];
-    a0[0][0] = pack_bf16(x[g * 16 + 2 * t], x[g * 16 + 2 * t + 1]);
-    a0[0][1] = pack_bf16(x[(g + 8) * 16 + 2 * t], x[(g + 8) * 16 + 2 * t + 1]);
-    a0[0][2] = pack_bf16(x[g * 16 + 2 * t + 8], x[g * 16 + 2 * t + 9]);
-    a0[0][3] = pack_bf16(x[(g + 8) * 16 + 2 * t + 8], x[(g + 8) * 16 + 2 * t + 9]);
-    float acc[8][4];
-    uint32_t a[4][4];
-    auto keep = [&](int layer) {
-        if (!z) return;
-        float* zz = z + layer * 16 * ML_H;
-#pragma unroll
-        for (int j = 0; j < 8; j++)
-        {
-            zz[g * ML_H + 8 * j + 2 * t] = acc[j][0]; zz[g * ML_H + 8 * j + 2 * t + 1] = acc[j][1];
-            zz[(g + 8) * ML_H + 8 * j + 2 * t] = acc[j][2]; zz[(g + 8) * ML_H + 8 * j + 2 * t + 1] = acc[j][3];
-        }
-    };
-    mlp_layer<1, 8>(a0, s.w1, s.b1, acc);
-    keep(0);
-    acc_to_operand<8>(acc, a);
-    mlp_layer<4, 8>(a, s.w2, s.b2, acc);
-    keep(1);
-    acc_to_operand<8>(acc, a);
-    mlp_layer<4, 8>(a, s.w3, s.b3, acc);
-    keep(2);
-    acc_to_operand<8>(acc, a);
-    float o[1][4];
-    mlp_layer<4, 1>(a, s.w4, s.b4, o);
-    if (2 * t < ML_OUT) { out[g * 4 + 2 * t] = o[0][0]; out[(g + 8) * 4 + 2 * t] = o[0][2]; }
-    if (2 * t + 1 < ML_OUT) { out[g * 4 + 2 * t + 1] = o[0][1]; out[(g + 8) * 4 + 2 * t + 1] = o[0][3]; }
+    uint32_t v[16];
+    tc_ld16(tmem_lane_base(t.tmem) + ycol, v);
+    tc_wait_ld();
+    for (int k = 0; k < ML_OUT; k++) y[k] = __uint_as_float(v[k]) + s.b4[k];
+}
+
+// CTA set-up of the inference kernels: weights, mbarrier, 128 tensor-memory columns
+struct __align__(128) MlpTcInferSmem
+{
+    MlpTcWeights w;
+    unsigned char x[ML_ROWS * 16 * 2];
+    unsigned char h[ML_ROWS * 64 * 2];
+    unsigned long long mbar;
+    uint32_t tmemSlot;
+};
+
+__device__ __forceinline__ TcCtx mlp_tc_begin(MlpTcInferSmem& s, uint32_t cols)
+{
+    TcCtx t;
+    if (threadIdx.x == 0) mbar_init(smem_addr(&s.mbar), 1);
+    t.tmem = tmem_alloc(&s.tmemSlot, cols);    // includes a CTA barrier
+    t.mbar = smem_addr(&s.mbar);
+    t.phase = 0;
+    t.ok = true;
+    return t;
 }
 
 // ------------------------------------------------------------- features
@@ -215,42 +273,45 @@ struct MlpArgs
     const float* norm;   // ML_NNORM
 };
 
-// warm start: features -> MLP -> position correction, 128 particles per CTA
-// (4 warps x 2 tiles of 16); pinned particles are left alone
+// warm start: features -> MLP -> position correction, tiles of 128 particles
+// (one per thread), CTAs persistent over the tiles; pinned particles are left
+// alone. A wait that gives up sets ST_TC_TIMEOUT and ends the CTA's work.
 __global__ void __launch_bounds__(128) k_mlp_warm(DevCloth c, Buffers b, MlpArgs ml)
 {
-    __shared__ MlpSmem s;
-    __shared__ float sx[128 * 16];
-    __shared__ float sy[128 * 4];
-    mlp_load_smem(s, ml.prm, ml.norm);
-    __syncthreads();
-    const int i = blockIdx.x * 128 + threadIdx.x;
-    float f[16];
-    if (i < c.N) ml_features(c, b, i, f);
-    else for (int k = 0; k < ML_IN; k++) f[k] = 0.f;
-#pragma unroll
-    for (int k = 0; k < ML_IN; k++) sx[threadIdx.x * 16 + k] = (f[k] - s.mean[k]) * s.istd[k];
-#pragma unroll
-    for (int k = ML_IN; k < 16; k++) sx[threadIdx.x * 16 + k] = 0.f;
-    __syncthreads();
-    const int w = threadIdx.x >> 5;
-    for (int tile = 0; tile < 2; tile++)
+    __shared__ MlpTcInferSmem s;
+    mlp_tc_load(s.w, nullptr, ml.prm, ml.norm);
+    TcCtx t = mlp_tc_begin(s, 128);
+    unsigned char* hs[3] = {s.h, s.h, s.h};
+    const uint32_t zc[3] = {0, 64, 0};
+    const int tiles = (c.N + ML_ROWS - 1) / ML_ROWS;
+    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x)
     {
-        const int row0 = w * 32 + tile * 16;
-        mlp_forward_tile(s, sx + row0 * 16, sy + row0 * 4, nullptr);
-    }
-    __syncthreads();
-    if (i < c.N)
-    {
-        float4 p = c.pos[i];
-        if (p.w > 0.f)
+        const int i = tile * ML_ROWS + (int)threadIdx.x;
+        float f[16];
+        if (i < c.N) ml_features(c, b, i, f);
+#pragma unroll
+        for (int k = 0; k < 16; k++) f[k] = (i < c.N && k < ML_IN) ? (f[k] - s.w.mean[k]) * s.w.istd[k] : 0.f;
+        put_row16(s.x, threadIdx.x, f);
+        if (!mlp_tc_forward(t, s.w, s.x, hs, zc, 64))
         {
-            p.x += sy[threadIdx.x * 4] * s.oscale[0];
-            p.y += sy[threadIdx.x * 4 + 1] * s.oscale[1];
-            p.z += sy[threadIdx.x * 4 + 2] * s.oscale[2];
-            c.pos[i] = p;
+            if (threadIdx.x == 0) atomicOr(c.status, ST_TC_TIMEOUT);
+            break;
+        }
+        float y[ML_OUT];
+        mlp_tc_outputs(t, s.w, 64, y);
+        if (i < c.N)
+        {
+            float4 p = c.pos[i];
+            if (p.w > 0.f)
+            {
+                p.x += y[0] * s.w.oscale[0];
+                p.y += y[1] * s.w.oscale[1];
+                p.z += y[2] * s.w.oscale[2];
+                c.pos[i] = p;
+            }
         }
     }
+    tmem_free(t.tmem, 128);
 }
 
 // the predicted positions, and (sample recording) every particle's raw features
@@ -280,139 +341,278 @@ __global__ void k_mlp_targets(DevCloth c, float* target)
 }
 
 // forward over raw feature rows (S x 12) -> outputs (S x 3, output scale applied)
-__global__ void __launch_bounds__(128) k_mlp_forward(const float* X, int S, MlpArgs ml, float* Y)
+__global__ void __launch_bounds__(128) k_mlp_forward(const float* X, int S, MlpArgs ml, float* Y, int* status)
 {
-    __shared__ MlpSmem s;
-    __shared__ float sx[128 * 16];
-    __shared__ float sy[128 * 4];
-    mlp_load_smem(s, ml.prm, ml.norm);
-    __syncthreads();
-    const int r = blockIdx.x * 128 + threadIdx.x;
+    __shared__ MlpTcInferSmem s;
+    mlp_tc_load(s.w, nullptr, ml.prm, ml.norm);
+    TcCtx t = mlp_tc_begin(s, 128);
+    unsigned char* hs[3] = {s.h, s.h, s.h};
+    const uint32_t zc[3] = {0, 64, 0};
+    const int tiles = (S + ML_ROWS - 1) / ML_ROWS;
+    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x)
+    {
+        const int r = tile * ML_ROWS + (int)threadIdx.x;
+        float f[16];
 #pragma unroll
-    for (int k = 0; k < 16; k++)
-        sx[threadIdx.x * 16 + k] = (r < S && k < ML_IN) ? (X[(size_t)r * ML_IN + k] - s.mean[k]) * s.istd[k] : 0.f;
-    __syncthreads();
-    const int w = threadIdx.x >> 5;
-    for (int tile = 0; tile < 2; tile++)
-        mlp_forward_tile(s, sx + (w * 32 + tile * 16) * 16, sy + (w * 32 + tile * 16) * 4, nullptr);
-    __syncthreads();
-    if (r < S)
-        for (int k = 0; k < ML_OUT; k++) Y[(size_t)r * ML_OUT + k] = sy[threadIdx.x * 4 + k] * s.oscale[k];
+        for (int k = 0; k < 16; k++) f[k] = (r < S && k < ML_IN) ? (X[(size_t)r * ML_IN + k] - s.w.mean[k]) * s.w.istd[k] : 0.f;
+        put_row16(s.x, threadIdx.x, f);
+        if (!mlp_tc_forward(t, s.w, s.x, hs, zc, 64))
+        {
+            if (threadIdx.x == 0 && status) atomicOr(status, 1);
+            break;
+        }
+        float y[ML_OUT];
+        mlp_tc_outputs(t, s.w, 64, y);
+        if (r < S)
+            for (int k = 0; k < ML_OUT; k++) Y[(size_t)r * ML_OUT + k] = y[k] * s.w.oscale[k];
+    }
+    tmem_free(t.tmem, 128);
 }
 
 // ------------------------------------------------------------ training
-// Gradients of the mean squared error between the network's output and
-// target / output scale, for 64 rows per CTA (4 warps x one 16-row tile);
-// accumulated into grad[ML_NPARAM] and loss[0] (both zeroed by the caller).
-constexpr int ML_ROWS = 64;
-struct MlpTrainSmem
+// Sum over a warp of 64 per-lane values: a butterfly in which each step halves
+// the columns a lane keeps, so that lane l ends with the sums of columns 2l and
+// 2l + 1 (62 shuffles instead of 64 x 5).
+__device__ __forceinline__ float2 warp_colsum64(const float (&v)[64])
 {
-    float x[ML_ROWS * 16];
-    float z[ML_ROWS / 16][3 * 16 * ML_H];   // per warp: pre-activations of the 3 hidden layers
-    float y[ML_ROWS * 4];
-    float d0[ML_ROWS * ML_H], d1[ML_ROWS * ML_H];
+    const int lane = threadIdx.x & 31;
+    float a[32];
+    {
+        const bool hi = lane & 16;
+#pragma unroll
+        for (int j = 0; j < 32; j++)
+        {
+            const float keep = hi ? v[j + 32] : v[j], send = hi ? v[j] : v[j + 32];
+            a[j] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+        }
+    }
+    float b16[16];
+    {
+        const bool hi = lane & 8;
+#pragma unroll
+        for (int j = 0; j < 16; j++)
+        {
+            const float keep = hi ? a[j + 16] : a[j], send = hi ? a[j] : a[j + 16];
+            b16[j] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+        }
+    }
+    float c8[8];
+    {
+        const bool hi = lane & 4;
+#pragma unroll
+        for (int j = 0; j < 8; j++)
+        {
+            const float keep = hi ? b16[j + 8] : b16[j], send = hi ? b16[j] : b16[j + 8];
+            c8[j] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+        }
+    }
+    float d4[4];
+    {
+        const bool hi = lane & 2;
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+        {
+            const float keep = hi ? c8[j + 4] : c8[j], send = hi ? c8[j] : c8[j + 4];
+            d4[j] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+        }
+    }
+    float e2[2];
+    {
+        const bool hi = lane & 1;
+#pragma unroll
+        for (int j = 0; j < 2; j++)
+        {
+            const float keep = hi ? d4[j + 2] : d4[j], send = hi ? d4[j] : d4[j + 2];
+            e2[j] = keep + __shfl_xor_sync(0xffffffffu, send, 1);
+        }
+    }
+    return make_float2(e2[0], e2[1]);
+}
+
+// dZ = dH * gelu'(Z + b) for this thread's row: dH and Z (no bias) from tensor
+// memory, dZ as BF16 into columns 0..63 of row r of the 128-column tile d, and
+// its per-column sums over the warp into bsum (lane l: columns 2l, 2l + 1)
+__device__ __forceinline__ void epilogue_dz(uint32_t lanes, uint32_t dhCol, uint32_t zCol, const float* bias,
+                                            unsigned char* d, int r, float2& bsum)
+{
+    float dz[64];
+#pragma unroll
+    for (int half = 0; half < 2; half++)
+    {
+        uint32_t vh[32], vz[32];
+        tc_ld32(lanes + dhCol + 32 * half, vh);
+        tc_ld32(lanes + zCol + 32 * half, vz);
+        tc_wait_ld();
+#pragma unroll
+        for (int j = 0; j < 32; j++)
+            dz[32 * half + j] = __uint_as_float(vh[j]) * gelu_grad(__uint_as_float(vz[j]) + bias[32 * half + j]);
+    }
+#pragma unroll
+    for (int c = 0; c < 8; c++)
+    {
+        uint4 q;
+        q.x = pack_bf16(dz[8 * c], dz[8 * c + 1]); q.y = pack_bf16(dz[8 * c + 2], dz[8 * c + 3]);
+        q.z = pack_bf16(dz[8 * c + 4], dz[8 * c + 5]); q.w = pack_bf16(dz[8 * c + 6], dz[8 * c + 7]);
+        *reinterpret_cast<uint4*>(d + core_off(r, 8 * c, 128)) = q;
+    }
+    const float2 s2 = warp_colsum64(dz);
+    bsum.x += s2.x;
+    bsum.y += s2.y;
+}
+
+// Tensor-memory columns of the training kernel (512 allocated)
+constexpr uint32_t TM_Z1 = 0, TM_Z2 = 64, TM_Z3 = 128, TM_Y = 192, TM_DH = 208;
+constexpr uint32_t TM_DW4 = 272, TM_DW3 = 336, TM_DW2 = 400, TM_DW1 = 464;
+
+struct __align__(128) MlpTcTrainSmem
+{
+    MlpTcWeights w;
+    MlpTcTrans t;
+    unsigned char x[ML_ROWS * 16 * 2];
+    unsigned char h1[ML_ROWS * 64 * 2], h2[ML_ROWS * 64 * 2], h3[ML_ROWS * 64 * 2];
+    // dY / dZ tile, 128 columns: 0..63 in use, 64..127 zero (the padded rows of
+    // the M = 128 weight-gradient products)
+    unsigned char d[ML_ROWS * 128 * 2];
+    unsigned long long mbar;
+    uint32_t tmemSlot;
 };
 
-__global__ void __launch_bounds__(128) k_mlp_grad(const float* X, const float* T, int S, MlpArgs ml, float* grad, float* loss)
+// Gradients of the mean squared error between the network's output and
+// target / output scale (mean over S x 3 elements), accumulated into grad[] and
+// loss[0] (both zeroed by the caller). CTAs are persistent over 128-row tiles;
+// the weight gradients of all their tiles are summed in tensor memory and added
+// to grad[] once per CTA. A wait that gives up sets *status (if given).
+__global__ void __launch_bounds__(128) k_mlp_grad(const float* X, const float* T, int S, MlpArgs ml, float* grad,
+                                                  float* loss, int* status)
 {
-    extern __shared__ __align__(16) unsigned char dyn[];
-    MlpSmem& s = *reinterpret_cast<MlpSmem*>(dyn);
-    MlpTrainSmem& a = *reinterpret_cast<MlpTrainSmem*>(dyn + ((sizeof(MlpSmem) + 15) / 16) * 16);
-    mlp_load_smem(s, ml.prm, ml.norm);
-    const int r0 = blockIdx.x * ML_ROWS;
-    for (int k = threadIdx.x; k < ML_ROWS * 16; k += blockDim.x)
-    {
-        const int r = r0 + k / 16, col = k % 16;
-        a.x[k] = (r < S && col < ML_IN) ? (X[(size_t)r * ML_IN + col] - ml.norm[col]) * ml.norm[ML_IN + col] : 0.f;
-    }
-    __syncthreads();
-    const int w = threadIdx.x >> 5;
-    mlp_forward_tile(s, a.x + w * 16 * 16, a.y + w * 16 * 4, a.z[w]);
-    __syncthreads();
-    // output layer: dL/dy for rows inside the batch (mean over S x 3 elements)
+    extern __shared__ __align__(1024) unsigned char dyn[];
+    MlpTcTrainSmem& s = *reinterpret_cast<MlpTcTrainSmem*>(dyn);
+    mlp_tc_load(s.w, &s.t, ml.prm, ml.norm);
+    for (int k = threadIdx.x; k < ML_ROWS * 128 * 2 / 16; k += blockDim.x)
+        reinterpret_cast<uint4*>(s.d)[k] = make_uint4(0u, 0u, 0u, 0u);
+    TcCtx t;
+    if (threadIdx.x == 0) mbar_init(smem_addr(&s.mbar), 1);
+    t.tmem = tmem_alloc(&s.tmemSlot, 512);
+    t.mbar = smem_addr(&s.mbar);
+    t.phase = 0;
+    const int r = threadIdx.x, lane = r & 31;
+    const uint32_t lanes = tmem_lane_base(t.tmem);
     const float inv = 1.f / (float)(S * ML_OUT);
-    float lsum = 0.f;
-    for (int k = threadIdx.x; k < ML_ROWS * 4; k += blockDim.x)
+    float2 db1 = make_float2(0.f, 0.f), db2 = db1, db3 = db1;
+    float db4[ML_OUT] = {0.f, 0.f, 0.f}, lsum = 0.f;
+    unsigned char* hs[3] = {s.h1, s.h2, s.h3};
+    const uint32_t zc[3] = {TM_Z1, TM_Z2, TM_Z3};
+    const int tiles = (S + ML_ROWS - 1) / ML_ROWS;
+    bool first = true, ok = true;
+    for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x)
     {
-        const int rr = k / 4, col = k % 4, r = r0 + rr;
-        float d = 0.f;
-        if (col < ML_OUT && r < S)
+        const int row = tile * ML_ROWS + r;
+        const bool live = row < S;
+        float f[16];
+#pragma unroll
+        for (int k = 0; k < 16; k++) f[k] = (live && k < ML_IN) ? (X[(size_t)row * ML_IN + k] - s.w.mean[k]) * s.w.istd[k] : 0.f;
+        put_row16(s.x, r, f);
+        if (!(ok = mlp_tc_forward(t, s.w, s.x, hs, zc, TM_Y))) break;
+        // output layer: dL/dy (zero for rows past S) into dY columns 0..2
+        float y[ML_OUT], dy[16];
+        mlp_tc_outputs(t, s.w, TM_Y, y);
+#pragma unroll
+        for (int k = 0; k < 16; k++) dy[k] = 0.f;
+        for (int k = 0; k < ML_OUT; k++)
+            if (live)
+            {
+                const float e = y[k] - T[(size_t)row * ML_OUT + k] / s.w.oscale[k];
+                lsum += e * e * inv;
+                dy[k] = 2.f * e * inv;
+            }
+        for (int k = 0; k < ML_OUT; k++)
         {
-            const float e = a.y[k] - T[(size_t)r * ML_OUT + col] / ml.norm[2 * ML_IN + col];
-            lsum += e * e;
-            d = 2.f * e * inv;
+            float v = dy[k];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            db4[k] += v;
         }
-        a.y[k] = d;
-    }
-    atomicAdd(loss, lsum * inv);
-    __syncthreads();
-    auto zat = [&](int layer, int r, int o) { return a.z[r / 16][layer * 16 * ML_H + (r % 16) * ML_H + o]; };
-    auto hat = [&](int layer, int r, int i) { return gelu(zat(layer, r, i)); };
-    // layer 4: grads, and dH3 = dY W4 (into d0)
-    for (int k = threadIdx.x; k < ML_OUT * ML_H; k += blockDim.x)
-    {
-        const int o = k / ML_H, i = k % ML_H;
-        float gsum = 0.f;
-        for (int r = 0; r < ML_ROWS; r++) gsum += a.y[r * 4 + o] * hat(2, r, i);
-        atomicAdd(&grad[ML_W4 + k], gsum);
-    }
-    if (threadIdx.x < ML_OUT)
-    {
-        float gsum = 0.f;
-        for (int r = 0; r < ML_ROWS; r++) gsum += a.y[r * 4 + threadIdx.x];
-        atomicAdd(&grad[ML_B4 + threadIdx.x], gsum);
-    }
-    for (int k = threadIdx.x; k < ML_ROWS * ML_H; k += blockDim.x)
-    {
-        const int r = k / ML_H, i = k % ML_H;
-        float d = 0.f;
-        for (int o = 0; o < ML_OUT; o++) d += a.y[r * 4 + o] * ml.prm[ML_W4 + o * ML_H + i];
-        a.d0[k] = d * gelu_grad(zat(2, r, i));      // dZ3
-    }
-    __syncthreads();
-    // hidden layers 3, 2: dW = dZ^T H_prev, db = sum dZ, dZ_prev = (dZ W) * gelu'(Z_prev)
-    float* dz = a.d0;
-    float* dn = a.d1;
-    for (int layer = 2; layer >= 1; layer--)
-    {
-        const int wo = layer == 2 ? ML_W3 : ML_W2, bo = layer == 2 ? ML_B3 : ML_B2;
-        for (int k = threadIdx.x; k < ML_H * ML_H; k += blockDim.x)
         {
-            const int o = k / ML_H, i = k % ML_H;
-            float gsum = 0.f;
-            for (int r = 0; r < ML_ROWS; r++) gsum += dz[r * ML_H + o] * hat(layer - 1, r, i);
-            atomicAdd(&grad[wo + k], gsum);
+            uint4 q0, q1;
+            q0.x = pack_bf16(dy[0], dy[1]); q0.y = pack_bf16(dy[2], 0.f); q0.z = 0u; q0.w = 0u;
+            q1 = make_uint4(0u, 0u, 0u, 0u);
+            *reinterpret_cast<uint4*>(s.d + core_off(r, 0, 128)) = q0;
+            for (int c = 1; c < 8; c++) *reinterpret_cast<uint4*>(s.d + core_off(r, 8 * c, 128)) = q1;
         }
-        if (threadIdx.x < ML_H)
+        // dH3 = dY W4 (K = 16) and dW4 += dY^T H3 (sum over the tile's rows)
+        tc_sync_for_mma();
+        if (r == 0)
         {
-            float gsum = 0.f;
-            for (int r = 0; r < ML_ROWS; r++) gsum += dz[r * ML_H + threadIdx.x];
-            atomicAdd(&grad[bo + threadIdx.x], gsum);
+            umma_bf16(t.tmem + TM_DH, desc_kmajor(smem_addr(s.d), 128), desc_kmajor(smem_addr(s.t.w4t), 16), IDESC_N64, 0);
+            for (int ks = 0; ks < ML_ROWS / 16; ks++)
+                umma_bf16(t.tmem + TM_DW4, desc_mnmajor(smem_addr(s.d) + ks * 2 * 2048, 128),
+                          desc_mnmajor(smem_addr(s.h3) + ks * 2 * 1024, 64), IDESC_GRAD_N64, (!first || ks > 0) ? 1u : 0u);
+            umma_commit(t.mbar);
         }
-        for (int k = threadIdx.x; k < ML_ROWS * ML_H; k += blockDim.x)
+        if (!(ok = t.wait())) break;
+        // hidden layers 3, 2, 1: dZ, then dH of the layer below and dW += dZ^T H
+        const float* bias[3] = {s.w.b1, s.w.b2, s.w.b3};
+        float2* dbs[3] = {&db1, &db2, &db3};
+        const unsigned char* wt[3] = {nullptr, s.t.w2t, s.t.w3t};
+        const uint32_t dwc[3] = {TM_DW1, TM_DW2, TM_DW3};
+        for (int l = 2; l >= 0 && ok; l--)
         {
-            const int r = k / ML_H, i = k % ML_H;
-            float d = 0.f;
-            for (int o = 0; o < ML_H; o++) d += dz[r * ML_H + o] * ml.prm[wo + o * ML_H + i];
-            dn[k] = d * gelu_grad(zat(layer - 1, r, i));
+            epilogue_dz(lanes, TM_DH, zc[l], bias[l], s.d, r, *dbs[l]);
+            tc_sync_for_mma();
+            if (r == 0)
+            {
+                if (l > 0)
+                    for (int ks = 0; ks < 4; ks++)
+                        umma_bf16(t.tmem + TM_DH, desc_kmajor(smem_addr(s.d) + 256 * ks, 128),
+                                  desc_kmajor(smem_addr(wt[l]) + 256 * ks, 64), IDESC_N64, ks > 0);
+                const unsigned char* hb = l > 0 ? hs[l - 1] : s.x;
+                const int hk = l > 0 ? 64 : 16;
+                for (int ks = 0; ks < ML_ROWS / 16; ks++)
+                    umma_bf16(t.tmem + dwc[l], desc_mnmajor(smem_addr(s.d) + ks * 2 * 2048, 128),
+                              desc_mnmajor(smem_addr(hb) + ks * 2 * hk * 16, hk), l > 0 ? IDESC_GRAD_N64 : IDESC_GRAD_N16,
+                              (!first || ks > 0) ? 1u : 0u);
+                umma_commit(t.mbar);
+            }
+            ok = t.wait();
         }
-        __syncthreads();
-        float* tmp = dz; dz = dn; dn = tmp;
+        first = false;
     }
-    // layer 1: dW1 = dZ1^T X, db1
-    for (int k = threadIdx.x; k < ML_H * ML_IN; k += blockDim.x)
+    if (!ok && threadIdx.x == 0 && status) atomicOr(status, 1);
+    // this CTA's sums: weight gradients (rows 0..63 = output units: warps 0, 1),
+    // bias gradients (lane l of each warp: units 2l, 2l + 1), loss
+    if (ok && !first)
     {
-        const int o = k / ML_IN, i = k % ML_IN;
-        float gsum = 0.f;
-        for (int r = 0; r < ML_ROWS; r++) gsum += dz[r * ML_H + o] * a.x[r * 16 + i];
-        atomicAdd(&grad[ML_W1 + k], gsum);
+        // tensor-memory loads are warp-collective: every warp loads, the warps
+        // holding rows 0..63 (output units) add them
+        const bool mine = r < 64;
+        uint32_t v[32];
+        for (int half = 0; half < 2; half++)
+        {
+            tc_ld32(lanes + TM_DW3 + 32 * half, v);
+            tc_wait_ld();
+            if (mine) for (int j = 0; j < 32; j++) atomicAdd(&grad[ML_W3 + r * ML_H + 32 * half + j], __uint_as_float(v[j]));
+            tc_ld32(lanes + TM_DW2 + 32 * half, v);
+            tc_wait_ld();
+            if (mine) for (int j = 0; j < 32; j++) atomicAdd(&grad[ML_W2 + r * ML_H + 32 * half + j], __uint_as_float(v[j]));
+            tc_ld32(lanes + TM_DW4 + 32 * half, v);
+            tc_wait_ld();
+            if (r < ML_OUT) for (int j = 0; j < 32; j++) atomicAdd(&grad[ML_W4 + r * ML_H + 32 * half + j], __uint_as_float(v[j]));
+        }
+        uint32_t v16[16];
+        tc_ld16(lanes + TM_DW1, v16);
+        tc_wait_ld();
+        if (mine) for (int j = 0; j < ML_IN; j++) atomicAdd(&grad[ML_W1 + r * ML_IN + j], __uint_as_float(v16[j]));
     }
-    if (threadIdx.x < ML_H)
+    if (ok && !first)
     {
-        float gsum = 0.f;
-        for (int r = 0; r < ML_ROWS; r++) gsum += dz[r * ML_H + threadIdx.x];
-        atomicAdd(&grad[ML_B1 + threadIdx.x], gsum);
+        atomicAdd(&grad[ML_B1 + 2 * lane], db1.x); atomicAdd(&grad[ML_B1 + 2 * lane + 1], db1.y);
+        atomicAdd(&grad[ML_B2 + 2 * lane], db2.x); atomicAdd(&grad[ML_B2 + 2 * lane + 1], db2.y);
+        atomicAdd(&grad[ML_B3 + 2 * lane], db3.x); atomicAdd(&grad[ML_B3 + 2 * lane + 1], db3.y);
+        if (lane == 0)
+            for (int k = 0; k < ML_OUT; k++) atomicAdd(&grad[ML_B4 + k], db4[k]);
+        for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+        if (lane == 0) atomicAdd(loss, lsum);
     }
+    tmem_free(t.tmem, 512);
 }
 
 // Adam (Kingma & Ba 2015) on the FP32 master weights; m and v follow the parameters

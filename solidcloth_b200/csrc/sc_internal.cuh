@@ -26,7 +26,7 @@ enum StatusBits {
     ST_COLOUR_OVERFLOW = 16,     // contact colouring needed more rounds than supported
     ST_MESH_STACK_OVERFLOW = 32,
     ST_BVH_STACK_OVERFLOW = 64,
-    ST_SYNC_TIMEOUT = 128,       // a neighbour wait of the tiled solver gave up (bounded spin)
+    ST_TC_TIMEOUT = 128,         // a tensor-core completion wait of the warm-start network gave up
 };
 
 struct SolverParams
@@ -76,6 +76,12 @@ struct DevCloth
     float4* meshN;              // render mesh normals
     float4* meshTriN;
     float4* triAngles;          // scratch: per-triangle angle weights
+    // static colours of the cloth's triangles and edges (proper colourings: one
+    // colour's triangles / edges share no particle); triangle and edge collider
+    // contacts take their triangle's / edge's colour, so they need no colouring pass
+    const uint8_t* triColour;   // T
+    const uint8_t* edgeColour;  // E
+    int nTriColours, nEdgeColours;
     float* scal;                // [0] max |pos - prev| (as float bits), [1..7] GS errors, [8] done flag
     int* status;
 };

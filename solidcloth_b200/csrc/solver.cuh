@@ -169,11 +169,30 @@ __global__ void __launch_bounds__(256) k_bends(DevCloth c, SolverParams P, int f
 }
 
 // --------------------------------------------------------- contact solves
+// Data that no solver kernel writes (the collider meshes, the contact slots'
+// collider ranges and counts, the colour orders, the start-of-substep
+// positions) is read through the non-coherent path, so that it stays in L1
+// across the colour phases and iterations: in a contact phase only the contact
+// record and the particles then pay the L2 latency.
+__device__ __forceinline__ V3 ldg3(const float4* p, uint32_t i) { const float4 a = __ldg(&p[i]); return mk(a.x, a.y, a.z); }
+template <typename T>
+__device__ __forceinline__ const T* ldg_ptr(const T* const* p)
+{
+    return reinterpret_cast<const T*>(__ldg(reinterpret_cast<const unsigned long long*>(p)));
+}
+// the fields of collider mesh k the contact solves read
+struct MeshView { const float4* v; const float4* n; const uint32_t* tri; const int4* edge; };
+__device__ __forceinline__ MeshView mesh_view(const Buffers& b, int k)
+{
+    const DevMesh* m = b.meshes + k;
+    return MeshView{ldg_ptr(&m->v), ldg_ptr(&m->n), ldg_ptr(&m->tri), ldg_ptr(&m->edge)};
+}
+
 // ComputeTriangleNormal(mesh, tri, coords, false): vertex normals blended by the
 // barycentric coordinates (Geometry/ClosestPointOnMesh.cpp:37-60).
-__device__ __forceinline__ V3 blended_normal(const DevMesh& m, int t, V3 w)
+__device__ __forceinline__ V3 blended_normal(const MeshView& m, int t, V3 w)
 {
-    V3 n0 = ld3(m.n, m.tri[3 * t]), n1 = ld3(m.n, m.tri[3 * t + 1]), n2 = ld3(m.n, m.tri[3 * t + 2]);
+    V3 n0 = ldg3(m.n, __ldg(&m.tri[3 * t])), n1 = ldg3(m.n, __ldg(&m.tri[3 * t + 1])), n2 = ldg3(m.n, __ldg(&m.tri[3 * t + 2]));
     return normalized(w.x * n0 + w.y * n1 + w.z * n2);
 }
 
@@ -187,13 +206,13 @@ __device__ __forceinline__ float vertex_contacts_one(const PA& pa, const DevClot
     float err = 0.f;
     float4 p4 = pa.ld(i);
     V3 p = mk(p4.x, p4.y, p4.z);
-    const V3 q = ld3(c.prev, i);
+    const V3 q = ldg3(c.prev, i);
     bool touched = false;
     const int2 cr = colliders_of(c, b, i);
     for (int ci = cr.x; ci < cr.x + cr.y; ci++)
     {
         const VColl& g = b.vcoll[ci];
-        const int n = b.vcCount[(size_t)g.countBase + (i - g.vBegin)];
+        const int n = __ldg(&b.vcCount[(size_t)__ldg(&g.countBase) + (i - __ldg(&g.vBegin))]);
         VC* slot = b.vc + g.slotBase + (size_t)(i - g.vBegin) * g.kmax;
         for (int k = 0; k < n; k++)
         {
@@ -201,10 +220,11 @@ __device__ __forceinline__ float vertex_contacts_one(const PA& pa, const DevClot
             V3 point = mk(v.point.x, v.point.y, v.point.z), normal = mk(v.normal.x, v.normal.y, v.normal.z);
             if (v.mesh >= 0)
             {
-                const DevMesh& m = b.meshes[v.mesh];
+                const MeshView m = mesh_view(b, v.mesh);
                 int t = v.feature;
                 V3 coords, cp;
-                closest_point_triangle(p, ld3(m.v, m.tri[3 * t]), ld3(m.v, m.tri[3 * t + 1]), ld3(m.v, m.tri[3 * t + 2]), cp, coords);
+                closest_point_triangle(p, ldg3(m.v, __ldg(&m.tri[3 * t])), ldg3(m.v, __ldg(&m.tri[3 * t + 1])),
+                                       ldg3(m.v, __ldg(&m.tri[3 * t + 2])), cp, coords);
                 point = cp;
                 normal = blended_normal(m, t, coords);
                 v.point = f4(point, 0.f); v.normal = f4(normal, 0.f);
@@ -265,10 +285,10 @@ __device__ float solve_edge_contact(const PA& pa, const DevCloth& c, const Solve
     V3 p = w1 * x1 + w2 * x2;
     if (k.mesh >= 0)
     {
-        const DevMesh& m = b.meshes[k.mesh];
-        int4 ed = m.edge[k.feature];
+        const MeshView m = mesh_view(b, k.mesh);
+        const int4 ed = __ldg(&m.edge[k.feature]);
         float s1, t;
-        closest_segm_segm(ld3(m.v, ed.x), ld3(m.v, ed.y), x1, x2, s1, t, point, p);
+        closest_segm_segm(ldg3(m.v, ed.x), ldg3(m.v, ed.y), x1, x2, s1, t, point, p);
         w1 = 1.0f - t; w2 = t;
         k.point = f4(point, 0.f);
     }
@@ -283,7 +303,7 @@ __device__ float solve_edge_contact(const PA& pa, const DevCloth& c, const Solve
     V3 disp = dLambda * normal;
     if (P.friction != 0)
     {
-        V3 p0 = w1 * ld3(c.prev, k.idx.x) + w2 * ld3(c.prev, k.idx.y);
+        V3 p0 = w1 * ldg3(c.prev, k.idx.x) + w2 * ldg3(c.prev, k.idx.y);
         V3 v12 = p - p0 - mk(0.f, 0.f, 0.f);
         float vnrel = dot(normal, v12);
         V3 vt = v12 - vnrel * normal;
@@ -322,7 +342,7 @@ __device__ float solve_tri_contact(const PA& pa, const DevCloth& c, const Solver
     V3 normal = n;
     if (k.mesh >= 0 && k.feature >= 0)
     {
-        V3 mnrm = ld3(b.meshes[k.mesh].n, k.feature);
+        V3 mnrm = ldg3(mesh_view(b, k.mesh).n, k.feature);
         if (dot(n, mnrm) < 0) normal = -n;
     }
     k.normal = f4(normal, 0.f);
@@ -336,7 +356,7 @@ __device__ float solve_tri_contact(const PA& pa, const DevCloth& c, const Solver
     V3 disp = dLambda * normal;
     if (P.friction != 0)
     {
-        V3 p0 = w1 * ld3(c.prev, k.idx.x) + w2 * ld3(c.prev, k.idx.y) + w3 * ld3(c.prev, k.idx.z);
+        V3 p0 = w1 * ldg3(c.prev, k.idx.x) + w2 * ldg3(c.prev, k.idx.y) + w3 * ldg3(c.prev, k.idx.z);
         V3 v12 = p - p0 - mk(0.f, 0.f, 0.f);
         float vnrel = dot(normal, v12);
         V3 vt = v12 - vnrel * normal;
@@ -632,7 +652,7 @@ __global__ void __launch_bounds__(GS_THREADS) k_gs_cluster(DevCloth c, SolverPar
                 range(plan.linkStart[col], plan.linkStart[col + 1], a, e);
                 for (int j = a + threadIdx.x; j < e; j += blockDim.x)
                 {
-                    const float err = link_project(pa, c.link[j], P);
+                    const float err = link_project(pa, __ldg(&c.link[j]), P);
                     if (track && err > 0.f) atomicMax((int*)&sErr[1], __float_as_int(err));
                 }
                 cl.sync();
@@ -687,7 +707,7 @@ __global__ void __launch_bounds__(GS_THREADS) k_gs_cluster(DevCloth c, SolverPar
                     range(s0, s1, a, e);
                     for (int j = a + threadIdx.x; j < e; j += blockDim.x)
                     {
-                        float err = solve_contact(pa, c, P, b, cls, cv.order[j]);
+                        float err = solve_contact(pa, c, P, b, cls, __ldg(&cv.order[j]));
                         if (track && err > 0.f) atomicMax((int*)&sErr[4 + cls], __float_as_int(err));
                     }
                 }
@@ -784,6 +804,10 @@ struct RegPos
     }
 };
 
+// Constraint records are constant for the whole launch: they are read through the
+// non-coherent path (ld.global.nc), which keeps them in the SM's L1 from one
+// iteration to the next (each thread sweeps the same records every iteration),
+// so only the particle loads pay the L2 latency in a colour phase.
 template <int TILE>
 __device__ __forceinline__ void fem_tiles(const DevCloth& c, const SolverParams& P, const float4* fem, int s0, int s1,
                                           int tid, int nth)
@@ -796,7 +820,7 @@ __device__ __forceinline__ void fem_tiles(const DevCloth& c, const SolverParams&
         for (int u = 0; u < TILE; u++)
         {
             const int j = min(base + u, s1 - 1);
-            r0[u] = fem[3 * j]; r1[u] = fem[3 * j + 1]; r2[u] = fem[3 * j + 2];
+            r0[u] = __ldg(&fem[3 * j]); r1[u] = __ldg(&fem[3 * j + 1]); r2[u] = __ldg(&fem[3 * j + 2]);
         }
 #pragma unroll
         for (int u = 0; u < TILE; u++)
@@ -827,7 +851,7 @@ __device__ __forceinline__ float bend_tiles(const DevCloth& c, const SolverParam
         uint4 bc[TILE];
         RegPos rp[TILE];
 #pragma unroll
-        for (int u = 0; u < TILE; u++) bc[u] = bend[min(base + u, s1 - 1)];
+        for (int u = 0; u < TILE; u++) bc[u] = __ldg(&bend[min(base + u, s1 - 1)]);
 #pragma unroll
         for (int u = 0; u < TILE; u++)
         {
@@ -884,7 +908,7 @@ __global__ void __launch_bounds__(NT) k_gs_grid(DevCloth c, SolverParams P, Buff
             {
                 for (int j = plan.linkStart[col] + tid; j < plan.linkStart[col + 1]; j += nth)
                 {
-                    const float err = link_project(pa, c.link[j], P);
+                    const float err = link_project(pa, __ldg(&c.link[j]), P);
                     if (track && err > 0.f) atomicMax((int*)&sErr[1], __float_as_int(err));
                 }
                 grid.sync();
@@ -928,7 +952,7 @@ __global__ void __launch_bounds__(NT) k_gs_grid(DevCloth c, SolverParams P, Buff
                 else
                     for (int j = s0 + tid; j < s1; j += nth)
                     {
-                        const float e = solve_contact(pa, c, P, b, cls, cv.order[j]);
+                        const float e = solve_contact(pa, c, P, b, cls, __ldg(&cv.order[j]));
                         if (track && e > 0.f) atomicMax((int*)&sErr[4 + cls], __float_as_int(e));
                     }
                 grid.sync();
@@ -993,7 +1017,6 @@ __global__ void __launch_bounds__(NT) k_gs_grid(DevCloth c, SolverParams P, Buff
 
 // variants the tuner chooses among: (threads per CTA, FEM tile, bend tile)
 using GridKernel = void (*)(DevCloth, SolverParams, Buffers, ColourArgs, GsPlan);
-using GridKernelT = void (*)(DevCloth, SolverParams, Buffers, ColourArgs, GsPlan, TilePlan);
 static const GridKernel kGridVariants[] = {
     k_gs_grid<256, 1, 1>, k_gs_grid<256, 2, 1>, k_gs_grid<256, 2, 2>, k_gs_grid<256, 4, 2>,
     k_gs_grid<512, 1, 1>, k_gs_grid<512, 2, 1>, k_gs_grid<512, 2, 2>, k_gs_grid<512, 4, 2>,
@@ -1038,231 +1061,6 @@ bool launch_gs_grid(cudaStream_t s, const DevCloth& c, const SolverParams& P, co
     at.val.cooperative = 1;
     cfg.attrs = &at; cfg.numAttrs = 1;
     return cudaLaunchKernelEx(&cfg, kGridVariants[variant], c, P, b, colour_args(b), plan) == cudaSuccess;
-}
-
-// ------------------------------------------------ tiled grid-resident solver
-// The grid-resident solver with spatial ownership: CTA t owns tile t of a
-// TilePlan (its particles and the constraints whose first particle it owns) and
-// sweeps only its own constraints of each colour; between colour phases it
-// publishes its progress and waits for its neighbour tiles' (the tiles whose
-// constraints share a particle with its own) instead of a grid-wide barrier.
-// Every CTA takes the same phase sequence. Two tiles run one colour's
-// constraints concurrently only when those share no particle (a colour), and a
-// tile starts phase k+1 only after every tile it shares a particle with has
-// finished phase k, so the result equals the grid solver's bit for bit. The
-// multi-particle contacts (any particles) and the exit / residual tests keep
-// grid-wide barriers. Waits are bounded (SYNC_SPIN_LIMIT polls): a wait that
-// gives up sets ST_SYNC_TIMEOUT and the CTA stops waiting from then on.
-template <int NT, int FT, int BT>
-__global__ void __launch_bounds__(NT) k_gs_tiled(DevCloth c, SolverParams P, Buffers b, ColourArgs ca, GsPlan plan,
-                                                 TilePlan tp)
-{
-    cg::grid_group grid = cg::this_grid();
-    __shared__ float sErr[8];
-    __shared__ int sGaveUp;
-    const int tile = blockIdx.x, T = tp.tiles;
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
-    const GlobalPos pa{c.pos};
-    const bool track = !P.fixedIterations;
-    const int nb0 = tp.nbrStart[tile], nb1 = tp.nbrStart[tile + 1];
-    const int q0 = tp.tileStart[tile], q1 = tp.tileStart[tile + 1];
-    unsigned phase = 0;
-    if (threadIdx.x < 8) sErr[threadIdx.x] = 0.f;
-    if (threadIdx.x == 0) sGaveUp = 0;
-    // end of a colour phase: publish it, then wait until every neighbour tile has
-    // finished it too
-    auto neighbour_sync = [&]() {
-        __syncthreads();
-        phase++;
-        if (threadIdx.x == 0)
-        {
-            __threadfence();
-            st_release_gpu(&tp.flags[tile], phase);
-        }
-        if (!sGaveUp)
-            for (int k = nb0 + (int)threadIdx.x; k < nb1; k += NT)
-            {
-                const unsigned* f = &tp.flags[tp.nbr[k]];
-                int spins = 0;
-                while (ld_acquire_gpu(f) < phase)
-                    if (++spins > SYNC_SPIN_LIMIT)
-                    {
-                        atomicOr(c.status, ST_SYNC_TIMEOUT);
-                        sGaveUp = 1;
-                        break;
-                    }
-            }
-        __threadfence();
-        __syncthreads();
-    };
-    if (P.resTol > 0.f)
-    {
-        for (int k = q0 + (int)threadIdx.x; k < q1; k += NT) { const int g = tp.ptcl[k]; c.xsnap[g] = c.pos[g]; }
-        grid.sync();
-    }
-    for (int k = 0; k < plan.iterations; k++)
-    {
-        if (P.fem)
-            for (int col = 0; col < plan.nFemCol; col++)
-            {
-                const int r = col * T + tile;
-                fem_tiles<FT>(c, P, tp.fem, tp.femStart[r], tp.femStart[r + 1], (int)threadIdx.x, NT);
-                neighbour_sync();
-            }
-        else
-            for (int col = 0; col < plan.nLinkCol; col++)
-            {
-                const int r = col * T + tile;
-                for (int j = tp.linkStart[r] + (int)threadIdx.x; j < tp.linkStart[r + 1]; j += NT)
-                {
-                    const float err = link_project(pa, tp.link[j], P);
-                    if (track && err > 0.f) atomicMax((int*)&sErr[1], __float_as_int(err));
-                }
-                neighbour_sync();
-            }
-        if (P.dihedral && k % P.bendFreq == 0)
-            for (int col = 0; col < plan.nBendCol; col++)
-            {
-                const int r = col * T + tile;
-                const float e = bend_tiles<BT>(c, P, tp.bend, tp.bendStart[r], tp.bendStart[r + 1], (int)threadIdx.x, NT);
-                if (track && e > 0.f) atomicMax((int*)&sErr[2], __float_as_int(e));
-                neighbour_sync();
-            }
-        if (b.numVColl > 0)
-        {
-            for (int q = q0 + (int)threadIdx.x; q < q1; q += NT)
-            {
-                const float e = vertex_contacts_one(pa, c, P, b, tp.ptcl[q]);
-                if (track && e > 0.f) atomicMax((int*)&sErr[3], __float_as_int(e));
-            }
-            neighbour_sync();
-        }
-        bool multi = false;
-        for (int cls = 0; cls < 4; cls++) multi |= *ca.cls[cls].count > 0;
-        if (multi)
-        {
-            grid.sync();         // the contacts may join any particles
-            for (int cls = 0; cls < 4; cls++)
-            {
-                const ClassView& cv = ca.cls[cls];
-                const int n = *cv.count;
-                if (n == 0) continue;
-                for (int col = 0; col < MAX_COLOURS; col++)
-                {
-                    const int s0 = cv.start[col], s1 = cv.start[col + 1];
-                    if (s0 == s1) continue;
-                    if (col == MAX_COLOURS - 1)
-                    {
-                        if (tid == 0)
-                            for (int i = 0; i < n; i++)
-                                if (cv.colour[i] == MAX_COLOURS - 1)
-                                {
-                                    const float e = solve_contact(pa, c, P, b, cls, i);
-                                    if (track && e > 0.f) atomicMax((int*)&sErr[4 + cls], __float_as_int(e));
-                                }
-                    }
-                    else
-                        for (int j = s0 + tid; j < s1; j += nth)
-                        {
-                            const float e = solve_contact(pa, c, P, b, cls, cv.order[j]);
-                            if (track && e > 0.f) atomicMax((int*)&sErr[4 + cls], __float_as_int(e));
-                        }
-                    grid.sync();
-                }
-            }
-        }
-        if (tid == 0) c.scal[9] = (float)(k + 1);
-        if (P.resTol > 0.f)
-        {
-            float r = 0.f;
-            for (int q = q0 + (int)threadIdx.x; q < q1; q += NT)
-            {
-                const int g = tp.ptcl[q];
-                const float4 x = c.pos[g], x0 = c.xsnap[g];
-                const float dx = x.x - x0.x, dy = x.y - x0.y, dz = x.z - x0.z;
-                r = fmaxf(r, sqrtf(dx * dx + dy * dy + dz * dz) * P.resScale);
-                c.xsnap[g] = x;
-            }
-            const unsigned u = __reduce_max_sync(0xffffffffu, __float_as_uint(r));
-            unsigned* word = reinterpret_cast<unsigned*>(c.scal + 11);
-            if ((threadIdx.x & 31) == 0 && u) atomicMax(word, u);
-            grid.sync();
-            const float res = __uint_as_float(__ldcg(word));
-            grid.sync();
-            if (tid == 0) *word = 0u;
-            if (res <= P.resTol) break;
-        }
-        if (track)
-        {
-            __syncthreads();
-            if (threadIdx.x < 8 && threadIdx.x >= 1 && sErr[threadIdx.x] > 0.f)
-                atomic_max_pos(&c.scal[threadIdx.x], sErr[threadIdx.x]);
-            grid.sync();
-            if (tid == 0)
-            {
-                const float eps = 0.01f;
-                float cb = c.scal[2], cv = c.scal[3], ce = c.scal[4], ct = c.scal[5], sct = c.scal[6], see = c.scal[7];
-                const float clk = P.fem ? 0.f : c.scal[1];
-                if (clk < 0.05f && cb < 0.005f && see < P.selfThreshold && sct < P.selfThreshold && cv < eps && ce < eps && ct < eps)
-                    c.scal[8] = 1.f;
-                c.scal[1] = 0.f;
-                for (int s2 = 3; s2 < 8; s2++) c.scal[s2] = 0.f;
-                if ((k + 1) % P.bendFreq == 0) c.scal[2] = 0.f;
-            }
-            if (threadIdx.x < 8) sErr[threadIdx.x] = 0.f;
-            grid.sync();
-            if (__ldcg(&c.scal[8]) != 0.f) break;
-        }
-    }
-    if (tid == 0) c.scal[10] += c.scal[9];
-    // velocity update of the tile's own particles (ClothPBD.cpp:314-321), after
-    // the neighbours' last phase (the last sync above covers it)
-    for (int q = q0 + (int)threadIdx.x; q < q1; q += NT)
-    {
-        const int g = tp.ptcl[q];
-        const float4 p = c.pos[g];
-        if (p.w == 0.f) continue;
-        const float4 q4 = c.prev[g];
-        V3 vel = P.invH * (mk(p.x, p.y, p.z) - mk(q4.x, q4.y, q4.z));
-        c.vel[g] = make_float4(vel.x, vel.y, vel.z, 0.f);
-    }
-}
-
-// tiled variants share the grid variants' (threads, FEM tile, bend tile) table
-static const GridKernelT kTiledVariants[] = {
-    k_gs_tiled<256, 1, 1>, k_gs_tiled<256, 2, 1>, k_gs_tiled<256, 2, 2>, k_gs_tiled<256, 4, 2>,
-    k_gs_tiled<512, 1, 1>, k_gs_tiled<512, 2, 1>, k_gs_tiled<512, 2, 2>, k_gs_tiled<512, 4, 2>,
-};
-
-int gs_tiled_max_blocks_per_sm(int v)
-{
-    int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kTiledVariants[v], kGridThreads[v], 0) != cudaSuccess) n = 0;
-    cudaGetLastError();
-    return n;
-}
-
-// one CTA per tile; false if the tiles cannot all be resident
-bool launch_gs_tiled(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b, GsPlan plan,
-                     const TilePlan& tp, int variant)
-{
-    int dev = 0, sms = 0, coop = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
-    const int maxB = gs_tiled_max_blocks_per_sm(variant);
-    if (!coop || maxB < 1 || tp.tiles < 1 || tp.tiles > maxB * sms) return false;
-    if (cudaMemsetAsync(tp.flags, 0, sizeof(unsigned) * (size_t)tp.tiles, s) != cudaSuccess) return false;
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(tp.tiles);
-    cfg.blockDim = dim3(kGridThreads[variant]);
-    cfg.dynamicSmemBytes = 0;
-    cfg.stream = s;
-    cudaLaunchAttribute at;
-    at.id = cudaLaunchAttributeCooperative;
-    at.val.cooperative = 1;
-    cfg.attrs = &at; cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, kTiledVariants[variant], c, P, b, colour_args(b), plan, tp) == cudaSuccess;
 }
 
 int gs_cluster_size(int N, int& shift, size_t& smem)
@@ -1349,5 +1147,4 @@ void launch_solve_multi_contacts(cudaStream_t s, const DevCloth& c, const Solver
 // this build's entry points
 static const SolverOps kSolverOps = {launch_fem, launch_links, launch_reset_link_error, launch_bends,
                                      launch_solve_vertex_contacts, launch_solve_multi_contacts, gs_cluster_size,
-                                     launch_gs_cluster, gs_grid_max_blocks_per_sm, launch_gs_grid,
-                                     gs_tiled_max_blocks_per_sm, launch_gs_tiled};
+                                     launch_gs_cluster, gs_grid_max_blocks_per_sm, launch_gs_grid};

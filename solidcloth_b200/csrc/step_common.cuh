@@ -60,17 +60,4 @@ static inline ColourArgs colour_args(const Buffers& b)
     return a;
 }
 
-// gpu-scope release store / acquire load of a progress word (neighbour sync of
-// the tiled solver)
-__device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v)
-{
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
-}
-__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p)
-{
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
 } // namespace sc

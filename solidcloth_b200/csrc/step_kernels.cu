@@ -17,6 +17,7 @@
 #include <cuda/atomic>
 #include <cstdio>
 #include <climits>
+#include <algorithm>
 
 namespace cg = cooperative_groups;
 
@@ -484,7 +485,7 @@ __global__ void k_tri_colliders(DevCloth c, SolverParams P, Buffers b, VColl g, 
     float tv3 = len(ld3(c.prev, i3) - ld3(c.pos, i3));
     float tvm = mx(tv1, mx(tv2, tv3));
     TC rec;
-    rec.idx = make_uint4(i1, i2, i3, 0);
+    rec.idx = make_uint4(i1, i2, i3, (uint32_t)t | ((uint32_t)min(slotColl, 255) << 24));   // .w: triangle, collider slot
     rec.lam = make_float2(0.f, 0.f);
     if (g.type == 4)
     {
@@ -535,7 +536,7 @@ __global__ void k_edge_colliders(DevCloth c, SolverParams P, Buffers b, VColl g,
     b.ecFlag[slot] = 0;
     V3 p = ld3(c.prev, ed.x), q = ld3(c.prev, ed.y);
     EC rec;
-    rec.idx = make_uint4(ed.x, ed.y, 0, 0);
+    rec.idx = make_uint4(ed.x, ed.y, (uint32_t)e, (uint32_t)slotColl);   // .z: edge, .w: collider slot
     rec.lam = make_float2(0.f, 0.f);
     if (g.type == 4)
     {
@@ -608,10 +609,10 @@ __device__ __forceinline__ unsigned long long contact_key(const DevCloth& c, con
     return ((unsigned long long)h << 32) | (uint32_t)i;
 }
 
+__device__ void place_by_colour(const ClassView& cv, int n);
+
 __device__ void colour_class(const DevCloth& c, const Buffers& b, const ClassView& cv, int* status)
 {
-    __shared__ int sHist[MAX_COLOURS + 1];
-    __shared__ int sCursor[MAX_COLOURS + 1];
     __shared__ int sRemaining;
     const int n = *cv.count;
     for (int i = threadIdx.x; i < n; i += blockDim.x) cv.colour[i] = -1;
@@ -662,7 +663,41 @@ __device__ void colour_class(const DevCloth& c, const Buffers& b, const ClassVie
         // last colour, which the solver runs on a single thread in list order
         if (threadIdx.x == 0) atomicOr(status, ST_COLOUR_OVERFLOW);
     }
-    // histogram + exclusive scan + placement
+    place_by_colour(cv, n);
+}
+
+// Triangle (class 1) and edge (class 0) collider contacts: the static colour of
+// their cloth triangle / edge, offset by nColours per collider slot (two
+// colliders can both touch one triangle); the last colour (MAX_COLOURS - 1) is
+// the serial bucket. Contacts of one colour share no particle.
+__device__ void static_colour_class(const DevCloth& c, const Buffers& b, const ClassView& cv)
+{
+    const int n = *cv.count;
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+    {
+        int col;
+        if (cv.kind == 1)
+        {
+            const uint32_t w = b.tcList[i].idx.w;
+            col = c.triColour[w & 0xffffffu] + c.nTriColours * (int)(w >> 24);
+        }
+        else
+        {
+            const uint4 x = b.ecList[i].idx;
+            col = c.edgeColour[x.z] + c.nEdgeColours * (int)x.w;
+        }
+        cv.colour[i] = min(col, MAX_COLOURS - 1);
+    }
+    __syncthreads();
+    place_by_colour(cv, n);
+}
+
+// histogram of the colours + exclusive scan + placement: order[] lists each
+// colour's contacts contiguously, start[] gives the colour ranges
+__device__ void place_by_colour(const ClassView& cv, int n)
+{
+    __shared__ int sHist[MAX_COLOURS + 1];
+    __shared__ int sCursor[MAX_COLOURS + 1];
     for (int k = threadIdx.x; k <= MAX_COLOURS; k += blockDim.x) sHist[k] = 0;
     __syncthreads();
     for (int i = threadIdx.x; i < n; i += blockDim.x)
@@ -690,7 +725,11 @@ __device__ void colour_class(const DevCloth& c, const Buffers& b, const ClassVie
 
 __global__ void __launch_bounds__(1024) k_colour(DevCloth c, Buffers b, ColourArgs a)
 {
-    for (int k = 0; k < 4; k++) colour_class(c, b, a.cls[k], c.status);
+    for (int k = 0; k < 4; k++)
+    {
+        if (a.cls[k].kind <= 1) static_colour_class(c, b, a.cls[k]);
+        else colour_class(c, b, a.cls[k], c.status);
+    }
 }
 
 // residual-target mode, per-colour path: after iteration `iter` the residual
@@ -2157,9 +2196,25 @@ namespace sc {
 
 static_assert(MLP_NPARAM == ML_NPARAM && MLP_NNORM == ML_NNORM, "MLP layout");
 
+static int mlp_sm_count()
+{
+    static int sms = 0;
+    if (sms == 0)
+    {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms < 1) sms = 1;
+    }
+    return sms;
+}
+
+// inference CTAs hold 128 tensor-memory columns (four fit an SM), persistent over tiles
+static int mlp_infer_grid(int rows) { return std::max(1, std::min((rows + ML_ROWS - 1) / ML_ROWS, 4 * mlp_sm_count())); }
+
 void launch_mlp_warm(cudaStream_t s, const DevCloth& c, const Buffers& b, const float* prm, const float* norm)
 {
-    k_mlp_warm<<<(c.N + 127) / 128, 128, 0, s>>>(c, b, MlpArgs{prm, norm});
+    k_mlp_warm<<<mlp_infer_grid(c.N), 128, 0, s>>>(c, b, MlpArgs{prm, norm});
 }
 
 void launch_mlp_features(cudaStream_t s, const DevCloth& c, const Buffers& b, float* feat)
@@ -2174,10 +2229,10 @@ void launch_mlp_targets(cudaStream_t s, const DevCloth& c, float* target)
 
 void launch_mlp_forward(cudaStream_t s, const float* X, int S, const float* prm, const float* norm, float* Y)
 {
-    k_mlp_forward<<<(S + 127) / 128, 128, 0, s>>>(X, S, MlpArgs{prm, norm}, Y);
+    k_mlp_forward<<<mlp_infer_grid(S), 128, 0, s>>>(X, S, MlpArgs{prm, norm}, Y, nullptr);
 }
 
-size_t mlp_grad_smem() { return ((sizeof(MlpSmem) + 15) / 16) * 16 + sizeof(MlpTrainSmem); }
+size_t mlp_grad_smem() { return sizeof(MlpTcTrainSmem); }
 
 bool launch_mlp_grad(cudaStream_t s, const float* X, const float* T, int S, const float* prm, const float* norm,
                      float* grad, float* loss)
@@ -2191,7 +2246,9 @@ bool launch_mlp_grad(cudaStream_t s, const float* X, const float* T, int S, cons
     }
     cudaMemsetAsync(grad, 0, sizeof(float) * ML_NPARAM, s);
     cudaMemsetAsync(loss, 0, sizeof(float), s);
-    k_mlp_grad<<<(S + ML_ROWS - 1) / ML_ROWS, 128, smem, s>>>(X, T, S, MlpArgs{prm, norm}, grad, loss);
+    // training CTAs hold all 512 tensor-memory columns of their SM: one per SM
+    const int grid = std::max(1, std::min((S + ML_ROWS - 1) / ML_ROWS, mlp_sm_count()));
+    k_mlp_grad<<<grid, 128, smem, s>>>(X, T, S, MlpArgs{prm, norm}, grad, loss, nullptr);
     return cudaGetLastError() == cudaSuccess;
 }
 

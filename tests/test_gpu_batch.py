@@ -28,7 +28,7 @@ def _standalone(sc, frames, state=None):
     return out
 
 
-@pytest.mark.parametrize("solver", ["auto", "grid", "tiled", "kernels"])
+@pytest.mark.parametrize("solver", ["auto", "grid", "kernels"])
 def test_batch_matches_standalone(solver):
     """Uneven instances (sides 8..24, own sphere SDF, 1-4 pinned corners, the
     continuous self-collision detector on): each instance of the batch equals the
@@ -40,8 +40,6 @@ def test_batch_matches_standalone(solver):
     assert b.size() == len(insts)
     if solver == "grid":
         b.model.set_grid_solver(0, 1)
-    elif solver == "tiled":
-        b.model.set_tiled_solver(2, 1)
     elif solver == "kernels":
         b.model.set_solver_mode(3)
     for _ in range(frames):

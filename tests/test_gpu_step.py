@@ -2,8 +2,9 @@
 
 Check mode: the oracle runs the reference's sequential Gauss-Seidel sweep in the
 order the coloured GPU sweep realises (constraint colour order from
-scGetConstraintOrder, contacts in the deterministic independent-set colouring),
-so the two agree to FP32 rounding of acosf (CUDA vs glibc) only.
+scGetConstraintOrder; self contacts in the deterministic independent-set
+colouring, triangle and edge collider contacts by the static colours of their
+cloth triangles / edges, scGetStaticColours), so the two agree bit for bit.
 """
 import copy
 
@@ -32,6 +33,7 @@ def _pair(sc, ccd=False, state=None):
     if not sc.params.fem:
         o.set_link_order(p.model.constraint_order(2)[0])
     o.set_contact_order(1)
+    o.set_static_colours(*p.model.static_colours())
     return w, p, o
 
 
@@ -276,8 +278,7 @@ def test_mass_spring_check_mode(dihedral, fixed):
 def test_solvers_are_bit_identical(scene):
     """The cluster-resident solver (one launch per substep, particles in
     distributed shared memory, records staged in shared memory or read from
-    global memory), every variant of the grid-resident cooperative solver and of
-    its tiled form (neighbour waits instead of grid barriers), the
+    global memory), every variant of the grid-resident cooperative solver, the
     one-kernel-per-colour path and the autotuner's choice are the same algorithm
     in the same order: bit-identical trajectories."""
     from solidcloth_b200 import api
@@ -298,8 +299,7 @@ def test_solvers_are_bit_identical(scene):
         sc, state = scenes.ccd_scene(16)
     out = []
     modes = [("cluster", True), ("cluster", False), ("kernels", False)]
-    modes += [("grid", (v, 1)) for v in range(len(api.grid_variants()))] + [("grid", (0, 2))]
-    modes += [("tiled", (v, 1)) for v in range(len(api.grid_variants()))] + [("tiled", (3, 2)), ("auto", None)]
+    modes += [("grid", (v, 1)) for v in range(len(api.grid_variants()))] + [("grid", (0, 2)), ("auto", None)]
     for mode, arg in modes:
         w, p = api.load_scene(sc)
         if mode == "cluster":
@@ -309,8 +309,6 @@ def test_solvers_are_bit_identical(scene):
             p.model.set_cluster_solver(False)
         elif mode == "grid":
             p.model.set_grid_solver(*arg)
-        elif mode == "tiled":
-            p.model.set_tiled_solver(*arg)
         if state is not None:
             p.model.set_state(*state)
         for _ in range(4):

@@ -132,9 +132,11 @@ def test_no_alloc_zero_area_triangle_matches_restatement():
     (Vector3::Normalize divides by a zero length); the others are unaffected."""
     from solidcloth_b200 import api
     L = api.lib()
-    pos = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [1, 1, 0.2], [2, 2, 0.4], [3, 3, 0.6], [5, 0, 0], [6, 0, 0],
-                    [5, 1, 0.1]], np.float32)
-    idx = np.array([0, 1, 2, 1, 3, 2, 3, 4, 5, 6, 7, 8], np.int32)      # triangle 2 is collinear
+    # triangle 2 is collinear, with exactly representable coordinates so that its
+    # edge vectors are exactly parallel and their cross product exactly zero
+    pos = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [1, 1, 0.25], [2, 2, 0.5], [3, 3, 0.75], [5, 0, 0], [6, 0, 0],
+                    [5, 1, 0.125]], np.float32)
+    idx = np.array([0, 1, 2, 1, 3, 2, 3, 4, 5, 6, 7, 8], np.int32)
     expect = _restated_normals(pos, idx)
     rc, normals = _call(L, pos, idx)
     assert rc == 0, L.scGetLastErrorString()
