@@ -275,6 +275,8 @@ SCEXP void scSetClusterSolver(scModel model, bool val);
 SCEXP void scSetSolverMode(scModel model, int mode);
 /* force grid variant `variant` (0 .. scGetGridVariants()-1) with blocksPerSm CTAs per SM */
 SCEXP void scSetGridSolver(scModel model, int variant, int blocksPerSm);
+/* force the cluster kernel with 1 (variant 0) or 2 (variant 1) constraints per thread */
+SCEXP void scSetClusterVariant(scModel model, int variant);
 /* out4 = {kind, grid variant, CTAs per SM, threads per CTA} of the solver in use;
    tuneMs (4 floats per candidate: kind, variant, CTAs per SM, ms per substep)
    gets up to cap candidates of the last tuning; returns the candidate count */

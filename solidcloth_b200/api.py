@@ -138,6 +138,7 @@ SIGNATURES = {
     "scSetClusterStaging": ([scModel, C.c_bool], None),
     "scSetSolverPrecision": ([scModel, C.c_int], None),
     "scSetResidualUnit": ([scModel, C.c_int], None),
+    "scSetClusterVariant": ([scModel, C.c_int], None),
     "scGetStaticColours": ([scModel, _i, _i, _i], C.c_int),
     "scGetSolverPrecision": ([scModel], C.c_int),
     "scCreateClothBatch": ([scCollisionWorld, C.POINTER(scClothPatch), C.c_int], scClothPatch),
@@ -334,6 +335,10 @@ class ClothModel:
         """0 autotuned, 1 cluster kernel, 2 grid kernel, 3 per-colour kernels"""
         lib().scSetSolverMode(self.h, int(mode))
         _check("scSetSolverMode")
+
+    def set_cluster_variant(self, variant: int):
+        lib().scSetClusterVariant(self.h, int(variant))
+        _check("scSetClusterVariant")
 
     def set_grid_solver(self, variant: int, blocks_per_sm: int):
         lib().scSetGridSolver(self.h, int(variant), int(blocks_per_sm))

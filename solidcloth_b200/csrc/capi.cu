@@ -659,6 +659,15 @@ void scSetGridSolver(scModel m, int variant, int blocksPerSm)
     M(m)->touch();
     M(m)->tunedVersion = M(m)->paramVersion;
 }
+void scSetClusterVariant(scModel m, int variant)
+{
+    if (!M(m) || variant < 0 || variant >= gs_cluster_variants()) { set_error(SC_ERR_ARG, "bad cluster solver variant"); return; }
+    M(m)->solverMode = SOLVE_CLUSTER;
+    M(m)->choice = {SOLVE_CLUSTER, variant, 0, 0.f};
+    M(m)->tuned = true;
+    M(m)->touch();
+    M(m)->tunedVersion = M(m)->paramVersion;
+}
 int scGetSolverChoice(scModel m, int* out4, float* tuneMs, int cap)
 {
     if (!M(m)) return 0;

@@ -1798,7 +1798,7 @@ bool ClothPatch::record_solve(cudaStream_t s, const SolverParams& P, const Solve
             plan.stage = 1;
             smem = staged;
         }
-        ops.cluster(s, c, P, b, plan, cluster, smem);   // includes the velocity update
+        ops.cluster(s, c, P, b, plan, cluster, smem, ch.variant);   // includes the velocity update
         return true;
     }
     if (ch.kind == SOLVE_GRID && planFits && ops.grid(s, c, P, b, plan, ch.variant, ch.blocksPerSm))
@@ -1862,7 +1862,7 @@ bool ClothPatch::autotune(float h)
     const bool fits = m.triColourStart.size() <= 65 && m.bendColourStart.size() <= 65 && m.linkColourStart.size() <= 65;
     const SolverOps& ops = solver_ops(m.prm.fastMath);
     if (fits && (m.solverMode == SOLVE_AUTO || m.solverMode == SOLVE_CLUSTER) && ops.cluster_size(m.N, shift, smem) > 0)
-        cand.push_back({SOLVE_CLUSTER, 0, 0, 0.f});
+        for (int v = 0; v < gs_cluster_variants(); v++) cand.push_back({SOLVE_CLUSTER, v, 0, 0.f});
     if (fits && (m.solverMode == SOLVE_AUTO || m.solverMode == SOLVE_GRID))
         for (int v = 0; v < gs_grid_variants(); v++)
         {

@@ -137,8 +137,10 @@ struct GsPlan
 // cluster size usable for N particles (0: too large or unsupported); sets the
 // log2 particles-per-CTA and the dynamic shared memory per CTA
 int gs_cluster_size(int N, int& shift, size_t& smem);
+// variant 0: one constraint per thread; 1: two (their loads overlap)
+int gs_cluster_variants();
 void launch_gs_cluster(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b, GsPlan plan,
-                       int clusterSize, size_t smem);
+                       int clusterSize, size_t smem, int variant);
 
 // grid-resident solver (cooperative launch, any cloth or batch size); variants
 // differ in threads per CTA and in constraints per thread (tiles)
@@ -162,7 +164,7 @@ struct SolverOps
     void (*vertex_contacts)(cudaStream_t, const DevCloth&, const SolverParams&, const Buffers&);
     void (*multi_contacts)(cudaStream_t, const DevCloth&, const SolverParams&, const Buffers&, int);
     int (*cluster_size)(int, int&, size_t&);
-    void (*cluster)(cudaStream_t, const DevCloth&, const SolverParams&, const Buffers&, GsPlan, int, size_t);
+    void (*cluster)(cudaStream_t, const DevCloth&, const SolverParams&, const Buffers&, GsPlan, int, size_t, int);
     int (*grid_max_blocks_per_sm)(int);
     bool (*grid)(cudaStream_t, const DevCloth&, const SolverParams&, const Buffers&, GsPlan, int, int);
 };

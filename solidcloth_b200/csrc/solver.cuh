@@ -555,6 +555,135 @@ struct ClusterPos
     __device__ __forceinline__ void st(uint32_t v, float4 x) const { *addr(v) = x; }
 };
 
+// particle accessor over a tile entry's own registers (the projection functions
+// load their particles first and store them last)
+struct RegPos
+{
+    uint32_t id[4];
+    mutable float4 v[4];
+    __device__ __forceinline__ float4 ld(uint32_t q) const
+    {
+        return q == id[0] ? v[0] : q == id[1] ? v[1] : q == id[2] ? v[2] : v[3];
+    }
+    __device__ __forceinline__ void st(uint32_t q, float4 x) const
+    {
+        if (q == id[0]) v[0] = x;
+        else if (q == id[1]) v[1] = x;
+        else if (q == id[2]) v[2] = x;
+        else v[3] = x;
+    }
+};
+
+// A thread of the cluster solver takes TILE consecutive constraints of its CTA's
+// chunk of a colour and issues all their particle loads (distributed shared
+// memory) before any projection, so their latencies overlap; the constraints of
+// a colour share no particle, so the result is unchanged.
+template <int TILE, class PA>
+__device__ __forceinline__ void cluster_fem(const PA& pa, const DevCloth& c, const SolverParams& P, const float4* staged,
+                                            int a, int e)
+{
+    if constexpr (TILE == 1)
+    {
+        // one constraint a thread: project straight through the accessor
+        for (int j = a + (int)threadIdx.x; j < e; j += (int)blockDim.x)
+        {
+            if (staged)
+            {
+                const float4* r = staged + 3 * (j - a);
+                fem_project(pa, r[0], r[1], r[2], P);
+            }
+            else
+                fem_project(pa, __ldg(&c.fem[3 * j]), __ldg(&c.fem[3 * j + 1]), __ldg(&c.fem[3 * j + 2]), P);
+        }
+        return;
+    }
+    for (int j0 = a + (int)threadIdx.x * TILE; j0 < e; j0 += (int)blockDim.x * TILE)
+    {
+        float4 r0[TILE], r1[TILE], r2[TILE];
+        RegPos rp[TILE];
+#pragma unroll
+        for (int u = 0; u < TILE; u++)
+        {
+            const int j = min(j0 + u, e - 1);
+            if (staged)
+            {
+                const float4* r = staged + 3 * (j - a);
+                r0[u] = r[0]; r1[u] = r[1]; r2[u] = r[2];
+            }
+            else
+            {
+                r0[u] = __ldg(&c.fem[3 * j]); r1[u] = __ldg(&c.fem[3 * j + 1]); r2[u] = __ldg(&c.fem[3 * j + 2]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < TILE; u++)
+        {
+            rp[u].id[0] = __float_as_uint(r0[u].x); rp[u].id[1] = __float_as_uint(r0[u].y);
+            rp[u].id[2] = __float_as_uint(r0[u].z); rp[u].id[3] = 0xffffffffu;
+            rp[u].v[0] = pa.ld(rp[u].id[0]); rp[u].v[1] = pa.ld(rp[u].id[1]); rp[u].v[2] = pa.ld(rp[u].id[2]);
+        }
+#pragma unroll
+        for (int u = 0; u < TILE; u++)
+            if (j0 + u < e) fem_project(rp[u], r0[u], r1[u], r2[u], P);
+#pragma unroll
+        for (int u = 0; u < TILE; u++)
+            if (j0 + u < e)
+            {
+                pa.st(rp[u].id[0], rp[u].v[0]); pa.st(rp[u].id[1], rp[u].v[1]); pa.st(rp[u].id[2], rp[u].v[2]);
+            }
+    }
+}
+
+template <int TILE, class PA>
+__device__ __forceinline__ float cluster_bends(const PA& pa, const DevCloth& c, const SolverParams& P, const uint4* staged,
+                                               int a, int e)
+{
+    float err = 0.f;
+    if constexpr (TILE == 1)
+    {
+        for (int j = a + (int)threadIdx.x; j < e; j += (int)blockDim.x)
+            err = fmaxf(err, bend_project(pa, staged ? staged[j - a] : __ldg(&c.bend[j]), P));
+        return err;
+    }
+    for (int j0 = a + (int)threadIdx.x * TILE; j0 < e; j0 += (int)blockDim.x * TILE)
+    {
+        uint4 bc[TILE];
+        RegPos rp[TILE];
+#pragma unroll
+        for (int u = 0; u < TILE; u++)
+        {
+            const int j = min(j0 + u, e - 1);
+            bc[u] = staged ? staged[j - a] : __ldg(&c.bend[j]);
+        }
+#pragma unroll
+        for (int u = 0; u < TILE; u++)
+        {
+            rp[u].id[0] = bc[u].x; rp[u].id[1] = bc[u].y; rp[u].id[2] = bc[u].z; rp[u].id[3] = bc[u].w;
+            rp[u].v[0] = pa.ld(bc[u].x); rp[u].v[1] = pa.ld(bc[u].y); rp[u].v[2] = pa.ld(bc[u].z); rp[u].v[3] = pa.ld(bc[u].w);
+        }
+        bool moved[TILE];
+#pragma unroll
+        for (int u = 0; u < TILE; u++)
+        {
+            moved[u] = false;
+            if (j0 + u < e)
+            {
+                const float ev = bend_project(rp[u], bc[u], P);
+                moved[u] = ev >= 0.f;
+                err = fmaxf(err, ev);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < TILE; u++)
+            if (moved[u])
+            {
+                pa.st(bc[u].x, rp[u].v[0]); pa.st(bc[u].y, rp[u].v[1]); pa.st(bc[u].z, rp[u].v[2]); pa.st(bc[u].w, rp[u].v[3]);
+            }
+    }
+    return err;
+}
+
+template <int TILE>
 __global__ void __launch_bounds__(GS_THREADS) k_gs_cluster(DevCloth c, SolverParams P, Buffers b, ColourArgs ca, GsPlan plan)
 {
     extern __shared__ float4 sPos[];
@@ -633,16 +762,7 @@ __global__ void __launch_bounds__(GS_THREADS) k_gs_cluster(DevCloth c, SolverPar
             {
                 int a, e;
                 range(plan.femStart[col], plan.femStart[col + 1], a, e);
-                for (int j = a + threadIdx.x; j < e; j += blockDim.x)
-                {
-                    if (plan.stage)
-                    {
-                        const float4* r = sFem + 3 * (sFemOff[col] + (j - a));
-                        fem_project(pa, r[0], r[1], r[2], P);
-                    }
-                    else
-                        fem_project(pa, c.fem[3 * j], c.fem[3 * j + 1], c.fem[3 * j + 2], P);
-                }
+                cluster_fem<TILE>(pa, c, P, plan.stage ? sFem + 3 * sFemOff[col] : nullptr, a, e);
                 cl.sync();
             }
         else
@@ -662,11 +782,8 @@ __global__ void __launch_bounds__(GS_THREADS) k_gs_cluster(DevCloth c, SolverPar
             {
                 int a, e;
                 range(plan.bendStart[col], plan.bendStart[col + 1], a, e);
-                for (int j = a + threadIdx.x; j < e; j += blockDim.x)
-                {
-                    float errv = bend_project(pa, plan.stage ? sBend[sBendOff[col] + (j - a)] : c.bend[j], P);
-                    if (track && errv > 0.f) atomicMax((int*)&sErr[2], __float_as_int(errv));
-                }
+                const float errv = cluster_bends<TILE>(pa, c, P, plan.stage ? sBend + sBendOff[col] : nullptr, a, e);
+                if (track && errv > 0.f) atomicMax((int*)&sErr[2], __float_as_int(errv));
                 cl.sync();
             }
         if (b.numVColl > 0)
@@ -785,24 +902,6 @@ __global__ void __launch_bounds__(GS_THREADS) k_gs_cluster(DevCloth c, SolverPar
 // projections' memory latencies overlap. Same phases and order as the
 // per-colour kernels: bit-identical results.
 
-// particle accessor over a tile entry's own registers (the projection functions
-// load their particles first and store them last)
-struct RegPos
-{
-    uint32_t id[4];
-    mutable float4 v[4];
-    __device__ __forceinline__ float4 ld(uint32_t q) const
-    {
-        return q == id[0] ? v[0] : q == id[1] ? v[1] : q == id[2] ? v[2] : v[3];
-    }
-    __device__ __forceinline__ void st(uint32_t q, float4 x) const
-    {
-        if (q == id[0]) v[0] = x;
-        else if (q == id[1]) v[1] = x;
-        else if (q == id[2]) v[2] = x;
-        else v[3] = x;
-    }
-};
 
 // Constraint records are constant for the whole launch: they are read through the
 // non-coherent path (ld.global.nc), which keeps them in the SM's L1 from one
@@ -1063,14 +1162,21 @@ bool launch_gs_grid(cudaStream_t s, const DevCloth& c, const SolverParams& P, co
     return cudaLaunchKernelEx(&cfg, kGridVariants[variant], c, P, b, colour_args(b), plan) == cudaSuccess;
 }
 
+// cluster solver variants: constraints per thread 1 or 2
+static const GridKernel kClusterVariants[] = {k_gs_cluster<1>, k_gs_cluster<2>};
+int gs_cluster_variants() { return 2; }
+
 int gs_cluster_size(int N, int& shift, size_t& smem)
 {
     static int supported = -1;
     if (supported < 0)
     {
         supported = 0;
-        cudaFuncSetAttribute(k_gs_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-        cudaFuncSetAttribute(k_gs_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, GS_SMEM_MAX);
+        for (auto k : kClusterVariants)
+        {
+            cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, GS_SMEM_MAX);
+        }
         for (int cs : {16, 8})
         {
             cudaLaunchConfig_t cfg = {};
@@ -1082,7 +1188,7 @@ int gs_cluster_size(int N, int& shift, size_t& smem)
             at.val.clusterDim.x = cs; at.val.clusterDim.y = 1; at.val.clusterDim.z = 1;
             cfg.attrs = &at; cfg.numAttrs = 1;
             int clusters = 0;
-            if (cudaOccupancyMaxActiveClusters(&clusters, k_gs_cluster, &cfg) == cudaSuccess && clusters > 0)
+            if (cudaOccupancyMaxActiveClusters(&clusters, kClusterVariants[1], &cfg) == cudaSuccess && clusters > 0)
             {
                 supported = cs;
                 break;
@@ -1101,7 +1207,7 @@ int gs_cluster_size(int N, int& shift, size_t& smem)
 }
 
 void launch_gs_cluster(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b, GsPlan plan,
-                       int clusterSize, size_t smem)
+                       int clusterSize, size_t smem, int variant)
 {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(clusterSize);
@@ -1112,7 +1218,7 @@ void launch_gs_cluster(cudaStream_t s, const DevCloth& c, const SolverParams& P,
     at.id = cudaLaunchAttributeClusterDimension;
     at.val.clusterDim.x = clusterSize; at.val.clusterDim.y = 1; at.val.clusterDim.z = 1;
     cfg.attrs = &at; cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, k_gs_cluster, c, P, b, colour_args(b), plan);
+    cudaLaunchKernelEx(&cfg, kClusterVariants[variant == 1 ? 1 : 0], c, P, b, colour_args(b), plan);
 }
 
 // ---------------------------------------------- per-colour path launchers

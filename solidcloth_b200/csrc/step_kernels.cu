@@ -196,11 +196,33 @@ struct PointHit { float dist; int tri; V3 cp, bary, normal; int region; };
 // only produce such results — every node nearer than the bound is visited in the
 // same order as by the unbounded search, so results below the bound (and ties
 // among them) are unchanged.
+// Leaf pre-filter of the nearest-feature searches: a primitive can change a
+// search's result only if its distance is below the best so far (minDist), and
+// its distance is at least the distance between the query and the primitive's
+// bounding box. Primitives whose box distance exceeds minDist by more than the
+// rounding of the exact computation (slack: 1e-4 of the coordinates' magnitude,
+// orders of magnitude above it) are skipped without the exact closest-point
+// computation; the searches return exactly what they return without it.
+__device__ __forceinline__ float skip_slack(V3 p)
+{
+    return 1e-4f * (1.f + fmaxf(fabsf(p.x), fmaxf(fabsf(p.y), fabsf(p.z))));
+}
+__device__ __forceinline__ bool cannot_improve(float boxDist, float minDist, float slack)
+{
+    return boxDist > minDist + slack;
+}
+__device__ __forceinline__ Box prim_box(V3 a, V3 b, V3 c)
+{
+    Box x = Box::empty(); x.add(a); x.add(b); x.add(c);
+    return x;
+}
+
 __device__ PointHit mesh_point_query(const DevMesh& m, V3 p, int* status, float bound)
 {
     PointHit r; r.dist = FLT_MAX; r.tri = -1; r.region = -1;
     r.cp = r.bary = r.normal = mk(0.f, 0.f, 0.f);
     float minDist = bound;
+    const float slack = skip_slack(p);
     int stNode[MESH_STACK]; float stDist[MESH_STACK];
     int sp = 0;
     int node = 0;
@@ -213,6 +235,7 @@ __device__ PointHit mesh_point_query(const DevMesh& m, V3 p, int* status, float 
             {
                 uint32_t t = m.tree.tris[pr.x + k];
                 V3 a = ld3(m.v, m.tri[3 * t]), b = ld3(m.v, m.tri[3 * t + 1]), cc = ld3(m.v, m.tri[3 * t + 2]);
+                if (cannot_improve(prim_box(a, b, cc).dist(p), minDist, slack)) continue;
                 V3 coords, pt;
                 int region = closest_point_triangle(p, a, b, cc, pt, coords);
                 V3 delta = p - pt;
@@ -260,6 +283,7 @@ __device__ VtxHit mesh_triangle_query(const DevMesh& m, V3 a, V3 b, V3 cc, int* 
     r.cpMesh = r.cpTri = r.bary = r.normal = mk(0.f, 0.f, 0.f);
     float minDist = bound;
     Box tb = Box::empty(); tb.add(a); tb.add(b); tb.add(cc);
+    const float slack = skip_slack(a);
     int stNode[MESH_STACK]; float stDist[MESH_STACK];
     int sp = 0, node = 0;
     while (true)
@@ -271,6 +295,7 @@ __device__ VtxHit mesh_triangle_query(const DevMesh& m, V3 a, V3 b, V3 cc, int* 
             {
                 uint32_t v = m.tree.verts[pr.z + k];
                 V3 pv = ld3(m.v, v);
+                if (cannot_improve(tb.dist(pv), minDist, slack)) continue;
                 V3 bary, cp;
                 int region = closest_point_triangle(pv, a, b, cc, cp, bary);
                 V3 delta = cp - pv;
@@ -324,6 +349,7 @@ __device__ SegHit mesh_segment_query(const DevMesh& m, V3 p, V3 q, int* status, 
     r.cs0 = r.cs1 = r.cm0 = r.cm1 = 0.f;
     float minDist = bound;
     Box eb = Box::empty(); eb.add(p); eb.add(q);
+    const float slack = skip_slack(p);
     int stNode[MESH_STACK]; float stDist[MESH_STACK];
     int sp = 0, node = 0;
     while (true)
@@ -336,6 +362,8 @@ __device__ SegHit mesh_segment_query(const DevMesh& m, V3 p, V3 q, int* status, 
                 uint32_t e = m.tree.edges[er.x + k];
                 int4 ed = m.edge[e];
                 V3 a = ld3(m.v, ed.x), b = ld3(m.v, ed.y);
+                Box pb = Box::empty(); pb.add(a); pb.add(b);
+                if (cannot_improve(pb.dist(eb), minDist, slack)) continue;
                 float ps, pm;
                 V3 cs, cm;
                 int region = closest_segm_segm(p, q, a, b, ps, pm, cs, cm);

@@ -67,7 +67,7 @@ class Dataset:
 
 
 def generate(num_drapes: int, n: int = 256, per_batch: int = 32, skip_frames: int = 4, record_frames: int = 3,
-             keep_every: int = 128, tol: float = 1e-4, max_iter: int = 100, seed0: int = 0) -> Dataset:
+             keep_every: int = 128, tol: float = 1e-4, max_iter: int = 100, seed0: int = 0, log=None) -> Dataset:
     """Simulate `num_drapes` drapes with the plain solver (update residual target
     `tol` in metres, at most `max_iter` iterations a substep) in batches, and keep
     every `keep_every`-th particle's (features, correction) of every substep of
@@ -76,8 +76,10 @@ def generate(num_drapes: int, n: int = 256, per_batch: int = 32, skip_frames: in
     t0 = time.time()
     xs, ts = [], []
     for b0 in range(0, num_drapes, per_batch):
+        tb = time.time()
         ds = [drape_scene(seed0 + k, n) for k in range(b0, min(num_drapes, b0 + per_batch))]
         b = api.load_batch(ds)
+        tl = time.time()
         b.model.set_fast_math(True)
         b.model.set_residual_target(tol, max_iter, metres=True)
         N = sum(d.num_vertices for d in ds)
@@ -95,6 +97,8 @@ def generate(num_drapes: int, n: int = 256, per_batch: int = 32, skip_frames: in
             ts.append(Tg[:, sel].reshape(-1, OUT).clone())
         b.model.set_sample_buffers(0, 0)
         b.free()
+        if log:
+            log(f"batch {b0 // per_batch}: set-up {tl - tb:.1f} s, frames {time.time() - tl:.1f} s")
     torch.cuda.synchronize()
     return Dataset(torch.cat(xs), torch.cat(ts), num_drapes, time.time() - t0)
 
@@ -222,7 +226,8 @@ def main(argv=None):
     ap.add_argument("--report", default=None)
     a = ap.parse_args(argv)
     torch.cuda.init()
-    ds = generate(a.drapes, n=a.n, per_batch=a.per_batch, tol=a.tol, max_iter=a.max_iter)
+    ds = generate(a.drapes, n=a.n, per_batch=a.per_batch, tol=a.tol, max_iter=a.max_iter,
+                  log=lambda m: print(m, flush=True))
     print(f"samples {ds.X.shape[0]} from {ds.drapes} drapes in {ds.seconds:.1f} s", flush=True)
     norm = fit_norm(ds.X, ds.T)
     t0 = time.time()
@@ -230,7 +235,8 @@ def main(argv=None):
     train_s = time.time() - t0
     np.savez(a.out, params=params, norm=norm, drapes=a.drapes, n=a.n, tol=a.tol, loss=np.array(hist))
     report = {"drapes": a.drapes, "n_train": a.n, "samples": int(ds.X.shape[0]), "generate_s": ds.seconds,
-              "train_s": train_s, "loss_per_epoch": hist, "tol": a.tol, "max_iter": a.max_iter, "eval": {}}
+              "train_s": train_s, "loss_per_epoch": hist, "tol": a.tol, "residual_unit": "m", "max_iter": a.max_iter,
+              "eval_max_iter": a.eval_max_iter, "eval": {}}
     for n in a.eval_n:
         rows = []
         for k in range(a.eval):

@@ -97,32 +97,32 @@ def grid_positions(n: int, inc: float, offset) -> np.ndarray:
     them in float32 (Physics/ClothPatch.cpp:150-190): column j at
     x_j = x_{j-1} + inc starting from -0.5*n*inc, row i at startY + inc*i."""
     off = np.asarray(offset, dtype=np.float32)
-    pos = np.zeros((n * n, 3), dtype=np.float32)
-    x = np.float32(np.float32(-0.5) * np.float32(n)) * np.float32(inc)
-    start = x
-    for j in range(n):
-        base = j * n
-        for i in range(n):
-            z = start if i == 0 else np.float32(start + np.float32(np.float32(inc) * np.float32(i)))
-            pos[base + i] = (np.float32(x + off[0]), np.float32(np.float32(0) + off[1]),
-                             np.float32(z + off[2]))
-        x = np.float32(x + np.float32(inc))
-    return pos
+    inc32 = np.float32(inc)
+    start = np.float32(np.float32(np.float32(-0.5) * np.float32(n)) * inc32)
+    xs = np.empty(n, dtype=np.float32)
+    x = start
+    for j in range(n):                 # the running float32 sum of the reference's loop
+        xs[j] = x
+        x = np.float32(x + inc32)
+    zs = (start + (inc32 * np.arange(n, dtype=np.float32)).astype(np.float32)).astype(np.float32)
+    zs[0] = start
+    pos = np.empty((n, n, 3), dtype=np.float32)
+    pos[:, :, 0] = (xs + off[0]).astype(np.float32)[:, None]
+    pos[:, :, 1] = np.float32(np.float32(0) + off[1])
+    pos[:, :, 2] = (zs + off[2]).astype(np.float32)[None, :]
+    return pos.reshape(n * n, 3)
 
 
 def grid_triangles(n: int) -> np.ndarray:
     """Triangle list of ClothPatch::Init(grid), alternating diagonals
     (Physics/ClothPatch.cpp:205-221)."""
-    tris = []
-    for j in range(1, n):
-        for i in range(1, n):
-            idx = j * n + i
-            a, b, c, d = idx - n - 1, idx - n, idx, idx - 1
-            if (i & 1) == (j & 1):
-                tris += [(a, c, b), (a, d, c)]
-            else:
-                tris += [(b, d, c), (d, b, a)]
-    return np.asarray(tris, dtype=np.uint32)
+    j, i = np.meshgrid(np.arange(1, n), np.arange(1, n), indexing="ij")
+    idx = j * n + i
+    a, b, c, d = idx - n - 1, idx - n, idx, idx - 1
+    same = (i & 1) == (j & 1)
+    t1 = np.where(same[..., None], np.stack([a, c, b], -1), np.stack([b, d, c], -1))
+    t2 = np.where(same[..., None], np.stack([a, d, c], -1), np.stack([d, b, a], -1))
+    return np.stack([t1, t2], 2).reshape(-1, 3).astype(np.uint32)
 
 
 def lumped_masses(n: int, inc: float, density: float, pinned) -> np.ndarray:

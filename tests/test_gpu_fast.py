@@ -127,13 +127,13 @@ def test_fast_solvers_agree(scene):
         sc = scenes.cfg0()
         sc.params.fem = False
         sc.params.stretch, sc.params.shear, sc.params.bend = 1e3, 5e2, 2.0
-    modes = [("cluster", None), ("kernels", None)] + [("grid", (v, 1)) for v in range(len(api.grid_variants()))]
+    modes = [("cluster", 0), ("cluster", 1), ("kernels", None)] + [("grid", (v, 1)) for v in range(len(api.grid_variants()))]
     out = []
     for mode, arg in modes:
         w, p = api.load_scene(sc)
         p.model.set_fast_math(True)
         if mode == "cluster":
-            p.model.set_cluster_solver(True)
+            p.model.set_cluster_variant(arg)
         elif mode == "kernels":
             p.model.set_cluster_solver(False)
         else:

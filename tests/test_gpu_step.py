@@ -298,13 +298,13 @@ def test_solvers_are_bit_identical(scene):
     else:
         sc, state = scenes.ccd_scene(16)
     out = []
-    modes = [("cluster", True), ("cluster", False), ("kernels", False)]
+    modes = [("cluster", True), ("cluster", False), ("cluster2", True), ("cluster2", False), ("kernels", False)]
     modes += [("grid", (v, 1)) for v in range(len(api.grid_variants()))] + [("grid", (0, 2)), ("auto", None)]
     for mode, arg in modes:
         w, p = api.load_scene(sc)
-        if mode == "cluster":
-            p.model.set_cluster_solver(True)
+        if mode in ("cluster", "cluster2"):
             p.model.set_cluster_staging(arg)
+            p.model.set_cluster_variant(1 if mode == "cluster2" else 0)     # last: forcing survives
         elif mode == "kernels":
             p.model.set_cluster_solver(False)
         elif mode == "grid":
