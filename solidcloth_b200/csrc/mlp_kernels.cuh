@@ -1,8 +1,8 @@
 // mlp_kernels.cuh — the learned warm start: a per-particle MLP
 // 12 -> 64 -> 64 -> 64 -> 3 (GELU) that predicts the Gauss-Seidel correction of a
 // substep from 1-ring features, so that plain iterations start closer to the
-// solution. It has no counterpart in the reference; the plain solver stays the
-// fallback and the judge (the residual decides when a substep is done).
+// solution. It has no counterpart in the reference; the plain iterations still
+// run after it, and the residual target decides when a substep is done.
 //
 // Every contraction runs on the fifth-generation tensor cores (tc05.cuh): tiles
 // of 128 particles (rows) per CTA, BF16 operands staged in shared memory, FP32

@@ -150,7 +150,7 @@ extern "C" int scComputeVertexNormalsNoAlloc(const float* vertices, int numVerti
     k_noalloc_normalise<<<nb, 256, 0, s>>>(acc, numVertices, normals);
     e = cudaGetLastError();
     if (e != cudaSuccess) { set_error(SC_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e)); return SC_ERR_CUDA; }
-    // the index check's verdict: read the device counter once the work is done
+    // the index check's outcome: read the device counter once the work is done
     int bad = 0;
     e = cudaMemcpyFromSymbolAsync(&bad, g_noalloc_bad_triangles, sizeof(int), 0, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);

@@ -5,8 +5,8 @@ The network (12 -> 64 -> 64 -> 64 -> 3, GELU, BF16 weights on the tensor cores)
 predicts, per particle, the correction the Gauss-Seidel loop will apply in a
 substep (solved minus predicted position) from features available right after
 the prediction. The library applies it before the loop; plain iterations then
-continue until the residual target, so the plain solver remains both fallback
-and judge. Everything runs on the GPU: samples come from the solver through
+continue until the residual target, so the plain solver still decides when a
+substep is done. Everything runs on the GPU: samples come from the solver through
 scSetSampleBuffers, gradients from scMlpGradients, updates from scMlpAdamStep.
 """
 from __future__ import annotations
@@ -166,7 +166,9 @@ def compare(drapes, params: np.ndarray | None, norm: np.ndarray | None, frames: 
     """Plain versus learned on the same drapes (a batch): Gauss-Seidel iterations a
     substep to reach the update residual target (the largest particle
     displacement of an iteration, in metres), and device-timed
-    vertex-substeps/s over the measured frames (after `skip` untimed frames)."""
+    vertex-substeps/s over the measured frames (after `skip` untimed frames).
+    constraint_residual_after is max |C| over the FEM constraints after the last
+    frame (scGetResidual), a check that both arms end in states of equal quality."""
     import torch
     out = {}
     for label, warm in (("plain", False), ("learned", True)):
@@ -192,7 +194,7 @@ def compare(drapes, params: np.ndarray | None, norm: np.ndarray | None, frames: 
         sub = drapes[0].params.substeps * frames
         N = sum(d.num_vertices for d in drapes)
         out[label] = {"iterations_per_substep": its / sub, "vertex_substeps_per_s": N * sub / (ms * 1e-3),
-                      "ms_per_frame": ms / frames, "residual_after": b.model.residual(), "status": b.status()}
+                      "ms_per_frame": ms / frames, "constraint_residual_after": b.model.residual(), "status": b.status()}
         b.free()
     return out
 

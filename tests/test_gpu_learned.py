@@ -1,0 +1,50 @@
+"""The trained warm start (solidcloth_b200/data/warmstart.npz: 2,000 drapes at
+256 x 256) against the plain solver on a held-out 256 x 256 drape, through the C
+ABI: Gauss-Seidel iterations a substep to the same update residual (the largest
+particle displacement of an iteration, 1e-4 m, cap 200).
+
+The learned warm start has no reference counterpart; it replaces iterations of
+the Gauss-Seidel loop (Physics/ClothPBD.cpp:332-361). The bar is the scope's: at
+least 2x fewer iterations at equal residual. Both arms must reach the residual
+(below the cap), and the learned arm's final constraint residual must not be
+worse than twice the plain arm's (the network does not buy iterations with a
+worse state)."""
+import numpy as np
+import pytest
+
+from solidcloth_b200 import learned
+from solidcloth_b200.build import PKG
+
+pytestmark = pytest.mark.gpu
+
+CAP = 200
+TOL = 1e-4        # metres
+
+
+def _weights():
+    z = np.load(PKG / "data" / "warmstart.npz")
+    return z["params"].astype(np.float32), z["norm"].astype(np.float32), int(z["n"])
+
+
+@pytest.mark.parametrize("seed", [30_000_000, 30_000_001])
+def test_trained_network_halves_iterations_on_held_out_256_drape(seed):
+    params, norm, n_train = _weights()
+    assert n_train == 256
+    d = learned.drape_scene(seed, 256)            # seeds the training never used (0 .. 1999)
+    r = learned.compare([d], params, norm, frames=3, skip=4, tol=TOL, max_iter=CAP)
+    plain, warm = r["plain"], r["learned"]
+    assert plain["status"] == 0 and warm["status"] == 0
+    assert plain["iterations_per_substep"] < CAP and warm["iterations_per_substep"] < CAP
+    ratio = plain["iterations_per_substep"] / warm["iterations_per_substep"]
+    assert ratio >= 2.0, r
+    assert warm["constraint_residual_after"] <= 2.0 * plain["constraint_residual_after"], r
+    assert warm["vertex_substeps_per_s"] > plain["vertex_substeps_per_s"], r
+
+
+def test_untrained_network_gives_no_gain():
+    """Control: the same comparison with the correction scaled to zero runs the
+    plain iteration count (the warm start's wiring adds nothing by itself)."""
+    params, norm, _ = _weights()
+    d = learned.drape_scene(30_000_002, 64, side=0.5)
+    r = learned.compare([d], params, learned.scaled(norm, 0.0), frames=2, skip=2, tol=TOL, max_iter=CAP)
+    assert abs(r["plain"]["iterations_per_substep"] - r["learned"]["iterations_per_substep"]) <= 0.5, r
