@@ -473,7 +473,9 @@ def run_ours(args):
     ch, _ = p.model.solver_choice()
     solver = {1: "k_gs_cluster (one substep's Gauss-Seidel loop + velocity, one cluster launch)",
               2: f"k_gs_grid variant {ch[1]} ({ch[3]} threads, {ch[2]} CTAs/SM; one substep's Gauss-Seidel loop + velocity, one cooperative launch)",
-              3: "k_fem / k_bends per colour (one substep's Gauss-Seidel loop)"}.get(ch[0], "solver")
+              3: "k_fem / k_bends per colour (one substep's Gauss-Seidel loop)",
+              4: f"k_gs_band ({ch[3]} threads per CTA, one {p.model.band_plan()[0]}-CTA cluster of particle bands; "
+                 f"one substep's Gauss-Seidel loop + velocity, one cluster launch)"}.get(ch[0], "solver")
     kernel_names = {"gs_solve": solver,
                     "ccd_broad_ee": "k_bvh_refit + k_ccd_broad_ee + k_ccd_broad_coop (edge-edge swept-box LBVH "
                                     "refit and query: one walk per lane, long lists one warp per query)",

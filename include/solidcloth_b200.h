@@ -266,11 +266,15 @@ SCEXP int scMlpAdamStep(float* params, const float* grad, float* m, float* v, in
    cluster with the particles in distributed shared memory, when the cloth fits
    (up to 131,072 particles); false: one kernel per colour. Same results. */
 SCEXP void scSetClusterSolver(scModel model, bool val);
-/* Solver for the Gauss-Seidel loop (additions, no reference counterpart; all
-   give the same results): 0 = autotuned at the first step (default: the fastest
-   of the cluster kernel, the grid-resident cooperative kernel's variants and the
-   per-colour kernels, timed on this cloth), 1 = cluster kernel (clothes up to
-   131,072 particles), 2 = grid kernel (tuned variant), 3 = per-colour kernels.
+/* Solver for the Gauss-Seidel loop (additions, no reference counterpart).
+   0 = autotuned at the first step (default: the fastest of the cluster kernel,
+   the grid-resident cooperative kernel's variants and the per-colour kernels,
+   timed on this cloth), 1 = cluster kernel (clothes up to 131,072 particles),
+   2 = grid kernel (tuned variant), 3 = per-colour kernels, 4 = band-parallel
+   kernel (clothes with a band plan, scGetBandPlan; its thread count timed at
+   the first step). Modes 0-3 give identical results (the colour order); the
+   band kernel sweeps in its own order (interior records of every band, then
+   boundary records), which scGetConstraintOrder reports while it is in use.
    scSetClusterSolver(true/false) is mode 1 / 3. */
 SCEXP void scSetSolverMode(scModel model, int mode);
 /* force grid variant `variant` (0 .. scGetGridVariants()-1) with blocksPerSm CTAs per SM */
@@ -281,6 +285,13 @@ SCEXP void scSetClusterVariant(scModel model, int variant);
    tuneMs (4 floats per candidate: kind, variant, CTAs per SM, ms per substep)
    gets up to cap candidates of the last tuning; returns the candidate count */
 SCEXP int scGetSolverChoice(scModel model, int* out4, float* tuneMs, int cap);
+/* force the band-parallel kernel with 256 (variant 0), 512 (1) or 1024 (2)
+   threads per CTA (addition; SC_ERR_UNSUPPORTED without a band plan) */
+SCEXP void scSetBandVariant(scModel model, int variant);
+/* Band plan of the band-parallel solver (addition): out4 = {CTAs of its
+   cluster (0: no plan), particles per band, halo particles, 1 if it is the
+   solver in use}; returns 1 if the cloth has a plan. */
+SCEXP int scGetBandPlan(scModel model, int* out4);
 /* Continuous-collision broad phase walk (additions): 0 = one tree walk per query
    (lane), 1 = warp packets (32 neighbouring queries walk together, broadcast
    node loads), -1 (default) = timed at the first step and the faster kept. Same

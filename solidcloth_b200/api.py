@@ -147,6 +147,8 @@ SIGNATURES = {
     "scSetSolverMode": ([scModel, C.c_int], None),
     "scSetGridSolver": ([scModel, C.c_int, C.c_int], None),
     "scGetSolverChoice": ([scModel, _i, _f, C.c_int], C.c_int),
+    "scGetBandPlan": ([scModel, _i], C.c_int),
+    "scSetBandVariant": ([scModel, C.c_int], None),
     "scGetGridVariants": ([_i, C.c_int], C.c_int),
     "scSetBroadPhaseMode": ([scModel, C.c_int], None),
     "scGetBroadPhaseMode": ([scModel, _f], C.c_int),
@@ -332,7 +334,8 @@ class ClothModel:
         lib().scSetClusterSolver(self.h, bool(on))
 
     def set_solver_mode(self, mode: int):
-        """0 autotuned, 1 cluster kernel, 2 grid kernel, 3 per-colour kernels"""
+        """0 autotuned (default), 1 cluster kernel, 2 grid kernel, 3 per-colour
+        kernels, 4 band kernel (its own order)"""
         lib().scSetSolverMode(self.h, int(mode))
         _check("scSetSolverMode")
 
@@ -343,6 +346,18 @@ class ClothModel:
     def set_grid_solver(self, variant: int, blocks_per_sm: int):
         lib().scSetGridSolver(self.h, int(variant), int(blocks_per_sm))
         _check("scSetGridSolver")
+
+    def set_band_variant(self, variant: int):
+        """force the band kernel with 256 / 512 / 1024 threads per CTA (variant 0 / 1 / 2)"""
+        lib().scSetBandVariant(self.h, int(variant))
+        _check("scSetBandVariant")
+
+    def band_plan(self):
+        """(CTAs of the band solver's cluster or 0, particles per band, halo
+        particles, in use) — scGetBandPlan"""
+        out = np.zeros(4, np.int32)
+        lib().scGetBandPlan(self.h, out.ctypes.data_as(_i))
+        return tuple(int(x) for x in out)
 
     def solver_choice(self):
         """(kind, variant, CTAs per SM, threads) in use, and the last tuning's candidates"""

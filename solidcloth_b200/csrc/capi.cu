@@ -645,7 +645,7 @@ void scSetSelfCCD(scModel m, bool v) { if (M(m)) { M(m)->prm.ccd = v; M(m)->touc
 void scSetClusterSolver(scModel m, bool v) { scSetSolverMode(m, v ? SOLVE_CLUSTER : SOLVE_KERNELS); }
 void scSetSolverMode(scModel m, int mode)
 {
-    if (!M(m) || mode < SOLVE_AUTO || mode > SOLVE_KERNELS) { set_error(SC_ERR_ARG, "solver mode must be 0..3"); return; }
+    if (!M(m) || mode < SOLVE_AUTO || mode > SOLVE_BAND) { set_error(SC_ERR_ARG, "solver mode must be 0..4"); return; }
     M(m)->solverMode = mode;
     M(m)->tuned = false;
     M(m)->touch();
@@ -668,6 +668,16 @@ void scSetClusterVariant(scModel m, int variant)
     M(m)->touch();
     M(m)->tunedVersion = M(m)->paramVersion;
 }
+void scSetBandVariant(scModel m, int variant)
+{
+    if (!M(m) || variant < 0 || variant >= gs_band_variants()) { set_error(SC_ERR_ARG, "bad band solver variant"); return; }
+    if (!M(m)->bandPlan.valid) { set_error(SC_ERR_UNSUPPORTED, "the cloth has no band plan"); return; }
+    M(m)->solverMode = SOLVE_BAND;
+    M(m)->choice = {SOLVE_BAND, variant, 0, 0.f};
+    M(m)->tuned = true;
+    M(m)->touch();
+    M(m)->tunedVersion = M(m)->paramVersion;
+}
 int scGetSolverChoice(scModel m, int* out4, float* tuneMs, int cap)
 {
     if (!M(m)) return 0;
@@ -676,6 +686,8 @@ int scGetSolverChoice(scModel m, int* out4, float* tuneMs, int cap)
     {
         int th = 0, ft = 0, bt = 0;
         if (ch.kind == SOLVE_GRID) gs_grid_variant_info(ch.variant, th, ft, bt);
+        if (ch.kind == SOLVE_BAND) th = gs_band_threads(ch.variant);
+        if (ch.kind == SOLVE_CLUSTER) th = GS_THREADS;
         out4[0] = ch.kind; out4[1] = ch.variant; out4[2] = ch.blocksPerSm; out4[3] = th;
     }
     const auto& log = M(m)->tuneLog;
@@ -686,6 +698,19 @@ int scGetSolverChoice(scModel m, int* out4, float* tuneMs, int cap)
             tuneMs[4 * k + 2] = (float)log[k].blocksPerSm; tuneMs[4 * k + 3] = log[k].ms;
         }
     return (int)log.size();
+}
+int scGetBandPlan(scModel m, int* out4)
+{
+    if (!M(m)) return 0;
+    const auto& bp = M(m)->bandPlan;
+    if (out4)
+    {
+        out4[0] = bp.valid ? bp.clusterSize : 0;
+        out4[1] = bp.valid ? (1 << bp.shift) : 0;
+        out4[2] = bp.valid ? bp.halo : 0;
+        out4[3] = M(m)->band_active() ? 1 : 0;
+    }
+    return bp.valid ? 1 : 0;
 }
 void scSetBroadPhaseMode(scModel m, int mode)
 {
@@ -845,8 +870,14 @@ int scGetSolverIterations(scModel m)
 int scGetConstraintOrder(scModel m, int kind, int* order, int* colourStart)
 {
     if (!M(m)) return 0;
-    const std::vector<int>& o = kind == 0 ? M(m)->triOrder : kind == 1 ? M(m)->bendOrder : M(m)->linkOrder;
-    const std::vector<int>& s = kind == 0 ? M(m)->triColourStart : kind == 1 ? M(m)->bendColourStart : M(m)->linkColourStart;
+    // the band solver's order while it is the one in use (solver mode 4 on a
+    // cloth with a band plan), else the colour order of the other solvers
+    const bool band = M(m)->band_active();
+    const auto& bp = M(m)->bandPlan;
+    const std::vector<int>& o = band ? (kind == 0 ? bp.triOrder : kind == 1 ? bp.bendOrder : bp.linkOrder)
+                                     : (kind == 0 ? M(m)->triOrder : kind == 1 ? M(m)->bendOrder : M(m)->linkOrder);
+    const std::vector<int>& s = band ? (kind == 0 ? bp.triStart : kind == 1 ? bp.bendStart : bp.linkStart)
+                                     : (kind == 0 ? M(m)->triColourStart : kind == 1 ? M(m)->bendColourStart : M(m)->linkColourStart);
     if (s.empty()) return 0;
     if (order) memcpy(order, o.data(), sizeof(int) * o.size());
     if (colourStart) memcpy(colourStart, s.data(), sizeof(int) * s.size());

@@ -37,6 +37,16 @@ const char* last_error_string() { return g_errMsg.c_str(); }
         }                                                                              \
     } while (0)
 
+// the same for functions without a result
+#define SC_CUDA_V(x)                                                                   \
+    do {                                                                               \
+        cudaError_t e_ = (x);                                                          \
+        if (e_ != cudaSuccess) {                                                       \
+            set_error(SC_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_));   \
+            return;                                                                    \
+        }                                                                              \
+    } while (0)
+
 // -------------------------------------------------------------------- mesh
 // Mesh::ComputeNormals, angle weighted (Geometry/Mesh.cpp:10-63)
 void HMesh::compute_normals()
@@ -740,6 +750,179 @@ void ClothModel::colour_constraints()
     }
 }
 
+// Band plan of the band-parallel solver (k_gs_band): the largest cluster (16, 8,
+// 4 or 2 CTAs) whose bands of 2^shift consecutive particles admit every FEM
+// triangle, bend and link either as an interior record of the band of its lowest
+// particle or as a boundary record reaching only the first `halo` particles of
+// the next band, where every band's boundary records touch their own band at
+// offsets >= halo. Grid clothes (particles row by row) satisfy it once a band
+// holds a few rows; batches never use it.
+void ClothModel::build_band_plan()
+{
+    bandPlan = BandPlan{};
+    if (!instV.empty() || N < 64) return;
+    struct Cls
+    {
+        int arity;
+        const std::vector<int>* order;
+        const std::vector<int>* start;
+        std::function<void(int, uint32_t*)> get;
+    };
+    const Cls cls[3] = {
+        {3, &triOrder, &triColourStart, [&](int i, uint32_t* v) { v[0] = tris[i].i1; v[1] = tris[i].i2; v[2] = tris[i].i3; }},
+        {4, &bendOrder, &bendColourStart, [&](int i, uint32_t* v) { v[0] = bends[i].x; v[1] = bends[i].y; v[2] = bends[i].z; v[3] = bends[i].w; }},
+        {2, &linkOrder, &linkColourStart, [&](int i, uint32_t* v) { v[0] = links[i].x; v[1] = links[i].y; }}};
+    for (int cs : {16, 8, 4, 2})
+    {
+        int shift = 0;
+        while (((size_t)1 << shift) * cs < (size_t)N) shift++;
+        const int vpc = 1 << shift;
+        if ((size_t)vpc * (cs - 1) >= (size_t)N) continue;            // a band would be empty
+        if ((size_t)vpc * sizeof(float4) > 128 * 1024) continue;
+        // part (0 interior, 1 boundary) of every record, the halo, and per band the
+        // smallest own-band offset its boundary records touch
+        int halo = 0;
+        bool ok = true;
+        std::vector<int> minOwn(cs, vpc);
+        std::vector<std::vector<uint8_t>> part(3);
+        for (int k = 0; k < 3 && ok; k++)
+        {
+            const Cls& q = cls[k];
+            const int n = (int)q.order->size();
+            part[k].assign(n, 0);
+            for (int r = 0; r < n && ok; r++)
+            {
+                uint32_t v[4];
+                q.get(r, v);
+                uint32_t lo = v[0], hi = v[0];
+                for (int a = 1; a < q.arity; a++) { lo = std::min(lo, v[a]); hi = std::max(hi, v[a]); }
+                const int b = (int)(lo >> shift), hb = (int)(hi >> shift);
+                if (hb == b) continue;
+                if (hb != b + 1) { ok = false; break; }
+                part[k][r] = 1;
+                for (int a = 0; a < q.arity; a++)
+                {
+                    const int o = (int)(v[a] & (uint32_t)(vpc - 1));
+                    if ((int)(v[a] >> shift) == b + 1) halo = std::max(halo, o + 1);
+                    else minOwn[b] = std::min(minOwn[b], o);
+                }
+            }
+        }
+        for (int b = 0; b < cs && ok; b++) ok = minOwn[b] >= halo;
+        if (!ok || halo > vpc) continue;
+        const int haloPad = (halo + 15) & ~15;
+        if (!gs_band_fits(cs, (size_t)(vpc + haloPad) * sizeof(float4))) continue;
+        // records in (band, part, colour, colour order) order with their offsets,
+        // and the reported order (part, colour, band, colour order)
+        BandPlan& bp = bandPlan;
+        bp.clusterSize = cs; bp.shift = shift; bp.halo = halo;
+        std::vector<int>* outOrder[3] = {&bp.triOrder, &bp.bendOrder, &bp.linkOrder};
+        std::vector<int>* outStart[3] = {&bp.triStart, &bp.bendStart, &bp.linkStart};
+        int* most[3] = {&bp.femMax, &bp.bendMax, &bp.linkMax};
+        std::vector<int> offs[3];
+        std::vector<int> devOrder[3];
+        for (int k = 0; k < 3; k++)
+        {
+            const Cls& q = cls[k];
+            const int nCol = std::max(1, (int)q.start->size() - 1), n = (int)q.order->size();
+            std::vector<int> colOf(n, 0), bandOf(n, 0);
+            for (int c = 0; c + 1 < (int)q.start->size(); c++)
+                for (int j = (*q.start)[c]; j < (*q.start)[c + 1]; j++) colOf[(*q.order)[j]] = c;
+            for (int r = 0; r < n; r++)
+            {
+                uint32_t v[4];
+                q.get(r, v);
+                uint32_t lo = v[0];
+                for (int a = 1; a < q.arity; a++) lo = std::min(lo, v[a]);
+                bandOf[r] = (int)(lo >> shift);
+            }
+            // position of each record in the colour order: ties keep it
+            std::vector<int> rank(n, 0);
+            for (int j = 0; j < n; j++) rank[(*q.order)[j]] = j;
+            std::vector<int> idx(n);
+            std::iota(idx.begin(), idx.end(), 0);
+            auto key = [&](int r) { return ((int64_t)(bandOf[r] * 2 + part[k][r]) * nCol + colOf[r]) * (int64_t)(n + 1) + rank[r]; };
+            std::sort(idx.begin(), idx.end(), [&](int x, int y) { return key(x) < key(y); });
+            devOrder[k] = idx;
+            offs[k].assign((size_t)cs * 2 * nCol + 1, 0);
+            for (int r = 0; r < n; r++) offs[k][(size_t)(bandOf[r] * 2 + part[k][r]) * nCol + colOf[r] + 1]++;
+            for (size_t g = 1; g < offs[k].size(); g++) offs[k][g] += offs[k][g - 1];
+            *most[k] = 0;
+            for (int b = 0; b < cs; b++) *most[k] = std::max(*most[k], offs[k][(size_t)(b + 1) * 2 * nCol] - offs[k][(size_t)b * 2 * nCol]);
+            auto key2 = [&](int r) { return ((int64_t)(part[k][r] * nCol + colOf[r]) * cs + bandOf[r]) * (int64_t)(n + 1) + rank[r]; };
+            std::vector<int> rep(n);
+            std::iota(rep.begin(), rep.end(), 0);
+            std::sort(rep.begin(), rep.end(), [&](int x, int y) { return key2(x) < key2(y); });
+            *outOrder[k] = rep;
+            outStart[k]->assign(1, 0);
+            for (int g = 0; g < 2 * nCol; g++)
+            {
+                int cnt = 0;
+                for (int b = 0; b < cs; b++)
+                    cnt += offs[k][(size_t)(b * 2 + g / nCol) * nCol + g % nCol + 1] - offs[k][(size_t)(b * 2 + g / nCol) * nCol + g % nCol];
+                if (cnt) outStart[k]->push_back(outStart[k]->back() + cnt);
+            }
+        }
+        // device arrays
+        BandView& v = bp.view;
+        v.shift = shift; v.halo = halo;
+        v.nFemCol = std::max(1, (int)triColourStart.size() - 1);
+        v.nBendCol = std::max(1, (int)bendColourStart.size() - 1);
+        v.nLinkCol = std::max(1, (int)linkColourStart.size() - 1);
+        int* doff[3];
+        for (int k = 0; k < 3; k++)
+        {
+            doff[k] = (int*)dalloc(sizeof(int) * offs[k].size());
+            SC_CUDA_V(cudaMemcpy(doff[k], offs[k].data(), sizeof(int) * offs[k].size(), cudaMemcpyHostToDevice));
+        }
+        v.femOff = doff[0]; v.bendOff = doff[1]; v.linkOff = doff[2];
+        const int T = (int)tris.size(), B = (int)bends.size(), L = (int)links.size();
+        std::vector<float4> fem(3 * (size_t)std::max(1, T));
+        for (int j = 0; j < T; j++)
+        {
+            const FemHost& t = tris[devOrder[0][j]];
+            fem[3 * j] = make_float4(bits_f(t.i1), bits_f(t.i2), bits_f(t.i3), t.du1);
+            fem[3 * j + 1] = make_float4(t.du2, t.dv1, t.dv2, t.invDet);
+            fem[3 * j + 2] = make_float4(t.lu2, t.lv2, t.lu0 * t.lv0, t.area);
+        }
+        std::vector<uint4> bd(std::max(1, B));
+        for (int j = 0; j < B; j++) bd[j] = bends[devOrder[1][j]];
+        std::vector<float4> lk(std::max(1, L));
+        for (int j = 0; j < L; j++)
+        {
+            const int li = devOrder[2][j];
+            lk[j] = make_float4(bits_f(links[li].x), bits_f(links[li].y), linkRest[li].x, linkRest[li].y);
+        }
+        float4* dfem = (float4*)dalloc(sizeof(float4) * fem.size());
+        uint4* dbend = (uint4*)dalloc(sizeof(uint4) * bd.size());
+        float4* dlink = (float4*)dalloc(sizeof(float4) * lk.size());
+        SC_CUDA_V(cudaMemcpy(dfem, fem.data(), sizeof(float4) * fem.size(), cudaMemcpyHostToDevice));
+        SC_CUDA_V(cudaMemcpy(dbend, bd.data(), sizeof(uint4) * bd.size(), cudaMemcpyHostToDevice));
+        SC_CUDA_V(cudaMemcpy(dlink, lk.data(), sizeof(float4) * lk.size(), cudaMemcpyHostToDevice));
+        v.fem = dfem; v.bend = dbend; v.link = dlink;
+        v.femMax = bp.femMax; v.bendMax = bp.bendMax; v.linkMax = bp.linkMax;
+        bp.valid = true;
+        return;
+    }
+}
+
+// dynamic shared memory of the band solver: own band, halo and the staged
+// records; chooses what to stage (FEM, then bends, then links) within the limit
+size_t ClothModel::band_smem()
+{
+    BandView& v = bandPlan.view;
+    size_t bytes = ((size_t)(1 << bandPlan.shift) + (size_t)((bandPlan.halo + 15) & ~15)) * sizeof(float4);
+    v.stageFem = v.stageBend = v.stageLink = 0;
+    if (!prm.stageRecords) return bytes;
+    const size_t fem = (size_t)3 * bandPlan.femMax * sizeof(float4), bend = (size_t)bandPlan.bendMax * sizeof(uint4),
+                 link = (size_t)bandPlan.linkMax * sizeof(float4);
+    auto fits = [&](size_t extra) { return bytes + extra <= (size_t)BAND_SMEM_MAX && gs_band_fits(bandPlan.clusterSize, bytes + extra); };
+    if (prm.fem && fits(fem)) { bytes += fem; v.stageFem = 1; }
+    if (prm.dihedral && fits(bend)) { bytes += bend; v.stageBend = 1; }
+    if (!prm.fem && fits(link)) { bytes += link; v.stageLink = 1; }
+    return bytes;
+}
+
 bool ClothModel::upload_topology(const HMesh& mesh)
 {
     release_device();
@@ -786,6 +969,7 @@ bool ClothModel::upload_topology(const HMesh& mesh)
     uint4* dbend = (uint4*)dalloc(sizeof(uint4) * B);
     if (B) SC_CUDA(cudaMemcpy(dbend, bd.data(), sizeof(uint4) * B, cudaMemcpyHostToDevice));
     dc.bend = dbend;
+    build_band_plan();
     // static colours of triangles (their FEM colours) and of collision-mesh edges
     // (greedy in index order; grids: a period-4 pattern when it needs fewer) for
     // the triangle and edge collider contacts
@@ -1769,6 +1953,9 @@ bool ClothPatch::record_solve(cudaStream_t s, const SolverParams& P, const Solve
         plan.nLinkCol = (int)m.linkColourStart.size() - 1;
         for (size_t k = 0; k < m.linkColourStart.size(); k++) plan.linkStart[k] = m.linkColourStart[k];
     }
+    if (ch.kind == SOLVE_BAND && m.band_active() &&
+        ops.band(s, c, P, b, plan, m.bandPlan.view, m.bandPlan.clusterSize, m.band_smem(), ch.variant))
+        return true;                                                 // includes the velocity update
     int shift = 0;
     size_t smem = 0;
     const int cluster = (ch.kind == SOLVE_CLUSTER && planFits) ? ops.cluster_size(m.N, shift, smem) : 0;
@@ -1842,7 +2029,8 @@ bool ClothPatch::autotune(float h)
     const SolverParams P = m.solver_params(h);
     std::vector<int> key = {m.N, m.dc.T, m.dc.B, m.prm.iterations, m.prm.dihedral, m.prm.fem, m.prm.fixedIterations,
                             (int)m.buf.numVColl, m.prm.bendFreq, (int)m.prm.stageRecords, m.solverMode,
-                            (int)m.prm.ccd, m.broadMode, (int)m.prm.fastMath};
+                            (int)m.prm.ccd, m.broadMode, (int)m.prm.fastMath, (int)m.band_active(),
+                            m.bandPlan.clusterSize, m.bandPlan.halo};
     key.insert(key.end(), m.triColourStart.begin(), m.triColourStart.end());
     key.insert(key.end(), m.bendColourStart.begin(), m.bendColourStart.end());
     {
@@ -1861,9 +2049,13 @@ bool ClothPatch::autotune(float h)
     int shift = 0; size_t smem = 0;
     const bool fits = m.triColourStart.size() <= 65 && m.bendColourStart.size() <= 65 && m.linkColourStart.size() <= 65;
     const SolverOps& ops = solver_ops(m.prm.fastMath);
-    if (fits && (m.solverMode == SOLVE_AUTO || m.solverMode == SOLVE_CLUSTER) && ops.cluster_size(m.N, shift, smem) > 0)
+    // the band solver (mode 4) sweeps in its own order: only its thread counts are timed
+    const bool band = m.band_active();
+    if (band)
+        for (int v = 0; v < gs_band_variants(); v++) cand.push_back({SOLVE_BAND, v, 0, 0.f});
+    if (!band && fits && (m.solverMode == SOLVE_AUTO || m.solverMode == SOLVE_CLUSTER) && ops.cluster_size(m.N, shift, smem) > 0)
         for (int v = 0; v < gs_cluster_variants(); v++) cand.push_back({SOLVE_CLUSTER, v, 0, 0.f});
-    if (fits && (m.solverMode == SOLVE_AUTO || m.solverMode == SOLVE_GRID))
+    if (!band && fits && (m.solverMode == SOLVE_AUTO || m.solverMode == SOLVE_GRID))
         for (int v = 0; v < gs_grid_variants(); v++)
         {
             const int mb = ops.grid_max_blocks_per_sm(v);
@@ -1875,7 +2067,7 @@ bool ClothPatch::autotune(float h)
                     if (!dup) cand.push_back({SOLVE_GRID, v, bps, 0.f});
                 }
         }
-    if (m.solverMode == SOLVE_AUTO) cand.push_back({SOLVE_KERNELS, 0, 0, 0.f});
+    if (!band && m.solverMode == SOLVE_AUTO) cand.push_back({SOLVE_KERNELS, 0, 0, 0.f});
     if (cand.empty()) cand.push_back({SOLVE_KERNELS, 0, 0, 0.f});
     const size_t bytes = sizeof(float4) * (size_t)m.N;
     float4* backup = nullptr;

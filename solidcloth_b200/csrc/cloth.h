@@ -109,7 +109,7 @@ struct HostParams
 struct BatchColl { std::shared_ptr<Collidable> coll; int vBegin, vCount, inst; };
 
 // solver selection (autotuned unless forced)
-enum SolverKind { SOLVE_AUTO = 0, SOLVE_CLUSTER = 1, SOLVE_GRID = 2, SOLVE_KERNELS = 3 };
+enum SolverKind { SOLVE_AUTO = 0, SOLVE_CLUSTER = 1, SOLVE_GRID = 2, SOLVE_KERNELS = 3, SOLVE_BAND = 4 };
 struct SolverChoice { int kind, variant, blocksPerSm; float ms; int broad; };
 
 struct FemHost { uint32_t i1, i2, i3; float du1, du2, dv1, dv2, det, invDet, lu0, lv0, su, sv, lu2, lv2, area; };
@@ -199,6 +199,21 @@ public:
     float broadMs[BROAD_WALKS] = {};            // tuned times of the broad-phase walks
     void colour_constraints();
     void touch() { paramVersion++; }
+
+    // band-parallel solver (k_gs_band): the plan, when the cloth admits one
+    // (build_band_plan); used when solver mode 4 is set
+    struct BandPlan
+    {
+        bool valid = false;
+        int clusterSize = 0, shift = 0, halo = 0;
+        int femMax = 0, bendMax = 0, linkMax = 0;          // most records of one band per class
+        std::vector<int> triOrder, bendOrder, linkOrder;   // its Gauss-Seidel order, (part, colour, band, record)
+        std::vector<int> triStart, bendStart, linkStart;   // (part, colour) group starts of that order
+        BandView view{};                                   // device arrays (in allocs)
+    } bandPlan;
+    void build_band_plan();
+    bool band_active() const { return bandPlan.valid && solverMode == SOLVE_BAND; }
+    size_t band_smem();
 };
 
 class ClothPatch

@@ -150,6 +150,35 @@ int gs_grid_max_blocks_per_sm(int variant);
 bool launch_gs_grid(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b, GsPlan plan,
                     int variant, int blocksPerSm);
 
+// band-parallel solver (one cluster per cloth, one launch per substep): the
+// particles in contiguous bands of 2^shift, one per CTA, resident in shared
+// memory; each class's records split per band into interior records (every
+// particle in the band) and boundary records (lowest particle in the band, the
+// others in it or among the first `halo` particles of the next band)
+struct BandView
+{
+    int shift, halo;
+    int nFemCol, nBendCol, nLinkCol;
+    // record offsets per (band, part, colour): [(band * 2 + part) * nCol + colour], nBands * 2 * nCol + 1 entries
+    const int* femOff;
+    const int* bendOff;
+    const int* linkOff;
+    // records in (band, part, colour, colour order) order: FEM 3 float4, bends uint4, links float4
+    const float4* fem;
+    const uint4* bend;
+    const float4* link;
+    // records staged in shared memory (1) or read through the non-coherent path (0),
+    // and the most records one band holds (the staging layout)
+    int stageFem, stageBend, stageLink;
+    int femMax, bendMax, linkMax;
+};
+constexpr int BAND_SMEM_MAX = 220 * 1024;  // dynamic shared memory per CTA of the band solver
+// threads-per-CTA variants of the band solver (same order, bit-identical results)
+int gs_band_variants();
+int gs_band_threads(int variant);
+// true if a cluster of clusterSize CTAs with smem bytes each can run the band solver
+bool gs_band_fits(int clusterSize, size_t smem);
+
 // The solver's entry points as one table per build of solver.cuh: IEEE division
 // and square root without FMA contraction (bit-exact with the reference's
 // operation order, the check-mode build) or the fast build (FMA contraction,
@@ -167,6 +196,8 @@ struct SolverOps
     void (*cluster)(cudaStream_t, const DevCloth&, const SolverParams&, const Buffers&, GsPlan, int, size_t, int);
     int (*grid_max_blocks_per_sm)(int);
     bool (*grid)(cudaStream_t, const DevCloth&, const SolverParams&, const Buffers&, GsPlan, int, int);
+    bool (*band)(cudaStream_t, const DevCloth&, const SolverParams&, const Buffers&, GsPlan, const BandView&, int, size_t,
+                 int);
 };
 const SolverOps& solver_ops(bool fast);
 

@@ -683,6 +683,107 @@ __device__ __forceinline__ float cluster_bends(const PA& pa, const DevCloth& c, 
     return err;
 }
 
+// The multi-particle contact classes inside a cluster-resident solver (edge,
+// triangle, self vertex-triangle, self edge-edge; Physics/ClothPBD.cpp:349-352):
+// each colour split into one contiguous chunk per CTA, particles through
+// distributed shared memory, a cluster barrier after every colour.
+template <class PA>
+__device__ __forceinline__ void cluster_contact_classes(const PA& pa, const DevCloth& c, const SolverParams& P,
+                                                        const Buffers& b, const ColourArgs& ca, int rank, int nRank,
+                                                        bool track, float* sErr)
+{
+    cg::cluster_group cl = cg::this_cluster();
+    for (int cls = 0; cls < 4; cls++)
+    {
+        const ClassView& cv = ca.cls[cls];
+        const int n = *cv.count;
+        if (n == 0) continue;
+        for (int col = 0; col < MAX_COLOURS; col++)
+        {
+            const int s0 = cv.start[col], s1 = cv.start[col + 1];
+            if (s0 == s1) continue;
+            if (col == MAX_COLOURS - 1)
+            {
+                // colours exhausted: one thread, list order (as the oracle)
+                if (rank == 0 && threadIdx.x == 0)
+                    for (int i = 0; i < n; i++)
+                        if (cv.colour[i] == MAX_COLOURS - 1)
+                        {
+                            float e = solve_contact(pa, c, P, b, cls, i);
+                            if (track && e > 0.f) atomicMax((int*)&sErr[4 + cls], __float_as_int(e));
+                        }
+            }
+            else
+            {
+                const int chunk = (s1 - s0 + nRank - 1) / nRank;
+                const int a = s0 + rank * chunk, e = min(s1, a + chunk);
+                for (int j = a + threadIdx.x; j < e; j += blockDim.x)
+                {
+                    float err = solve_contact(pa, c, P, b, cls, __ldg(&cv.order[j]));
+                    if (track && err > 0.f) atomicMax((int*)&sErr[4 + cls], __float_as_int(err));
+                }
+            }
+            cl.sync();
+        }
+    }
+}
+
+// End of one Gauss-Seidel iteration of a cluster-resident solver whose CTA holds
+// the particles [v0, v0 + vpc) in sPos: the iteration count, the update residual
+// test (residual-target mode) and the reference's exit test
+// (Physics/ClothPBD.cpp:354-361). True when the loop ends.
+__device__ __forceinline__ bool cluster_iteration_end(const DevCloth& c, const SolverParams& P, const float4* sPos,
+                                                      int v0, uint32_t vpc, int rank, int k, bool track, float* sErr)
+{
+    cg::cluster_group cl = cg::this_cluster();
+    if (threadIdx.x == 0 && rank == 0) c.scal[9] = (float)(k + 1);
+    if (P.resTol > 0.f)
+    {
+        // residual-target mode: the largest displacement of this iteration (own
+        // particles, against the snapshot), cluster-wide; then the next snapshot
+        float r = 0.f;
+        for (uint32_t v = threadIdx.x; v < vpc; v += blockDim.x)
+        {
+            const int g = v0 + (int)v;
+            if (g >= c.N) continue;
+            const float4 x = sPos[v], x0 = c.xsnap[g];
+            const float dx = x.x - x0.x, dy = x.y - x0.y, dz = x.z - x0.z;
+            r = fmaxf(r, sqrtf(dx * dx + dy * dy + dz * dz) * P.resScale);
+            c.xsnap[g] = x;
+        }
+        const unsigned u = __reduce_max_sync(0xffffffffu, __float_as_uint(r));
+        unsigned* word = reinterpret_cast<unsigned*>(c.scal + 11);
+        if ((threadIdx.x & 31) == 0 && u) atomicMax(word, u);
+        cl.sync();
+        const float res = __uint_as_float(__ldcg(word));
+        cl.sync();
+        if (rank == 0 && threadIdx.x == 0) *word = 0u;
+        if (res <= P.resTol) return true;
+    }
+    if (track)
+    {
+        // SolveGS exit test (Physics/ClothPBD.cpp:354-361) on cluster-wide maxima
+        if (threadIdx.x < 8 && threadIdx.x >= 1 && sErr[threadIdx.x] > 0.f)
+            atomic_max_pos(&c.scal[threadIdx.x], sErr[threadIdx.x]);
+        cl.sync();
+        if (rank == 0 && threadIdx.x == 0)
+        {
+            const float eps = 0.01f;
+            float cb = c.scal[2], cv = c.scal[3], ce = c.scal[4], ct = c.scal[5], sct = c.scal[6], see = c.scal[7];
+            const float clk = P.fem ? 0.f : c.scal[1];
+            if (clk < 0.05f && cb < 0.005f && see < P.selfThreshold && sct < P.selfThreshold && cv < eps && ce < eps && ct < eps)
+                c.scal[8] = 1.f;
+            c.scal[1] = 0.f;
+            for (int s = 3; s < 8; s++) c.scal[s] = 0.f;          // per-iteration maxima
+            if ((k + 1) % P.bendFreq == 0) c.scal[2] = 0.f;       // recomputed by the next bend sweep
+        }
+        if (threadIdx.x < 8) sErr[threadIdx.x] = 0.f;
+        cl.sync();
+        if (__ldcg(&c.scal[8]) != 0.f) return true;
+    }
+    return false;
+}
+
 template <int TILE>
 __global__ void __launch_bounds__(GS_THREADS) k_gs_cluster(DevCloth c, SolverParams P, Buffers b, ColourArgs ca, GsPlan plan)
 {
@@ -798,88 +899,225 @@ __global__ void __launch_bounds__(GS_THREADS) k_gs_cluster(DevCloth c, SolverPar
             }
             cl.sync();
         }
-        for (int cls = 0; cls < 4; cls++)
-        {
-            const ClassView& cv = ca.cls[cls];
-            const int n = *cv.count;
-            if (n == 0) continue;
-            for (int col = 0; col < MAX_COLOURS; col++)
-            {
-                const int s0 = cv.start[col], s1 = cv.start[col + 1];
-                if (s0 == s1) continue;
-                if (col == MAX_COLOURS - 1)
-                {
-                    // colours exhausted: one thread, list order (as the oracle)
-                    if (rank == 0 && threadIdx.x == 0)
-                        for (int i = 0; i < n; i++)
-                            if (cv.colour[i] == MAX_COLOURS - 1)
-                            {
-                                float e = solve_contact(pa, c, P, b, cls, i);
-                                if (track && e > 0.f) atomicMax((int*)&sErr[4 + cls], __float_as_int(e));
-                            }
-                }
-                else
-                {
-                    int a, e;
-                    range(s0, s1, a, e);
-                    for (int j = a + threadIdx.x; j < e; j += blockDim.x)
-                    {
-                        float err = solve_contact(pa, c, P, b, cls, __ldg(&cv.order[j]));
-                        if (track && err > 0.f) atomicMax((int*)&sErr[4 + cls], __float_as_int(err));
-                    }
-                }
-                cl.sync();
-            }
-        }
-        if (threadIdx.x == 0 && rank == 0) c.scal[9] = (float)(k + 1);
-        if (P.resTol > 0.f)
-        {
-            // residual-target mode: the largest displacement of this iteration (own
-            // particles, against the snapshot), cluster-wide; then the next snapshot
-            float r = 0.f;
-            for (uint32_t v = threadIdx.x; v < vpc; v += blockDim.x)
-            {
-                const int g = v0 + (int)v;
-                if (g >= c.N) continue;
-                const float4 x = sPos[v], x0 = c.xsnap[g];
-                const float dx = x.x - x0.x, dy = x.y - x0.y, dz = x.z - x0.z;
-                r = fmaxf(r, sqrtf(dx * dx + dy * dy + dz * dz) * P.resScale);
-                c.xsnap[g] = x;
-            }
-            const unsigned u = __reduce_max_sync(0xffffffffu, __float_as_uint(r));
-            unsigned* word = reinterpret_cast<unsigned*>(c.scal + 11);
-            if ((threadIdx.x & 31) == 0 && u) atomicMax(word, u);
-            cl.sync();
-            const float res = __uint_as_float(__ldcg(word));
-            cl.sync();
-            if (rank == 0 && threadIdx.x == 0) *word = 0u;
-            if (res <= P.resTol) break;
-        }
-        if (track)
-        {
-            // SolveGS exit test (Physics/ClothPBD.cpp:354-361) on cluster-wide maxima
-            if (threadIdx.x < 8 && threadIdx.x >= 1 && sErr[threadIdx.x] > 0.f)
-                atomic_max_pos(&c.scal[threadIdx.x], sErr[threadIdx.x]);
-            cl.sync();
-            if (rank == 0 && threadIdx.x == 0)
-            {
-                const float eps = 0.01f;
-                float cb = c.scal[2], cv = c.scal[3], ce = c.scal[4], ct = c.scal[5], sct = c.scal[6], see = c.scal[7];
-                const float clk = P.fem ? 0.f : c.scal[1];
-                if (clk < 0.05f && cb < 0.005f && see < P.selfThreshold && sct < P.selfThreshold && cv < eps && ce < eps && ct < eps)
-                    c.scal[8] = 1.f;
-                c.scal[1] = 0.f;
-                for (int s = 3; s < 8; s++) c.scal[s] = 0.f;          // per-iteration maxima
-                if ((k + 1) % P.bendFreq == 0) c.scal[2] = 0.f;       // recomputed by the next bend sweep
-            }
-            if (threadIdx.x < 8) sErr[threadIdx.x] = 0.f;
-            cl.sync();
-            if (__ldcg(&c.scal[8]) != 0.f) break;
-        }
+        cluster_contact_classes(pa, c, P, b, ca, rank, nRank, track, sErr);
+        if (cluster_iteration_end(c, P, sPos, v0, vpc, rank, k, track, sErr)) break;
     }
     if (rank == 0 && threadIdx.x == 0) c.scal[10] += c.scal[9];
     // write back own particles and update their velocities (ClothPBD.cpp:314-321)
     for (uint32_t v = threadIdx.x; v < vpc; v += blockDim.x)
+    {
+        const int g = v0 + (int)v;
+        if (g >= c.N) continue;
+        const float4 p = sPos[v];
+        c.pos[g] = p;
+        if (p.w == 0.f) continue;
+        const float4 q = c.prev[g];
+        V3 vel = P.invH * (mk(p.x, p.y, p.z) - mk(q.x, q.y, q.z));
+        c.vel[g] = make_float4(vel.x, vel.y, vel.z, 0.f);
+    }
+}
+
+// ---------------------------------------------------- band-parallel solver
+// One cluster per cloth; CTA r owns the particles [r 2^shift, (r + 1) 2^shift)
+// (a band), resident in its shared memory for the whole substep. Each class's
+// records (FEM triangles, bends, links) are split per band into interior
+// records (all particles in the band) and boundary records (lowest particle in
+// the band, the others in it or among the first `halo` particles of the next
+// band). A sweep runs, in every CTA at once, the band's interior records colour
+// by colour on its own shared memory with CTA barriers between colours; then,
+// after a cluster barrier, each CTA copies the next band's first `halo`
+// particles into a local buffer, runs its boundary records colour by colour on
+// its band and that buffer, and copies the buffer back before a second cluster
+// barrier. Interior record sets of different bands share no particle; neither
+// do boundary sets, because the host admits a plan only if the boundary records
+// of every band touch their own band at offsets >= halo (beyond the part the
+// previous band copies). The launch therefore computes the sequential
+// Gauss-Seidel sweep in the order (part, band, colour, record), which equals
+// (part, colour, band, record): two colour phases per class sweep end in a
+// cluster barrier instead of every colour. The contact classes run as in the
+// cluster solver (chunks, distributed shared memory, a cluster barrier per
+// colour); vertex contacts touch one particle each and run on the owner CTA.
+
+// particle accessor of a band CTA: its own band, then the copied head of the next
+struct BandPos
+{
+    float4* own;
+    float4* halo;
+    uint32_t v0, v1;
+    __device__ __forceinline__ float4* addr(uint32_t g) const { return g < v1 ? own + (g - v0) : halo + (g - v1); }
+    __device__ __forceinline__ float4 ld(uint32_t g) const { return *addr(g); }
+    __device__ __forceinline__ void st(uint32_t g, float4 x) const { *addr(g) = x; }
+};
+
+// one record of class KIND (0 FEM: three float4; 1 bend: a uint4; 2 link: a
+// float4), from shared memory (staged: index relative to the band's first
+// record) or through the non-coherent path
+template <int KIND>
+struct BandRec { float4 r[KIND == 0 ? 3 : 1]; };
+
+template <int KIND>
+__device__ __forceinline__ BandRec<KIND> band_load(const BandView& bv, const float4* staged, int base, int j)
+{
+    BandRec<KIND> q;
+    if constexpr (KIND == 0)
+    {
+        if (staged)
+        {
+            const float4* r = staged + 3 * (j - base);
+            q.r[0] = r[0]; q.r[1] = r[1]; q.r[2] = r[2];
+        }
+        else
+        {
+            q.r[0] = __ldg(&bv.fem[3 * j]); q.r[1] = __ldg(&bv.fem[3 * j + 1]); q.r[2] = __ldg(&bv.fem[3 * j + 2]);
+        }
+    }
+    else if constexpr (KIND == 1)
+        q.r[0] = staged ? staged[j - base] : __ldg(reinterpret_cast<const float4*>(bv.bend) + j);
+    else
+        q.r[0] = staged ? staged[j - base] : __ldg(&bv.link[j]);
+    return q;
+}
+
+template <int KIND>
+__device__ __forceinline__ float band_apply(const BandPos& pa, const SolverParams& P, const BandRec<KIND>& q)
+{
+    if constexpr (KIND == 0)
+    {
+        fem_project(pa, q.r[0], q.r[1], q.r[2], P);
+        return 0.f;
+    }
+    else if constexpr (KIND == 1)
+    {
+        const float4 f = q.r[0];
+        return bend_project(pa, make_uint4(__float_as_uint(f.x), __float_as_uint(f.y), __float_as_uint(f.z),
+                                           __float_as_uint(f.w)), P);
+    }
+    else
+        return link_project(pa, q.r[0], P);
+}
+
+// one sweep of a class over the cluster: 2 nCol steps (interior colours, then
+// boundary colours); each thread's first record of the next step is loaded
+// before the current step's projections, so its latency overlaps them. Returns
+// this thread's largest projection error.
+template <int KIND, int NT>
+__device__ __forceinline__ float band_sweep(const BandPos& pa, const SolverParams& P, const BandView& bv,
+                                            const float4* staged, int band, int nb, float4* nextHead)
+{
+    cg::cluster_group cl = cg::this_cluster();
+    const int nCol = KIND == 0 ? bv.nFemCol : KIND == 1 ? bv.nBendCol : bv.nLinkCol;
+    const int* off = (KIND == 0 ? bv.femOff : KIND == 1 ? bv.bendOff : bv.linkOff) + band * 2 * nCol;
+    const int base = __ldg(&off[0]);
+    const int tid = (int)threadIdx.x;
+    const bool hasNext = band + 1 < nb;
+    float err = 0.f;
+    int a = __ldg(&off[0]), e = __ldg(&off[1]);
+    BandRec<KIND> cur;
+    if (a + tid < e) cur = band_load<KIND>(bv, staged, base, a + tid);
+    for (int step = 0; step < 2 * nCol; step++)
+    {
+        // off[step] .. off[step + 1] is this band's step: (part, colour) = (step / nCol, step % nCol)
+        int a2 = 0, e2 = 0;
+        BandRec<KIND> nxt;
+        if (step + 1 < 2 * nCol)
+        {
+            a2 = __ldg(&off[step + 1]); e2 = __ldg(&off[step + 2]);
+            if (a2 + tid < e2) nxt = band_load<KIND>(bv, staged, base, a2 + tid);
+        }
+        if (step == nCol)
+        {
+            cl.sync();                 // every band's interior records are done
+            if (hasNext)
+                for (int i = tid; i < bv.halo; i += NT) pa.halo[i] = nextHead[i];
+            __syncthreads();
+        }
+        if (a + tid < e) err = fmaxf(err, band_apply<KIND>(pa, P, cur));
+        for (int j = a + tid + NT; j < e; j += NT) err = fmaxf(err, band_apply<KIND>(pa, P, band_load<KIND>(bv, staged, base, j)));
+        if (step + 1 != nCol) __syncthreads();
+        cur = nxt;
+        a = a2; e = e2;
+    }
+    if (hasNext)
+        for (int i = tid; i < bv.halo; i += NT) nextHead[i] = pa.halo[i];
+    cl.sync();                         // the heads are back with their owners
+    return err;
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT) k_gs_band(DevCloth c, SolverParams P, Buffers b, ColourArgs ca, GsPlan plan,
+                                                BandView bv)
+{
+    extern __shared__ float4 sPos[];
+    __shared__ float sErr[8];
+    cg::cluster_group cl = cg::this_cluster();
+    const int band = (int)cl.block_rank(), nb = (int)cl.num_blocks();
+    const uint32_t vpc = 1u << bv.shift;
+    const int v0 = band * (int)vpc;
+    // shared memory: own band | halo (rounded to 16 particles) | staged FEM | bends | links
+    float4* sHalo = sPos + vpc;
+    float4* sFem = sHalo + ((bv.halo + 15) & ~15);
+    float4* sBend = sFem + (bv.stageFem ? 3 * bv.femMax : 0);
+    float4* sLink = sBend + (bv.stageBend ? bv.bendMax : 0);
+    float4* nextHead = band + 1 < nb ? cl.map_shared_rank(sPos, band + 1) : nullptr;
+    for (uint32_t v = threadIdx.x; v < vpc; v += NT)
+    {
+        const int g = v0 + (int)v;
+        if (g < c.N) sPos[v] = c.pos[g];
+    }
+    auto stage = [&](int nCol, const int* off, const float4* src, int perRec, float4* dst) {
+        const int a = __ldg(&off[band * 2 * nCol]), e = __ldg(&off[(band + 1) * 2 * nCol]);
+        for (int j = a * perRec + (int)threadIdx.x; j < e * perRec; j += NT) dst[j - a * perRec] = __ldg(&src[j]);
+    };
+    if (bv.stageFem) stage(bv.nFemCol, bv.femOff, bv.fem, 3, sFem);
+    if (bv.stageBend) stage(bv.nBendCol, bv.bendOff, reinterpret_cast<const float4*>(bv.bend), 1, sBend);
+    if (bv.stageLink) stage(bv.nLinkCol, bv.linkOff, bv.link, 1, sLink);
+    if (threadIdx.x < 8) sErr[threadIdx.x] = 0.f;
+    cl.sync();
+    const BandPos pa{sPos, sHalo, (uint32_t)v0, (uint32_t)v0 + vpc};
+    const ClusterPos cpa{sPos, (uint32_t)bv.shift, vpc - 1};
+    const bool track = !P.fixedIterations;
+    if (P.resTol > 0.f)
+    {
+        for (uint32_t v = threadIdx.x; v < vpc; v += NT)
+            if (v0 + (int)v < c.N) c.xsnap[v0 + v] = sPos[v];
+        __syncthreads();
+    }
+    for (int k = 0; k < plan.iterations; k++)
+    {
+        if (P.fem)
+            band_sweep<0, NT>(pa, P, bv, bv.stageFem ? sFem : nullptr, band, nb, nextHead);
+        else
+        {
+            const float e = band_sweep<2, NT>(pa, P, bv, bv.stageLink ? sLink : nullptr, band, nb, nextHead);
+            if (track && e > 0.f) atomicMax((int*)&sErr[1], __float_as_int(e));
+        }
+        if (P.dihedral && k % P.bendFreq == 0)
+        {
+            const float e = band_sweep<1, NT>(pa, P, bv, bv.stageBend ? sBend : nullptr, band, nb, nextHead);
+            if (track && e > 0.f) atomicMax((int*)&sErr[2], __float_as_int(e));
+        }
+        if (b.numVColl > 0)
+        {
+            // each CTA solves the vertex contacts of its own particles
+            for (uint32_t v = threadIdx.x; v < vpc; v += NT)
+            {
+                const int g = v0 + (int)v;
+                if (g >= c.N) continue;
+                const float err = vertex_contacts_one(pa, c, P, b, g);
+                if (track && err > 0.f) atomicMax((int*)&sErr[3], __float_as_int(err));
+            }
+        }
+        // the contact classes reach any particle: all vertex contacts first
+        bool contacts = false;
+        for (int cls = 0; cls < 4; cls++) contacts |= *ca.cls[cls].count > 0;
+        if (contacts) cl.sync();
+        else __syncthreads();
+        cluster_contact_classes(cpa, c, P, b, ca, band, nb, track, sErr);
+        if (cluster_iteration_end(c, P, sPos, v0, vpc, band, k, track, sErr)) break;
+    }
+    if (band == 0 && threadIdx.x == 0) c.scal[10] += c.scal[9];
+    // write back own particles and update their velocities (ClothPBD.cpp:314-321)
+    for (uint32_t v = threadIdx.x; v < vpc; v += NT)
     {
         const int g = v0 + (int)v;
         if (g >= c.N) continue;
@@ -1221,6 +1459,68 @@ void launch_gs_cluster(cudaStream_t s, const DevCloth& c, const SolverParams& P,
     cudaLaunchKernelEx(&cfg, kClusterVariants[variant == 1 ? 1 : 0], c, P, b, colour_args(b), plan);
 }
 
+// ---------------------------------------------- band solver launchers
+using BandKernel = void (*)(DevCloth, SolverParams, Buffers, ColourArgs, GsPlan, BandView);
+static const BandKernel kBandVariants[] = {k_gs_band<256>, k_gs_band<512>, k_gs_band<1024>};
+static const int kBandThreads[] = {256, 512, 1024};
+
+int gs_band_variants() { return 3; }
+int gs_band_threads(int variant) { return (variant >= 0 && variant < 3) ? kBandThreads[variant] : 0; }
+
+// kernel attributes (once per process): non-portable cluster sizes, the shared memory limit
+static void band_attributes()
+{
+    static std::once_flag once;
+    std::call_once(once, [] {
+        for (auto k : kBandVariants)
+        {
+            cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, BAND_SMEM_MAX);
+        }
+        cudaGetLastError();
+    });
+}
+
+static cudaLaunchConfig_t band_config(int clusterSize, int threads, size_t smem, cudaStream_t s, cudaLaunchAttribute* at)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(clusterSize);
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    at->id = cudaLaunchAttributeClusterDimension;
+    at->val.clusterDim.x = clusterSize; at->val.clusterDim.y = 1; at->val.clusterDim.z = 1;
+    cfg.attrs = at; cfg.numAttrs = 1;
+    return cfg;
+}
+
+// a cluster of clusterSize CTAs with smem bytes each fits for some variant
+bool gs_band_fits(int clusterSize, size_t smem)
+{
+    if (smem > (size_t)BAND_SMEM_MAX) return false;
+    band_attributes();
+    bool ok = false;
+    for (int v = 0; v < 3 && !ok; v++)
+    {
+        cudaLaunchAttribute at;
+        cudaLaunchConfig_t cfg = band_config(clusterSize, kBandThreads[v], smem, nullptr, &at);
+        int clusters = 0;
+        ok = cudaOccupancyMaxActiveClusters(&clusters, kBandVariants[v], &cfg) == cudaSuccess && clusters > 0;
+    }
+    cudaGetLastError();
+    return ok;
+}
+
+bool launch_gs_band(cudaStream_t s, const DevCloth& c, const SolverParams& P, const Buffers& b, GsPlan plan,
+                    const BandView& bv, int clusterSize, size_t smem, int variant)
+{
+    if (variant < 0 || variant >= 3) return false;
+    band_attributes();
+    cudaLaunchAttribute at;
+    cudaLaunchConfig_t cfg = band_config(clusterSize, kBandThreads[variant], smem, s, &at);
+    return cudaLaunchKernelEx(&cfg, kBandVariants[variant], c, P, b, colour_args(b), plan, bv) == cudaSuccess;
+}
+
 // ---------------------------------------------- per-colour path launchers
 void launch_reset_link_error(cudaStream_t s, const DevCloth& c)
 {
@@ -1253,4 +1553,4 @@ void launch_solve_multi_contacts(cudaStream_t s, const DevCloth& c, const Solver
 // this build's entry points
 static const SolverOps kSolverOps = {launch_fem, launch_links, launch_reset_link_error, launch_bends,
                                      launch_solve_vertex_contacts, launch_solve_multi_contacts, gs_cluster_size,
-                                     launch_gs_cluster, gs_grid_max_blocks_per_sm, launch_gs_grid};
+                                     launch_gs_cluster, gs_grid_max_blocks_per_sm, launch_gs_grid, launch_gs_band};

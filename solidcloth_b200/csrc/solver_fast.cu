@@ -11,6 +11,7 @@
 #include "step_common.cuh"
 #include <cooperative_groups.h>
 #include <cstdio>
+#include <mutex>
 
 namespace cg = cooperative_groups;
 

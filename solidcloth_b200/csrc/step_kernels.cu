@@ -16,6 +16,7 @@
 #include <cooperative_groups.h>
 #include <cuda/atomic>
 #include <cstdio>
+#include <mutex>
 #include <climits>
 #include <algorithm>
 

@@ -68,11 +68,13 @@ def _pairs_match(sc, p, pos, prev, vel):
     return len(ovt), len(oee)
 
 
-def _run_check_mode(sc, frames, per_substep_state=True):
+def _run_check_mode(sc, frames, per_substep_state=True, solver_mode=0):
     """GPU and oracle side by side; returns the GPU patch, the oracle and the
     state before the last substep (for the broad-phase comparison)"""
     from solidcloth_b200 import api
     w, p = api.load_scene(sc)
+    if solver_mode:
+        p.model.set_solver_mode(solver_mode)
     o = _oracle_for(sc, p)
     for f in range(frames):
         p.step(sc.dt)
@@ -110,6 +112,21 @@ def test_cfg1_128_drape_check_mode():
     assert nvt > 100_000 and nee > 100_000
     assert p1.status() & ~16 == 0
     p1.free()
+    p.free()
+
+
+@pytest.mark.parametrize("n", [128, 256])
+def test_band_solver_check_mode_at_config_sizes(n):
+    """The band-parallel solver (solver mode 4: one 16-CTA cluster, particle
+    bands resident in shared memory, interior then boundary records) on the
+    128x128 SDF drape and the 256x256 icosphere drape: bit-identical to the
+    oracle run in the band order, frame by frame."""
+    sc = scenes.cfg1() if n == 128 else scenes.cfg2()
+    sc.positions[:, 1] -= np.float32(0.398 if n == 128 else 0.49)
+    w, p, o = _run_check_mode(sc, 1, solver_mode=4)
+    cs, per_band, halo, used = p.model.band_plan()
+    assert used == 1 and cs == 16 and per_band * cs == n * n and 0 < halo <= 2 * n + 2
+    assert p.model.solver_choice()[0][0] == 4
     p.free()
 
 

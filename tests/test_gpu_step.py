@@ -18,11 +18,13 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-5          # metres; per-constraint parity bound of the spec, applied to positions
 
 
-def _pair(sc, ccd=False, state=None):
+def _pair(sc, ccd=False, state=None, solver_mode=0):
     from solidcloth_b200 import api
     from oracle.bridge import PortCloth
     PortCloth.set_portable_math(True)
     w, p = api.load_scene(sc, ccd=ccd)
+    if solver_mode:
+        p.model.set_solver_mode(solver_mode)
     o = PortCloth.from_scene(sc)
     o._fn("set_ccd")(o.h, int(ccd))
     if state is not None:
@@ -68,10 +70,16 @@ def test_cfg0_check_mode():
     assert np.allclose(p.model.velocities(), o.state()[2], atol=1e-3)
 
 
-def test_colouring_is_valid():
+@pytest.mark.parametrize("mode", [0, 4])
+def test_colouring_is_valid(mode):
+    """Every group of the reported order is an independent set: the colours of
+    the colour order (the default), the (part, colour) groups of the band order
+    (solver mode 4); the band groups are the colour classes split into interior
+    and boundary records."""
     sc = scenes.cfg0()
     from solidcloth_b200 import api
     w, p = api.load_scene(sc)
+    p.model.set_solver_mode(mode)
     tris = p.model.tris()
     order, start = p.model.constraint_order(0)
     assert sorted(order.tolist()) == list(range(len(tris)))
@@ -80,13 +88,18 @@ def test_colouring_is_valid():
         assert len(np.unique(ids)) == ids.size, "two triangles of one colour share a particle"
     bends = p.model.bends()
     order, start = p.model.constraint_order(1)
+    assert sorted(order.tolist()) == list(range(len(bends)))
     for c in range(len(start) - 1):
         ids = bends[order[start[c]:start[c + 1]]].reshape(-1)
         assert len(np.unique(ids)) == ids.size
     # grid bends take the period-4 colouring: 16 colours, the most bends sharing
     # one particle (index-order greedy needs 18-19 on these grids)
     per = np.bincount(bends.reshape(-1), minlength=sc.num_vertices).max()
-    assert len(start) - 1 == per == 16
+    if mode == 0:
+        assert len(start) - 1 == per == 16
+    else:
+        assert p.model.band_plan()[3] == 1
+        assert 16 < len(start) - 1 <= 32
 
 
 def test_topology_matches_oracle():
@@ -278,9 +291,12 @@ def test_mass_spring_check_mode(dihedral, fixed):
 def test_solvers_are_bit_identical(scene):
     """The cluster-resident solver (one launch per substep, particles in
     distributed shared memory, records staged in shared memory or read from
-    global memory), every variant of the grid-resident cooperative solver, the
-    one-kernel-per-colour path and the autotuner's choice are the same algorithm
-    in the same order: bit-identical trajectories."""
+    global memory), every variant of the grid-resident cooperative solver and the
+    one-kernel-per-colour path are the same algorithm in the same (colour) order:
+    bit-identical trajectories, the autotuner's choice among them included. The
+    band-parallel solver's variants (256, 512 and 1024 threads, records staged or
+    not) and its tuned choice sweep in the band order: bit-identical among
+    themselves and to the oracle run in that order."""
     from solidcloth_b200 import api
     state = None
     if scene == "cfg0":
@@ -297,29 +313,51 @@ def test_solvers_are_bit_identical(scene):
         state = scenes.folded(sc, gap=0.004)
     else:
         sc, state = scenes.ccd_scene(16)
-    out = []
-    modes = [("cluster", True), ("cluster", False), ("cluster2", True), ("cluster2", False), ("kernels", False)]
-    modes += [("grid", (v, 1)) for v in range(len(api.grid_variants()))] + [("grid", (0, 2)), ("auto", None)]
-    for mode, arg in modes:
-        w, p = api.load_scene(sc)
-        if mode in ("cluster", "cluster2"):
-            p.model.set_cluster_staging(arg)
-            p.model.set_cluster_variant(1 if mode == "cluster2" else 0)     # last: forcing survives
-        elif mode == "kernels":
-            p.model.set_cluster_solver(False)
-        elif mode == "grid":
-            p.model.set_grid_solver(*arg)
-        if state is not None:
-            p.model.set_state(*state)
-        for _ in range(4):
-            p.step(sc.dt)
-            p.update_mesh()
-        out.append((p.model.positions(), p.model.velocities(), p.status() & ~16))
-        p.free()
-    for o, m in zip(out, modes):
-        assert o[2] == 0, m
-    for o, m in zip(out[1:], modes[1:]):
-        assert _same(out[0][0], o[0]) and _same(out[0][1], o[1]), m
+    colour = [("cluster", True), ("cluster", False), ("cluster2", True), ("cluster2", False), ("kernels", False)]
+    colour += [("grid", (v, 1)) for v in range(len(api.grid_variants()))] + [("grid", (0, 2)), ("auto", None)]
+    band = [("band", (v, st)) for v in range(3) for st in (True, False)] + [("band_tuned", None)]
+    w, p = api.load_scene(sc)
+    has_band = p.model.band_plan()[0] > 0
+    p.free()
+    groups = [colour] + ([band] if has_band else [])
+    for group in groups:
+        out = []
+        for mode, arg in group:
+            w, p = api.load_scene(sc)
+            if mode in ("cluster", "cluster2"):
+                p.model.set_cluster_staging(arg)
+                p.model.set_cluster_variant(1 if mode == "cluster2" else 0)     # last: forcing survives
+            elif mode == "kernels":
+                p.model.set_cluster_solver(False)
+            elif mode == "grid":
+                p.model.set_grid_solver(*arg)
+            elif mode == "band":
+                p.model.set_cluster_staging(arg[1])
+                p.model.set_band_variant(arg[0])
+            elif mode == "band_tuned":
+                p.model.set_solver_mode(4)
+            if state is not None:
+                p.model.set_state(*state)
+            o = None
+            if mode == "band_tuned" and not sc.ccd:
+                # the band solver against the oracle in the band order
+                _, p2, o = _pair(sc, ccd=False, state=state, solver_mode=4)
+                p.free()
+                p = p2
+            for _ in range(4):
+                p.step(sc.dt)
+                p.update_mesh()
+                if o is not None:
+                    o.step(sc.dt)
+                    assert _same(p.model.positions(), o.positions()), (mode, float(np.abs(p.model.positions() - o.positions()).max()))
+            if mode == "band_tuned":
+                assert p.model.band_plan()[3] == 1 and p.model.solver_choice()[0][0] == 4
+            out.append((p.model.positions(), p.model.velocities(), p.status() & ~16))
+            p.free()
+        for o, m in zip(out, group):
+            assert o[2] == 0, m
+        for o, m in zip(out[1:], group[1:]):
+            assert _same(out[0][0], o[0]) and _same(out[0][1], o[1]), m
 
 
 def test_early_exit_mode_matches_oracle():
