@@ -335,11 +335,12 @@ def run_reference(args):
     print(json.dumps(line))
 
 
-def _learned_ab(drapes: int = 2, n: int = 256):
+def _learned_ab(drapes: int = 4, n: int = 256):
     """iterations a substep to the residual target (update residual: the largest
     particle displacement of a Gauss-Seidel iteration, <= 1e-4 m, cap 200) and
     device-timed vertex-substeps/s, plain versus learned warm start, on held-out
-    256 x 256 drapes (seeds the training never saw)"""
+    256 x 256 drapes (the first of learned.TEST_SEEDS: seeds neither the training
+    nor the output-scale calibration saw)"""
     from solidcloth_b200 import learned
     path = ROOT / "solidcloth_b200" / "data" / "warmstart.npz"
     if not path.exists():
@@ -347,22 +348,30 @@ def _learned_ab(drapes: int = 2, n: int = 256):
     z = np.load(path)
     params, norm = z["params"].astype(np.float32), z["norm"].astype(np.float32)
     tol, cap = 1e-4, 200
-    rows = [learned.compare([learned.drape_scene(20_000_000 + k, n)], params, norm, frames=3, skip=4,
-                            tol=tol, max_iter=cap)
-            for k in range(drapes)]
-    plain_it = float(np.mean([r["plain"]["iterations_per_substep"] for r in rows]))
-    learn_it = float(np.mean([r["learned"]["iterations_per_substep"] for r in rows]))
-    plain_v = float(np.mean([r["plain"]["vertex_substeps_per_s"] for r in rows]))
-    learn_v = float(np.mean([r["learned"]["vertex_substeps_per_s"] for r in rows]))
+    seeds = learned.TEST_SEEDS[:drapes]
+    rows = [learned.compare([learned.drape_scene(sd, n)], params, norm, frames=3, skip=4, tol=tol, max_iter=cap)
+            for sd in seeds]
+    per = [{"seed": sd, "plain": r["plain"]["iterations_per_substep"], "learned": r["learned"]["iterations_per_substep"]}
+           for sd, r in zip(seeds, rows)]
+    s = learned.summary(per)
+    plain_it = float(np.mean([x["plain"] for x in per]))
+    learn_it = float(np.mean([x["learned"] for x in per]))
+    plain_ms = float(np.sum([r["plain"]["ms_per_frame"] for r in rows]))
+    learn_ms = float(np.sum([r["learned"]["ms_per_frame"] for r in rows]))
+    N = n * n
+    subs = 8
     return {"workload": f"{drapes} held-out {n}x{n} drapes (1.5 m) over a sphere SDF, 8 substeps, continuous "
                         f"self-collision, fast solver build; trained on {int(z['drapes'])} drapes at "
-                        f"{int(z['n'])}x{int(z['n'])}",
+                        f"{int(z['n'])}x{int(z['n'])}, correction scaled by "
+                        f"{float(z['output_scale']) if 'output_scale' in z else 1.0:g} (calibrated on other drapes)",
             "residual": f"update residual (largest particle displacement of an iteration, metres) <= {tol:g}, cap {cap}",
             "plain_iterations_per_substep": plain_it, "learned_iterations_per_substep": learn_it,
-            "iteration_ratio": plain_it / learn_it if learn_it else None,
+            "iteration_ratio": s["aggregate"], "iteration_ratio_median": s["median"],
+            "iteration_ratio_per_drape": s["ratios"],
             "plain_residual_reached": all(r["plain"]["iterations_per_substep"] < cap for r in rows),
-            "plain_vertex_substeps_per_s": plain_v, "learned_vertex_substeps_per_s": learn_v,
-            "throughput_ratio": learn_v / plain_v if plain_v else None}
+            "plain_vertex_substeps_per_s": N * subs * len(rows) / (plain_ms * 1e-3),
+            "learned_vertex_substeps_per_s": N * subs * len(rows) / (learn_ms * 1e-3),
+            "throughput_ratio": plain_ms / learn_ms if learn_ms else None}
 
 
 def run_ours(args):
@@ -537,8 +546,39 @@ def run_ours(args):
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
             from oracle.bridge import available
-            if available("ref"):
-                ref_sc = sc.mine[len(sc.mine) // 2] if isinstance(sc, _Batch) else sc
+            if available("ref") and isinstance(sc, _Batch):
+                # a batch: whole first frames of instances spread over the list,
+                # until about 10 s of reference time
+                picks = sc.mine[::max(1, len(sc.mine) // 64)]
+                units = secs = 0.0
+                used = []
+                with _reference_output_to_stderr():
+                    for inst in picks:
+                        v1, s1, cores = cpu_reference_rate(inst, frames=1)
+                        units += v1 * s1
+                        secs += s1
+                        used.append(inst)
+                        if secs >= 10.0:
+                            break
+                ref_sc = used[len(used) // 2]
+                cpu = {"value": units / secs, "unit": UNIT, "cores": cores, "kind": "reference", "cpu": _cpu_model(),
+                       "sample": f"the first frame ({ref_sc.params.substeps} substeps) of {len(used)} of the "
+                                 f"{len(sc.mine)} instances, spread over the list ({int(sum(x.num_vertices for x in used))} "
+                                 f"vertices, {secs:.1f} s), the reference's own C++ (oracle/_ref, OpenMP {cores} threads)"}
+                if available("ref_serial"):
+                    units1 = secs1 = 0.0
+                    with _reference_output_to_stderr():
+                        for inst in used:
+                            v1, s1, _ = cpu_reference_rate(inst, serial=True, substeps=inst.params.substeps)
+                            units1 += v1 * s1
+                            secs1 += s1
+                    cpu["single_thread"] = {
+                        "value": units1 / secs1, "unit": UNIT, "cores": 1,
+                        "sample": f"the first {ref_sc.params.substeps} substeps of the same {len(used)} instances "
+                                  f"({secs1:.1f} s), the reference built without OpenMP (oracle/_ref/libscref_serial.so), "
+                                  f"as its C-ABI library ships"}
+            elif available("ref"):
+                ref_sc = sc
                 with _reference_output_to_stderr():
                     v, secs, cores = cpu_reference_rate(ref_sc, frames=1)
                 cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "reference", "cpu": _cpu_model(),
