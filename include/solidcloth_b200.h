@@ -367,6 +367,11 @@ SCEXP void scSynchronize(scClothPatch patch);
 SCEXP void* scGetCudaStream(scClothPatch patch);
 /* kernel nodes in the frame graph of the last scStepCloth (launches per frame) */
 SCEXP int scGetGraphKernelCount(scClothPatch patch);
+/* on != 0: scStepCloth launches the substeps' kernels one by one on the patch
+   stream instead of replaying the captured frame graph (same kernels, same
+   results; for profilers that cannot see kernels inside graphs); section timing
+   (scSetKernelTiming) records nothing meanwhile. Default 0. */
+SCEXP void scSetDirectLaunch(scClothPatch patch, int on);
 /* Time `reps` back-to-back constraint sweeps (kind 0: all FEM colours of one
    iteration, 1: all bend colours) captured as one graph, with CUDA events on
    the patch stream; returns milliseconds per sweep, or a negative value on error.

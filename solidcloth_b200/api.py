@@ -182,6 +182,7 @@ SIGNATURES = {
     "scSynchronize": ([scClothPatch], None),
     "scGetCudaStream": ([scClothPatch], C.c_void_p),
     "scGetGraphKernelCount": ([scClothPatch], C.c_int),
+    "scSetDirectLaunch": ([scClothPatch, C.c_int], None),
     "scProfileSweep": ([scClothPatch, C.c_int, C.c_int], C.c_float),
     "scProbeClusterPhase": ([C.c_int, C.c_int], C.c_float),
     "scSetKernelTiming": ([scClothPatch, C.c_int], C.c_bool),
@@ -577,6 +578,11 @@ class ClothPatch:
 
     def graph_kernel_count(self) -> int:
         return lib().scGetGraphKernelCount(self.h)
+
+    def set_direct_launch(self, on: bool):
+        """launch each substep's kernels directly instead of replaying the frame graph"""
+        lib().scSetDirectLaunch(self.h, int(bool(on)))
+        _check("scSetDirectLaunch")
 
     def profile_sweep(self, kind: int, reps: int = 50) -> float:
         ms = lib().scProfileSweep(self.h, int(kind), int(reps))

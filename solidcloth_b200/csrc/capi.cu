@@ -1070,6 +1070,12 @@ void scSynchronize(scClothPatch p) { if (P(p)) P(p)->sync(); }
 
 void* scGetCudaStream(scClothPatch p) { return P(p) ? (void*)P(p)->stream : nullptr; }
 
+void scSetDirectLaunch(scClothPatch p, int on)
+{
+    if (!P(p)) { set_error(SC_ERR_ARG, "null patch"); return; }
+    P(p)->sync();
+    P(p)->directLaunch = on != 0;
+}
 int scGetGraphKernelCount(scClothPatch p)
 {
     if (!P(p) || !P(p)->graph) return 0;

@@ -2216,6 +2216,24 @@ bool ClothPatch::step(float dt)
     if (!m.ensure_buffers(world, stream)) return false;
     const int n = numSteps;
     const float h = dt / n;
+    if (directLaunch)
+    {
+        // the same substeps, launched one kernel at a time (no graph, no section timing)
+        if (m.solverMode == SOLVE_KERNELS) m.choice = {SOLVE_KERNELS, 0, 0, 0.f};
+        else if (!m.tuned || m.tunedVersion != m.paramVersion)
+        {
+            if (!autotune(h)) return false;
+            m.tunedVersion = m.paramVersion;
+        }
+        const int frames = timingFrames;
+        timingFrames = 0;
+        recordingSubstep = 0;
+        for (int i = 0; i < n; i++) record_substep(h);
+        timingFrames = frames;
+        SC_CUDA(cudaGetLastError());
+        hostStateDirty = true;
+        return true;
+    }
     if (!graph || graphDt != dt || graphSteps != n || graphParamVersion != m.paramVersion || graphWorldVersion != world.version)
     {
         if (graph) { cudaGraphExecDestroy(graph); graph = nullptr; }

