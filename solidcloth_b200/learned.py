@@ -169,12 +169,21 @@ def compare(drapes, params: np.ndarray | None, norm: np.ndarray | None, frames: 
     displacement of an iteration, in metres), and device-timed
     vertex-substeps/s over the measured frames (after `skip` untimed frames).
     constraint_residual_after is max |C| over the FEM constraints after the last
-    frame (scGetResidual), a check that both arms end in states of equal quality."""
+    frame (scGetResidual), a check that both arms end in states of equal quality.
+    Both arms run one fixed solver kernel (the cluster solver for one drape, the
+    grid solver's first variant for a batch) rather than the autotuner's choice:
+    in the fast build the solvers agree only within the projection tolerance,
+    and iteration counts to a max-norm residual amplify such differences, so a
+    timing-dependent choice would make the counts differ from run to run."""
     import torch
     out = {}
     for label, warm in (("plain", False), ("learned", True)):
         b = api.load_batch(drapes) if len(drapes) > 1 else api.load_scene(drapes[0])[1]
         b.model.set_fast_math(fast)
+        if len(drapes) > 1:
+            b.model.set_grid_solver(0, 1)
+        else:
+            b.model.set_cluster_variant(0)
         b.model.set_residual_target(tol, max_iter, metres=True)
         if warm:
             b.model.set_warm_start(params, norm)
