@@ -761,6 +761,8 @@ void ClothModel::build_band_plan()
 {
     bandPlan = BandPlan{};
     if (!instV.empty() || N < 64) return;
+    // the kernel keeps a band's record offsets in shared memory: at most 64 colours a class
+    if (triColourStart.size() > 65 || bendColourStart.size() > 65 || linkColourStart.size() > 65) return;
     struct Cls
     {
         int arity;

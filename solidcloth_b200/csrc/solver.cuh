@@ -1002,16 +1002,16 @@ __device__ __forceinline__ float band_apply(const BandPos& pa, const SolverParam
 // this thread's largest projection error.
 template <int KIND, int NT>
 __device__ __forceinline__ float band_sweep(const BandPos& pa, const SolverParams& P, const BandView& bv,
-                                            const float4* staged, int band, int nb, float4* nextHead)
+                                            const float4* staged, int band, int nb, float4* nextHead, const int* off)
 {
+    // off: this band's 2 nCol + 1 record offsets of the class, in shared memory
     cg::cluster_group cl = cg::this_cluster();
     const int nCol = KIND == 0 ? bv.nFemCol : KIND == 1 ? bv.nBendCol : bv.nLinkCol;
-    const int* off = (KIND == 0 ? bv.femOff : KIND == 1 ? bv.bendOff : bv.linkOff) + band * 2 * nCol;
-    const int base = __ldg(&off[0]);
+    const int base = off[0];
     const int tid = (int)threadIdx.x;
     const bool hasNext = band + 1 < nb;
     float err = 0.f;
-    int a = __ldg(&off[0]), e = __ldg(&off[1]);
+    int a = off[0], e = off[1];
     BandRec<KIND> cur;
     if (a + tid < e) cur = band_load<KIND>(bv, staged, base, a + tid);
     for (int step = 0; step < 2 * nCol; step++)
@@ -1021,7 +1021,7 @@ __device__ __forceinline__ float band_sweep(const BandPos& pa, const SolverParam
         BandRec<KIND> nxt;
         if (step + 1 < 2 * nCol)
         {
-            a2 = __ldg(&off[step + 1]); e2 = __ldg(&off[step + 2]);
+            a2 = off[step + 1]; e2 = off[step + 2];
             if (a2 + tid < e2) nxt = band_load<KIND>(bv, staged, base, a2 + tid);
         }
         if (step == nCol)
@@ -1071,6 +1071,14 @@ __global__ void __launch_bounds__(NT) k_gs_band(DevCloth c, SolverParams P, Buff
     if (bv.stageFem) stage(bv.nFemCol, bv.femOff, bv.fem, 3, sFem);
     if (bv.stageBend) stage(bv.nBendCol, bv.bendOff, reinterpret_cast<const float4*>(bv.bend), 1, sBend);
     if (bv.stageLink) stage(bv.nLinkCol, bv.linkOff, bv.link, 1, sLink);
+    // this band's record offsets of each class (at most 64 colours a class)
+    __shared__ int sOff[3][129];
+    {
+        const int nc[3] = {bv.nFemCol, bv.nBendCol, bv.nLinkCol};
+        const int* src[3] = {bv.femOff, bv.bendOff, bv.linkOff};
+        for (int k = 0; k < 3; k++)
+            for (int j = (int)threadIdx.x; j <= 2 * nc[k] && j < 129; j += NT) sOff[k][j] = __ldg(&src[k][band * 2 * nc[k] + j]);
+    }
     if (threadIdx.x < 8) sErr[threadIdx.x] = 0.f;
     cl.sync();
     const BandPos pa{sPos, sHalo, (uint32_t)v0, (uint32_t)v0 + vpc};
@@ -1085,15 +1093,15 @@ __global__ void __launch_bounds__(NT) k_gs_band(DevCloth c, SolverParams P, Buff
     for (int k = 0; k < plan.iterations; k++)
     {
         if (P.fem)
-            band_sweep<0, NT>(pa, P, bv, bv.stageFem ? sFem : nullptr, band, nb, nextHead);
+            band_sweep<0, NT>(pa, P, bv, bv.stageFem ? sFem : nullptr, band, nb, nextHead, sOff[0]);
         else
         {
-            const float e = band_sweep<2, NT>(pa, P, bv, bv.stageLink ? sLink : nullptr, band, nb, nextHead);
+            const float e = band_sweep<2, NT>(pa, P, bv, bv.stageLink ? sLink : nullptr, band, nb, nextHead, sOff[2]);
             if (track && e > 0.f) atomicMax((int*)&sErr[1], __float_as_int(e));
         }
         if (P.dihedral && k % P.bendFreq == 0)
         {
-            const float e = band_sweep<1, NT>(pa, P, bv, bv.stageBend ? sBend : nullptr, band, nb, nextHead);
+            const float e = band_sweep<1, NT>(pa, P, bv, bv.stageBend ? sBend : nullptr, band, nb, nextHead, sOff[1]);
             if (track && e > 0.f) atomicMax((int*)&sErr[2], __float_as_int(e));
         }
         if (b.numVColl > 0)
