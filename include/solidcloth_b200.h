@@ -200,6 +200,13 @@ SCEXP void scSetStretchStiffness(scModel model, float val);
 SCEXP void scSetPoisson(scModel model, float val);
 SCEXP void scSetDragCoeff(scModel model, float val);
 SCEXP void scSetDihedral(scModel model, bool val);
+/* ClothModel::SetSolver / GetSolver (Physics/ClothModel.h:137-138; C++ members, not
+   in the reference's C API): the SolverType ClothModelPBD::Step dispatches on
+   (Physics/ClothPBD.cpp:293-298). 1 SOLVER_GAUSS_SEIDEL (default), 0 SOLVER_JACOBI
+   (SolveJacobi: links only, omega 0.5), 2-4 the conjugate-residual SolveCR (links
+   only). Other values are rejected (SC_ERR_ARG). */
+SCEXP void scSetSolverType(scModel model, int type);
+SCEXP int scGetSolverType(scModel model);
 SCEXP void scSetSelfShrink(scModel model, float val);
 SCEXP void scSetNumSteps(scClothPatch patch, int val);
 SCEXP int scGetNumSteps(scClothPatch patch);

@@ -58,6 +58,7 @@ def _load(path: Path, prefix: str):
         "init_grid": ([C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int, C.c_int], None),
         "set_params": ([C.c_void_p, _f, C.c_int], None),
         "set_ccd": ([C.c_void_p, C.c_int], None),
+        "set_solver": ([C.c_void_p, C.c_int], None),
         "num_particles": ([C.c_void_p], C.c_int), "num_tris": ([C.c_void_p], C.c_int),
         "num_bends": ([C.c_void_p], C.c_int), "num_edges": ([C.c_void_p], C.c_int),
         "set_positions": ([C.c_void_p, _f], None),
@@ -158,6 +159,7 @@ class CpuCloth:
             self._fn("add_mesh")(self.h, v.shape[0], _fp(v), idx.size // 3, _up(idx))
         pa = s.params.as_array()
         self._fn("set_params")(self.h, _fp(pa), pa.size)
+        self._fn("set_solver")(self.h, int(getattr(s.params, "solver", 1)))
         off = s.offset
         self._fn("init_grid")(self.h, s.n, s.n, float(s.inc), float(off[0]), float(off[1]), float(off[2]), 1,
                               int(s.attached))

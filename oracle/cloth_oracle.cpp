@@ -1683,6 +1683,84 @@ struct Cloth
         lastIterations = k;
     }
 
+    /* ClothModel::SolverType (Physics/ClothModel.h:23-30): 0 SOLVER_JACOBI,
+       1 SOLVER_GAUSS_SEIDEL (default), otherwise SolveCR (Physics/ClothPBD.cpp:293-298) */
+    int solver = 1;
+
+    /* ClothModelPBD::SolveJacobi / SolveLinksJacobi (Physics/ClothPBD.cpp:616-661):
+       every link's displacement from the same positions, omega 0.5, then applied
+       in link order; links only (no FEM, bends or contacts) */
+    void solve_jacobi(float h)
+    {
+        const float h2 = h * h;
+        const float k = h2 * area * unit;
+        const float omega = 0.5f;
+        std::vector<V3> disp(links.size());
+        for (int it = 0; it < iterations; ++it)
+        {
+            for (size_t i = 0; i < links.size(); i++)
+            {
+                const Link& lk = links[i];
+                const float mu = 1.f / (invMass[lk.i1] + invMass[lk.i2]);
+                V3 delta = pos[lk.i1] - pos[lk.i2];
+                const float len0 = lk.len;
+                const float l = len(delta);
+                delta = (1 / l) * delta;
+                const float err = l - len0;
+                const float epsilon = len0 / (k * lk.stiffness);
+                const float s = 1.f / (1.f + mu * epsilon);
+                const float lambda = err * mu * s;
+                disp[i] = (omega * lambda) * delta;
+            }
+            for (size_t i = 0; i < links.size(); i++)
+            {
+                const Link& l = links[i];
+                pos[l.i1] = pos[l.i1] - invMass[l.i1] * disp[i];
+                pos[l.i2] = pos[l.i2] + invMass[l.i2] * disp[i];
+            }
+        }
+        lastIterations = iterations;
+    }
+
+    /* ClothModelPBD::SolveCR (Physics/ClothPBD.cpp:371-496) as compiled, with
+       SKIP_ALPHA and SKIP_BETA defined: per iteration each link's error and unit
+       direction, d = r + beta d with beta = (iter / (iterations - 1))^0.6, and the
+       step alpha0 * d along the direction, applied in link order */
+    void solve_cr(float h, float alpha0)
+    {
+        (void)h;
+        const size_t nl = links.size();
+        if (nl == 0) return;
+        std::vector<float> r(nl), d(nl, 0.f);
+        std::vector<V3> normal(nl);
+        for (int iter = 0; iter < iterations; iter++)
+        {
+            for (size_t i = 0; i < nl; i++)
+            {
+                const Link& l = links[i];
+                V3 delta = pos[l.i2] - pos[l.i1];
+                const float c = (len(delta) - l.len) * l.stiffness * unit;
+                const float ln = len(delta);
+                delta = (1.f / ln) * delta;
+                normal[i] = delta;
+                r[i] = -c;
+            }
+            float beta = (float)iter / (float)(iterations - 1);
+            beta = std::pow(beta, 0.6f);
+            for (size_t i = 0; i < nl; i++) d[i] = r[i] + beta * d[i];
+            const float alpha = alpha0;
+            for (size_t i = 0; i < nl; i++)
+            {
+                const Link& l = links[i];
+                const float dLambda = alpha * d[i];
+                const V3 disp = dLambda * normal[i];
+                pos[l.i1] = pos[l.i1] - invMass[l.i1] * disp;
+                pos[l.i2] = pos[l.i2] + invMass[l.i2] * disp;
+            }
+        }
+        lastIterations = iterations;
+    }
+
     void velocity(float h)
     {
         const float invH = 1.f / h;
@@ -1697,7 +1775,9 @@ struct Cloth
     {
         predict(h);
         detect(ccd);
-        solve_gs(h);
+        if (solver == 1) solve_gs(h);
+        else if (solver == 0) solve_jacobi(h);
+        else solve_cr(h, 0.1f);
         velocity(h);
     }
 
@@ -2088,6 +2168,7 @@ void orc_set_params(void* h, const float* p, int n)
 }
 
 void orc_set_ccd(void* h, int on) { ((Cloth*)h)->ccd = on != 0; }
+void orc_set_solver(void* h, int type) { ((Cloth*)h)->solver = type; }
 int orc_num_particles(void* h) { return ((Cloth*)h)->N; }
 int orc_num_tris(void* h) { return (int)((Cloth*)h)->tris.size(); }
 int orc_num_bends(void* h) { return (int)((Cloth*)h)->bends.size(); }

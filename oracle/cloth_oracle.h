@@ -22,6 +22,8 @@ void orc_add_mesh(void* h, int nv, const float* verts, int nt, const unsigned* i
 void orc_init_grid(void* h, int divX, int divY, float inc, float ox, float oy, float oz, int horizontal, int attached);
 void orc_set_params(void* h, const float* p, int n);
 void orc_set_ccd(void* h, int on);
+/* ClothModel::SetSolver: 0 Jacobi, 1 Gauss-Seidel (default), 2.. conjugate residual */
+void orc_set_solver(void* h, int type);
 int orc_num_particles(void* h);
 int orc_num_tris(void* h);
 int orc_num_bends(void* h);

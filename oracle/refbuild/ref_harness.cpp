@@ -395,6 +395,8 @@ void ref_predict_detect(void* h, float hh, int runCCD)
         s->ccd.Detect();
 }
 
+/* ClothModel::SetSolver (Physics/ClothModel.h:138): the SolverType of ClothModelPBD::Step */
+void ref_set_solver(void* h, int type) { Model((RefScene*)h).SetSolver((SolverType)type); }
 int ref_solver_iterations(void* h) { return Model((RefScene*)h).mStats.iterations; }
 
 /* ---- contact lists ---- */

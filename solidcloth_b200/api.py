@@ -105,6 +105,8 @@ SIGNATURES = {
     "scSetNumIterations": ([scModel, C.c_int], None),
     "scGetUseFEM": ([scModel], C.c_bool),
     "scSetUseFEM": ([scModel, C.c_bool], None),
+    "scSetSolverType": ([scModel, C.c_int], None),
+    "scGetSolverType": ([scModel], C.c_int),
     "scGetClothTree": ([scModel], C.c_void_p),
     "scAddMouseSpring": ([scModel, C.c_int, C.c_int, C.c_int, scVector3, scVector3], None),
     "scUpdateMouseSpring": ([scModel, scVector3], None),
@@ -291,6 +293,7 @@ class ClothModel:
         L.scSetDihedral(self.h, bool(p.dihedral))
         L.scSetFixedIterations(self.h, bool(p.fixed_iterations))
         L.scSetDragCoeff(self.h, p.drag)
+        L.scSetSolverType(self.h, int(getattr(p, "solver", 1)))
         _check("set_params")
 
     def set_masses(self, masses):
@@ -333,6 +336,10 @@ class ClothModel:
 
     def set_cluster_solver(self, on: bool):
         lib().scSetClusterSolver(self.h, bool(on))
+
+    def solver_type(self) -> int:
+        """ClothModel::GetSolver: 0 Jacobi, 1 Gauss-Seidel, 2-4 conjugate residual"""
+        return int(lib().scGetSolverType(self.h))
 
     def set_solver_mode(self, mode: int):
         """0 autotuned (default), 1 cluster kernel, 2 grid kernel, 3 per-colour

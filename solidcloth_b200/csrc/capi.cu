@@ -591,6 +591,13 @@ void scSetStretchStiffness(scModel m, float v) { if (M(m)) { M(m)->prm.stretch =
 void scSetPoisson(scModel m, float v) { if (M(m)) { M(m)->prm.poisson = v; M(m)->touch(); } }
 void scSetDragCoeff(scModel m, float v) { if (M(m)) { M(m)->prm.drag = v; M(m)->touch(); } }
 void scSetDihedral(scModel m, bool v) { if (M(m)) { M(m)->prm.dihedral = v; M(m)->touch(); } }
+void scSetSolverType(scModel m, int type)
+{
+    if (!M(m) || type < 0 || type > 4) { set_error(SC_ERR_ARG, "solver type must be 0..4"); return; }
+    M(m)->prm.solverType = type;
+    M(m)->touch();
+}
+int scGetSolverType(scModel m) { return M(m) ? M(m)->prm.solverType : 1; }
 void scSetSelfShrink(scModel m, float v) { if (M(m)) { M(m)->prm.selfShrink = v; M(m)->touch(); } }
 void scSetNumSteps(scClothPatch p, int v)
 {

@@ -966,6 +966,38 @@ bool ClothModel::upload_topology(const HMesh& mesh)
     SC_CUDA(cudaMemcpy(dlink, lk.data(), sizeof(float4) * lk.size(), cudaMemcpyHostToDevice));
     dc.link = dlink;
     dc.L = L;
+    // the Jacobi and conjugate-residual solves: links in index order, each
+    // particle's incident links in increasing index
+    {
+        std::vector<float4> lo(std::max(1, L));
+        std::vector<int> start(N + 1, 0), inc(std::max(1, 2 * L));
+        for (int k = 0; k < L; k++)
+        {
+            lo[k] = make_float4(bits_f(links[k].x), bits_f(links[k].y), linkRest[k].x, linkRest[k].y);
+            start[links[k].x + 1]++;
+            start[links[k].y + 1]++;
+        }
+        for (int i = 0; i < N; i++) start[i + 1] += start[i];
+        std::vector<int> fill(start.begin(), start.end() - 1);
+        for (int k = 0; k < L; k++)
+        {
+            inc[fill[links[k].x]++] = k << 1;
+            inc[fill[links[k].y]++] = (k << 1) | 1;
+        }
+        LinkSolve& ls = linkSolve;
+        ls.L = L;
+        float4* a = (float4*)dalloc(sizeof(float4) * lo.size());
+        SC_CUDA(cudaMemcpy(a, lo.data(), sizeof(float4) * lo.size(), cudaMemcpyHostToDevice));
+        ls.link = a;
+        ls.disp = (float4*)dalloc(sizeof(float4) * lo.size());
+        ls.d = (float*)dalloc(sizeof(float) * lo.size());
+        int* st = (int*)dalloc(sizeof(int) * start.size());
+        int* ic = (int*)dalloc(sizeof(int) * inc.size());
+        SC_CUDA(cudaMemcpy(st, start.data(), sizeof(int) * start.size(), cudaMemcpyHostToDevice));
+        SC_CUDA(cudaMemcpy(ic, inc.data(), sizeof(int) * inc.size(), cudaMemcpyHostToDevice));
+        ls.incStart = st;
+        ls.inc = ic;
+    }
     std::vector<uint4> bd(B);
     for (int k = 0; k < B; k++) bd[k] = bends[bendOrder[k]];
     uint4* dbend = (uint4*)dalloc(sizeof(uint4) * B);
@@ -1940,6 +1972,26 @@ bool ClothPatch::record_solve(cudaStream_t s, const SolverParams& P, const Solve
     const DevCloth& c = m.dc;
     Buffers& b = m.buf;
     const SolverOps& ops = solver_ops(m.prm.fastMath);
+    if (m.prm.solverType != 1)
+    {
+        // ClothModelPBD::Step with SOLVER_JACOBI or another non-Gauss-Seidel type
+        // (Physics/ClothPBD.cpp:293-298): links only, fixed iterations; always the
+        // IEEE kernels
+        if (m.prm.solverType == 0) launch_solve_jacobi(s, c, P, m.linkSolve);
+        else
+        {
+            std::vector<float> beta(std::max(1, P.iterations));
+            for (int k = 0; k < P.iterations; k++)
+            {
+                const float t = (float)k / (float)(P.iterations - 1);
+                beta[k] = std::pow(t, 0.6f);
+            }
+            launch_solve_cr(s, c, P, m.linkSolve, beta.data());
+        }
+        launch_iteration_total(s, c);
+        launch_velocity(s, c, P);
+        return true;
+    }
     // the reference's loop tests its exit conditions after the body, so it always
     // runs at least one iteration (Physics/ClothPBD.cpp:335-362)
     const int iterations = m.prm.iterations > 1 ? m.prm.iterations : 1;
@@ -2028,6 +2080,7 @@ static std::vector<std::pair<std::vector<int>, SolverChoice>> g_tuneCache;
 bool ClothPatch::autotune(float h)
 {
     ClothModel& m = model;
+    if (m.prm.solverType != 1) { m.tuned = true; return true; }   // the Jacobi / CR solves have no variants
     const SolverParams P = m.solver_params(h);
     std::vector<int> key = {m.N, m.dc.T, m.dc.B, m.prm.iterations, m.prm.dihedral, m.prm.fem, m.prm.fixedIterations,
                             (int)m.buf.numVColl, m.prm.bendFreq, (int)m.prm.stageRecords, m.solverMode,

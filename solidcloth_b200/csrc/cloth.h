@@ -103,6 +103,7 @@ struct HostParams
     bool fastMath = false;       // solver build: false = IEEE (bit-exact), true = FMA + approximate div/sqrt
     float resTol = 0.f;          // > 0: Gauss-Seidel runs until the residual is <= resTol (iterations = cap)
     bool resMetres = false;      // update residual in metres (true) or in mean rest edge lengths
+    int solverType = 1;          // ClothModel::SolverType: 0 Jacobi, 1 Gauss-Seidel, other: conjugate residual
 };
 
 // a collider acting on the particles [vBegin, vBegin + vCount) of batch instance `inst`
@@ -212,6 +213,7 @@ public:
         BandView view{};                                   // device arrays (in allocs)
     } bandPlan;
     void build_band_plan();
+    LinkSolve linkSolve{};                      // Jacobi / conjugate-residual link solves (uploaded with the links)
     bool band_active() const { return bandPlan.valid && solverMode == SOLVE_BAND; }
     size_t band_smem();
 };

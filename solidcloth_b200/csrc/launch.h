@@ -114,6 +114,23 @@ void launch_ccd(cudaStream_t s, cudaStream_t side, cudaEvent_t fork, cudaEvent_t
 void launch_compact_self(cudaStream_t s, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join, const DevCloth& c,
                          const SolverParams& P, const Buffers& b, bool self, bool ccd);
 void launch_reset_gs(cudaStream_t s, const DevCloth& c);
+
+// The reference's other link solvers (ClothModel::SetSolver, Physics/ClothPBD.cpp:293-298):
+// links in index order, per-link displacements, and each particle's incident links
+// in increasing link index ((link << 1) | 1 where the particle is the link's i2)
+struct LinkSolve
+{
+    int L;
+    const float4* link;     // L: i1, i2 (bits), rest length, stiffness; link index order
+    float4* disp;           // L: this iteration's displacement of each link
+    float* d;               // L: conjugate-residual search direction
+    const int* incStart;    // N + 1
+    const int* inc;         // 2 L
+};
+// SolveJacobi: `iterations` rounds of SolveLinksJacobi (omega 0.5)
+void launch_solve_jacobi(cudaStream_t s, const DevCloth& c, const SolverParams& P, const LinkSolve& ls);
+// SolveCR (alpha0 0.1): beta[k] of iteration k, (k / (iterations - 1))^0.6, computed by the caller
+void launch_solve_cr(cudaStream_t s, const DevCloth& c, const SolverParams& P, const LinkSolve& ls, const float* beta);
 // max |C| over warp / weft / shear constraints, as float bits into *out
 void launch_residual(cudaStream_t s, const DevCloth& c, unsigned* out);
 // residual-target mode for the per-colour path: residual + exit flag after an iteration

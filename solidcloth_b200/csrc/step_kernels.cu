@@ -57,6 +57,95 @@ __global__ void k_velocity(DevCloth c, SolverParams P)
     c.vel[i] = make_float4(v.x, v.y, v.z, 0.f);
 }
 
+// ------------------------------------------ Jacobi and conjugate-residual link solves
+// ClothModelPBD::SolveLinksJacobi, first loop (Physics/ClothPBD.cpp:616-639): every
+// link's displacement from the same positions (no guard against two pinned ends,
+// as the reference)
+__global__ void k_jacobi_disp(DevCloth c, LinkSolve ls, float k, float omega)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ls.L) return;
+    const float4 r = ls.link[i];
+    const float4 a = c.pos[__float_as_uint(r.x)], b = c.pos[__float_as_uint(r.y)];
+    const float mu = 1.f / (a.w + b.w);
+    V3 delta = mk(a.x, a.y, a.z) - mk(b.x, b.y, b.z);
+    const float len0 = r.z;
+    const float l = len(delta);
+    delta = (1.f / l) * delta;
+    const float err = l - len0;
+    const float epsilon = len0 / (k * r.w);
+    const float s = 1.f / (1.f + mu * epsilon);
+    const float lambda = err * mu * s;
+    const V3 d = (omega * lambda) * delta;
+    ls.disp[i] = make_float4(d.x, d.y, d.z, 0.f);
+}
+
+// SolveCR per link as compiled (SKIP_ALPHA, SKIP_BETA; Physics/ClothPBD.cpp:371-379,
+// 405-411, 440-447, 486-494): error and unit direction from the same positions,
+// d = r + beta d, displacement alpha d along the direction
+__global__ void k_cr_disp(DevCloth c, LinkSolve ls, float unit, float beta, float alpha)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ls.L) return;
+    const float4 r = ls.link[i];
+    const float4 a = c.pos[__float_as_uint(r.x)], b = c.pos[__float_as_uint(r.y)];
+    V3 delta = mk(b.x, b.y, b.z) - mk(a.x, a.y, a.z);
+    const float cc = (len(delta) - r.z) * r.w * unit;
+    const float ln = len(delta);
+    delta = (1.f / ln) * delta;
+    const float res = -cc;
+    const float d = res + beta * ls.d[i];
+    ls.d[i] = d;
+    const float dLambda = alpha * d;
+    const V3 disp = dLambda * delta;
+    ls.disp[i] = make_float4(disp.x, disp.y, disp.z, 0.f);
+}
+
+// the apply loop of both (Physics/ClothPBD.cpp:641-650, 486-494): particle i1 of a
+// link moves by -invMass disp, i2 by +invMass disp, in link order; each particle
+// takes its incident links in increasing index, which is the sequential loop's
+// order of updates to it
+__global__ void k_link_apply(DevCloth c, LinkSolve ls, int iterationsDone)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p == 0 && iterationsDone > 0) c.scal[9] = (float)iterationsDone;
+    if (p >= c.N) return;
+    const float4 x = c.pos[p];
+    V3 q = mk(x.x, x.y, x.z);
+    const float w = x.w;
+    const int e0 = ls.incStart[p], e1 = ls.incStart[p + 1];
+    if (e0 == e1) return;
+    for (int j = e0; j < e1; j++)
+    {
+        const int e = ls.inc[j];
+        const float4 d = ls.disp[e >> 1];
+        const V3 t = w * mk(d.x, d.y, d.z);
+        q = (e & 1) ? q + t : q - t;
+    }
+    c.pos[p] = make_float4(q.x, q.y, q.z, w);
+}
+
+void launch_solve_jacobi(cudaStream_t s, const DevCloth& c, const SolverParams& P, const LinkSolve& ls)
+{
+    const float k = P.h2 * P.area * P.unit;
+    for (int it = 0; it < P.iterations; it++)
+    {
+        if (ls.L > 0) k_jacobi_disp<<<blocks_for(ls.L), 256, 0, s>>>(c, ls, k, 0.5f);
+        k_link_apply<<<blocks_for(c.N), 256, 0, s>>>(c, ls, it + 1 == P.iterations ? P.iterations : 0);
+    }
+}
+
+void launch_solve_cr(cudaStream_t s, const DevCloth& c, const SolverParams& P, const LinkSolve& ls, const float* beta)
+{
+    if (ls.L == 0) return;
+    cudaMemsetAsync(ls.d, 0, sizeof(float) * (size_t)ls.L, s);
+    for (int it = 0; it < P.iterations; it++)
+    {
+        k_cr_disp<<<blocks_for(ls.L), 256, 0, s>>>(c, ls, P.unit, beta[it], 0.1f);
+        k_link_apply<<<blocks_for(c.N), 256, 0, s>>>(c, ls, it + 1 == P.iterations ? P.iterations : 0);
+    }
+}
+
 #include "solver.cuh"     // projections, contact solves and the solver kernels (IEEE build)
 
 // ----------------------------------------------------------- normals

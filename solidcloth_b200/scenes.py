@@ -48,6 +48,7 @@ class Params:
     dihedral: bool = True
     fixed_iterations: bool = True
     drag: float = 1.0
+    solver: int = 1     # ClothModel::SolverType: 0 Jacobi, 1 Gauss-Seidel, 2 conjugate residual (not in as_array)
 
     def as_array(self) -> np.ndarray:
         return np.array([self.unit, self.thickness, self.tolerance, self.shear, self.bend,

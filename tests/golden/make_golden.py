@@ -132,6 +132,33 @@ def case_links():
     return out
 
 
+def solver_scenes():
+    """The reference's other link solvers (ClothModel::SetSolver): SolveJacobi on
+    the mass-spring cloth with dihedral bending (stretch and shear links), eight
+    frames; SolveCR one frame of one substep x 3 iterations (finite), and its
+    default 4 x 10 frame (the solve diverges to NaN in the reference itself)."""
+    jac = links_scene(True)
+    jac.params.solver = 0
+    cr = links_scene(True)
+    cr.params.solver = 2
+    cr.params.substeps, cr.params.iterations = 1, 3
+    cr_div = links_scene(True)
+    cr_div.params.solver = 2
+    return [("jacobi", jac, 8), ("cr", cr, 1), ("cr_diverging", cr_div, 1)]
+
+
+def case_solvers():
+    out = {}
+    for name, sc, frames in solver_scenes():
+        r = RefCloth.from_scene(sc)
+        for f in range(frames):
+            r.step(sc.dt)
+        pos, prev, vel, _ = r.state()
+        out[f"{name}_pos"] = pos
+        out[f"{name}_vel"] = vel
+    return out
+
+
 def case_sdf_mesh():
     """SDF::CreateFromMesh of a level-2 icosphere (radius 0.25) on a 16^3-cell grid"""
     from oracle.bridge import ref_sdf_from_mesh
@@ -143,7 +170,7 @@ def case_sdf_mesh():
 
 
 CASES = {"cfg0": case_cfg0, "sdf": case_sdf, "self": case_self, "ccd": case_ccd, "mesh": case_mesh,
-         "links": case_links, "sdf_mesh": case_sdf_mesh}
+         "links": case_links, "sdf_mesh": case_sdf_mesh, "solvers": case_solvers}
 
 
 if __name__ == "__main__":

@@ -307,6 +307,44 @@ def test_port_matches_reference_links(fixed, ref_threads):
         assert np.array_equal(bits(r.positions()), bits(o.positions())), dih
 
 
+# ------------------------------------------- Jacobi and conjugate residual
+def _same_or_both_nan(a, b):
+    a, b = np.asarray(a, np.float32), np.asarray(b, np.float32)
+    return np.array_equal(np.isnan(a), np.isnan(b)) and np.array_equal(bits(np.nan_to_num(a)), bits(np.nan_to_num(b)))
+
+
+def test_golden_solvers():
+    """SolveJacobi and SolveCR (Physics/ClothPBD.cpp:371-496, 616-661), chosen by
+    ClothModel::SetSolver: the oracle against fixtures from the reference build,
+    bit for bit (where the reference's conjugate-residual solve diverges, NaN
+    where it has NaN)."""
+    P = port()
+    P.set_portable_math(False)
+    g = np.load(GOLD / "solvers.npz")
+    for name, sc, frames in golden_module().solver_scenes():
+        o = P.from_scene(sc)
+        for _ in range(frames):
+            o.step(sc.dt)
+        pos, prev, vel, _ = o.state()
+        assert _same_or_both_nan(pos, g[f"{name}_pos"]), name
+        assert _same_or_both_nan(vel, g[f"{name}_vel"]), name
+    assert np.isfinite(g["jacobi_pos"]).all() and np.isfinite(g["cr_pos"]).all()
+    assert np.isnan(g["cr_diverging_pos"]).any()
+
+
+def test_port_matches_reference_solvers(ref_threads):
+    """Live: the Jacobi and conjugate-residual solves bit-exact against the
+    reference build, frame by frame."""
+    R, P = ref(), port()
+    P.set_portable_math(False)
+    for name, sc, frames in golden_module().solver_scenes():
+        r, o = R.from_scene(sc), P.from_scene(sc)
+        for f in range(frames):
+            r.step(sc.dt)
+            o.step(sc.dt)
+            assert _same_or_both_nan(r.positions(), o.positions()), (name, f)
+
+
 # ------------------------------------------------------------- mesh cloth
 def test_port_matches_reference_mesh_cloth(ref_threads):
     """ClothPatch::Init(mesh) (Physics/ClothPatch.cpp:42-133) in the reference
